@@ -1,0 +1,497 @@
+"""CPU oracle for the AL-DVC hot path (test infrastructure only).
+
+This module is the checker: only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg import it.  The product package
+``pyaldvc_b200`` never imports, links or calls anything under ``oracle/``.
+
+The per-node kernels are a plain-C FP64 restatement (``aldvc_oracle.c``) of
+pyALDVC's Numba CPU kernels; the orchestration around them is restated here
+in NumPy/SciPy.  Every function cites the reference file:line it follows
+(paths inside the pyALDVC project, ``src/al_dvc/...``).  Parity with the
+reference is pinned by ``tests/golden/*.npz`` (made by
+``tests/golden/make_golden.py``, which imports the reference).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+from scipy import sparse
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liborc_aldvc.so")
+_lib = None
+
+STATUS_CONVERGED, STATUS_MAX_ITER, STATUS_OUT_OF_BOUNDS, STATUS_INVALID_SUBSET = 0, 1, 2, 3
+STATUS_SINGULAR, STATUS_NAN, STATUS_SKIPPED, STATUS_STALLED = 4, 5, 6, 7
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+
+def build() -> str:
+    """Compile the C oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_num_threads.restype = _I
+        L.orc_set_num_threads.argtypes = [_I]
+        L.orc_sample_points.argtypes = [_P, _I64, _I64, _I64, _P, _P, _P, _I64, _I, _P]
+        L.orc_gradients.argtypes = [_P, _I64, _I64, _I64, _I64, _P, _P, _P]
+        L.orc_compose_warp.argtypes = [_P, _P]
+        L.orc_compose_warp.restype = _I
+        L.orc_precompute.argtypes = [_P, _I64, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _I64, _I64, _I64, _P, _P, _I64, _D, _D,
+                                     _P, _P, _P, _P, _P, _P]
+        L.orc_icgn12.argtypes = [_P, _I64, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _I64, _I64, _I64, _I, _P, _P, _D, _D, _I,
+                                 _I, _P, _P, _D, _I, _P, _P, _I64, _P, _P, _P, _P]
+        L.orc_icgn3.argtypes = [_P, _I64, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _I64, _I64, _I64, _I, _P, _P, _P,
+                                _D, _D, _D, _I, _I, _D, _D, _I, _P, _P, _I64, _P, _P, _P, _P]
+        L.orc_zncc_direct.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]
+        _lib = L
+    return _lib
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _vol_args(f, gx, gy, gz, mask):
+    """Placeholders follow the reference: (1,1,1) gradients = on-the-fly stencil, (1,1,1) mask = no mask
+    (numba_kernels._grad_at :188-212, _no_mask :314-317)."""
+    f = _f32(f)
+    stored = np.shape(gx) == f.shape
+    gx, gy, gz = (_f32(a) for a in (gx, gy, gz))
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    m = m if m.shape == f.shape else None
+    return f, gx, gy, gz, int(stored), m
+
+
+def _split(n, split_index, split_keep):
+    if split_index is None or split_keep is None:
+        return None, None, 0
+    si = np.ascontiguousarray(split_index, dtype=np.int64)
+    sk = np.ascontiguousarray(split_keep, dtype=np.uint8)
+    return si, sk, int(sk.shape[1]) if sk.ndim == 2 else 0
+
+
+# --------------------------------------------------------------------------- interpolation / gradients
+def sample_points(vol, zs, ys, xs, mode):
+    """interp_kernels.sample_points (:139-152)."""
+    vol = _f32(vol)
+    zs, ys, xs = (np.ascontiguousarray(a, dtype=np.float64) for a in (zs, ys, xs))
+    out = np.empty(zs.shape[0])
+    lib().orc_sample_points(_ptr(vol), *vol.shape, _ptr(zs), _ptr(ys), _ptr(xs), zs.shape[0], int(mode), _ptr(out))
+    return out
+
+
+def compute_gradients(f, border=3):
+    """io/volume_ops._gradient_stencil7 (:124-155) / compute_gradients (:177-197)."""
+    f = _f32(f)
+    gx, gy, gz = (np.empty_like(f) for _ in range(3))
+    lib().orc_gradients(_ptr(f), *f.shape, int(border), _ptr(gx), _ptr(gy), _ptr(gz))
+    return gx, gy, gz
+
+
+def compose_warp(P, dP):
+    """numba_kernels.compose_warp_inplace (:145-180) on a copy."""
+    P = np.array(P, dtype=np.float64)
+    dP = np.ascontiguousarray(dP, dtype=np.float64)
+    ok = lib().orc_compose_warp(_ptr(P), _ptr(dP))
+    return P, bool(ok)
+
+
+# --------------------------------------------------------------------------- local kernels
+def precompute_nodes(coords, hx, hy, hz, f, gx, gy, gz, mask, min_valid_ratio, cond_max, stride=1, split_index=None,
+                     split_keep=None):
+    """numba_kernels.precompute_nodes (:499-509)."""
+    coords = np.ascontiguousarray(coords, dtype=np.int64)
+    N = coords.shape[0]
+    f, gx, gy, gz, stored, m = _vol_args(f, gx, gy, gz, mask)
+    si, sk, kb = _split(N, split_index, split_keep)
+    H = np.zeros((N, 12, 12))
+    L = np.zeros((N, 12, 12))
+    mf = np.zeros(N)
+    bf = np.ones(N)
+    nv = np.zeros(N, dtype=np.int64)
+    valid = np.zeros(N, dtype=np.uint8)
+    lib().orc_precompute(_ptr(coords), N, int(hx), int(hy), int(hz), int(stride), _ptr(f), _ptr(gx), _ptr(gy), _ptr(gz), stored,
+                         _ptr(m), *f.shape, _ptr(si), _ptr(sk), kb, float(min_valid_ratio), float(cond_max), _ptr(H), _ptr(L),
+                         _ptr(mf), _ptr(bf), _ptr(nv), _ptr(valid))
+    return H, L, mf, bf, nv, valid.astype(bool)
+
+
+def icgn_12dof_parallel(coords, P0, hx, hy, hz, f, gx, gy, gz, mask, g, mode, L_all, meanf_all, bottomf_all, valid, tol, dp_tol,
+                        max_iter, patience, stride=1, H_all=None, pattern=None, noise_gain=0.0, predictive=True,
+                        split_index=None, split_keep=None):
+    """numba_kernels.icgn_12dof_parallel (:1211-1278); meanf_all is unused there too (the statistics are dynamic)."""
+    coords = np.ascontiguousarray(coords, dtype=np.int64)
+    N = coords.shape[0]
+    f, gx, gy, gz, stored, m = _vol_args(f, gx, gy, gz, mask)
+    g = _f32(g)
+    P0 = np.ascontiguousarray(P0, dtype=np.float64).reshape(N, 12)
+    L_all = np.ascontiguousarray(L_all, dtype=np.float64)
+    valid = np.ascontiguousarray(valid, dtype=np.uint8)
+    use_noise = H_all is not None and pattern is not None and noise_gain > 0.0
+    H_arr = np.ascontiguousarray(H_all, dtype=np.float64) if use_noise else None
+    pat = np.ascontiguousarray(pattern, dtype=np.float64) if use_noise else None
+    si, sk, kb = _split(N, split_index, split_keep)
+    P_out = np.empty((N, 12))
+    n_iter = np.zeros(N, dtype=np.int32)
+    status = np.zeros(N, dtype=np.int8)
+    zncc = np.zeros(N)
+    lib().orc_icgn12(_ptr(coords), N, _ptr(P0), int(hx), int(hy), int(hz), int(stride), _ptr(f), _ptr(gx), _ptr(gy), _ptr(gz),
+                     stored, _ptr(m), _ptr(g), *f.shape, int(mode), _ptr(L_all), _ptr(valid), float(tol), float(dp_tol),
+                     int(max_iter), int(patience), _ptr(H_arr), _ptr(pat), float(noise_gain if use_noise else 0.0),
+                     int(bool(predictive)), _ptr(si), _ptr(sk), kb, _ptr(P_out), _ptr(n_iter), _ptr(status), _ptr(zncc))
+    return P_out, n_iter, status, zncc
+
+
+def icgn_3dof_parallel(coords, U_old, F_fixed, vdual, hx, hy, hz, f, gx, gy, gz, mask, g, mode, H_all, meanf_all, bottomf_all,
+                       valid, mu, tol, dp_tol, max_iter, patience, stride=1, n_full=0.0, noise_gain=0.0, predictive=True,
+                       split_index=None, split_keep=None):
+    """numba_kernels.icgn_3dof_parallel (:1281-1346)."""
+    coords = np.ascontiguousarray(coords, dtype=np.int64)
+    N = coords.shape[0]
+    f, gx, gy, gz, stored, m = _vol_args(f, gx, gy, gz, mask)
+    g = _f32(g)
+    U_old = np.ascontiguousarray(U_old, dtype=np.float64).reshape(N, 3)
+    F_fixed = np.ascontiguousarray(F_fixed, dtype=np.float64).reshape(N, 9)
+    vdual = np.ascontiguousarray(vdual, dtype=np.float64).reshape(N, 3)
+    H_all = np.ascontiguousarray(H_all, dtype=np.float64)
+    bottomf_all = np.ascontiguousarray(bottomf_all, dtype=np.float64)
+    valid = np.ascontiguousarray(valid, dtype=np.uint8)
+    si, sk, kb = _split(N, split_index, split_keep)
+    U_out = np.empty((N, 3))
+    n_iter = np.zeros(N, dtype=np.int32)
+    status = np.zeros(N, dtype=np.int8)
+    zncc = np.zeros(N)
+    lib().orc_icgn3(_ptr(coords), N, _ptr(U_old), _ptr(F_fixed), _ptr(vdual), int(hx), int(hy), int(hz), int(stride), _ptr(f),
+                    _ptr(gx), _ptr(gy), _ptr(gz), stored, _ptr(m), _ptr(g), *f.shape, int(mode), _ptr(H_all), _ptr(bottomf_all),
+                    _ptr(valid), float(mu), float(tol), float(dp_tol), int(max_iter), int(patience), float(n_full),
+                    float(noise_gain if noise_gain > 0.0 else 0.0), int(bool(predictive)), _ptr(si), _ptr(sk), kb, _ptr(U_out),
+                    _ptr(n_iter), _ptr(status), _ptr(zncc))
+    return U_out, n_iter, status, zncc
+
+
+# --------------------------------------------------------------------------- integer search
+def zncc_direct(f, g, coords, hx, hy, hz, rx, ry, rz, wx0, wy0, wz0, t_ok, out):
+    """integer_search._zncc_direct (:44-151): fills ``out`` (n, vz, vy, vx) in place."""
+    f, g = _f32(f), _f32(g)
+    coords = np.ascontiguousarray(coords, dtype=np.int64)
+    wx0, wy0, wz0 = (np.ascontiguousarray(a, dtype=np.int64) for a in (wx0, wy0, wz0))
+    t_ok = np.ascontiguousarray(t_ok, dtype=np.uint8)
+    buf = out if (out.dtype == np.float64 and out.flags.c_contiguous) else np.empty(out.shape)
+    lib().orc_zncc_direct(_ptr(f), _ptr(g), *f.shape, _ptr(coords), coords.shape[0], int(hx), int(hy), int(hz), int(rx), int(ry),
+                          int(rz), _ptr(wx0), _ptr(wy0), _ptr(wz0), _ptr(t_ok), _ptr(buf))
+    if buf is not out:
+        out[...] = buf
+
+
+def _quadratic_pinv():
+    """Pseudo-inverse of the 27-point quadratic design (integer_search.py:210-227)."""
+    dz, dy, dx = np.meshgrid([-1, 0, 1], [-1, 0, 1], [-1, 0, 1], indexing="ij")
+    dx, dy, dz = dx.ravel().astype(float), dy.ravel().astype(float), dz.ravel().astype(float)
+    D = np.column_stack([np.ones(27), dx, dy, dz, dx * dy, dx * dz, dy * dz, dx**2, dy**2, dz**2])
+    return np.linalg.pinv(D)
+
+
+_PINV = _quadratic_pinv()
+_NB = [a.ravel()[None, :] for a in np.meshgrid([-1, 0, 1], [-1, 0, 1], [-1, 0, 1], indexing="ij")]
+
+
+def subvoxel_peak(neigh):
+    """integer_search._subvoxel_peak (:297-321)."""
+    n = neigh.shape[0]
+    coef = neigh @ _PINV.T
+    a = coef[:, 1:4]
+    H = np.empty((n, 3, 3))
+    H[:, 0, 0] = 2 * coef[:, 7]
+    H[:, 1, 1] = 2 * coef[:, 8]
+    H[:, 2, 2] = 2 * coef[:, 9]
+    H[:, 0, 1] = H[:, 1, 0] = coef[:, 4]
+    H[:, 0, 2] = H[:, 2, 0] = coef[:, 5]
+    H[:, 1, 2] = H[:, 2, 1] = coef[:, 6]
+    out = np.zeros((n, 3))
+    det = np.linalg.det(H)
+    ok = np.abs(det) > 1e-12
+    if ok.any():
+        sol = np.linalg.solve(H[ok], -a[ok][:, :, None])[:, :, 0]
+        good = np.all(np.abs(sol) <= 1.0, axis=1) & np.all(np.isfinite(sol), axis=1)
+        tmp = np.zeros((int(ok.sum()), 3))
+        tmp[good] = sol[good]
+        out[ok] = tmp
+    return out
+
+
+def ncc_search(f, g, coords, subset, radius, shift0=None, chunk=4096):
+    """integer_search.ncc_search (:329-483) with the direct engine (FP64 map) for every size."""
+    f, g = _f32(f), _f32(g)
+    nz, ny, nx = f.shape
+    coords = np.asarray(coords, dtype=np.int64)
+    N = coords.shape[0]
+    hx, hy, hz = (int(w) // 2 for w in subset)
+    rx, ry, rz = (int(r) for r in radius)
+    sx, sy, sz = 2 * hx + 1, 2 * hy + 1, 2 * hz + 1
+    wx, wy, wz = sx + 2 * rx, sy + 2 * ry, sz + 2 * rz
+    if shift0 is None:
+        shift0 = np.zeros((N, 3), dtype=np.int64)
+    shift0 = np.asarray(np.round(shift0), dtype=np.int64)
+    disp = np.full((N, 3), np.nan)
+    cc = np.full(N, np.nan)
+    pce = np.full(N, np.nan)
+    clipped = np.zeros(N, dtype=bool)
+    ok = np.zeros(N, dtype=bool)
+    out = {"disp": disp, "cc": cc, "pce": pce, "clipped": clipped, "ok": ok}
+    if wx > nx or wy > ny or wz > nz:
+        return out
+    cx, cy, cz = coords[:, 0], coords[:, 1], coords[:, 2]
+    t_ok = (cx - hx >= 0) & (cx + hx < nx) & (cy - hy >= 0) & (cy + hy < ny) & (cz - hz >= 0) & (cz + hz < nz)
+    dx0 = cx + shift0[:, 0] - hx - rx
+    dy0 = cy + shift0[:, 1] - hy - ry
+    dz0 = cz + shift0[:, 2] - hz - rz
+    wx0 = np.clip(dx0, 0, nx - wx)
+    wy0 = np.clip(dy0, 0, ny - wy)
+    wz0 = np.clip(dz0, 0, nz - wz)
+    free_lo = np.column_stack([dx0 >= 0, dy0 >= 0, dz0 >= 0])
+    free_hi = np.column_stack([dx0 <= nx - wx, dy0 <= ny - wy, dz0 <= nz - wz])
+    idx_all = np.flatnonzero(t_ok)
+    vz, vy, vx = 2 * rz + 1, 2 * ry + 1, 2 * rx + 1
+    for start in range(0, idx_all.size, chunk):
+        ids = idx_all[start:start + chunk]
+        n = ids.size
+        ncc = np.empty((n, vz, vy, vx))
+        zncc_direct(f, g, coords[ids], hx, hy, hz, rx, ry, rz, wx0[ids], wy0[ids], wz0[ids], np.ones(n, dtype=bool), ncc)
+        t_norm = np.where(ncc[:, 0, 0, 0] > -1.5, 1.0, 0.0)
+        ncc[ncc < -1.0] = 0.0
+        flat = ncc.reshape(n, -1)
+        pk = np.argmax(flat, axis=1)
+        pz, py, px = np.unravel_index(pk, ncc.shape[1:])
+        peak_val = flat[np.arange(n), pk]
+        cmin = flat - flat.min(axis=1, keepdims=True)
+        energy = np.mean(cmin * cmin, axis=1)
+        pk_min = cmin[np.arange(n), pk]
+        pce_k = np.divide(pk_min * pk_min, energy, out=np.zeros(n), where=energy > 1e-30)
+        lo, hi = free_lo[ids], free_hi[ids]
+        if rx > 0 or ry > 0 or rz > 0:
+            on_edge = (((px == 0) & lo[:, 0]) | ((px == 2 * rx) & hi[:, 0]) | ((py == 0) & lo[:, 1]) | ((py == 2 * ry) & hi[:, 1])
+                       | ((pz == 0) & lo[:, 2]) | ((pz == 2 * rz) & hi[:, 2]))
+        else:
+            on_edge = np.zeros(n, dtype=bool)
+        sub = np.zeros((n, 3))
+        at_border = (px == 0) | (px == 2 * rx) | (py == 0) | (py == 2 * ry) | (pz == 0) | (pz == 2 * rz)
+        interior = ~at_border & (rx > 0) & (ry > 0) & (rz > 0)
+        if interior.any():
+            ii = np.flatnonzero(interior)
+            neigh = ncc[ii[:, None], pz[ii][:, None] + _NB[0], py[ii][:, None] + _NB[1], px[ii][:, None] + _NB[2]]
+            sub[ii] = subvoxel_peak(neigh)
+        disp[ids, 0] = wx0[ids] + px + hx - cx[ids] + sub[:, 0]
+        disp[ids, 1] = wy0[ids] + py + hy - cy[ids] + sub[:, 1]
+        disp[ids, 2] = wz0[ids] + pz + hz - cz[ids] + sub[:, 2]
+        cc[ids] = peak_val
+        pce[ids] = pce_k
+        clipped[ids] = on_edge
+        ok[ids] = np.isfinite(peak_val) & (t_norm > 1e-10)
+    disp[~ok] = np.nan
+    return out
+
+
+def ncc_search_expanding(f, g, coords, subset, radius, shift0=None, auto_expand=True, max_expand=3):
+    """integer_search.ncc_search_expanding (:486-524)."""
+    res = ncc_search(f, g, coords, subset, radius, shift0)
+    res["expansions"] = 0
+    res["radius"] = tuple(int(r) for r in radius)
+    rad = res["radius"]
+    for _ in range(max_expand if auto_expand else 0):
+        sel = res["clipped"] & res["ok"]
+        n_ok = int(res["ok"].sum())
+        if n_ok == 0 or sel.sum() <= 0.05 * n_ok:
+            break
+        rad = tuple(2 * r for r in rad)
+        sub_shift = None if shift0 is None else np.asarray(shift0)[sel]
+        sub = ncc_search(f, g, coords[sel], subset, rad, sub_shift)
+        if not sub["ok"].any():
+            break
+        idx = np.flatnonzero(sel)[sub["ok"]]
+        for key in ("disp", "cc", "pce", "clipped", "ok"):
+            res[key][idx] = sub[key][sub["ok"]]
+        res["expansions"] += 1
+        res["radius"] = rad
+    return res
+
+
+# --------------------------------------------------------------------------- global step (hex8 FEM)
+_HEX8_SIGNS = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1], [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]],
+                       dtype=np.float64)
+
+
+def hex8_box_matrices(spacing, order=2):
+    """mesh/hex8.hex8_box_matrices (:74-105): element K, M, G_j of an axis-aligned box."""
+    if order == 1:
+        p1, w1 = np.array([0.0]), np.array([2.0])
+    elif order == 2:
+        gp = 1.0 / np.sqrt(3.0)
+        p1, w1 = np.array([-gp, gp]), np.array([1.0, 1.0])
+    elif order == 3:
+        gp = np.sqrt(3.0 / 5.0)
+        p1, w1 = np.array([-gp, 0.0, gp]), np.array([5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0])
+    else:
+        raise ValueError(order)
+    hx, hy, hz = (float(s) for s in spacing)
+    inv_jac = np.diag([2.0 / hx, 2.0 / hy, 2.0 / hz])
+    det_j = (hx / 2.0) * (hy / 2.0) * (hz / 2.0)
+    s = _HEX8_SIGNS
+    K = np.zeros((8, 8))
+    M = np.zeros((8, 8))
+    G = np.zeros((3, 8, 8))
+    for k, wk in zip(p1, w1):
+        for j, wj in zip(p1, w1):
+            for i, wi in zip(p1, w1):
+                ksi, eta, zeta = i, j, k
+                N = 0.125 * (1 + s[:, 0] * ksi) * (1 + s[:, 1] * eta) * (1 + s[:, 2] * zeta)
+                dN = np.empty((8, 3))
+                dN[:, 0] = 0.125 * s[:, 0] * (1 + s[:, 1] * eta) * (1 + s[:, 2] * zeta)
+                dN[:, 1] = 0.125 * (1 + s[:, 0] * ksi) * s[:, 1] * (1 + s[:, 2] * zeta)
+                dN[:, 2] = 0.125 * (1 + s[:, 0] * ksi) * (1 + s[:, 1] * eta) * s[:, 2]
+                dN = dN @ inv_jac
+                wj_ = wi * wj * wk * det_j
+                K += wj_ * (dN @ dN.T)
+                M += wj_ * np.outer(N, N)
+                for a in range(3):
+                    G[a] += wj_ * np.outer(dN[:, a], N)
+    return {"K": K, "M": M, "G": G}
+
+
+def grid_elements(grid_shape):
+    """mesh/grid_mesh.mesh_setup element connectivity (:79-103), node n = iz*ny*nx + iy*nx + ix."""
+    nz, ny, nx = grid_shape
+    iz, iy, ix = (a.ravel() for a in np.meshgrid(np.arange(nz - 1), np.arange(ny - 1), np.arange(nx - 1), indexing="ij"))
+
+    def nid(a, b, c):
+        return c * ny * nx + b * nx + a
+
+    return np.column_stack([nid(ix, iy, iz), nid(ix + 1, iy, iz), nid(ix + 1, iy + 1, iz), nid(ix, iy + 1, iz),
+                            nid(ix, iy, iz + 1), nid(ix + 1, iy, iz + 1), nid(ix + 1, iy + 1, iz + 1),
+                            nid(ix, iy + 1, iz + 1)]).astype(np.int64)
+
+
+def fem_operators(grid_shape, spacing, elem_active=None, order=2):
+    """global_operators.build_fem_operators (:58-71) over the active elements."""
+    n = int(np.prod(grid_shape))
+    elems = grid_elements(grid_shape)
+    if elem_active is not None:
+        elems = elems[np.asarray(elem_active, dtype=bool)]
+    box = hex8_box_matrices(spacing, order)
+
+    def scatter(Ke):
+        E = elems.shape[0]
+        rows = np.broadcast_to(elems[:, :, None], (E, 8, 8)).ravel()
+        cols = np.broadcast_to(elems[:, None, :], (E, 8, 8)).ravel()
+        vals = np.broadcast_to(Ke[None], (E, 8, 8)).ravel()
+        return sparse.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+
+    Kg, M = scatter(box["K"]), scatter(box["M"])
+    G = tuple(scatter(box["G"][j]) for j in range(3))
+    mL = np.asarray(M.sum(axis=1)).ravel()
+    active = np.zeros(n, dtype=bool)
+    active[np.unique(elems)] = True
+    return {"Kg": Kg, "M": M, "G": G, "mL": mL, "active": active, "n_nodes": n}
+
+
+def global_system(ops, beta, mu, alpha=0.0):
+    """subpb2_solver.build_global_system (:45-74), PCG branch."""
+    A_full = ((beta + alpha) * ops["Kg"] + mu * ops["M"]).tocsr()
+    act = np.flatnonzero(ops["active"])
+    A = A_full[act][:, act].tocsr()
+    d = A.diagonal()
+    inv_diag = np.where(np.abs(d) > 1e-300, 1.0 / d, 1.0)
+    return {"A": A, "inv_diag": inv_diag, "active_idx": act, "beta": beta, "mu": mu, "alpha": alpha, "ops": ops}
+
+
+def pcg_multi(A, B, inv_diag, tol, max_iter, X0=None):
+    """subpb2_solver.pcg_multi (:77-108): Jacobi-PCG for several right-hand sides."""
+    X = np.zeros_like(B) if X0 is None else X0.copy()
+    R = B - A @ X
+    Z = inv_diag[:, None] * R
+    P = Z.copy()
+    rz = np.einsum("ij,ij->j", R, Z)
+    bnorm = np.linalg.norm(B, axis=0)
+    bnorm[bnorm == 0] = 1.0
+    it = 0
+    for it in range(1, max_iter + 1):
+        AP = A @ P
+        denom = np.einsum("ij,ij->j", P, AP)
+        denom[denom == 0] = np.inf
+        alpha = rz / denom
+        X += P * alpha
+        R -= AP * alpha
+        if np.all(np.linalg.norm(R, axis=0) / bnorm < tol):
+            break
+        Z = inv_diag[:, None] * R
+        rz_new = np.einsum("ij,ij->j", R, Z)
+        beta = rz_new / np.where(rz == 0, np.inf, rz)
+        P = Z + P * beta
+        rz = rz_new
+    return X, it
+
+
+def global_rhs(ops, beta, mu, alpha, U1, F1, W, v):
+    """subpb2_solver.global_rhs (:111-130)."""
+    n = ops["n_nodes"]
+    FmW = np.asarray(F1, dtype=np.float64).reshape(n, 3, 3) - np.asarray(W, dtype=np.float64).reshape(n, 3, 3)
+    Umv = np.asarray(U1, dtype=np.float64).reshape(n, 3) - np.asarray(v, dtype=np.float64).reshape(n, 3)
+    b = mu * (ops["M"] @ Umv)
+    for j in range(3):
+        b += beta * (ops["G"][j] @ FmW[:, :, j])
+    if alpha != 0.0:
+        b += alpha * (ops["Kg"] @ np.asarray(U1, dtype=np.float64).reshape(n, 3))
+    return b
+
+
+def solve_subpb2(system, U1, F1, W, v, tol=1e-8, max_iter=500):
+    """subpb2_solver.solve_subpb2 (:133-155) with the PCG solver."""
+    ops = system["ops"]
+    b = global_rhs(ops, system["beta"], system["mu"], system["alpha"], U1, F1, W, v)
+    U1 = np.asarray(U1, dtype=np.float64).reshape(ops["n_nodes"], 3)
+    act = system["active_idx"]
+    X, it = pcg_multi(system["A"], b[act], system["inv_diag"], tol, max_iter, X0=U1[act])
+    U2 = U1.copy()
+    U2[act] = X
+    return U2, it
+
+
+def nodal_gradient(ops, U):
+    """global_operators.nodal_gradient (:151-170), FEM branch: F_ij = (G_j^T u_i) / m_L, NaN off the active set."""
+    n = ops["n_nodes"]
+    U = np.asarray(U, dtype=np.float64).reshape(n, 3)
+    F = np.empty((n, 3, 3))
+    safe = np.where(ops["mL"] > 1e-15, ops["mL"], 1.0)
+    for j in range(3):
+        GT = ops["G"][j].T
+        for i in range(3):
+            F[:, i, j] = (GT @ U[:, i]) / safe
+    F[~ops["active"]] = np.nan
+    return F

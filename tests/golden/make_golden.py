@@ -1,0 +1,254 @@
+"""Generate the golden fixtures that pin the CPU oracle to the reference.
+
+Run in a container that holds the pyALDVC sources (read-only) at
+``$ALDVC_REFERENCE/src`` (default ``/root/reference/src``)::
+
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py
+
+It imports the reference package, runs its own Numba CPU kernels on seeded
+bead volumes from ``pyaldvc_b200.synthetic`` and stores inputs + outputs as
+small ``.npz`` files next to this script.  The tests only read the fixtures;
+nothing at test time needs the reference.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(os.environ.get("ALDVC_REFERENCE", "/root/reference"), "src"))
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
+
+from al_dvc.core.config import dvcpara_default  # noqa: E402
+from al_dvc.core.data_structures import P_from_UF  # noqa: E402
+from al_dvc.io.volume_ops import compute_gradients, normalize_volume, prefilter_bspline  # noqa: E402
+from al_dvc.mesh.grid_mesh import build_grid_axes as ref_grid_axes  # noqa: E402
+from al_dvc.mesh.grid_mesh import mesh_setup  # noqa: E402
+from al_dvc.solver import integer_search as ris  # noqa: E402
+from al_dvc.solver import numba_kernels as nk  # noqa: E402
+from al_dvc.solver.global_operators import build_fem_operators, nodal_gradient  # noqa: E402
+from al_dvc.solver.interp_kernels import sample_points  # noqa: E402
+from al_dvc.solver.subpb2_solver import build_global_system, global_rhs, solve_subpb2  # noqa: E402
+from al_dvc.solver.uncertainty import STENCIL_NOISE_GAIN, noise_hessian_pattern  # noqa: E402
+
+from pyaldvc_b200 import synthetic as syn  # noqa: E402
+
+SHAPE = (32, 34, 36)  # (nz, ny, nx), non-cubic on purpose
+F_TRUE = np.array([[0.015, 0.004, 0.0], [0.003, -0.01, 0.002], [0.0, -0.002, 0.012]])
+T_TRUE = (1.3, -0.7, 0.4)
+CENTRE = ((SHAPE[2] - 1) / 2, (SHAPE[1] - 1) / 2, (SHAPE[0] - 1) / 2)
+
+
+def volumes():
+    disp = syn.affine(F_TRUE, T_TRUE, CENTRE)
+    pair = syn.bead_pair(SHAPE, density=0.03, sigma=1.5, seed=11, disp=disp, noise=0.01)
+    f = normalize_volume(pair.f)
+    g = normalize_volume(pair.g)
+    return f, g, disp
+
+
+def main():
+    f, g, disp = volumes()
+    gx, gy, gz = compute_gradients(f)
+    g_bs = prefilter_bspline(g)
+    f_bs = prefilter_bspline(f)
+    out = {"f": f, "g": g, "gx": gx, "gy": gy, "gz": gz, "g_bspline": g_bs, "f_bspline": f_bs}
+
+    # --- interpolation (interp_kernels.sample_points) ---
+    rng = np.random.default_rng(0)
+    npts = 300
+    zs = rng.uniform(0.5, SHAPE[0] - 2.5, npts)
+    ys = rng.uniform(0.5, SHAPE[1] - 2.5, npts)
+    xs = rng.uniform(0.5, SHAPE[2] - 2.5, npts)
+    out.update(pts_z=zs, pts_y=ys, pts_x=xs)
+    for mode in (0, 1, 2):
+        src = f_bs if mode == 2 else f
+        out[f"interp_{mode}"] = sample_points(src, zs, ys, xs, mode)
+
+    # --- warp composition ---
+    Pc = rng.normal(0, 0.05, 12)
+    dPc = rng.normal(0, 0.02, 12)
+    P1 = Pc.copy()
+    nk.compose_warp_inplace(P1, dPc)
+    out.update(compose_P=Pc, compose_dP=dPc, compose_out=P1)
+
+    # --- node grid (winsize 10, step 6) ---
+    x0, y0, z0 = ref_grid_axes(dvcpara_default().voi, SHAPE, (10, 10, 10), (6, 6, 6))
+    mesh = mesh_setup(x0, y0, z0)
+    coords = np.round(mesh.coordinates).astype(np.int64)
+    out.update(coords=coords, grid_shape=np.array(mesh.grid_shape), x0=x0, y0=y0, z0=z0)
+    N = coords.shape[0]
+    U_true = np.column_stack(disp(coords[:, 0].astype(float), coords[:, 1].astype(float), coords[:, 2].astype(float)))
+    out["U_true"] = U_true
+
+    mask = np.ones(SHAPE, dtype=np.uint8)
+    mask[:, :, 20:] = 0  # a slab of non-material: the last node column loses its subsets
+    out["mask"] = mask
+    placeholder = np.zeros((1, 1, 1), dtype=np.float32)
+    nomask = np.ones((1, 1, 1), dtype=np.uint8)
+
+    # split rows for the masked case (subset splitting)
+    cand = np.arange(N)
+    rows, n_keep, n_inmask = nk.build_split_rows(coords, cand, 5, 5, 5, 1, mask, 0)
+    split_index = np.arange(N, dtype=np.int64)
+    out.update(split_keep=rows, split_index=split_index)
+
+    pre_cases = {
+        "plain": dict(h=(5, 5, 5), stride=1, grads="stored", mask=False, split=False),
+        "aniso": dict(h=(4, 5, 6), stride=1, grads="stored", mask=False, split=False),
+        "masked": dict(h=(5, 5, 5), stride=1, grads="stored", mask=True, split=False),
+        "stride2": dict(h=(5, 5, 5), stride=2, grads="stored", mask=False, split=False),
+        "otf": dict(h=(5, 5, 5), stride=1, grads="otf", mask=False, split=False),
+        "split": dict(h=(5, 5, 5), stride=1, grads="stored", mask=True, split=True),
+    }
+    contexts = {}
+    for name, c in pre_cases.items():
+        hx, hy, hz = c["h"]
+        gxa, gya, gza = (gx, gy, gz) if c["grads"] == "stored" else (placeholder,) * 3
+        m = mask if c["mask"] else nomask
+        kw = {"split_index": split_index, "split_keep": rows} if c["split"] else {}
+        H, L, mf, bf, nv, valid = nk.precompute_nodes(coords, hx, hy, hz, f, gxa, gya, gza, m, 0.5, 1e12, c["stride"], **kw)
+        for k, v in zip(("H", "L", "meanf", "bottomf", "n_valid", "valid"), (H, L, mf, bf, nv, valid)):
+            out[f"pre_{name}_{k}"] = v
+        contexts[name] = (c, gxa, gya, gza, m, kw, H, L, mf, bf, valid)
+
+    # --- 12-DOF IC-GN ---
+    P0 = P_from_UF(np.round(U_true) + np.array([0.2, -0.1, 0.15]), np.zeros((N, 3, 3)))
+    P0_special = P0.copy()
+    P0_special[0, 9] = np.nan  # NaN start -> status 5
+    P0_special[1, 9] = 60.0  # warps outside the volume -> status 2
+    P0_far = P0.copy()
+    P0_far[:, 9:] = np.round(U_true) + np.array([3.5, -3.5, 2.45])  # far start: some nodes stall, some leave the volume
+    out["P0"] = P0
+    out["P0_special"] = P0_special
+    out["P0_far"] = P0_far
+    icgn_cases = {
+        "cubic": dict(pre="plain", mode=1),
+        "linear": dict(pre="plain", mode=0),
+        "bspline": dict(pre="plain", mode=2),
+        "aniso": dict(pre="aniso", mode=1),
+        "masked": dict(pre="masked", mode=1),
+        "stride2": dict(pre="stride2", mode=1),
+        "otf": dict(pre="otf", mode=1),
+        "split": dict(pre="split", mode=1),
+        "noise": dict(pre="plain", mode=1, noise=True),
+        "nopredict": dict(pre="plain", mode=1, predictive=False),
+        "special": dict(pre="plain", mode=1, special=True),
+        "stall": dict(pre="plain", mode=1, patience=1, far=True),
+        "maxiter": dict(pre="plain", mode=1, max_iter=2, tol=1e-9, dp_tol=1e-12, patience=0),
+    }
+    for name, c in icgn_cases.items():
+        cc, gxa, gya, gza, m, kw, H, L, mf, bf, valid = contexts[c["pre"]]
+        hx, hy, hz = cc["h"]
+        gsrc = g_bs if c["mode"] == 2 else g
+        pattern = noise_hessian_pattern((hx, hy, hz), cc["stride"])
+        gain = STENCIL_NOISE_GAIN if c.get("noise") else 0.0
+        P_start = P0_special if c.get("special") else (P0_far if c.get("far") else P0)
+        res = nk.icgn_12dof_parallel(coords, P_start.copy(), hx, hy, hz, f, gxa, gya, gza, m, gsrc, c["mode"], L, mf, bf, valid,
+                                     c.get("tol", 1e-2), c.get("dp_tol", 1e-3), c.get("max_iter", 100), c.get("patience", 5),
+                                     cc["stride"], H, pattern, gain, c.get("predictive", True), **kw)
+        for k, v in zip(("P", "n_iter", "status", "zncc"), res):
+            out[f"icgn12_{name}_{k}"] = v
+        out[f"icgn12_{name}_pattern"] = pattern
+
+    # --- 3-DOF IC-GN (ADMM subproblem 1) ---
+    U_old = U_true + np.array([0.25, -0.2, 0.15])
+    F_fixed = np.tile(F_TRUE, (N, 1, 1))
+    vdual = np.column_stack([0.02 * np.sin(np.arange(N)), 0.01 * np.cos(np.arange(N)), np.zeros(N)])
+    out.update(U_old=U_old, F_fixed=F_fixed, vdual=vdual)
+    icgn3_cases = {
+        "cubic": dict(pre="plain", mode=1),
+        "linear": dict(pre="plain", mode=0),
+        "masked": dict(pre="masked", mode=1),
+        "noise": dict(pre="plain", mode=1, noise=True),
+        "split": dict(pre="split", mode=1),
+        "stride2": dict(pre="stride2", mode=2),
+    }
+    for name, c in icgn3_cases.items():
+        cc, gxa, gya, gza, m, kw, H, L, mf, bf, valid = contexts[c["pre"]]
+        hx, hy, hz = cc["h"]
+        gsrc = g_bs if c["mode"] == 2 else g
+        pattern = noise_hessian_pattern((hx, hy, hz), cc["stride"])
+        gain = STENCIL_NOISE_GAIN if c.get("noise") else 0.0
+        res = nk.icgn_3dof_parallel(coords, U_old, F_fixed, vdual, hx, hy, hz, f, gxa, gya, gza, m, gsrc, c["mode"], H, mf, bf, valid,
+                                    1e-3, 1e-2, 1e-3, 100, 5, cc["stride"], float(pattern[9, 9]), gain, True, **kw)
+        for k, v in zip(("U", "n_iter", "status", "zncc"), res):
+            out[f"icgn3_{name}_{k}"] = v
+        out[f"icgn3_{name}_n_full"] = float(pattern[9, 9])
+
+    # --- integer search ---
+    hx = hy = hz = 4
+    rx, ry, rz = 3, 2, 3
+    sx, sy, sz = 2 * hx + 1, 2 * hy + 1, 2 * hz + 1
+    wx, wy, wz = sx + 2 * rx, sy + 2 * ry, sz + 2 * rz
+    wx0 = np.clip(coords[:, 0] + 1 - hx - rx, 0, SHAPE[2] - wx)
+    wy0 = np.clip(coords[:, 1] - 1 - hy - ry, 0, SHAPE[1] - wy)
+    wz0 = np.clip(coords[:, 2] - hz - rz, 0, SHAPE[0] - wz)
+    t_ok = np.ones(N, dtype=np.bool_)
+    t_ok[3] = False
+    zmap = np.empty((N, 2 * rz + 1, 2 * ry + 1, 2 * rx + 1))
+    ris._zncc_direct(f, g, coords, hx, hy, hz, rx, ry, rz, wx0, wy0, wz0, t_ok, zmap)
+    out.update(zncc_map=zmap, zncc_wx0=wx0, zncc_wy0=wy0, zncc_wz0=wz0, zncc_t_ok=t_ok, zncc_h=np.array([hx, hy, hz]),
+               zncc_r=np.array([rx, ry, rz]))
+    flat = f.copy()
+    flat[:, :, :] = 1.0  # flat template -> map of -2, never ok
+    zmap_flat = np.empty((2, 2 * rz + 1, 2 * ry + 1, 2 * rx + 1))
+    ris._zncc_direct(flat, g, coords[:2], hx, hy, hz, rx, ry, rz, wx0[:2], wy0[:2], wz0[:2], np.ones(2, bool), zmap_flat)
+    out["zncc_map_flat"] = zmap_flat
+
+    searches = {
+        "r3": dict(subset=(8, 8, 8), radius=(3, 3, 3), shift=None),
+        "shift": dict(subset=(8, 8, 8), radius=(2, 2, 2), shift=np.round(U_true).astype(np.int64)),
+        "aniso": dict(subset=(6, 8, 10), radius=(3, 2, 1), shift=None),
+        "r1": dict(subset=(8, 8, 8), radius=(1, 1, 1), shift=None),
+    }
+    for name, c in searches.items():
+        res = ris.ncc_search(f, g, coords, c["subset"], c["radius"], c["shift"], backend="numba")
+        for k in ("disp", "cc", "pce", "clipped", "ok"):
+            out[f"ncc_{name}_{k}"] = res[k]
+    res = ris.ncc_search_expanding(f, g, coords, (8, 8, 8), (1, 1, 1), None, True, 3, backend="numba")
+    for k in ("disp", "cc", "pce", "clipped", "ok"):
+        out[f"nccx_{k}"] = res[k]
+    out["nccx_expansions"] = res["expansions"]
+    out["nccx_radius"] = np.array(res["radius"])
+
+    # --- global step (hex8 FEM, PCG) ---
+    gm = mesh_setup(np.arange(6) * 6.0, np.arange(5) * 7.0, np.arange(4) * 5.0)
+    nn = gm.n_nodes
+    node_valid = np.ones(nn, dtype=bool)
+    node_valid[[7, 8, 33]] = False
+    elems = gm.elements.copy()
+    bad = ~node_valid[elems].all(axis=1)
+    elems[bad, :] = -1
+    gm.elements = elems
+    gm.node_valid = node_valid
+    ops = build_fem_operators(gm, 2)
+    para = dvcpara_default(global_solver="pcg", pcg_tol=1e-10, pcg_max_iter=500)
+    rng = np.random.default_rng(5)
+    U1 = rng.normal(0, 0.5, (nn, 3))
+    F1 = rng.normal(0, 0.01, (nn, 3, 3))
+    W = rng.normal(0, 0.002, (nn, 3, 3))
+    v = rng.normal(0, 0.05, (nn, 3))
+    system = build_global_system(ops, 1e-3, 1e-3, 0.0, para)
+    U2, info = solve_subpb2(system, U1, F1, W, v)
+    Fg = nodal_gradient(ops, U2)
+    b = global_rhs(ops, 1e-3, 1e-3, 0.0, U1, F1, W, v)
+    out.update(pcg_elem_active=~bad, pcg_grid_shape=np.array(gm.grid_shape), pcg_spacing=np.array(gm.spacing), pcg_U1=U1,
+               pcg_F1=F1, pcg_W=W, pcg_v=v, pcg_U2=U2, pcg_iters=info["iterations"], pcg_F=Fg, pcg_rhs=b,
+               pcg_active=ops.active)
+    system2 = build_global_system(ops, 0.05, 1e-3, 0.01, para)
+    U2b, infob = solve_subpb2(system2, U1, F1, W, v)
+    out.update(pcg_alpha_U2=U2b, pcg_alpha_iters=infob["iterations"])
+
+    path = os.path.join(HERE, "golden_kernels.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
+if __name__ == "__main__":
+    main()
