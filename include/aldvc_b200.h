@@ -1,0 +1,178 @@
+/*
+ * aldvc_b200 -- C ABI of the B200 (sm_100a) AL-DVC hot-path library.
+ *
+ * Every entry point takes device pointers, sizes and a cudaStream_t (passed
+ * as void*), enqueues its work on that stream and returns an int: 0 on
+ * success, a negative code on an argument or CUDA error (the message is in
+ * aldvc_last_error()).  Numerical failures of single nodes are never errors:
+ * they are per-node status codes, as in the reference.  Nothing here
+ * allocates device memory except where a function says so; scratch memory
+ * is a caller-provided workspace sized by the matching *_workspace_size().
+ *
+ * Reference interfaces replaced (pyALDVC v1.2.1, src/al_dvc/...):
+ *   aldvc_precompute  <- solver/cuda_kernels.py:1635 precompute_nodes_cuda
+ *                        (contract of solver/numba_kernels.py:499 precompute_nodes)
+ *   aldvc_icgn12      <- solver/cuda_kernels.py:1397 icgn_12dof_cuda
+ *                        (contract of solver/numba_kernels.py:1211 icgn_12dof_parallel)
+ *   aldvc_icgn3       <- solver/cuda_kernels.py:1518 icgn_3dof_cuda
+ *                        (contract of solver/numba_kernels.py:1281 icgn_3dof_parallel)
+ *   aldvc_ncc_map     <- solver/cuda_kernels.py:1713 zncc_direct_cuda
+ *                        (contract of solver/integer_search.py:44 _zncc_direct)
+ *   aldvc_ncc_search  <- solver/integer_search.py:329 ncc_search (map, argmax, PCE,
+ *                        clipped flag and sub-voxel refinement on the device)
+ *   aldvc_global_rhs  <- solver/subpb2_solver.py:111 global_rhs
+ *   aldvc_pcg_hex8    <- solver/subpb2_solver.py:77 pcg_multi over
+ *                        solver/subpb2_solver.py:45 build_global_system (hex8 FEM)
+ *   aldvc_nodal_gradient <- solver/global_operators.py:151 nodal_gradient (FEM)
+ *   aldvc_gradients   <- io/volume_ops.py:124 _gradient_stencil7
+ */
+#ifndef ALDVC_B200_H
+#define ALDVC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALDVC_ABI_VERSION 1
+
+/* status codes of a node (pyALDVC core/data_structures.py:26-43) */
+#define ALDVC_CONVERGED 0
+#define ALDVC_MAX_ITER 1
+#define ALDVC_OUT_OF_BOUNDS 2
+#define ALDVC_INVALID_SUBSET 3
+#define ALDVC_SINGULAR 4
+#define ALDVC_NAN 5
+#define ALDVC_SKIPPED 6
+#define ALDVC_STALLED 7
+
+/* error codes returned by the entry points */
+#define ALDVC_OK 0
+#define ALDVC_ERR_ARG -1
+#define ALDVC_ERR_CUDA -2
+#define ALDVC_ERR_WORKSPACE -3
+#define ALDVC_ERR_UNSUPPORTED -4
+
+/* IC-GN kernel variants */
+#define ALDVC_BATCHED 0 /* persistent work-queue kernel, subset bricks in shared memory */
+#define ALDVC_PLAIN 1   /* one node per block, two passes through a global sample buffer */
+
+/* Reference frame and deformed frame of one correlation (all device pointers). */
+typedef struct aldvc_volumes {
+    const float *f;       /* reference volume (nz, ny, nx) */
+    const float *gx;      /* reference gradients (nz, ny, nx); NULL: 7-point stencil on f in the kernels */
+    const float *gy;
+    const float *gz;
+    const uint8_t *mask;  /* reference mask (nz, ny, nx), 0 = not material; NULL: every voxel counts */
+    const float *g;       /* deformed volume prepared for the interpolation mode; NaN voxels are excluded */
+    int64_t nz, ny, nx;
+} aldvc_volumes;
+
+/* Subset geometry shared by every node of a call. */
+typedef struct aldvc_subset {
+    int32_t hx, hy, hz;          /* half-widths (winsize // 2) */
+    int32_t stride;              /* sample every stride-th voxel per axis (>= 1) */
+    int32_t mode;                /* 0 trilinear, 1 Keys cubic (a = -0.5), 2 cubic B-spline on prefiltered g */
+    int32_t reserved;
+    const int64_t *split_index;  /* (N,) row of split_keep per node, -1 = whole subset; NULL: no splitting */
+    const uint8_t *split_keep;   /* (rows, keep_bytes) packed keep bits in sampling order */
+    int64_t keep_bytes;
+} aldvc_subset;
+
+/* IC-GN controls (pyALDVC core/config.py:76-95 field meanings). */
+typedef struct aldvc_icgn_params {
+    double tol;           /* relative gradient-norm tolerance (icgn_tol) */
+    double dp_tol;        /* parameter-increment tolerance in voxels (icgn_dp_tol) */
+    int32_t max_iter;     /* icgn_max_iter */
+    int32_t patience;     /* icgn_patience, 0 disables the stall rule */
+    double noise_gain;    /* > 0 (with H_all and pattern): noise-corrected Hessian steps */
+    int32_t predictive;   /* icgn_predictive_stop */
+    int32_t variant;      /* ALDVC_BATCHED or ALDVC_PLAIN */
+    int32_t threads;      /* threads per block: 0 = library default */
+    int32_t brick_floats; /* batched: shared-memory brick capacity in floats, 0 = library default */
+    double mu;            /* 3-DOF: ADMM penalty */
+    double n_full;        /* 3-DOF: sampled voxels of a full subset (noise-correction scale) */
+} aldvc_icgn_params;
+
+/* Uniform hex8 node grid of the global step, node n = iz*ny*nx + iy*nx + ix. */
+typedef struct aldvc_hex8_mesh {
+    int64_t nx, ny, nz;            /* nodes per axis */
+    double sx, sy, sz;             /* node spacing (element edge lengths) */
+    const uint8_t *elem_active;    /* ((nz-1)(ny-1)(nx-1),) 1 = element kept; NULL: all kept */
+    int32_t gauss_order;           /* 1, 2 or 3 */
+    int32_t reserved;
+} aldvc_hex8_mesh;
+
+/* ---------------------------------------------------------------- library */
+int aldvc_abi_version(void);
+const char *aldvc_last_error(void);
+/* name of device `device`, its SM count and compute capability; returns ALDVC_OK */
+int aldvc_device_info(int device, char *name, int name_len, int *sm_count, int *cc_major, int *cc_minor);
+
+/* ---------------------------------------------------------------- volume preprocessing */
+/* 7-point central-difference gradients, zero within `border` voxels of a face */
+int aldvc_gradients(const float *f, int64_t nz, int64_t ny, int64_t nx, int32_t border, float *gx, float *gy, float *gz,
+                    void *stream);
+
+/* ---------------------------------------------------------------- local subset solver */
+/* Per-node Hessian H (N,12,12), its Cholesky factor L (N,12,12), meanf, bottomf, n_valid, valid. */
+int aldvc_precompute(const aldvc_volumes *vol, const aldvc_subset *sub, const int64_t *coords, int64_t n_nodes,
+                     double min_valid_ratio, double cond_max, double *H_all, double *L_all, double *meanf, double *bottomf,
+                     int64_t *n_valid, uint8_t *valid, void *stream);
+
+/* bytes of workspace aldvc_icgn12/aldvc_icgn3 need for `n_nodes` nodes with these params */
+size_t aldvc_icgn_workspace_size(const aldvc_subset *sub, int64_t n_nodes, const aldvc_icgn_params *prm);
+
+/* 12-DOF IC-GN.  H_all/pattern may be NULL unless prm->noise_gain > 0; meanf_all is the precompute mean
+ * (only used to centre the single-pass sums).  Outputs: P_out (N,12), n_iter (N,), status (N,), zncc (N,). */
+int aldvc_icgn12(const aldvc_volumes *vol, const aldvc_subset *sub, const int64_t *coords, int64_t n_nodes, const double *P0,
+                 const double *L_all, const double *H_all, const double *pattern, const double *meanf_all, const uint8_t *valid,
+                 const aldvc_icgn_params *prm, void *workspace, size_t workspace_bytes, double *P_out, int32_t *n_iter,
+                 int8_t *status, double *zncc, void *stream);
+
+/* 3-DOF translation IC-GN with the ADMM proximal term (subproblem 1).  F_fixed (N,3,3), U_old/vdual (N,3). */
+int aldvc_icgn3(const aldvc_volumes *vol, const aldvc_subset *sub, const int64_t *coords, int64_t n_nodes, const double *U_old,
+                const double *F_fixed, const double *vdual, const double *H_all, const double *meanf_all,
+                const double *bottomf_all, const uint8_t *valid, const aldvc_icgn_params *prm, void *workspace,
+                size_t workspace_bytes, double *U_out, int32_t *n_iter, int8_t *status, double *zncc, void *stream);
+
+/* ---------------------------------------------------------------- integer search */
+/* ZNCC maps out (n, 2rz+1, 2ry+1, 2rx+1) float32 of centred templates against windows starting at
+ * (wx0, wy0, wz0); t_ok == 0 or a flat template gives a map of -2 (the reference contract). */
+int aldvc_ncc_map(const float *f, const float *g, int64_t nz, int64_t ny, int64_t nx, const int64_t *coords, int64_t n_nodes,
+                  int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz, const int64_t *wx0, const int64_t *wy0,
+                  const int64_t *wz0, const uint8_t *t_ok, float *out, void *stream);
+
+size_t aldvc_ncc_search_workspace_size(int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz);
+
+/* Whole single-level search: template size (2h+1) per axis, search radius r, optional integer prior
+ * shift0 (N,3) [x,y,z] (NULL = 0).  disp (N,3) [x,y,z] (NaN where not ok), cc, pce (N,), clipped, ok (N,). */
+int aldvc_ncc_search(const float *f, const float *g, int64_t nz, int64_t ny, int64_t nx, const int64_t *coords,
+                     int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz,
+                     const int64_t *shift0, void *workspace, size_t workspace_bytes, double *disp, double *cc, double *pce,
+                     uint8_t *clipped, uint8_t *ok, void *stream);
+
+/* ---------------------------------------------------------------- global step (ADMM subproblem 2) */
+/* b = beta sum_j G_j (F1 - W)[:,:,j] + mu M (U1 - v) + alpha Kg U1, all (N,3) / (N,3,3) FP64 */
+int aldvc_global_rhs(const aldvc_hex8_mesh *mesh, double beta, double mu, double alpha, const double *U1, const double *F1,
+                     const double *W, const double *v, double *b, void *stream);
+
+size_t aldvc_pcg_workspace_size(const aldvc_hex8_mesh *mesh);
+
+/* Jacobi-PCG on A = (beta + alpha) Kg + mu M restricted to the nodes of the kept elements, three
+ * right-hand sides B (N,3) at once from X0 (N,3); X (N,3) keeps X0 off the active set.  iters (device
+ * int32) receives the iteration count, err (device int32) a nonzero code if a grid barrier gave up. */
+int aldvc_pcg_hex8(const aldvc_hex8_mesh *mesh, double beta, double mu, double alpha, const double *B, const double *X0,
+                   double tol, int32_t max_iter, void *workspace, size_t workspace_bytes, double *X, int32_t *iters,
+                   int32_t *err, void *stream);
+
+/* F (N,3,3) = (G_j^T u_i) / m_L on the active nodes, NaN elsewhere */
+int aldvc_nodal_gradient(const aldvc_hex8_mesh *mesh, const double *U, double *F, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALDVC_B200_H */

@@ -1,0 +1,1230 @@
+// 12-DOF and 3-DOF inverse-compositional Gauss-Newton subset solvers (pyALDVC numba_kernels.py:517-1208).
+//
+// Two forms of the same method:
+//
+//  * BATCHED -- a persistent kernel: one CTA per SM slot pulls node indices from a device work counter and
+//    iterates each node to its own exit.  Per iteration the warped subset is covered by one or more
+//    z-chunks; each chunk's deformed-volume box is staged in shared memory with coalesced row loads and
+//    every subset voxel samples it there.  The residual of the ZNSSD criterion is linear in the sampled
+//    value, so one pass accumulates all moments (sum SD_k, SD_k f, SD_k g, f, f^2, g, g^2, f g) and the
+//    gradient b and the ZNCC follow from them in FP64 -- no per-voxel sample buffer, no second pass.
+//    Intensities are centred (f - meanf_precomputed, g - meang_previous) so the moments do not cancel.
+//
+//  * PLAIN -- one block per node, the layout of the reference's numba-cuda kernels: pass 1 samples g from
+//    global memory into a per-node global buffer and reduces the statistics, pass 2 re-reads the buffer
+//    and reduces the gradient.  It is the comparison baseline for the batched form.
+//
+// Both accumulate in FP32 per thread (<= S / threads voxels each), reduce in FP32 within a warp and in
+// FP64 across warps; thread 0 runs the per-iteration control in FP64 (Cholesky solve, stopping rules,
+// warp composition) exactly as the reference does.
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace aldvc {
+
+struct IcgnArgs {
+    // volumes
+    const float* f;
+    const float* gx;
+    const float* gy;
+    const float* gz;
+    const uint8_t* mask;
+    const float* g;
+    int nz, ny, nx;
+    // subset
+    int hx, hy, hz, stride, nX, nY, nZ;
+    const int64_t* split_index;
+    const uint8_t* split_keep;
+    int64_t keep_bytes;
+    // nodes
+    const int64_t* coords;
+    int64_t n_nodes;
+    int64_t node_base;  // plain: first node of this launch
+    const uint8_t* valid;
+    const double* meanf;
+    // 12-DOF
+    const double* P0;
+    const double* L;
+    const double* H;
+    const double* pattern;
+    // 3-DOF
+    const double* U_old;
+    const double* F_fixed;
+    const double* vdual;
+    const double* bottomf;
+    double mu, n_full;
+    // controls
+    double tol, dp_tol, noise_gain;
+    int max_iter, patience, predictive;
+    // outputs
+    double* P_out;  // 12-DOF (N,12) / 3-DOF (N,3)
+    int32_t* n_iter;
+    int8_t* status;
+    double* zncc;
+    // scratch
+    int* counter;       // batched work queue
+    float* gbuf;        // plain: (blocks, S)
+    int brick_cap;      // batched: floats of the shared brick
+};
+
+// ----------------------------------------------------------------------------- per-node control state
+struct Ctl12 {
+    double P[12], P_best[12];
+    double norm_init, last_dp, dp_prev, best_zncc, best_dp, zncc;
+    int stall;
+    double half_scale;
+};
+
+struct Ctl3 {
+    double P[12];
+    double Hinv[3][3];
+    double u_old[3], vd[3];
+    double bf2, norm_init, last_dn, dn_prev, best_dn, zncc;
+    int stall;
+    const double* H;
+};
+
+// Sums of one iteration after the block reduction (FP64, shifted moments).
+struct Moments {
+    int64_t n, nref;
+    int oob;
+    double Sg, Sgg, Sf, Sff, Sfg;
+    double SD[12], SDf[12], SDg[12];
+};
+
+// Statistics of the dynamic valid set (numba_kernels._warp_and_sample :586-598) and the gradient
+// b_k = bottomf * sum SD_k * res with res = (f - mf)/bf - (g - mg)/bg, from the shifted moments.
+// Returns 0 = ok, ST_OOB or ST_INVALID.
+__device__ __noinline__ int finish_moments(const Moments& m, double cf, double cg, int nb, double* b, double& bf, double& bg, double& s_cc,
+                              int64_t& n_valid) {
+    n_valid = m.n;
+    if (m.oob) return ST_OOB;
+    if (m.n < MIN_SUBSET_VOXELS || (double)m.n < MIN_VALID_FRACTION * (double)m.nref) return ST_INVALID;
+    const double n = (double)m.n;
+    const double mg = m.Sg / n, mf = m.Sf / n;
+    double ssg = m.Sgg - n * mg * mg;
+    if (ssg < 0.0) ssg = 0.0;
+    double ssf = m.Sff - n * mf * mf;
+    if (ssf < 0.0) ssf = 0.0;
+    bg = sqrt(ssg > 1e-30 ? ssg : 1e-30);
+    bf = sqrt(ssf > 1e-30 ? ssf : 1e-30);
+    const double r = bf / bg;
+    for (int k = 0; k < nb; ++k) b[k] = (m.SDf[k] - mf * m.SD[k]) - r * (m.SDg[k] - mg * m.SD[k]);
+    s_cc = m.Sfg - n * mf * mg;
+    (void)cf;
+    (void)cg;
+    return 0;
+}
+
+__device__ __noinline__ bool corrected_chol12(const double* H, const double* pattern, double corr, double* H0, double* L0) {
+    double limit = 1.0;
+    for (int i = 9; i < 12; ++i) {
+        const double c = corr * pattern[i * 12 + i];
+        if (c > 0.0) {
+            const double lim = (1.0 - MIN_CORRECTED_FRACTION) * H[i * 12 + i] / c;
+            if (lim < limit) limit = lim;
+        }
+    }
+    if (limit <= 0.0) return false;
+    for (int i = 0; i < 144; ++i) H0[i] = H[i] - corr * limit * pattern[i];
+    return chol12(H0, L0);
+}
+
+// One 12-DOF control step after the sampling pass (numba_kernels._icgn_12dof_single :686-790).
+// Returns -1 to continue, else the final status; writes zncc_out on finish.
+__device__ __noinline__ int control12(Ctl12& s, const double* b_in, double bottomf_d, double bottomg, double s_cc, int64_t n_valid,
+                         const double* L, const double* H, const double* pattern, double noise_gain, double tol, double dp_tol,
+                         int patience, int predictive, double& zncc_out) {
+    double b[12], negb[12], dP[12];
+    double norm_abs = 0.0;
+    for (int k = 0; k < 12; ++k) {
+        b[k] = b_in[k];
+        norm_abs += b[k] * b[k];
+    }
+    norm_abs = sqrt(norm_abs);
+    if (!isfinite(norm_abs)) {
+        zncc_out = nan("");
+        return ST_NAN;
+    }
+    if (s.norm_init < 0.0) s.norm_init = norm_abs;
+    const double norm_rel = s.norm_init > 1e-300 ? norm_abs / s.norm_init : 0.0;
+    const double inv_bf = 1.0 / bottomf_d, inv_bg = 1.0 / bottomg;
+    const double zncc = s_cc * inv_bf * inv_bg;
+    s.zncc = zncc;
+    if (norm_rel < tol || norm_abs < ABS_TOL) {
+        zncc_out = zncc;
+        return ST_CONVERGED;
+    }
+    for (int k = 0; k < 12; ++k) negb[k] = -b[k];
+    bool use_corr = false;
+    double H0[144], L0[144];
+    const double n_full = pattern ? pattern[9 * 12 + 9] : 0.0;
+    if (noise_gain > 0.0 && n_full > 0.0 && s.last_dp < NOISE_CORR_STEP && H) {
+        const double s2 = (1.0 - zncc > 0.0 ? 1.0 - zncc : 0.0) * bottomf_d * bottomf_d / (double)n_valid;
+        const double corr = noise_gain * s2 * ((double)n_valid / n_full);
+        use_corr = corrected_chol12(H, pattern, corr, H0, L0);
+    }
+    chol_solve12(use_corr ? L0 : L, negb, dP);
+    double dp_norm = 0.0;
+    for (int k = 0; k < 9; ++k) {
+        const double v = dP[k] * s.half_scale;
+        dp_norm += v * v;
+    }
+    for (int k = 9; k < 12; ++k) dp_norm += dP[k] * dP[k];
+    dp_norm = sqrt(dp_norm);
+    if (!isfinite(dp_norm)) {
+        zncc_out = nan("");
+        return ST_NAN;
+    }
+    s.last_dp = dp_norm;
+    if (dp_norm < dp_tol) {
+        zncc_out = zncc;
+        return ST_CONVERGED;
+    }
+    if (predictive && s.dp_prev > 0.0 && dp_norm < PREDICT_CONTRACTION * s.dp_prev && dp_norm * dp_norm < dp_tol * s.dp_prev) {
+        zncc_out = zncc;
+        if (!compose_warp(s.P, dP)) return ST_SINGULAR;
+        return ST_CONVERGED;
+    }
+    s.dp_prev = dp_norm;
+    bool improved = zncc > s.best_zncc + STALL_ZNCC_EPS;
+    if (improved) {
+        s.best_zncc = zncc;
+        for (int k = 0; k < 12; ++k) s.P_best[k] = s.P[k];
+    }
+    if (dp_norm < s.best_dp * STALL_STEP_DECAY) {
+        s.best_dp = dp_norm;
+        improved = true;
+    }
+    if (improved) {
+        s.stall = 0;
+    } else {
+        s.stall += 1;
+        if (patience > 0 && s.stall >= patience) {
+            for (int k = 0; k < 12; ++k) s.P[k] = s.P_best[k];
+            zncc_out = s.best_zncc;
+            return ST_STALLED;
+        }
+    }
+    if (!compose_warp(s.P, dP)) {
+        zncc_out = zncc;
+        return ST_SINGULAR;
+    }
+    return -1;
+}
+
+// numba_kernels._build_h3 (:910-928)
+__device__ __noinline__ bool build_h3(const double* H, double bf2, double mu, double corr, double Hinv[3][3]) {
+    double H3[3][3], Hd[3][3];
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) H3[i][j] = H[(9 + i) * 12 + 9 + j] * 2.0 / bf2;
+        const double limit_i = (1.0 - MIN_CORRECTED_FRACTION) * H[(9 + i) * 12 + 9 + i];
+        const double cc = corr < limit_i ? corr : limit_i;
+        H3[i][i] -= cc * 2.0 / bf2;
+        H3[i][i] += mu;
+    }
+    const double md = H3[1][1] > H3[2][2] ? H3[1][1] : H3[2][2];
+    const double max_diag = H3[0][0] > md ? H3[0][0] : md;
+    if (!(max_diag > 0.0)) return false;
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) Hd[i][j] = H3[i][j];
+        Hd[i][i] += LM_DAMPING_3DOF * max_diag;
+    }
+    return inv3(Hd, Hinv) != 0.0;
+}
+
+// One 3-DOF control step (numba_kernels._icgn_3dof_single :1033-1080).
+__device__ __noinline__ int control3(Ctl3& s, const double* b_in, double bottomf_d, double bottomg, double s_cc, int64_t n_valid, double mu,
+                        double noise_gain, double tol, double dp_tol, int patience, int predictive, double& zncc_out) {
+    double tb[3], dt[3];
+    double norm_abs = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        tb[k] = b_in[k] * 2.0 / s.bf2 + mu * (s.P[9 + k] - s.u_old[k] - s.vd[k]);
+        norm_abs += tb[k] * tb[k];
+    }
+    norm_abs = sqrt(norm_abs);
+    if (!isfinite(norm_abs)) {
+        zncc_out = nan("");
+        return ST_NAN;
+    }
+    if (s.norm_init < 0.0) s.norm_init = norm_abs;
+    const double norm_rel = s.norm_init > 1e-300 ? norm_abs / s.norm_init : 0.0;
+    const double zncc = s_cc * (1.0 / bottomf_d) * (1.0 / bottomg);
+    s.zncc = zncc;
+    if (norm_rel < tol || norm_abs < mu * 1e-4) {
+        zncc_out = zncc;
+        return ST_CONVERGED;
+    }
+    if (noise_gain > 0.0 && s.last_dn < NOISE_CORR_STEP) {
+        const double s2 = (1.0 - zncc > 0.0 ? 1.0 - zncc : 0.0) * bottomf_d * bottomf_d / (double)n_valid;
+        if (!build_h3(s.H, s.bf2, mu, noise_gain * s2 * (double)n_valid, s.Hinv)) build_h3(s.H, s.bf2, mu, 0.0, s.Hinv);
+    }
+    for (int i = 0; i < 3; ++i) {
+        double t = 0.0;
+        for (int j = 0; j < 3; ++j) t += s.Hinv[i][j] * tb[j];
+        dt[i] = -t;
+    }
+    const double dn = sqrt(dt[0] * dt[0] + dt[1] * dt[1] + dt[2] * dt[2]);
+    if (!isfinite(dn)) {
+        zncc_out = nan("");
+        return ST_NAN;
+    }
+    s.last_dn = dn;
+    if (dn < dp_tol) {
+        zncc_out = zncc;
+        return ST_CONVERGED;
+    }
+    const double a00 = 1.0 + s.P[0], a01 = s.P[1], a02 = s.P[2];
+    const double a10 = s.P[3], a11 = 1.0 + s.P[4], a12 = s.P[5];
+    const double a20 = s.P[6], a21 = s.P[7], a22 = 1.0 + s.P[8];
+    if (predictive && s.dn_prev > 0.0 && dn < PREDICT_CONTRACTION * s.dn_prev && dn * dn < dp_tol * s.dn_prev) {
+        s.P[9] -= a00 * dt[0] + a01 * dt[1] + a02 * dt[2];
+        s.P[10] -= a10 * dt[0] + a11 * dt[1] + a12 * dt[2];
+        s.P[11] -= a20 * dt[0] + a21 * dt[1] + a22 * dt[2];
+        zncc_out = zncc;
+        return ST_CONVERGED;
+    }
+    s.dn_prev = dn;
+    if (dn < s.best_dn * STALL_STEP_DECAY) {
+        s.best_dn = dn;
+        s.stall = 0;
+    } else {
+        s.stall += 1;
+        if (patience > 0 && s.stall >= patience) {
+            zncc_out = zncc;
+            return ST_STALLED;
+        }
+    }
+    s.P[9] -= a00 * dt[0] + a01 * dt[1] + a02 * dt[2];
+    s.P[10] -= a10 * dt[0] + a11 * dt[1] + a12 * dt[2];
+    s.P[11] -= a20 * dt[0] + a21 * dt[1] + a22 * dt[2];
+    return -1;
+}
+
+// ----------------------------------------------------------------------------- node set-up / write-back (thread 0)
+// Returns true when the node is to be iterated; otherwise its outputs are already written.
+template <int NDOF>
+__device__ __noinline__ bool node_begin(const IcgnArgs& a, int64_t node, Ctl12& c12, Ctl3& c3) {
+    if (NDOF == 12) {
+        const double* P0 = a.P0 + node * 12;
+        double* Po = a.P_out + node * 12;
+        bool finite = true;
+        for (int k = 0; k < 12; ++k) {
+            const double v = P0[k];
+            Po[k] = v;
+            c12.P[k] = v;
+            c12.P_best[k] = v;
+            finite = finite && isfinite(v);
+        }
+        a.n_iter[node] = 0;
+        a.zncc[node] = nan("");
+        if (!a.valid[node]) {
+            a.status[node] = ST_INVALID;
+            return false;
+        }
+        if (!finite) {
+            a.status[node] = ST_NAN;
+            return false;
+        }
+        c12.norm_init = -1.0;
+        c12.last_dp = 1e300;
+        c12.dp_prev = -1.0;
+        c12.best_zncc = -2.0;
+        c12.best_dp = 1e300;
+        c12.zncc = nan("");
+        c12.stall = 0;
+        c12.half_scale = (double)max(a.hx, max(a.hy, a.hz));
+        return true;
+    } else {
+        double* Uo = a.P_out + node * 3;
+        bool finite = true;
+        for (int k = 0; k < 9; ++k) {
+            c3.P[k] = a.F_fixed[node * 9 + k];
+            finite = finite && isfinite(c3.P[k]);
+        }
+        for (int k = 0; k < 3; ++k) {
+            const double u = a.U_old[node * 3 + k];
+            Uo[k] = u;
+            c3.P[9 + k] = u;
+            c3.u_old[k] = u;
+            c3.vd[k] = a.vdual[node * 3 + k];
+            finite = finite && isfinite(u);
+        }
+        a.n_iter[node] = 0;
+        a.zncc[node] = nan("");
+        if (!a.valid[node]) {
+            a.status[node] = ST_INVALID;
+            return false;
+        }
+        if (!finite) {
+            a.status[node] = ST_NAN;
+            return false;
+        }
+        double bf = a.bottomf[node];
+        double bf2 = bf * bf;
+        if (bf2 < 1e-30) bf2 = 1e-30;
+        c3.bf2 = bf2;
+        c3.H = a.H + node * 144;
+        if (!build_h3(c3.H, bf2, a.mu, 0.0, c3.Hinv)) {
+            a.status[node] = ST_SINGULAR;
+            return false;
+        }
+        c3.norm_init = -1.0;
+        c3.last_dn = 1e300;
+        c3.dn_prev = -1.0;
+        c3.best_dn = 1e300;
+        c3.zncc = nan("");
+        c3.stall = 0;
+        return true;
+    }
+}
+
+template <int NDOF>
+__device__ __noinline__ void node_end(const IcgnArgs& a, int64_t node, const Ctl12& c12, const Ctl3& c3, int it, int st, double zc) {
+    if (NDOF == 12) {
+        for (int k = 0; k < 12; ++k) a.P_out[node * 12 + k] = c12.P[k];
+    } else {
+        for (int k = 0; k < 3; ++k) a.P_out[node * 3 + k] = c3.P[9 + k];
+    }
+    a.n_iter[node] = it;
+    a.status[node] = (int8_t)st;
+    a.zncc[node] = zc;
+}
+
+// ----------------------------------------------------------------------------- sampling helpers
+// Sampling box of subset planes [zc0, zc1) under warp P: voxel bounds of every tap plus one voxel of
+// margin for FP32 rounding, clamped to the volume.  Also reports whether all 8 corners lie in the
+// admissible domain (then no voxel can leave it: the warp is affine).
+struct Box {
+    int x0, y0, z0, bx, by, bz;
+    bool corners_in;
+};
+
+__device__ __noinline__ Box warp_box(const IcgnArgs& a, const double* P, int64_t xc, int64_t yc, int64_t zc, int zc0, int zc1, int mode) {
+    const double a00 = 1.0 + P[0], a01 = P[1], a02 = P[2], a10 = P[3], a11 = 1.0 + P[4], a12 = P[5], a20 = P[6], a21 = P[7],
+                 a22 = 1.0 + P[8];
+    const double tx = (double)xc + P[9], ty = (double)yc + P[10], tz = (double)zc + P[11];
+    const double Xs[2] = {(double)-a.hx, (double)(-a.hx + (a.nX - 1) * a.stride)};
+    const double Ys[2] = {(double)-a.hy, (double)(-a.hy + (a.nY - 1) * a.stride)};
+    const double Zs[2] = {(double)(-a.hz + zc0 * a.stride), (double)(-a.hz + (zc1 - 1) * a.stride)};
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    bool in = true;
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int k = 0; k < 2; ++k) {
+                const double X = Xs[i], Y = Ys[j], Z = Zs[k];
+                const double p[3] = {a00 * X + a01 * Y + a02 * Z + tx, a10 * X + a11 * Y + a12 * Z + ty,
+                                     a20 * X + a21 * Y + a22 * Z + tz};
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = fmin(lo[d], p[d]);
+                    hi[d] = fmax(hi[d], p[d]);
+                }
+                in = in && margin_ok(p[2], p[1], p[0], a.nz, a.ny, a.nx);
+            }
+    const int tl = mode == 0 ? 0 : 1, th = mode == 0 ? 1 : 2;  // taps below / above floor(x)
+    const int n[3] = {a.nx, a.ny, a.nz};
+    int b0[3], b1[3];
+    for (int d = 0; d < 3; ++d) {
+        // finite guard: a NaN warp never reaches here (checked at node start / after compose)
+        double l = fmax(fmin(lo[d], 1e9), -1e9), h = fmax(fmin(hi[d], 1e9), -1e9);
+        long long f0 = (long long)floor(l) - tl - 1, f1 = (long long)floor(h) + th + 1;
+        // both ends inside the volume, so the staged rows are always readable
+        f0 = f0 < 0 ? 0 : (f0 > n[d] - 1 ? n[d] - 1 : f0);
+        f1 = f1 > n[d] - 1 ? n[d] - 1 : (f1 < 0 ? 0 : f1);
+        if (f1 < f0) f1 = f0;
+        b0[d] = (int)f0;
+        b1[d] = (int)f1;
+    }
+    Box bx;
+    bx.x0 = b0[0];
+    bx.y0 = b0[1];
+    bx.z0 = b0[2];
+    bx.bx = b1[0] - b0[0] + 1;
+    bx.by = b1[1] - b0[1] + 1;
+    bx.bz = b1[2] - b0[2] + 1;
+    bx.corners_in = in;
+    return bx;
+}
+
+// Interpolate at a position relative to a brick origin (pitch bx, plane bxy, extent ex/ey/ez).
+// Indices are clamped into the brick so no read can leave it.
+template <int MODE>
+__device__ __forceinline__ float sample_rel(const float* __restrict__ base, int bx, int bxy, int ex, int ey, int ez, float xr,
+                                            float yr, float zr) {
+    int ix = __float2int_rd(xr), iy = __float2int_rd(yr), iz = __float2int_rd(zr);
+    const float fx = xr - (float)ix, fy = yr - (float)iy, fz = zr - (float)iz;
+    if (MODE == 0) {
+        ix = min(max(ix, 0), ex - 2);
+        iy = min(max(iy, 0), ey - 2);
+        iz = min(max(iz, 0), ez - 2);
+        return sample_brick<0>(base, bx, bxy, ix, iy, iz, fx, fy, fz);
+    }
+    ix = min(max(ix, 1), ex - 3);
+    iy = min(max(iy, 1), ey - 3);
+    iz = min(max(iz, 1), ez - 3);
+    return sample_brick<MODE>(base, bx, bxy, ix, iy, iz, fx, fy, fz);
+}
+
+// Per-thread FP32 moments of the single-pass accumulation.
+template <int NDOF>
+struct Acc {
+    static constexpr int NB = NDOF == 12 ? 12 : 3;
+    float Sg, Sgg, Sf, Sff, Sfg;
+    float SD[NB], SDf[NB], SDg[NB];
+    int n, nref, oob;
+    __device__ void zero() {
+        Sg = Sgg = Sf = Sff = Sfg = 0.0f;
+#pragma unroll
+        for (int k = 0; k < NB; ++k) SD[k] = SDf[k] = SDg[k] = 0.0f;
+        n = nref = oob = 0;
+    }
+    __device__ __forceinline__ void add(float fs, float gs, float q0, float q1, float q2, float X, float Y, float Z) {
+        Sg += gs;
+        Sgg += gs * gs;
+        Sf += fs;
+        Sff += fs * fs;
+        Sfg += fs * gs;
+        const float q[3] = {q0, q1, q2};
+        if (NDOF == 12) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float qf = q[i] * fs, qg = q[i] * gs;
+                SD[3 * i] += q[i] * X;
+                SD[3 * i + 1] += q[i] * Y;
+                SD[3 * i + 2] += q[i] * Z;
+                SD[9 + i] += q[i];
+                SDf[3 * i] += qf * X;
+                SDf[3 * i + 1] += qf * Y;
+                SDf[3 * i + 2] += qf * Z;
+                SDf[9 + i] += qf;
+                SDg[3 * i] += qg * X;
+                SDg[3 * i + 1] += qg * Y;
+                SDg[3 * i + 2] += qg * Z;
+                SDg[9 + i] += qg;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                SD[i] += q[i];
+                SDf[i] += q[i] * fs;
+                SDg[i] += q[i] * gs;
+            }
+        }
+        ++n;
+    }
+};
+
+// Cross-warp FP64 totals in a fixed order (deterministic), thread 0 only.
+__device__ __noinline__ void total_moments(double (*red)[48], int (*redi)[3], int nw, int nb, Moments& out) {
+    double t[5 + 3 * 12];
+    for (int i = 0; i < 5 + 3 * nb; ++i) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[w][i];
+        t[i] = s;
+    }
+    int64_t nn = 0, nrr = 0;
+    int oo = 0;
+    for (int w = 0; w < nw; ++w) {
+        nn += redi[w][0];
+        nrr += redi[w][1];
+        oo |= redi[w][2];
+    }
+    out.n = nn;
+    out.nref = nrr;
+    out.oob = oo;
+    out.Sg = t[0];
+    out.Sgg = t[1];
+    out.Sf = t[2];
+    out.Sff = t[3];
+    out.Sfg = t[4];
+    for (int k = 0; k < nb; ++k) {
+        out.SD[k] = t[5 + k];
+        out.SDf[k] = t[5 + nb + k];
+        out.SDg[k] = t[5 + 2 * nb + k];
+    }
+}
+
+// Reduce the per-thread moments into FP64 totals in shared memory (all threads call; totals valid
+// after the final __syncthreads in thread 0's view and everyone else's).
+template <int NDOF, int THREADS>
+__device__ void reduce_moments(Acc<NDOF>& acc, double (*red)[48], int (*redi)[3], Moments& out) {
+    constexpr int NB = Acc<NDOF>::NB;
+    constexpr int NW = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float v[5 + 3 * NB];
+    v[0] = acc.Sg;
+    v[1] = acc.Sgg;
+    v[2] = acc.Sf;
+    v[3] = acc.Sff;
+    v[4] = acc.Sfg;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        v[5 + k] = acc.SD[k];
+        v[5 + NB + k] = acc.SDf[k];
+        v[5 + 2 * NB + k] = acc.SDg[k];
+    }
+#pragma unroll
+    for (int i = 0; i < 5 + 3 * NB; ++i) {
+        const float s = warp_sum(v[i]);
+        if (lane == 0) red[warp][i] = (double)s;
+    }
+    const int n = warp_sum_i(acc.n), nr = warp_sum_i(acc.nref);
+    const int oob = __any_sync(0xffffffffu, acc.oob != 0) ? 1 : 0;
+    if (lane == 0) {
+        redi[warp][0] = n;
+        redi[warp][1] = nr;
+        redi[warp][2] = oob;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) total_moments(red, redi, NW, NB, out);
+}
+
+// ----------------------------------------------------------------------------- batched persistent kernel
+struct SharedCtl {
+    double P[12];
+    float A[9];
+    float t[3];  // translation relative to the brick origin
+    int box[6];  // x0 y0 z0 bx by bz
+    int zc1;
+    int use_brick;
+    int slow;
+    int state;  // 0: iterate, 1: node finished
+    int64_t node;
+    float cf, cg;
+};
+
+template <int MODE, bool STORED, int NDOF, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(IcgnArgs a) {
+    extern __shared__ __align__(16) float brick[];
+    __shared__ SharedCtl sc;
+    __shared__ double red[THREADS / 32][48];
+    __shared__ int redi[THREADS / 32][3];
+    __shared__ Moments mom;
+    __shared__ double Ls[144];
+
+    const int tid = threadIdx.x;
+    const int64_t sxy = (int64_t)a.nx * a.ny;
+    const int nXY = a.nX * a.nY;
+    Ctl12 c12;  // live in thread 0 only
+    Ctl3 c3;
+
+    for (;;) {
+        __syncthreads();  // every thread has finished reading the previous node's control block
+        if (tid == 0) {
+            const int q = atomicAdd(a.counter, 1);
+            sc.node = q < a.n_nodes ? (int64_t)q : -1;
+            sc.state = 1;
+            if (sc.node >= 0) {
+                const int64_t node = sc.node;
+                if (node_begin<NDOF>(a, node, c12, c3)) {
+                    sc.state = 0;
+                    const double* P = NDOF == 12 ? c12.P : c3.P;
+                    for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+                    sc.cf = (float)a.meanf[node];
+                    sc.cg = sc.cf;
+                }
+            }
+        }
+        __syncthreads();
+        const int64_t node = sc.node;
+        if (node < 0) break;
+        if (sc.state != 0) continue;
+        if (NDOF == 12) {
+            for (int i = tid; i < 144; i += THREADS) Ls[i] = a.L[node * 144 + i];
+        }
+        const int64_t xc = a.coords[3 * node], yc = a.coords[3 * node + 1], zcn = a.coords[3 * node + 2];
+        const int64_t srow = a.split_index ? a.split_index[node] : -1;
+        const uint8_t* keep = srow >= 0 ? a.split_keep + srow * a.keep_bytes : nullptr;
+        // a subset that crosses a volume face (only possible for nodes the caller marks valid against the
+        // precompute's verdict) reads no voxel outside the volume: those voxels are skipped
+        const bool inside = xc - a.hx >= 0 && xc + a.hx < a.nx && yc - a.hy >= 0 && yc + a.hy < a.ny && zcn - a.hz >= 0 &&
+                            zcn + a.hz < a.nz;
+        __syncthreads();
+
+        int it = 1;
+        for (; it <= a.max_iter; ++it) {
+            Acc<NDOF> acc;
+            acc.zero();
+            int zc0 = 0;
+            while (zc0 < a.nZ) {
+                if (tid == 0) {
+                    // largest chunk of subset planes whose box fits in the brick
+                    int lo = zc0 + 1, hi = a.nZ, best = zc0 + 1;
+                    Box bb = warp_box(a, sc.P, xc, yc, zcn, zc0, hi, MODE);
+                    bool fits = (long long)bb.bx * bb.by * bb.bz <= a.brick_cap;
+                    if (fits) {
+                        best = hi;
+                    } else {
+                        while (lo <= hi) {
+                            const int mid = (lo + hi) / 2;
+                            Box t = warp_box(a, sc.P, xc, yc, zcn, zc0, mid, MODE);
+                            if ((long long)t.bx * t.by * t.bz <= a.brick_cap) {
+                                best = mid;
+                                bb = t;
+                                lo = mid + 1;
+                            } else {
+                                hi = mid - 1;
+                            }
+                        }
+                        bb = warp_box(a, sc.P, xc, yc, zcn, zc0, best, MODE);
+                    }
+                    const bool use = (long long)bb.bx * bb.by * bb.bz <= a.brick_cap;
+                    sc.use_brick = use ? 1 : 0;
+                    sc.zc1 = best;
+                    sc.slow = bb.corners_in ? 0 : 1;
+                    if (!use) {  // a single plane does not fit: sample the global volume directly
+                        bb.x0 = 0;
+                        bb.y0 = 0;
+                        bb.z0 = 0;
+                        bb.bx = a.nx;
+                        bb.by = a.ny;
+                        bb.bz = a.nz;
+                    }
+                    sc.box[0] = bb.x0;
+                    sc.box[1] = bb.y0;
+                    sc.box[2] = bb.z0;
+                    sc.box[3] = bb.bx;
+                    sc.box[4] = bb.by;
+                    sc.box[5] = bb.bz;
+                    const double* P = sc.P;
+                    sc.A[0] = (float)(1.0 + P[0]);
+                    sc.A[1] = (float)P[1];
+                    sc.A[2] = (float)P[2];
+                    sc.A[3] = (float)P[3];
+                    sc.A[4] = (float)(1.0 + P[4]);
+                    sc.A[5] = (float)P[5];
+                    sc.A[6] = (float)P[6];
+                    sc.A[7] = (float)P[7];
+                    sc.A[8] = (float)(1.0 + P[8]);
+                    sc.t[0] = (float)(((double)xc - bb.x0) + P[9]);
+                    sc.t[1] = (float)(((double)yc - bb.y0) + P[10]);
+                    sc.t[2] = (float)(((double)zcn - bb.z0) + P[11]);
+                }
+                __syncthreads();
+                const int zc1 = sc.zc1;
+                const int bx0 = sc.box[0], by0 = sc.box[1], bz0 = sc.box[2];
+                const int BX = sc.box[3], BY = sc.box[4], BZ = sc.box[5];
+                const bool use_brick = sc.use_brick != 0;
+                const bool slow = sc.slow != 0;
+                if (use_brick) {
+                    // coalesced row loads of the box into shared memory
+                    const int rows = BY * BZ;
+                    const int warp = tid >> 5, lane = tid & 31;
+                    for (int r = warp; r < rows; r += THREADS / 32) {
+                        const int ry = r % BY, rz = r / BY;
+                        const float* src = a.g + (int64_t)(bz0 + rz) * sxy + (int64_t)(by0 + ry) * a.nx + bx0;
+                        float* dst = brick + r * BX;
+                        for (int x = lane; x < BX; x += 32) dst[x] = __ldg(src + x);
+                    }
+                    __syncthreads();
+                }
+                const float* base = use_brick ? brick : a.g;
+                const int pitch = use_brick ? BX : a.nx;
+                const int plane = use_brick ? BX * BY : (int)sxy;
+                const float A0 = sc.A[0], A1 = sc.A[1], A2 = sc.A[2], A3 = sc.A[3], A4 = sc.A[4], A5 = sc.A[5], A6 = sc.A[6],
+                            A7 = sc.A[7], A8 = sc.A[8];
+                const float T0 = sc.t[0], T1 = sc.t[1], T2 = sc.t[2];
+                const float cf = sc.cf, cg = sc.cg;
+                // voxels of planes [zc0, zc1) in sampling order
+                const int v0 = zc0 * nXY, v1 = zc1 * nXY;
+                for (int v = v0 + tid; v < v1; v += THREADS) {
+                    const int iz = v / nXY, rem = v - iz * nXY;
+                    const int iy = rem / a.nX, ix = rem - iy * a.nX;
+                    const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+                    const int64_t xx = xc + dx, yy = yc + dy, zz = zcn + dz;
+                    bool k;
+                    if (keep || !inside) {
+                        k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
+                        if (k) k = keep ? kept_bit(keep, v) : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0);
+                    } else {
+                        k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0;
+                    }
+                    if (!k) continue;
+                    acc.nref += 1;
+                    const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+                    if (slow) {
+                        const double* P = sc.P;
+                        const double xw = (1.0 + P[0]) * dx + P[1] * dy + P[2] * dz + ((double)xc + P[9]);
+                        const double yw = P[3] * dx + (1.0 + P[4]) * dy + P[5] * dz + ((double)yc + P[10]);
+                        const double zw = P[6] * dx + P[7] * dy + (1.0 + P[8]) * dz + ((double)zcn + P[11]);
+                        if (!margin_ok(zw, yw, xw, a.nz, a.ny, a.nx)) {
+                            acc.oob = 1;
+                            continue;
+                        }
+                    }
+                    const float xr = A0 * X + A1 * Y + A2 * Z + T0;
+                    const float yr = A3 * X + A4 * Y + A5 * Z + T1;
+                    const float zr = A6 * X + A7 * Y + A8 * Z + T2;
+                    const float gv = sample_rel<MODE>(base, pitch, plane, BX, BY, BZ, xr, yr, zr);
+                    if (gv != gv) continue;  // NaN: masked out in the deformed frame
+                    const int64_t o = zz * sxy + yy * a.nx + xx;
+                    const float fv = __ldg(a.f + o);
+                    float q0, q1, q2;
+                    if (STORED) {
+                        q0 = __ldg(a.gx + o);
+                        q1 = __ldg(a.gy + o);
+                        q2 = __ldg(a.gz + o);
+                    } else {
+                        grad_otf(a.f, a.nz, a.ny, a.nx, (int)zz, (int)yy, (int)xx, q0, q1, q2);
+                    }
+                    acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
+                }
+                zc0 = zc1;
+                __syncthreads();  // the next chunk overwrites the brick
+            }
+            reduce_moments<NDOF, THREADS>(acc, red, redi, mom);
+            if (tid == 0) {
+                double b[12], bf, bg, s_cc;
+                int64_t nv;
+                const int st0 = finish_moments(mom, sc.cf, sc.cg, NDOF == 12 ? 12 : 3, b, bf, bg, s_cc, nv);
+                int st;
+                double zc = nan("");
+                if (st0 != 0) {
+                    st = st0;  // OOB / invalid subset: zncc stays NaN
+                } else if (NDOF == 12) {
+                    st = control12(c12, b, bf, bg, s_cc, nv, Ls, a.H ? a.H + node * 144 : nullptr, a.pattern, a.noise_gain, a.tol,
+                                   a.dp_tol, a.patience, a.predictive, zc);
+                } else {
+                    st = control3(c3, b, bf, bg, s_cc, nv, a.mu, a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+                }
+                if (st >= 0) {
+                    node_end<NDOF>(a, node, c12, c3, it, st, zc);
+                    sc.state = 1;
+                } else {
+                    const double* P = NDOF == 12 ? c12.P : c3.P;
+                    for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+                    sc.cg = (float)((double)sc.cg + mom.Sg / (double)mom.n);  // centre g on this iteration's mean
+                    if (it == a.max_iter) {
+                        const double zc_last = NDOF == 12 ? c12.zncc : c3.zncc;
+                        node_end<NDOF>(a, node, c12, c3, a.max_iter, ST_MAX_ITER, zc_last);
+                        sc.state = 1;
+                    }
+                }
+            }
+            __syncthreads();
+            if (sc.state != 0) break;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------- plain one-node-per-block kernel
+template <int MODE, bool STORED, int NDOF>
+__global__ void __launch_bounds__(256) icgn_plain_kernel(IcgnArgs a) {
+    constexpr int THREADS = 256;
+    constexpr int NB = NDOF == 12 ? 12 : 3;
+    __shared__ SharedCtl sc;
+    __shared__ double red[THREADS / 32][48];
+    __shared__ int redi[THREADS / 32][3];
+    __shared__ Moments mom;
+    __shared__ double stat[4];  // meanf_d, meang, inv_bf, inv_bg
+    __shared__ double Ls[144];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t node = a.node_base + blockIdx.x;
+    if (node >= a.n_nodes) return;
+    const int64_t sxy = (int64_t)a.nx * a.ny;
+    const int nXY = a.nX * a.nY;
+    const int S = nXY * a.nZ;
+    float* gbuf = a.gbuf + (int64_t)blockIdx.x * S;
+    Ctl12 c12;
+    Ctl3 c3;
+    if (tid == 0) {
+        sc.state = node_begin<NDOF>(a, node, c12, c3) ? 0 : 1;
+        if (sc.state == 0) {
+            const double* P = NDOF == 12 ? c12.P : c3.P;
+            for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+            sc.cf = (float)a.meanf[node];
+        }
+    }
+    __syncthreads();
+    if (sc.state != 0) return;
+    if (NDOF == 12)
+        for (int i = tid; i < 144; i += THREADS) Ls[i] = a.L[node * 144 + i];
+    const int64_t xc = a.coords[3 * node], yc = a.coords[3 * node + 1], zcn = a.coords[3 * node + 2];
+    const int64_t srow = a.split_index ? a.split_index[node] : -1;
+    const uint8_t* keep = srow >= 0 ? a.split_keep + srow * a.keep_bytes : nullptr;
+    const bool inside = xc - a.hx >= 0 && xc + a.hx < a.nx && yc - a.hy >= 0 && yc + a.hy < a.ny && zcn - a.hz >= 0 &&
+                        zcn + a.hz < a.nz;
+    __syncthreads();
+
+    for (int it = 1; it <= a.max_iter; ++it) {
+        if (tid == 0) {
+            const Box bb = warp_box(a, sc.P, xc, yc, zcn, 0, a.nZ, MODE);
+            sc.slow = bb.corners_in ? 0 : 1;
+            const double* P = sc.P;
+            sc.A[0] = (float)(1.0 + P[0]);
+            sc.A[1] = (float)P[1];
+            sc.A[2] = (float)P[2];
+            sc.A[3] = (float)P[3];
+            sc.A[4] = (float)(1.0 + P[4]);
+            sc.A[5] = (float)P[5];
+            sc.A[6] = (float)P[6];
+            sc.A[7] = (float)P[7];
+            sc.A[8] = (float)(1.0 + P[8]);
+            sc.t[0] = (float)((double)xc + P[9]);
+            sc.t[1] = (float)((double)yc + P[10]);
+            sc.t[2] = (float)((double)zcn + P[11]);
+        }
+        __syncthreads();
+        // pass 1: sample into the global buffer, statistics of the valid set
+        Acc<NDOF> acc;
+        acc.zero();
+        const bool slow = sc.slow != 0;
+        const float cf = sc.cf;
+        for (int v = tid; v < S; v += THREADS) {
+            const int iz = v / nXY, rem = v - iz * nXY;
+            const int iy = rem / a.nX, ix = rem - iy * a.nX;
+            const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+            const int64_t xx = xc + dx, yy = yc + dy, zz = zcn + dz;
+            bool k;
+            if (keep || !inside) {
+                k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
+                if (k) k = keep ? kept_bit(keep, v) : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0);
+            } else {
+                k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0;
+            }
+            if (!k) {
+                gbuf[v] = nanf("");
+                continue;
+            }
+            acc.nref += 1;
+            const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+            if (slow) {
+                const double* P = sc.P;
+                const double xw = (1.0 + P[0]) * dx + P[1] * dy + P[2] * dz + ((double)xc + P[9]);
+                const double yw = P[3] * dx + (1.0 + P[4]) * dy + P[5] * dz + ((double)yc + P[10]);
+                const double zw = P[6] * dx + P[7] * dy + (1.0 + P[8]) * dz + ((double)zcn + P[11]);
+                if (!margin_ok(zw, yw, xw, a.nz, a.ny, a.nx)) {
+                    acc.oob = 1;
+                    gbuf[v] = nanf("");
+                    continue;
+                }
+            }
+            // absolute positions (the reference's layout: no brick)
+            const float xr = sc.A[0] * X + sc.A[1] * Y + sc.A[2] * Z + sc.t[0];
+            const float yr = sc.A[3] * X + sc.A[4] * Y + sc.A[5] * Z + sc.t[1];
+            const float zr = sc.A[6] * X + sc.A[7] * Y + sc.A[8] * Z + sc.t[2];
+            const float gv = sample_rel<MODE>(a.g, a.nx, (int)sxy, a.nx, a.ny, a.nz, xr, yr, zr);
+            gbuf[v] = gv;
+            if (gv != gv) continue;
+            const float fv = __ldg(a.f + zz * sxy + yy * a.nx + xx) - cf;
+            const float gs = gv - cf;
+            acc.Sg += gs;
+            acc.Sgg += gs * gs;
+            acc.Sf += fv;
+            acc.Sff += fv * fv;
+            acc.n += 1;
+        }
+        reduce_moments<NDOF, THREADS>(acc, red, redi, mom);
+        if (tid == 0) {
+            int st = 0;
+            if (mom.oob)
+                st = ST_OOB;
+            else if (mom.n < MIN_SUBSET_VOXELS || (double)mom.n < MIN_VALID_FRACTION * (double)mom.nref)
+                st = ST_INVALID;
+            if (st != 0) {
+                node_end<NDOF>(a, node, c12, c3, it, st, nan(""));
+                sc.state = 1;
+            } else {
+                const double n = (double)mom.n;
+                const double mg = mom.Sg / n, mf = mom.Sf / n;
+                double ssg = mom.Sgg - n * mg * mg, ssf = mom.Sff - n * mf * mf;
+                ssg = ssg < 0.0 ? 0.0 : ssg;
+                ssf = ssf < 0.0 ? 0.0 : ssf;
+                stat[0] = (double)cf + mf;
+                stat[1] = (double)cf + mg;
+                stat[2] = sqrt(ssf > 1e-30 ? ssf : 1e-30);
+                stat[3] = sqrt(ssg > 1e-30 ? ssg : 1e-30);
+            }
+        }
+        __syncthreads();
+        if (sc.state != 0) return;
+        // pass 2: residual and gradient from the buffer
+        const float mfd = (float)stat[0], mgd = (float)stat[1];
+        const float ibf = (float)(1.0 / stat[2]), ibg = (float)(1.0 / stat[3]);
+        float b[NB];
+#pragma unroll
+        for (int k = 0; k < NB; ++k) b[k] = 0.0f;
+        float scc = 0.0f;
+        for (int v = tid; v < S; v += THREADS) {
+            const float gv = gbuf[v];
+            if (gv != gv) continue;
+            const int iz = v / nXY, rem = v - iz * nXY;
+            const int iy = rem / a.nX, ix = rem - iy * a.nX;
+            const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+            const int64_t o = (zcn + dz) * sxy + (yc + dy) * a.nx + (xc + dx);
+            const float fd = __ldg(a.f + o) - mfd;
+            const float gd = gv - mgd;
+            scc += fd * gd;
+            const float res = fd * ibf - gd * ibg;
+            float q0, q1, q2;
+            if (STORED) {
+                q0 = __ldg(a.gx + o);
+                q1 = __ldg(a.gy + o);
+                q2 = __ldg(a.gz + o);
+            } else {
+                grad_otf(a.f, a.nz, a.ny, a.nx, (int)(zcn + dz), (int)(yc + dy), (int)(xc + dx), q0, q1, q2);
+            }
+            const float r0 = q0 * res, r1 = q1 * res, r2 = q2 * res;
+            if (NDOF == 12) {
+                const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+                b[0] += r0 * X;
+                b[1] += r0 * Y;
+                b[2] += r0 * Z;
+                b[3] += r1 * X;
+                b[4] += r1 * Y;
+                b[5] += r1 * Z;
+                b[6] += r2 * X;
+                b[7] += r2 * Y;
+                b[8] += r2 * Z;
+                b[9] += r0;
+                b[10] += r1;
+                b[11] += r2;
+            } else {
+                b[0] += r0;
+                b[1] += r1;
+                b[2] += r2;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NB; ++k) {
+            const float s = warp_sum(b[k]);
+            if (lane == 0) red[warp][k] = (double)s;
+        }
+        {
+            const float s = warp_sum(scc);
+            if (lane == 0) red[warp][NB] = (double)s;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double bt[12], sccd = 0.0;
+            for (int k = 0; k < NB; ++k) {
+                double s = 0.0;
+                for (int w = 0; w < THREADS / 32; ++w) s += red[w][k];
+                bt[k] = s * stat[2];  // b *= bottomf (numba_kernels.py:727-729)
+            }
+            for (int w = 0; w < THREADS / 32; ++w) sccd += red[w][NB];
+            double zc = nan("");
+            int st;
+            if (NDOF == 12)
+                st = control12(c12, bt, stat[2], stat[3], sccd, mom.n, Ls, a.H ? a.H + node * 144 : nullptr, a.pattern,
+                               a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+            else
+                st = control3(c3, bt, stat[2], stat[3], sccd, mom.n, a.mu, a.noise_gain, a.tol, a.dp_tol, a.patience,
+                              a.predictive, zc);
+            if (st >= 0) {
+                node_end<NDOF>(a, node, c12, c3, it, st, zc);
+                sc.state = 1;
+            } else {
+                const double* P = NDOF == 12 ? c12.P : c3.P;
+                for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+                if (it == a.max_iter) {
+                    node_end<NDOF>(a, node, c12, c3, a.max_iter, ST_MAX_ITER, NDOF == 12 ? c12.zncc : c3.zncc);
+                    sc.state = 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (sc.state != 0) return;
+    }
+}
+
+// ----------------------------------------------------------------------------- launch plumbing
+constexpr int PLAIN_CHUNK = 8192;  // nodes per plain launch (sample buffer rows)
+
+struct LaunchCfg {
+    int threads;
+    int brick_cap;
+};
+
+static LaunchCfg batched_cfg(const aldvc_icgn_params* prm) {
+    LaunchCfg c;
+    c.threads = prm->threads > 0 ? prm->threads : 256;
+    if (c.threads != 256 && c.threads != 512) c.threads = 256;
+    c.brick_cap = prm->brick_floats > 0 ? prm->brick_floats : 24 * 1024;
+    return c;
+}
+
+template <int MODE, bool STORED, int NDOF, int THREADS>
+static int launch_batched_t(const IcgnArgs& a, int brick_cap, cudaStream_t s) {
+    auto kern = icgn_batched_kernel<MODE, STORED, NDOF, THREADS>;
+    const size_t smem = (size_t)brick_cap * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "icgn batched: shared memory attribute");
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "icgn batched: occupancy");
+    if (per_sm < 1) return arg_fail("icgn batched: brick does not fit in shared memory");
+    long long grid = (long long)per_sm * sm_count();
+    if (grid > a.n_nodes) grid = a.n_nodes;
+    kern<<<(unsigned)grid, THREADS, smem, s>>>(a);
+    return check_launch("icgn batched");
+}
+
+template <int MODE, bool STORED, int NDOF>
+static int launch_batched_m(const IcgnArgs& a, const LaunchCfg& c, cudaStream_t s) {
+    switch (c.threads) {
+        case 512: return launch_batched_t<MODE, STORED, NDOF, 512>(a, c.brick_cap, s);
+        default: return launch_batched_t<MODE, STORED, NDOF, 256>(a, c.brick_cap, s);
+    }
+}
+
+template <int MODE, bool STORED, int NDOF>
+static int launch_plain_m(IcgnArgs a, cudaStream_t s) {
+    for (int64_t start = 0; start < a.n_nodes; start += PLAIN_CHUNK) {
+        a.node_base = start;
+        const int64_t n = std::min<int64_t>(PLAIN_CHUNK, a.n_nodes - start);
+        icgn_plain_kernel<MODE, STORED, NDOF><<<(unsigned)n, 256, 0, s>>>(a);
+        const int rc = check_launch("icgn plain");
+        if (rc) return rc;
+    }
+    return ALDVC_OK;
+}
+
+template <int NDOF>
+static int dispatch(const IcgnArgs& a, int mode, bool stored, int variant, const LaunchCfg& c, cudaStream_t s) {
+    if (variant == ALDVC_PLAIN) {
+        if (mode == 0) return stored ? launch_plain_m<0, true, NDOF>(a, s) : launch_plain_m<0, false, NDOF>(a, s);
+        if (mode == 1) return stored ? launch_plain_m<1, true, NDOF>(a, s) : launch_plain_m<1, false, NDOF>(a, s);
+        return stored ? launch_plain_m<2, true, NDOF>(a, s) : launch_plain_m<2, false, NDOF>(a, s);
+    }
+    if (mode == 0) return stored ? launch_batched_m<0, true, NDOF>(a, c, s) : launch_batched_m<0, false, NDOF>(a, c, s);
+    if (mode == 1) return stored ? launch_batched_m<1, true, NDOF>(a, c, s) : launch_batched_m<1, false, NDOF>(a, c, s);
+    return stored ? launch_batched_m<2, true, NDOF>(a, c, s) : launch_batched_m<2, false, NDOF>(a, c, s);
+}
+
+static int fill_common(IcgnArgs& a, const aldvc_volumes* vol, const aldvc_subset* sub, const int64_t* coords, int64_t n,
+                       const aldvc_icgn_params* prm) {
+    ALDVC_REQUIRE(vol && sub && prm, "icgn: null descriptor");
+    ALDVC_REQUIRE(vol->f && vol->g && coords, "icgn: null volume/coords pointer");
+    ALDVC_REQUIRE(sub->hx >= 0 && sub->hy >= 0 && sub->hz >= 0 && sub->stride >= 1, "icgn: bad subset");
+    ALDVC_REQUIRE(sub->mode >= 0 && sub->mode <= 2, "icgn: mode must be 0, 1 or 2");
+    ALDVC_REQUIRE(vol->nz >= 4 && vol->ny >= 4 && vol->nx >= 4 && vol->nx * vol->ny < (1LL << 31) && vol->nz < (1 << 30),
+                  "icgn: bad volume shape");
+    ALDVC_REQUIRE(n < (1LL << 31), "icgn: too many nodes");
+    ALDVC_REQUIRE(prm->max_iter >= 1, "icgn: max_iter must be >= 1");
+    const bool stored = vol->gx && vol->gy && vol->gz;
+    ALDVC_REQUIRE(stored || (!vol->gx && !vol->gy && !vol->gz), "icgn: give all three gradients or none");
+    ALDVC_REQUIRE(!sub->split_index || (sub->split_keep && sub->keep_bytes > 0), "icgn: split rows missing");
+    std::memset(&a, 0, sizeof(a));
+    a.f = vol->f;
+    a.gx = vol->gx;
+    a.gy = vol->gy;
+    a.gz = vol->gz;
+    a.mask = vol->mask;
+    a.g = vol->g;
+    a.nz = (int)vol->nz;
+    a.ny = (int)vol->ny;
+    a.nx = (int)vol->nx;
+    a.hx = sub->hx;
+    a.hy = sub->hy;
+    a.hz = sub->hz;
+    a.stride = sub->stride;
+    a.nX = (2 * sub->hx) / sub->stride + 1;
+    a.nY = (2 * sub->hy) / sub->stride + 1;
+    a.nZ = (2 * sub->hz) / sub->stride + 1;
+    a.split_index = sub->split_index;
+    a.split_keep = sub->split_keep;
+    a.keep_bytes = sub->keep_bytes;
+    a.coords = coords;
+    a.n_nodes = n;
+    a.tol = prm->tol;
+    a.dp_tol = prm->dp_tol;
+    a.noise_gain = prm->noise_gain;
+    a.max_iter = prm->max_iter;
+    a.patience = prm->patience;
+    a.predictive = prm->predictive;
+    a.mu = prm->mu;
+    a.n_full = prm->n_full;
+    return ALDVC_OK;
+}
+
+static size_t workspace_bytes(const aldvc_subset* sub, int64_t n, const aldvc_icgn_params* prm) {
+    size_t b = 256;  // work counter
+    if (prm && prm->variant == ALDVC_PLAIN && sub) {
+        const int64_t S = subset_count(sub->hx, sub->hy, sub->hz, std::max(1, sub->stride));
+        b += (size_t)std::min<int64_t>(n, PLAIN_CHUNK) * (size_t)S * sizeof(float);
+    }
+    return b;
+}
+
+static int run(IcgnArgs& a, int ndof, int mode, bool stored, const aldvc_icgn_params* prm, void* ws, size_t ws_bytes,
+               const aldvc_subset* sub, cudaStream_t s) {
+    const size_t need = workspace_bytes(sub, a.n_nodes, prm);
+    if (!ws || ws_bytes < need) {
+        set_error("icgn: workspace of %zu bytes needed, %zu given", need, ws_bytes);
+        return ALDVC_ERR_WORKSPACE;
+    }
+    a.counter = (int*)ws;
+    a.gbuf = (float*)((char*)ws + 256);
+    const LaunchCfg c = batched_cfg(prm);
+    a.brick_cap = c.brick_cap;
+    if (prm->variant != ALDVC_PLAIN) {
+        const size_t smem = (size_t)c.brick_cap * sizeof(float);
+        if (smem + 8192 > (size_t)max_smem_optin()) return arg_fail("icgn: brick_floats exceeds the shared memory per block");
+        cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
+        if (e != cudaSuccess) return cuda_fail(e, "icgn: counter reset");
+    }
+    return ndof == 12 ? dispatch<12>(a, mode, stored, prm->variant, c, s) : dispatch<3>(a, mode, stored, prm->variant, c, s);
+}
+
+}  // namespace aldvc
+
+using namespace aldvc;
+
+extern "C" size_t aldvc_icgn_workspace_size(const aldvc_subset* sub, int64_t n_nodes, const aldvc_icgn_params* prm) {
+    return workspace_bytes(sub, n_nodes, prm);
+}
+
+extern "C" int aldvc_icgn12(const aldvc_volumes* vol, const aldvc_subset* sub, const int64_t* coords, int64_t n_nodes,
+                            const double* P0, const double* L_all, const double* H_all, const double* pattern,
+                            const double* meanf_all, const uint8_t* valid, const aldvc_icgn_params* prm, void* workspace,
+                            size_t workspace_bytes_, double* P_out, int32_t* n_iter, int8_t* status, double* zncc, void* stream) {
+    IcgnArgs a;
+    int rc = fill_common(a, vol, sub, coords, n_nodes, prm);
+    if (rc) return rc;
+    ALDVC_REQUIRE(P0 && L_all && meanf_all && valid && P_out && n_iter && status && zncc, "aldvc_icgn12: null pointer");
+    const bool noise = prm->noise_gain > 0.0 && H_all && pattern;
+    if (n_nodes <= 0) return ALDVC_OK;
+    a.P0 = P0;
+    a.L = L_all;
+    a.H = noise ? H_all : nullptr;
+    a.pattern = noise ? pattern : nullptr;
+    a.noise_gain = noise ? prm->noise_gain : 0.0;
+    a.meanf = meanf_all;
+    a.valid = valid;
+    a.P_out = P_out;
+    a.n_iter = n_iter;
+    a.status = status;
+    a.zncc = zncc;
+    return run(a, 12, sub->mode, vol->gx != nullptr, prm, workspace, workspace_bytes_, sub, (cudaStream_t)stream);
+}
+
+extern "C" int aldvc_icgn3(const aldvc_volumes* vol, const aldvc_subset* sub, const int64_t* coords, int64_t n_nodes,
+                           const double* U_old, const double* F_fixed, const double* vdual, const double* H_all,
+                           const double* meanf_all, const double* bottomf_all, const uint8_t* valid, const aldvc_icgn_params* prm,
+                           void* workspace, size_t workspace_bytes_, double* U_out, int32_t* n_iter, int8_t* status, double* zncc,
+                           void* stream) {
+    IcgnArgs a;
+    int rc = fill_common(a, vol, sub, coords, n_nodes, prm);
+    if (rc) return rc;
+    ALDVC_REQUIRE(U_old && F_fixed && vdual && H_all && meanf_all && bottomf_all && valid && U_out && n_iter && status && zncc,
+                  "aldvc_icgn3: null pointer");
+    if (n_nodes <= 0) return ALDVC_OK;
+    a.U_old = U_old;
+    a.F_fixed = F_fixed;
+    a.vdual = vdual;
+    a.H = H_all;
+    a.meanf = meanf_all;
+    a.bottomf = bottomf_all;
+    a.valid = valid;
+    a.P_out = U_out;
+    a.n_iter = n_iter;
+    a.status = status;
+    a.zncc = zncc;
+    a.noise_gain = prm->noise_gain > 0.0 ? prm->noise_gain : 0.0;
+    return run(a, 3, sub->mode, vol->gx != nullptr, prm, workspace, workspace_bytes_, sub, (cudaStream_t)stream);
+}

@@ -1,0 +1,44 @@
+// Host-side plumbing shared by the entry points: error reporting and launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/aldvc_b200.h"
+
+namespace aldvc {
+
+void set_error(const char* fmt, ...);
+
+inline int cuda_fail(cudaError_t e, const char* where) {
+    set_error("%s: %s", where, cudaGetErrorString(e));
+    return ALDVC_ERR_CUDA;
+}
+
+inline int arg_fail(const char* msg) {
+    set_error("%s", msg);
+    return ALDVC_ERR_ARG;
+}
+
+// Enqueue check after a launch: a launch error is reported, an earlier asynchronous error is left
+// for the caller's next synchronisation.
+inline int check_launch(const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, where);
+    return ALDVC_OK;
+}
+
+int sm_count();
+int max_smem_optin();
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace aldvc
+
+#define ALDVC_REQUIRE(cond, msg) \
+    do {                          \
+        if (!(cond)) return aldvc::arg_fail(msg); \
+    } while (0)

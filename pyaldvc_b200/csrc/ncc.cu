@@ -1,0 +1,623 @@
+// Integer-voxel NCC search (pyALDVC solver/integer_search.py:44-151, 297-483).
+//
+// aldvc_ncc_map: the zncc_direct contract.  One CTA per (node, tile of offsets); the centred template
+//   (FP32, minus its FP64 mean) sits in shared memory, each thread owns one offset and accumulates the
+//   cross term and the window's box sums in one sweep over the template.  Window values are centred on
+//   the template mean; per template plane the FP32 partial sums are flushed into FP64 totals.
+//
+// aldvc_ncc_search: window placement, map, first-maximum argmax (C order), PCE, clipped flag, FP64
+//   re-scoring of every offset within NEAR_TIE of the FP32 maximum and of the 27-point neighbourhood of
+//   the winner, quadratic sub-voxel fit -- all on the device, in node chunks through a workspace.
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace aldvc {
+
+constexpr int NCC_THREADS = 256;
+constexpr float NEAR_TIE = 2e-4f;  // FP32 map error bound used to pick FP64 re-score candidates
+constexpr int MAX_CAND = 64;
+
+__constant__ double c_pinv[10 * 27];  // pseudo-inverse of the 27-point quadratic design (integer_search.py:210-227)
+
+struct NccGeom {
+    int nz, ny, nx;
+    int hx, hy, hz, rx, ry, rz;
+    int sx, sy, sz, vx, vy, vz, wx, wy, wz;
+    int n_tpl, nmap;
+};
+
+__host__ inline NccGeom make_geom(int64_t nz, int64_t ny, int64_t nx, int hx, int hy, int hz, int rx, int ry, int rz) {
+    NccGeom g;
+    g.nz = (int)nz;
+    g.ny = (int)ny;
+    g.nx = (int)nx;
+    g.hx = hx;
+    g.hy = hy;
+    g.hz = hz;
+    g.rx = rx;
+    g.ry = ry;
+    g.rz = rz;
+    g.sx = 2 * hx + 1;
+    g.sy = 2 * hy + 1;
+    g.sz = 2 * hz + 1;
+    g.vx = 2 * rx + 1;
+    g.vy = 2 * ry + 1;
+    g.vz = 2 * rz + 1;
+    g.wx = g.sx + 2 * rx;
+    g.wy = g.sy + 2 * ry;
+    g.wz = g.sz + 2 * rz;
+    g.n_tpl = g.sx * g.sy * g.sz;
+    g.nmap = g.vx * g.vy * g.vz;
+    return g;
+}
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum_d(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    return s;
+}
+
+// Centred template into shared memory (FP32) and its FP64 mean and sum of squares.
+// Returns false (for every thread) when the template is flat.
+__device__ bool load_template(const float* __restrict__ f, const NccGeom& G, int64_t x0, int64_t y0, int64_t z0, float* T,
+                              double* red, double& mf, double& ssf) {
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < G.n_tpl; i += blockDim.x) {
+        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
+        const float v = __ldg(f + (z0 - G.hz + k) * sxy + (y0 - G.hy + j) * G.nx + (x0 - G.hx + ii));
+        T[i] = v;
+        s += (double)v;
+    }
+    s = block_sum_d(s, red);
+    mf = s / (double)G.n_tpl;
+    double q = 0.0;
+    for (int i = threadIdx.x; i < G.n_tpl; i += blockDim.x) {
+        const double d = (double)T[i] - mf;
+        q += d * d;
+        T[i] = (float)d;
+    }
+    ssf = block_sum_d(q, red);
+    __syncthreads();
+    return !(ssf < 1e-20);
+}
+
+// ZNCC of one offset from FP32 sums (cross term and window box sums), reference normalisation.
+__device__ __forceinline__ float ncc_value(double sfg, double sg, double sgg, double n_tpl, double ssf) {
+    const double var = sgg - sg * sg / n_tpl;
+    if (var < 1e-20) return 0.0f;
+    double v = sfg / sqrt(var * ssf);
+    v = v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v);
+    return (float)v;
+}
+
+// One thread: the sums of one offset over the template (shared T), window read from global g.
+__device__ __forceinline__ void offset_sums(const float* __restrict__ g, const NccGeom& G, const float* T, int64_t zb, int64_t yb,
+                                            int64_t xb, float pilot, double& sfg, double& sg, double& sgg) {
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    sfg = sg = sgg = 0.0;
+    for (int k = 0; k < G.sz; ++k) {
+        float a = 0.0f, b = 0.0f, c = 0.0f;
+        const float* Tk = T + k * G.sx * G.sy;
+        for (int j = 0; j < G.sy; ++j) {
+            const float* gr = g + (zb + k) * sxy + (yb + j) * G.nx + xb;
+            const float* Tr = Tk + j * G.sx;
+            for (int i = 0; i < G.sx; ++i) {
+                const float v = __ldg(gr + i) - pilot;
+                a = fmaf(Tr[i], v, a);
+                b += v;
+                c = fmaf(v, v, c);
+            }
+        }
+        sfg += a;
+        sg += b;
+        sgg += c;
+    }
+}
+
+struct MapArgs {
+    const float* f;
+    const float* g;
+    const int64_t* coords;
+    const int64_t* wx0;
+    const int64_t* wy0;
+    const int64_t* wz0;
+    const uint8_t* t_ok;
+    float* out;
+    int64_t node_base, n_nodes;
+    NccGeom G;
+};
+
+// grid (tiles, nodes); dynamic smem = template floats
+__global__ void __launch_bounds__(NCC_THREADS) ncc_map_kernel(MapArgs a) {
+    extern __shared__ float T[];
+    __shared__ double red[NCC_THREADS / 32];
+    __shared__ double s_stat[2];
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    if (node >= a.n_nodes) return;
+    float* out = a.out + (int64_t)blockIdx.y * G.nmap;
+    const int d = blockIdx.x * NCC_THREADS + threadIdx.x;
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    // a template or window outside the volume is treated like t_ok == 0 (no read leaves the volume)
+    const int64_t wx0 = a.wx0[node], wy0 = a.wy0[node], wz0 = a.wz0[node];
+    const bool placed = x0 - G.hx >= 0 && x0 + G.hx < G.nx && y0 - G.hy >= 0 && y0 + G.hy < G.ny && z0 - G.hz >= 0 &&
+                        z0 + G.hz < G.nz && wx0 >= 0 && wx0 + G.wx <= G.nx && wy0 >= 0 && wy0 + G.wy <= G.ny && wz0 >= 0 &&
+                        wz0 + G.wz <= G.nz;
+    if (!a.t_ok[node] || !placed) {
+        if (d < G.nmap) out[d] = -2.0f;
+        return;
+    }
+    double mf, ssf;
+    const bool textured = load_template(a.f, G, x0, y0, z0, T, red, mf, ssf);
+    if (threadIdx.x == 0) {
+        s_stat[0] = mf;
+        s_stat[1] = ssf;
+    }
+    __syncthreads();
+    if (d >= G.nmap) return;
+    if (!textured) {
+        out[d] = -2.0f;
+        return;
+    }
+    const int dz = d / (G.vy * G.vx), r = d - dz * G.vy * G.vx, dy = r / G.vx, dx = r - dy * G.vx;
+    double sfg, sg, sgg;
+    offset_sums(a.g, G, T, wz0 + dz, wy0 + dy, wx0 + dx, (float)s_stat[0], sfg, sg, sgg);
+    out[d] = ncc_value(sfg, sg, sgg, (double)G.n_tpl, s_stat[1]);
+}
+
+// ----------------------------------------------------------------------------- fused search
+struct SearchArgs {
+    const float* f;
+    const float* g;
+    const int64_t* coords;
+    const int64_t* shift0;
+    int64_t n_nodes, node_base;
+    NccGeom G;
+    // per-node placement (workspace)
+    int64_t* wx0;
+    int64_t* wy0;
+    int64_t* wz0;
+    uint8_t* t_ok;
+    uint8_t* freeb;  // bits: lo x,y,z (1,2,4), hi x,y,z (8,16,32)
+    const float* map;  // chunk maps
+    double* disp;
+    double* cc;
+    double* pce;
+    uint8_t* clipped;
+    uint8_t* ok;
+};
+
+// integer_search.py:374-386 window placement
+__global__ void ncc_place_kernel(SearchArgs a) {
+    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (n >= a.n_nodes) return;
+    const NccGeom& G = a.G;
+    const int64_t cx = a.coords[3 * n], cy = a.coords[3 * n + 1], cz = a.coords[3 * n + 2];
+    const int64_t sx0 = a.shift0 ? a.shift0[3 * n] : 0, sy0 = a.shift0 ? a.shift0[3 * n + 1] : 0,
+                  sz0 = a.shift0 ? a.shift0[3 * n + 2] : 0;
+    a.t_ok[n] = (cx - G.hx >= 0) && (cx + G.hx < G.nx) && (cy - G.hy >= 0) && (cy + G.hy < G.ny) && (cz - G.hz >= 0) &&
+                (cz + G.hz < G.nz);
+    const int64_t dx0 = cx + sx0 - G.hx - G.rx, dy0 = cy + sy0 - G.hy - G.ry, dz0 = cz + sz0 - G.hz - G.rz;
+    auto clip = [](int64_t v, int64_t hi) { return v < 0 ? 0 : (v > hi ? hi : v); };
+    a.wx0[n] = clip(dx0, G.nx - G.wx);
+    a.wy0[n] = clip(dy0, G.ny - G.wy);
+    a.wz0[n] = clip(dz0, G.nz - G.wz);
+    uint8_t fb = 0;
+    fb |= dx0 >= 0 ? 1 : 0;
+    fb |= dy0 >= 0 ? 2 : 0;
+    fb |= dz0 >= 0 ? 4 : 0;
+    fb |= dx0 <= G.nx - G.wx ? 8 : 0;
+    fb |= dy0 <= G.ny - G.wy ? 16 : 0;
+    fb |= dz0 <= G.nz - G.wz ? 32 : 0;
+    a.freeb[n] = fb;
+}
+
+// FP64 value of one offset, the reference's arithmetic (FP64 template, float32-rounded squares).
+__device__ double rescore(const SearchArgs& a, int64_t node, const float* Tf, double mf, double ssf, int dz, int dy, int dx,
+                          double* red) {
+    const NccGeom& G = a.G;
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    const int64_t zb = a.wz0[node] + dz, yb = a.wy0[node] + dy, xb = a.wx0[node] + dx;
+    double sfg = 0.0, sg = 0.0, sgg = 0.0;
+    for (int i = threadIdx.x; i < G.n_tpl; i += blockDim.x) {
+        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
+        const float v = __ldg(a.g + (zb + k) * sxy + (yb + j) * G.nx + (xb + ii));
+        const float vv = v * v;
+        sg += (double)v;
+        sgg += (double)vv;
+        // template value in FP64: f - mean, re-read so no FP32 rounding of the centred value enters
+        const float fv = __ldg(a.f + (a.coords[3 * node + 2] - G.hz + k) * sxy + (a.coords[3 * node + 1] - G.hy + j) * G.nx +
+                               (a.coords[3 * node] - G.hx + ii));
+        sfg += ((double)fv - mf) * (double)v;
+    }
+    (void)Tf;
+    sfg = block_sum_d(sfg, red);
+    sg = block_sum_d(sg, red);
+    sgg = block_sum_d(sgg, red);
+    const double var = sgg - sg * sg / (double)G.n_tpl;
+    if (var < 1e-20) return 0.0;
+    double v = sfg / sqrt(var * ssf);
+    return v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v);
+}
+
+// one CTA per node of the chunk
+__global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
+    __shared__ double red[NCC_THREADS / 32];
+    __shared__ float s_max;
+    __shared__ int s_cand[MAX_CAND];
+    __shared__ int s_ncand;
+    __shared__ double s_neigh[27];
+    __shared__ int s_pk;
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.x;
+    if (node >= a.n_nodes) return;
+    const float* map = a.map + (int64_t)blockIdx.x * G.nmap;
+    const int tid = threadIdx.x;
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    if (!a.t_ok[node]) {
+        if (tid == 0) {
+            for (int c = 0; c < 3; ++c) a.disp[3 * node + c] = nan("");
+            a.cc[node] = nan("");
+            a.pce[node] = nan("");
+            a.clipped[node] = 0;
+            a.ok[node] = 0;
+        }
+        return;
+    }
+    // flat template: the map is -2 everywhere (integer_search.py:420-421)
+    const bool flat = map[0] < -1.5f;
+    // FP32 maximum with the first-index tie rule; the -2 marker counts as 0
+    float best = -3.0f;
+    int bidx = 0x7fffffff;
+    float mn = 3.0f;
+    for (int i = tid; i < G.nmap; i += blockDim.x) {
+        float v = map[i];
+        v = v < -1.0f ? 0.0f : v;
+        if (v > best || (v == best && i < bidx)) {
+            best = v;
+            bidx = i;
+        }
+        mn = fminf(mn, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+        if (ob > best || (ob == best && oi < bidx)) {
+            best = ob;
+            bidx = oi;
+        }
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    __shared__ float s_best[NCC_THREADS / 32], s_mn[NCC_THREADS / 32];
+    __shared__ int s_bidx[NCC_THREADS / 32];
+    if ((tid & 31) == 0) {
+        s_best[tid >> 5] = best;
+        s_bidx[tid >> 5] = bidx;
+        s_mn[tid >> 5] = mn;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        float b = s_best[0], m = s_mn[0];
+        int bi = s_bidx[0];
+        for (int w = 1; w < NCC_THREADS / 32; ++w) {
+            if (s_best[w] > b || (s_best[w] == b && s_bidx[w] < bi)) {
+                b = s_best[w];
+                bi = s_bidx[w];
+            }
+            m = fminf(m, s_mn[w]);
+        }
+        s_max = b;
+        s_pk = bi;
+        s_best[0] = m;
+        s_ncand = 0;
+    }
+    __syncthreads();
+    const float vmax = s_max, vmin = s_best[0];
+    // candidates within the FP32 error bound of the maximum, kept in C order
+    if (!flat) {
+        for (int i = tid; i < G.nmap; i += blockDim.x) {
+            float v = map[i];
+            v = v < -1.0f ? 0.0f : v;
+            if (v >= vmax - NEAR_TIE) {
+                const int slot = atomicAdd(&s_ncand, 1);
+                if (slot < MAX_CAND) s_cand[slot] = i;
+            }
+        }
+    }
+    __syncthreads();
+    // template statistics in FP64 (the reference's centred template, integer_search.py:73-88)
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    double sf = 0.0;
+    for (int i = tid; i < G.n_tpl; i += blockDim.x) {
+        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
+        sf += (double)__ldg(a.f + (z0 - G.hz + k) * sxy + (y0 - G.hy + j) * G.nx + (x0 - G.hx + ii));
+    }
+    sf = block_sum_d(sf, red);
+    const double mf = sf / (double)G.n_tpl;
+    double q = 0.0;
+    for (int i = tid; i < G.n_tpl; i += blockDim.x) {
+        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
+        const double d = (double)__ldg(a.f + (z0 - G.hz + k) * sxy + (y0 - G.hy + j) * G.nx + (x0 - G.hx + ii)) - mf;
+        q += d * d;
+    }
+    const double ssf = block_sum_d(q, red);
+    int pk = s_pk;
+    double peak = (double)vmax;
+    if (!flat) {
+        // FP64 re-score of the candidates; first maximum in C order wins (np.argmax)
+        const int nc = min(s_ncand, MAX_CAND);
+        if (tid == 0) {  // order the candidates (C order)
+            for (int i = 1; i < nc; ++i) {
+                const int v = s_cand[i];
+                int j = i - 1;
+                while (j >= 0 && s_cand[j] > v) {
+                    s_cand[j + 1] = s_cand[j];
+                    --j;
+                }
+                s_cand[j + 1] = v;
+            }
+        }
+        __syncthreads();
+        double bv = -3.0;
+        int bi = pk;
+        for (int c = 0; c < nc; ++c) {
+            const int i = s_cand[c];
+            const int dz = i / (G.vy * G.vx), r = i - dz * G.vy * G.vx, dy = r / G.vx, dx = r - dy * G.vx;
+            const double v = rescore(a, node, nullptr, mf, ssf, dz, dy, dx, red);
+            if (v > bv) {
+                bv = v;
+                bi = i;
+            }
+        }
+        if (nc > 0) {
+            pk = bi;
+            peak = bv;
+        }
+    } else {
+        peak = 0.0;
+        pk = 0;
+    }
+    const int pz = pk / (G.vy * G.vx), pr = pk - pz * G.vy * G.vx, py = pr / G.vx, px = pr - py * G.vx;
+    // PCE on the min-shifted FP32 map (integer_search.py:448-452)
+    double e = 0.0;
+    const float cmin = flat ? 0.0f : vmin;
+    for (int i = tid; i < G.nmap; i += blockDim.x) {
+        float v = map[i];
+        v = v < -1.0f ? 0.0f : v;
+        const double dv = (double)v - (double)cmin;
+        e += dv * dv;
+    }
+    e = block_sum_d(e, red) / (double)G.nmap;
+    // sub-voxel refinement on FP64 neighbours (integer_search.py:467-473, 297-321)
+    const bool at_border = px == 0 || px == 2 * G.rx || py == 0 || py == 2 * G.ry || pz == 0 || pz == 2 * G.rz;
+    const bool interior = !at_border && G.rx > 0 && G.ry > 0 && G.rz > 0 && !flat;
+    double sub[3] = {0.0, 0.0, 0.0};
+    if (interior) {
+        for (int t = 0; t < 27; ++t) {
+            const int dzz = t / 9 - 1, dyy = (t / 3) % 3 - 1, dxx = t % 3 - 1;
+            const double v = (dzz == 0 && dyy == 0 && dxx == 0) ? peak
+                                                                : rescore(a, node, nullptr, mf, ssf, pz + dzz, py + dyy, px + dxx, red);
+            if (tid == 0) s_neigh[t] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double coef[10];
+            for (int r = 0; r < 10; ++r) {
+                double s = 0.0;
+                for (int t = 0; t < 27; ++t) s += c_pinv[r * 27 + t] * s_neigh[t];
+                coef[r] = s;
+            }
+            double H[3][3] = {{2 * coef[7], coef[4], coef[5]}, {coef[4], 2 * coef[8], coef[6]}, {coef[5], coef[6], 2 * coef[9]}};
+            double Hi[3][3];
+            const double det = inv3(H, Hi);
+            if (fabs(det) > 1e-12) {
+                double sol[3];
+                bool good = true;
+                for (int i = 0; i < 3; ++i) {
+                    sol[i] = -(Hi[i][0] * coef[1] + Hi[i][1] * coef[2] + Hi[i][2] * coef[3]);
+                    good = good && isfinite(sol[i]) && fabs(sol[i]) <= 1.0;
+                }
+                if (good)
+                    for (int i = 0; i < 3; ++i) sub[i] = sol[i];
+            }
+        }
+    }
+    if (tid == 0) {
+        const double pmin = peak - (double)cmin;
+        const double pce = e > 1e-30 ? pmin * pmin / e : 0.0;
+        const uint8_t fb = a.freeb[node];
+        bool on_edge = false;
+        if (G.rx > 0 || G.ry > 0 || G.rz > 0)
+            on_edge = (px == 0 && (fb & 1)) || (px == 2 * G.rx && (fb & 8)) || (py == 0 && (fb & 2)) ||
+                      (py == 2 * G.ry && (fb & 16)) || (pz == 0 && (fb & 4)) || (pz == 2 * G.rz && (fb & 32));
+        const bool okv = isfinite(peak) && !flat;
+        a.ok[node] = okv ? 1 : 0;
+        a.cc[node] = peak;
+        a.pce[node] = pce;
+        a.clipped[node] = on_edge ? 1 : 0;
+        if (okv) {
+            a.disp[3 * node + 0] = (double)(a.wx0[node] + px + G.hx - x0) + sub[0];
+            a.disp[3 * node + 1] = (double)(a.wy0[node] + py + G.hy - y0) + sub[1];
+            a.disp[3 * node + 2] = (double)(a.wz0[node] + pz + G.hz - z0) + sub[2];
+        } else {
+            for (int c = 0; c < 3; ++c) a.disp[3 * node + c] = nan("");
+        }
+    }
+}
+
+static int upload_pinv() {
+    static bool done = false;
+    if (done) return ALDVC_OK;
+    // least-squares quadratic on the 3x3x3 grid: pinv(D) = (D^T D)^-1 D^T, columns
+    // [1, x, y, z, xy, xz, yz, x^2, y^2, z^2], rows of D in C order over (dz, dy, dx)
+    double D[27][10];
+    for (int t = 0; t < 27; ++t) {
+        const double z = t / 9 - 1, y = (t / 3) % 3 - 1, x = t % 3 - 1;
+        const double row[10] = {1, x, y, z, x * y, x * z, y * z, x * x, y * y, z * z};
+        for (int c = 0; c < 10; ++c) D[t][c] = row[c];
+    }
+    double N[10][20];
+    for (int i = 0; i < 10; ++i) {
+        for (int j = 0; j < 10; ++j) {
+            double s = 0.0;
+            for (int t = 0; t < 27; ++t) s += D[t][i] * D[t][j];
+            N[i][j] = s;
+        }
+        for (int j = 0; j < 10; ++j) N[i][10 + j] = i == j ? 1.0 : 0.0;
+    }
+    for (int c = 0; c < 10; ++c) {  // Gauss-Jordan with partial pivoting
+        int p = c;
+        for (int r = c + 1; r < 10; ++r)
+            if (std::fabs(N[r][c]) > std::fabs(N[p][c])) p = r;
+        for (int j = 0; j < 20; ++j) std::swap(N[c][j], N[p][j]);
+        const double d = N[c][c];
+        for (int j = 0; j < 20; ++j) N[c][j] /= d;
+        for (int r = 0; r < 10; ++r)
+            if (r != c) {
+                const double m = N[r][c];
+                for (int j = 0; j < 20; ++j) N[r][j] -= m * N[c][j];
+            }
+    }
+    double P[10 * 27];
+    for (int i = 0; i < 10; ++i)
+        for (int t = 0; t < 27; ++t) {
+            double s = 0.0;
+            for (int j = 0; j < 10; ++j) s += N[i][10 + j] * D[t][j];
+            P[i * 27 + t] = s;
+        }
+    cudaError_t e = cudaMemcpyToSymbol(c_pinv, P, sizeof(P));
+    if (e != cudaSuccess) return cuda_fail(e, "ncc: pinv upload");
+    done = true;
+    return ALDVC_OK;
+}
+
+static size_t tpl_smem(const NccGeom& G) { return (size_t)G.n_tpl * sizeof(float); }
+
+static int launch_map(const MapArgs& m, int64_t n_chunk, cudaStream_t s) {
+    const size_t smem = tpl_smem(m.G);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(ncc_map_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc map: shared memory attribute");
+    }
+    const unsigned tiles = (unsigned)((m.G.nmap + NCC_THREADS - 1) / NCC_THREADS);
+    for (int64_t done = 0; done < n_chunk; done += 65535) {
+        MapArgs mm = m;
+        mm.node_base = m.node_base + done;
+        mm.out = m.out + done * m.G.nmap;
+        const unsigned ny = (unsigned)std::min<int64_t>(65535, n_chunk - done);
+        ncc_map_kernel<<<dim3(tiles, ny), NCC_THREADS, smem, s>>>(mm);
+        const int rc = check_launch("ncc map");
+        if (rc) return rc;
+    }
+    return ALDVC_OK;
+}
+
+static int check_geom(const NccGeom& G) {
+    if (G.hx < 0 || G.hy < 0 || G.hz < 0 || G.rx < 0 || G.ry < 0 || G.rz < 0) return arg_fail("ncc: negative half-width or radius");
+    if ((int64_t)G.nx * G.ny >= (1LL << 31)) return arg_fail("ncc: volume plane too large");
+    if (tpl_smem(G) + 4096 > (size_t)max_smem_optin()) return arg_fail("ncc: template larger than shared memory");
+    return ALDVC_OK;
+}
+
+static int64_t search_chunk(const NccGeom& G, int64_t n) {
+    const int64_t per = (int64_t)G.nmap * 4;
+    int64_t c = (256LL << 20) / std::max<int64_t>(per, 1);
+    c = std::max<int64_t>(1, std::min<int64_t>(c, n));
+    return c;
+}
+
+}  // namespace aldvc
+
+using namespace aldvc;
+
+extern "C" int aldvc_ncc_map(const float* f, const float* g, int64_t nz, int64_t ny, int64_t nx, const int64_t* coords,
+                             int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz,
+                             const int64_t* wx0, const int64_t* wy0, const int64_t* wz0, const uint8_t* t_ok, float* out,
+                             void* stream) {
+    ALDVC_REQUIRE(f && g && coords && wx0 && wy0 && wz0 && t_ok && out, "aldvc_ncc_map: null pointer");
+    const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
+    int rc = check_geom(G);
+    if (rc) return rc;
+    if (n_nodes <= 0) return ALDVC_OK;
+    MapArgs m{f, g, coords, wx0, wy0, wz0, t_ok, out, 0, n_nodes, G};
+    return launch_map(m, n_nodes, (cudaStream_t)stream);
+}
+
+extern "C" size_t aldvc_ncc_search_workspace_size(int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry,
+                                                  int32_t rz) {
+    const NccGeom G = make_geom(1, 1, 1, hx, hy, hz, rx, ry, rz);
+    const int64_t n = std::max<int64_t>(n_nodes, 1);
+    const int64_t chunk = search_chunk(G, n);
+    return align_up((size_t)n * 32, 256) + (size_t)chunk * G.nmap * sizeof(float);
+}
+
+extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int64_t ny, int64_t nx, const int64_t* coords,
+                                int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz,
+                                const int64_t* shift0, void* workspace, size_t workspace_bytes, double* disp, double* cc,
+                                double* pce, uint8_t* clipped, uint8_t* ok, void* stream) {
+    ALDVC_REQUIRE(f && g && coords && disp && cc && pce && clipped && ok, "aldvc_ncc_search: null pointer");
+    const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
+    int rc = check_geom(G);
+    if (rc) return rc;
+    ALDVC_REQUIRE(G.wx <= G.nx && G.wy <= G.ny && G.wz <= G.nz, "aldvc_ncc_search: search window larger than the volume");
+    if (n_nodes <= 0) return ALDVC_OK;
+    const size_t need = aldvc_ncc_search_workspace_size(n_nodes, hx, hy, hz, rx, ry, rz);
+    if (!workspace || workspace_bytes < need) {
+        set_error("aldvc_ncc_search: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+        return ALDVC_ERR_WORKSPACE;
+    }
+    rc = upload_pinv();
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* w = (char*)workspace;
+    SearchArgs a;
+    a.f = f;
+    a.g = g;
+    a.coords = coords;
+    a.shift0 = shift0;
+    a.n_nodes = n_nodes;
+    a.node_base = 0;
+    a.G = G;
+    a.wx0 = (int64_t*)w;
+    a.wy0 = a.wx0 + n_nodes;
+    a.wz0 = a.wy0 + n_nodes;
+    a.t_ok = (uint8_t*)(a.wz0 + n_nodes);
+    a.freeb = a.t_ok + n_nodes;
+    float* map = (float*)(w + align_up((size_t)n_nodes * 32, 256));
+    a.map = map;
+    a.disp = disp;
+    a.cc = cc;
+    a.pce = pce;
+    a.clipped = clipped;
+    a.ok = ok;
+    ncc_place_kernel<<<(unsigned)((n_nodes + 255) / 256), 256, 0, s>>>(a);
+    rc = check_launch("ncc place");
+    if (rc) return rc;
+    const int64_t chunk = search_chunk(G, n_nodes);
+    for (int64_t start = 0; start < n_nodes; start += chunk) {
+        const int64_t n = std::min(chunk, n_nodes - start);
+        MapArgs m{f, g, coords, a.wx0, a.wy0, a.wz0, a.t_ok, map, start, n_nodes, G};
+        rc = launch_map(m, n, s);
+        if (rc) return rc;
+        SearchArgs b = a;
+        b.node_base = start;
+        for (int64_t done = 0; done < n; done += 65535) {
+            SearchArgs bb = b;
+            bb.node_base = start + done;
+            bb.map = map + done * G.nmap;
+            ncc_peak_kernel<<<(unsigned)std::min<int64_t>(65535, n - done), NCC_THREADS, 0, s>>>(bb);
+            rc = check_launch("ncc peak");
+            if (rc) return rc;
+        }
+    }
+    return ALDVC_OK;
+}

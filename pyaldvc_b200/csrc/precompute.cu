@@ -1,0 +1,232 @@
+// Per-node precomputation of the local solver: Gauss-Newton Hessian, its FP64 Cholesky factor and the
+// ZNSSD normalisation of the reference subset (pyALDVC numba_kernels._precompute_one :326-418).
+//
+// One CTA per node.  H[(i,j),(k,l)] = sum g_i g_k X_j X_l with X = (X, Y, Z, 1) has only 6 x 10 = 60
+// distinct sums (Kronecker structure of the steepest-descent images), accumulated per thread in FP32
+// over <= S/256 voxels, reduced across the warp in FP32 and across warps in FP64.  Sum f and sum f^2
+// are taken relative to the centre voxel so the variance does not cancel for offset intensities.
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace aldvc {
+
+constexpr int PRE_THREADS = 256;
+constexpr int PRE_NSUM = 60 + 2;  // 60 Hessian moments, sum(f - c), sum((f - c)^2)
+
+struct PreArgs {
+    const float* f;
+    const float* gx;
+    const float* gy;
+    const float* gz;
+    const uint8_t* mask;
+    int nz, ny, nx;
+    int hx, hy, hz, stride;
+    const int64_t* split_index;
+    const uint8_t* split_keep;
+    int64_t keep_bytes;
+    const int64_t* coords;
+    int64_t n_nodes;
+    double min_valid_ratio, cond_max;
+    double* H;
+    double* L;
+    double* meanf;
+    double* bottomf;
+    int64_t* n_valid;
+    uint8_t* valid;
+};
+
+// (i,k) pair index of the gradient products gg: 00 01 02 11 12 22
+__device__ __forceinline__ int gg_index(int i, int k) {
+    if (i > k) {
+        int t = i;
+        i = k;
+        k = t;
+    }
+    return i == 0 ? k : (i == 1 ? 2 + k : 5);
+}
+
+// (j,l) pair index of the coordinate products xx over (X, Y, Z, 1): 00 01 02 03 11 12 13 22 23 33
+__device__ __forceinline__ int xx_index(int j, int l) {
+    if (j > l) {
+        int t = j;
+        j = l;
+        l = t;
+    }
+    const int base[4] = {0, 4, 7, 9};
+    return base[j] + (l - j);
+}
+
+template <bool STORED>
+__global__ void __launch_bounds__(PRE_THREADS) precompute_kernel(PreArgs a) {
+    const int64_t node = blockIdx.x;
+    if (node >= a.n_nodes) return;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    __shared__ double red[PRE_THREADS / 32][PRE_NSUM];
+    __shared__ int red_n[PRE_THREADS / 32];
+    __shared__ double tot[PRE_NSUM];
+
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    const int64_t r = a.split_index ? a.split_index[node] : -1;
+    const bool use_keep = r >= 0;
+    const uint8_t* keep = use_keep ? a.split_keep + r * a.keep_bytes : nullptr;
+    double* H = a.H + node * 144;
+    double* L = a.L + node * 144;
+
+    const bool inside = x0 - a.hx >= 0 && x0 + a.hx < a.nx && y0 - a.hy >= 0 && y0 + a.hy < a.ny && z0 - a.hz >= 0 &&
+                        z0 + a.hz < a.nz;
+    if (!use_keep && !inside) {
+        for (int i = tid; i < 144; i += PRE_THREADS) {
+            H[i] = 0.0;
+            L[i] = 0.0;
+        }
+        if (tid == 0) {
+            a.meanf[node] = 0.0;
+            a.bottomf[node] = 1.0;
+            a.n_valid[node] = 0;
+            a.valid[node] = 0;
+        }
+        return;
+    }
+    const int64_t sxy = (int64_t)a.nx * a.ny;
+    // pilot value for the f moments: the centre voxel (clamped into the volume)
+    auto clampi = [](int64_t v, int64_t hi) -> int64_t { return v < 0 ? 0 : (v > hi ? hi : v); };
+    const int64_t cz = clampi(z0, a.nz - 1), cy = clampi(y0, a.ny - 1), cx = clampi(x0, a.nx - 1);
+    const float pilot = __ldg(a.f + cz * sxy + cy * a.nx + cx);
+
+    float acc[PRE_NSUM];
+#pragma unroll
+    for (int i = 0; i < PRE_NSUM; ++i) acc[i] = 0.0f;
+    int n = 0;
+
+    const int nX = (2 * a.hx) / a.stride + 1, nY = (2 * a.hy) / a.stride + 1, nZ = (2 * a.hz) / a.stride + 1;
+    const int S = nX * nY * nZ;
+    // mixed-radix step of PRE_THREADS voxels through (iz, iy, ix)
+    const int st_z = PRE_THREADS / (nX * nY), rem = PRE_THREADS % (nX * nY);
+    const int st_y = rem / nX, st_x = rem % nX;
+    int ix = tid % nX, iy = (tid / nX) % nY, iz = tid / (nX * nY);
+    for (int v = tid; v < S; v += PRE_THREADS) {
+        const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+        const int64_t xx = x0 + dx, yy = y0 + dy, zz = z0 + dz;
+        bool k;
+        if (use_keep) {
+            k = kept_bit(keep, v) && xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
+        } else {
+            k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0;
+        }
+        if (k) {
+            const int64_t o = zz * sxy + yy * a.nx + xx;
+            const float fv = __ldg(a.f + o) - pilot;
+            float g0, g1, g2;
+            if (STORED) {
+                g0 = __ldg(a.gx + o);
+                g1 = __ldg(a.gy + o);
+                g2 = __ldg(a.gz + o);
+            } else {
+                grad_otf(a.f, a.nz, a.ny, a.nx, (int)zz, (int)yy, (int)xx, g0, g1, g2);
+            }
+            const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+            const float gg[6] = {g0 * g0, g0 * g1, g0 * g2, g1 * g1, g1 * g2, g2 * g2};
+            const float xq[10] = {X * X, X * Y, X * Z, X, Y * Y, Y * Z, Y, Z * Z, Z, 1.0f};
+#pragma unroll
+            for (int p = 0; p < 6; ++p)
+#pragma unroll
+                for (int q = 0; q < 10; ++q) acc[p * 10 + q] += gg[p] * xq[q];
+            acc[60] += fv;
+            acc[61] += fv * fv;
+            ++n;
+        }
+        ix += st_x;
+        if (ix >= nX) {
+            ix -= nX;
+            ++iy;
+        }
+        iy += st_y;
+        if (iy >= nY) {
+            iy -= nY;
+            ++iz;
+        }
+        iz += st_z;
+    }
+    // FP32 within the warp, FP64 across warps (fixed order: deterministic)
+#pragma unroll
+    for (int i = 0; i < PRE_NSUM; ++i) {
+        const float s = warp_sum(acc[i]);
+        if (lane == 0) red[warp][i] = (double)s;
+    }
+    n = warp_sum_i(n);
+    if (lane == 0) red_n[warp] = n;
+    __syncthreads();
+    if (tid < PRE_NSUM) {
+        double s = 0.0;
+        for (int w = 0; w < PRE_THREADS / 32; ++w) s += red[w][tid];
+        tot[tid] = s;
+    }
+    __syncthreads();
+    if (tid != 0) return;
+    int64_t nv = 0;
+    for (int w = 0; w < PRE_THREADS / 32; ++w) nv += red_n[w];
+    // assemble H over SD = [g0 X, g0 Y, g0 Z, g1 X, g1 Y, g1 Z, g2 X, g2 Y, g2 Z, g0, g1, g2]
+    auto comp = [](int a_) { return a_ < 9 ? a_ / 3 : a_ - 9; };
+    auto coord = [](int a_) { return a_ < 9 ? a_ % 3 : 3; };
+    double Hl[144];
+    for (int p = 0; p < 12; ++p)
+        for (int q = 0; q < 12; ++q) Hl[p * 12 + q] = tot[gg_index(comp(p), comp(q)) * 10 + xx_index(coord(p), coord(q))];
+    for (int i = 0; i < 144; ++i) H[i] = Hl[i];
+    a.n_valid[node] = nv;
+    const int64_t total = subset_count(a.hx, a.hy, a.hz, a.stride);
+    double Ll[144];
+    for (int i = 0; i < 144; ++i) Ll[i] = 0.0;
+    bool ok = !(nv < 27 || (double)nv < a.min_valid_ratio * (double)total);
+    double meanf = 0.0, bottomf = 1.0;
+    if (ok) {
+        const double m_rel = tot[60] / (double)nv;
+        meanf = (double)pilot + m_rel;
+        double ssf = tot[61] - (double)nv * m_rel * m_rel;
+        if (ssf < 0.0) ssf = 0.0;
+        bottomf = sqrt(ssf > 1e-30 ? ssf : 1e-30);
+        if (bottomf < 1e-10) ok = false;
+        if (ok) ok = chol12(Hl, Ll);
+        if (ok) {
+            double dmin = Ll[0], dmax = Ll[0];
+            for (int i = 1; i < 12; ++i) {
+                const double d = Ll[i * 12 + i];
+                dmin = d < dmin ? d : dmin;
+                dmax = d > dmax ? d : dmax;
+            }
+            if (dmin <= 0.0 || (dmax / dmin) * (dmax / dmin) > a.cond_max) ok = false;
+        }
+    }
+    for (int i = 0; i < 144; ++i) L[i] = Ll[i];
+    a.meanf[node] = meanf;
+    a.bottomf[node] = bottomf;
+    a.valid[node] = ok ? 1 : 0;
+}
+
+}  // namespace aldvc
+
+using namespace aldvc;
+
+extern "C" int aldvc_precompute(const aldvc_volumes* vol, const aldvc_subset* sub, const int64_t* coords, int64_t n_nodes,
+                                double min_valid_ratio, double cond_max, double* H_all, double* L_all, double* meanf,
+                                double* bottomf, int64_t* n_valid, uint8_t* valid, void* stream) {
+    ALDVC_REQUIRE(vol && sub, "aldvc_precompute: null descriptor");
+    ALDVC_REQUIRE(vol->f && coords && H_all && L_all && meanf && bottomf && n_valid && valid, "aldvc_precompute: null pointer");
+    ALDVC_REQUIRE(sub->hx >= 0 && sub->hy >= 0 && sub->hz >= 0 && sub->stride >= 1, "aldvc_precompute: bad subset");
+    ALDVC_REQUIRE(vol->nz > 0 && vol->ny > 0 && vol->nx > 0 && vol->nz < (1 << 30) && vol->ny < (1 << 30) && vol->nx < (1 << 30),
+                  "aldvc_precompute: bad volume shape");
+    const bool stored = vol->gx && vol->gy && vol->gz;
+    ALDVC_REQUIRE(stored || (!vol->gx && !vol->gy && !vol->gz), "aldvc_precompute: give all three gradients or none");
+    ALDVC_REQUIRE(!sub->split_index || (sub->split_keep && sub->keep_bytes > 0), "aldvc_precompute: split rows missing");
+    if (n_nodes <= 0) return ALDVC_OK;
+    ALDVC_REQUIRE(n_nodes < (1LL << 31), "aldvc_precompute: too many nodes");
+    PreArgs a{vol->f, vol->gx, vol->gy, vol->gz, vol->mask, (int)vol->nz, (int)vol->ny, (int)vol->nx, sub->hx, sub->hy, sub->hz,
+              sub->stride, sub->split_index, sub->split_keep, sub->keep_bytes, coords, n_nodes, min_valid_ratio, cond_max,
+              H_all, L_all, meanf, bottomf, n_valid, valid};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (stored)
+        precompute_kernel<true><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);
+    else
+        precompute_kernel<false><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);
+    return check_launch("aldvc_precompute");
+}

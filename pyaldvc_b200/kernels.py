@@ -1,0 +1,224 @@
+"""Device-level API: torch CUDA tensors in, torch CUDA tensors out, every call through the C ABI.
+
+PyTorch provides device memory, the current stream and the caching allocator for workspaces;
+the arithmetic is the library's.  All calls are stream-ordered on ``torch.cuda.current_stream()``
+and return without synchronising, so they can be chained (and captured in a CUDA graph).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+BATCHED = _lib.BATCHED
+PLAIN = _lib.PLAIN
+INTERP_MODE_BY_NAME = {"linear": 0, "cubic": 1, "bspline": 2}
+
+
+def lib():
+    return _lib.load()
+
+
+def stream_handle() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def dev(a, dtype: torch.dtype) -> torch.Tensor:
+    """A contiguous CUDA tensor of ``dtype`` (host arrays are copied)."""
+    if isinstance(a, torch.Tensor):
+        t = a if a.is_cuda else a.to("cuda", non_blocking=False)
+        t = t.to(dtype) if t.dtype != dtype else t
+        return t.contiguous()
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def _p(t: torch.Tensor | None):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _workspace(nbytes: int) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device="cuda")
+
+
+def volumes_struct(f, gx, gy, gz, mask, g) -> _lib.Volumes:
+    nz, ny, nx = f.shape
+    return _lib.Volumes(f.data_ptr(), None if gx is None else gx.data_ptr(), None if gy is None else gy.data_ptr(),
+                        None if gz is None else gz.data_ptr(), None if mask is None else mask.data_ptr(),
+                        None if g is None else g.data_ptr(), nz, ny, nx)
+
+
+def subset_struct(half, stride, mode, split_index=None, split_keep=None) -> _lib.Subset:
+    hx, hy, hz = (int(h) for h in half)
+    if split_index is not None and split_keep is not None:
+        return _lib.Subset(hx, hy, hz, int(stride), int(mode), 0, split_index.data_ptr(), split_keep.data_ptr(),
+                           int(split_keep.shape[1]))
+    return _lib.Subset(hx, hy, hz, int(stride), int(mode), 0, None, None, 0)
+
+
+# --------------------------------------------------------------------------- preprocessing
+def gradients(f: torch.Tensor, border: int = 3):
+    """Stencil-7 gradients of a (nz, ny, nx) float32 CUDA volume."""
+    f = dev(f, torch.float32)
+    gx, gy, gz = (torch.empty_like(f) for _ in range(3))
+    nz, ny, nx = f.shape
+    _lib.check(lib().aldvc_gradients(_p(f), nz, ny, nx, int(border), _p(gx), _p(gy), _p(gz), stream_handle()),
+               "aldvc_gradients")
+    return gx, gy, gz
+
+
+# --------------------------------------------------------------------------- local solver
+def precompute(coords, half, f, gx, gy, gz, mask, min_valid_ratio, cond_max, stride=1, split_index=None, split_keep=None):
+    """Device ``precompute_nodes``: returns (H (N,12,12), L (N,12,12), meanf, bottomf, n_valid, valid) tensors."""
+    coords = dev(coords, torch.int64)
+    N = coords.shape[0]
+    d = coords.device
+    H = torch.empty((N, 12, 12), dtype=torch.float64, device=d)
+    L = torch.empty((N, 12, 12), dtype=torch.float64, device=d)
+    mf = torch.empty(N, dtype=torch.float64, device=d)
+    bf = torch.empty(N, dtype=torch.float64, device=d)
+    nv = torch.empty(N, dtype=torch.int64, device=d)
+    valid = torch.empty(N, dtype=torch.uint8, device=d)
+    vol = volumes_struct(f, gx, gy, gz, mask, None)
+    sub = subset_struct(half, stride, 0, split_index, split_keep)
+    _lib.check(lib().aldvc_precompute(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, float(min_valid_ratio),
+                                      float(cond_max), _p(H), _p(L), _p(mf), _p(bf), _p(nv), _p(valid), stream_handle()),
+               "aldvc_precompute")
+    return H, L, mf, bf, nv, valid
+
+
+def icgn_params(tol, dp_tol, max_iter, patience, noise_gain=0.0, predictive=True, variant=BATCHED, threads=0, brick_floats=0,
+                mu=0.0, n_full=0.0) -> _lib.IcgnParams:
+    return _lib.IcgnParams(float(tol), float(dp_tol), int(max_iter), int(patience), float(noise_gain), int(bool(predictive)),
+                           int(variant), int(threads), int(brick_floats), float(mu), float(n_full))
+
+
+def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol, dp_tol, max_iter, patience, stride=1, H=None,
+           pattern=None, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED, threads=0,
+           brick_floats=0):
+    """Device 12-DOF IC-GN; returns (P (N,12), n_iter, status, zncc) tensors."""
+    coords = dev(coords, torch.int64)
+    N = coords.shape[0]
+    d = coords.device
+    P0 = dev(P0, torch.float64).reshape(N, 12)
+    P = torch.empty((N, 12), dtype=torch.float64, device=d)
+    n_iter = torch.empty(N, dtype=torch.int32, device=d)
+    status = torch.empty(N, dtype=torch.int8, device=d)
+    zncc = torch.empty(N, dtype=torch.float64, device=d)
+    vol = volumes_struct(f, gx, gy, gz, mask, g)
+    sub = subset_struct(half, stride, mode, split_index, split_keep)
+    prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats)
+    ws_n = lib().aldvc_icgn_workspace_size(ctypes.byref(sub), N, ctypes.byref(prm))
+    ws = _workspace(ws_n)
+    use_noise = noise_gain > 0.0 and H is not None and pattern is not None
+    Hd = dev(H, torch.float64) if use_noise else None
+    pat = dev(pattern, torch.float64) if use_noise else None
+    _lib.check(lib().aldvc_icgn12(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, _p(P0), _p(L), _p(Hd), _p(pat), _p(meanf),
+                                  _p(valid), ctypes.byref(prm), _p(ws), ws.numel(), _p(P), _p(n_iter), _p(status), _p(zncc),
+                                  stream_handle()), "aldvc_icgn12")
+    return P, n_iter, status, zncc
+
+
+def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, meanf, bottomf, valid, mu, tol, dp_tol, max_iter,
+          patience, stride=1, n_full=0.0, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED,
+          threads=0, brick_floats=0):
+    """Device 3-DOF IC-GN (ADMM subproblem 1); returns (U (N,3), n_iter, status, zncc) tensors."""
+    coords = dev(coords, torch.int64)
+    N = coords.shape[0]
+    d = coords.device
+    U_old = dev(U_old, torch.float64).reshape(N, 3)
+    F_fixed = dev(F_fixed, torch.float64).reshape(N, 9)
+    vdual = dev(vdual, torch.float64).reshape(N, 3)
+    U = torch.empty((N, 3), dtype=torch.float64, device=d)
+    n_iter = torch.empty(N, dtype=torch.int32, device=d)
+    status = torch.empty(N, dtype=torch.int8, device=d)
+    zncc = torch.empty(N, dtype=torch.float64, device=d)
+    vol = volumes_struct(f, gx, gy, gz, mask, g)
+    sub = subset_struct(half, stride, mode, split_index, split_keep)
+    prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats, mu, n_full)
+    ws = _workspace(lib().aldvc_icgn_workspace_size(ctypes.byref(sub), N, ctypes.byref(prm)))
+    _lib.check(lib().aldvc_icgn3(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, _p(U_old), _p(F_fixed), _p(vdual), _p(H),
+                                 _p(meanf), _p(bottomf), _p(valid), ctypes.byref(prm), _p(ws), ws.numel(), _p(U), _p(n_iter),
+                                 _p(status), _p(zncc), stream_handle()), "aldvc_icgn3")
+    return U, n_iter, status, zncc
+
+
+# --------------------------------------------------------------------------- integer search
+def ncc_map(f, g, coords, half, radius, wx0, wy0, wz0, t_ok) -> torch.Tensor:
+    """Device ``_zncc_direct``: (N, 2rz+1, 2ry+1, 2rx+1) float32 maps."""
+    coords = dev(coords, torch.int64)
+    N = coords.shape[0]
+    hx, hy, hz = (int(h) for h in half)
+    rx, ry, rz = (int(r) for r in radius)
+    out = torch.empty((N, 2 * rz + 1, 2 * ry + 1, 2 * rx + 1), dtype=torch.float32, device=coords.device)
+    wx0, wy0, wz0 = (dev(a, torch.int64) for a in (wx0, wy0, wz0))
+    t_ok = dev(t_ok, torch.uint8)
+    nz, ny, nx = f.shape
+    _lib.check(lib().aldvc_ncc_map(_p(f), _p(g), nz, ny, nx, _p(coords), N, hx, hy, hz, rx, ry, rz, _p(wx0), _p(wy0), _p(wz0),
+                                   _p(t_ok), _p(out), stream_handle()), "aldvc_ncc_map")
+    return out
+
+
+def ncc_search(f, g, coords, half, radius, shift0=None) -> dict:
+    """Device single-level search; returns dict of tensors disp (N,3), cc, pce, clipped, ok."""
+    coords = dev(coords, torch.int64)
+    N = coords.shape[0]
+    d = coords.device
+    hx, hy, hz = (int(h) for h in half)
+    rx, ry, rz = (int(r) for r in radius)
+    sh = None if shift0 is None else dev(shift0, torch.int64).reshape(N, 3)
+    disp = torch.empty((N, 3), dtype=torch.float64, device=d)
+    cc = torch.empty(N, dtype=torch.float64, device=d)
+    pce = torch.empty(N, dtype=torch.float64, device=d)
+    clipped = torch.empty(N, dtype=torch.uint8, device=d)
+    ok = torch.empty(N, dtype=torch.uint8, device=d)
+    ws = _workspace(lib().aldvc_ncc_search_workspace_size(N, hx, hy, hz, rx, ry, rz))
+    nz, ny, nx = f.shape
+    _lib.check(lib().aldvc_ncc_search(_p(f), _p(g), nz, ny, nx, _p(coords), N, hx, hy, hz, rx, ry, rz, _p(sh), _p(ws),
+                                      ws.numel(), _p(disp), _p(cc), _p(pce), _p(clipped), _p(ok), stream_handle()),
+               "aldvc_ncc_search")
+    return {"disp": disp, "cc": cc, "pce": pce, "clipped": clipped, "ok": ok}
+
+
+# --------------------------------------------------------------------------- global step
+def mesh_struct(grid_shape, spacing, elem_active=None, gauss_order=2) -> _lib.Hex8Mesh:
+    nz, ny, nx = (int(s) for s in grid_shape)
+    sx, sy, sz = (float(s) for s in spacing)
+    return _lib.Hex8Mesh(nx, ny, nz, sx, sy, sz, None if elem_active is None else elem_active.data_ptr(), int(gauss_order), 0)
+
+
+def global_rhs(grid_shape, spacing, elem_active, beta, mu, alpha, U1, F1, W, v, gauss_order=2) -> torch.Tensor:
+    U1 = dev(U1, torch.float64).reshape(-1, 3)
+    N = U1.shape[0]
+    F1, W = (dev(a, torch.float64).reshape(N, 9) for a in (F1, W))
+    v = dev(v, torch.float64).reshape(N, 3)
+    b = torch.empty((N, 3), dtype=torch.float64, device=U1.device)
+    m = mesh_struct(grid_shape, spacing, elem_active, gauss_order)
+    _lib.check(lib().aldvc_global_rhs(ctypes.byref(m), float(beta), float(mu), float(alpha), _p(U1), _p(F1), _p(W), _p(v), _p(b),
+                                      stream_handle()), "aldvc_global_rhs")
+    return b
+
+
+def pcg_hex8(grid_shape, spacing, elem_active, beta, mu, alpha, B, X0, tol, max_iter, gauss_order=2):
+    """Jacobi-PCG on the hex8 system; returns (X (N,3), iters (device int32), err (device int32))."""
+    B = dev(B, torch.float64).reshape(-1, 3)
+    X0 = dev(X0, torch.float64).reshape(-1, 3)
+    X = torch.empty_like(B)
+    iters = torch.zeros(1, dtype=torch.int32, device=B.device)
+    err = torch.zeros(1, dtype=torch.int32, device=B.device)
+    m = mesh_struct(grid_shape, spacing, elem_active, gauss_order)
+    ws = _workspace(lib().aldvc_pcg_workspace_size(ctypes.byref(m)))
+    _lib.check(lib().aldvc_pcg_hex8(ctypes.byref(m), float(beta), float(mu), float(alpha), _p(B), _p(X0), float(tol), int(max_iter),
+                                    _p(ws), ws.numel(), _p(X), _p(iters), _p(err), stream_handle()), "aldvc_pcg_hex8")
+    return X, iters, err
+
+
+def nodal_gradient(grid_shape, spacing, elem_active, U, gauss_order=2) -> torch.Tensor:
+    U = dev(U, torch.float64).reshape(-1, 3)
+    F = torch.empty((U.shape[0], 3, 3), dtype=torch.float64, device=U.device)
+    m = mesh_struct(grid_shape, spacing, elem_active, gauss_order)
+    _lib.check(lib().aldvc_nodal_gradient(ctypes.byref(m), _p(U), _p(F), stream_handle()), "aldvc_nodal_gradient")
+    return F
