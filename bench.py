@@ -1,0 +1,427 @@
+"""Benchmark: nodes/s of a full AL-DVC pass on one B200 (batched form), beside the plain form and the CPU oracle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config 5] [--impl reference]
+
+A step is one full pass (normalise, gradients, NCC initial guess with cleaning, precompute, 12-DOF local
+IC-GN with outlier filling, ADMM: global hex8 PCG + 3-DOF subproblem 1) over the configuration's volume
+pair, inputs resident in HBM.  Rank 0 prints one JSON line.  With N > 1 (torchrun) every rank runs its own
+replica of the workload (weak scaling; the pass needs no exchange between replicas); the value is the
+nodes of all ranks over the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "nodes/s full AL-DVC pass at <=0.01 vox RMS err; batched vs plain form, 1 B200"
+WORKLOAD = {
+    1: "64^3 bead pair, translation, ws20/st8, trilinear, NCC +-4, local IC-GN (125 nodes)",
+    2: "128^3 bead pair, 2% z strain + sine, ws24/st6, tricubic, NCC +-8, local IC-GN (4096 nodes)",
+    3: "256^3 uint16 bead pair, 5 deg rotation + 1% hydrostatic, sphere ROI r110, ws16x16x24/st8, 3 ADMM (graph)",
+    5: "1024x1024x306 uint16 confocal-like bead pair, Boussinesq indentation, ws32/st12, NCC +-16, tricubic, 3 ADMM",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=1, help="timed passes of the plain form (0 skips it)")
+    ap.add_argument("--cpu-nodes", type=int, default=8, help="node block edge of the CPU baseline sample (cube root)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+
+        sm = np.array([num(r[0]) for r in self.rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.nanmedian(sm)), "sm_max_mhz": num(self.rows[0][1]), "power_w_max":
+                float(np.nanmax([num(r[2]) for r in self.rows])), "reasons": reasons, "samples": len(self.rows)}
+
+
+# --------------------------------------------------------------------------- CPU baseline (oracle, FP64)
+def node_block(mesh_shape, edge: int):
+    """Flat indices of an edge^3 block of nodes at the centre of the node grid."""
+    nz, ny, nx = mesh_shape
+    e = [min(edge, s) for s in (nz, ny, nx)]
+    st = [(s - k) // 2 for s, k in zip((nz, ny, nx), e)]
+    iz, iy, ix = np.meshgrid(*[np.arange(a, a + k) for a, k in zip(st, e)], indexing="ij")
+    return (iz * ny * nx + iy * nx + ix).ravel()
+
+
+def cpu_sample(f, g, coords, p, block, threads: int):
+    """The per-node chain of the pass on the host cores for the nodes ``block`` of ``coords``: NCC search, precompute,
+    12-DOF IC-GN and (with the global step) two 3-DOF passes.  Volumes are cropped to the box the block touches.
+    Returns (seconds, n_nodes, results)."""
+    from oracle import oracle as orc
+
+    orc.set_num_threads(threads)
+    c = coords[block]
+    half = tuple(int(w) // 2 for w in p.winsize)
+    sub0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
+    h0 = tuple(int(w) // 2 for w in sub0)
+    reach = [max(h + 8, h0_ + r + 2) + 8 for h, h0_, r in zip(half, h0, p.search_radius)]
+    lo = np.maximum(c.min(axis=0) - reach, 0)
+    hi = np.minimum(c.max(axis=0) + reach + 1, [f.shape[2], f.shape[1], f.shape[0]])
+    fs = np.ascontiguousarray(f[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]])
+    gs = np.ascontiguousarray(g[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]])
+    cl = (c - lo).astype(np.int64)
+    mode = {"linear": 0, "cubic": 1}[p.interp_method]
+    t0 = time.perf_counter()
+    gx, gy, gz = orc.compute_gradients(fs)
+    res = orc.ncc_search(fs, gs, cl, sub0, p.search_radius)
+    U0 = np.where(np.isfinite(res["disp"]), res["disp"], 0.0)
+    H, L, mf, bf, nv, valid = orc.precompute_nodes(cl, *half, fs, gx, gy, gz, np.ones((1, 1, 1), np.uint8), p.min_valid_ratio,
+                                                   p.hessian_cond_max, p.subset_stride)
+    P0 = np.zeros((cl.shape[0], 12))
+    P0[:, 9:] = U0
+    P, it, st, zc = orc.icgn_12dof_parallel(cl, P0, *half, fs, gx, gy, gz, np.ones((1, 1, 1), np.uint8), gs, mode, L, mf, bf, valid,
+                                            p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride)
+    U = P[:, 9:]
+    if p.use_global_step:
+        F = P[:, :9].reshape(-1, 3, 3)
+        v = np.zeros_like(U)
+        for _ in range(2, p.admm_max_iter + 1):
+            U, it3, st3, zc3 = orc.icgn_3dof_parallel(cl, U, F, v, *half, fs, gx, gy, gz, np.ones((1, 1, 1), np.uint8), gs, mode, H,
+                                                      mf, bf, valid, p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
+                                                      p.icgn_patience, p.subset_stride)
+    dt = time.perf_counter() - t0
+    return dt, int(cl.shape[0]), {"P": P, "status": st, "U0": U0}
+
+
+def run_reference(args):
+    """CPU arm: the FP64 oracle of the reference's CPU path on the host cores, bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from pyaldvc_b200 import configs, mesh
+
+    p = configs.params(args.config)
+    shape = configs.shape_of(args.config)
+    x0, y0, z0 = mesh.build_grid_axes(shape, p.winsize, p.winstepsize)
+    coords = np.round(mesh.grid_coords(x0, y0, z0)).astype(np.int64)
+    grid_shape = (len(z0), len(y0), len(x0))
+    f, g = _host_volumes(args.config)
+    threads = os.cpu_count() or 1
+    block = node_block(grid_shape, args.cpu_nodes)
+    for _ in range(max(0, args.warmup and 1)):
+        cpu_sample(f, g, coords, p, block[:8], threads)
+    times = []
+    n = 0
+    for _ in range(args.steps):
+        dt, n, _ = cpu_sample(f, g, coords, p, block, threads)
+        times.append(dt)
+    value = n / float(np.mean(times))
+    sample = f"{n} nodes ({args.cpu_nodes}^3 block at the grid centre) per step, FP64 oracle, {threads} threads"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD[args.config], "config_index": args.config, "nodes_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def _peaks() -> dict:
+    """Peaks for the roofline.  The hot kernels are FP32 CUDA-core bound; the measured-peaks file holds HBM and
+    bf16 tensor figures only, so the FP32 peak is the nominal rate of the device (SMs x 128 FP32 lanes x 2 x max clock)."""
+    import torch
+
+    props = torch.cuda.get_device_properties(0)
+    mhz = 1965.0
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    hbm = None
+    if os.path.exists(path):
+        with open(path) as fh:
+            mp = json.load(fh)
+        mhz = float(mp.get("sm_max_mhz", mhz))
+        hbm = mp.get("hbm_gbs")
+    fp32 = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+    return {"fp32_tflops": fp32, "hbm_gbs": hbm,
+            "fp32_source": f"nominal FP32 CUDA-core rate: {props.multi_processor_count} SMs x 128 lanes x 2 flop x {mhz:.0f} MHz"}
+
+
+def _normalize_np(v):
+    a = np.asarray(v, dtype=np.float64)
+    nz, ny, nx = a.shape
+    pilot = float(a[nz // 2, ny // 2, nx // 2])
+    d = a - pilot
+    ms = d.mean()
+    sd = np.sqrt(max((d * d).mean() - ms * ms, 0.0))
+    sd = sd if sd >= 1e-12 else 1.0
+    return ((a - (pilot + ms)) * (1.0 / sd)).astype(np.float32)
+
+
+def _host_volumes(cfg: int):
+    """Normalised host volumes of the configuration (for the CPU arm)."""
+    from pyaldvc_b200 import configs
+
+    if cfg == 5:
+        import torch
+
+        if torch.cuda.is_available():
+            f, g, _, _ = configs.device_pair(cfg)
+            from pyaldvc_b200 import kernels as K
+
+            return K.normalize(f).cpu().numpy(), K.normalize(g).cpu().numpy()
+        raise RuntimeError("configuration 5 is rendered on the device")
+    pair = configs.host_pair(cfg)
+    return _normalize_np(pair.f), _normalize_np(pair.g)
+
+
+# --------------------------------------------------------------------------- B200 arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from pyaldvc_b200 import configs
+    from pyaldvc_b200 import kernels as K
+    from pyaldvc_b200.cuda_kernels import cuda_available, unavailable_reason
+    from pyaldvc_b200.pipeline import Tracer, run_pass
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    if not cuda_available():
+        raise RuntimeError(f"B200 library unusable: {unavailable_reason()}")
+
+    cfg = args.config
+    p = configs.params(cfg)
+    f, g, mask, disp = configs.device_pair(cfg, seed=1000 + 17 * rank)
+    torch.cuda.synchronize()
+
+    def one_pass(variant=K.BATCHED, tracer=None):
+        p.variant = variant
+        return run_pass(f, g, p, mask, tracer=tracer)
+
+    for _ in range(args.warmup):
+        res = one_pass()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K passes, inputs resident in HBM
+    lib = K.lib()
+    tracers = [Tracer() for _ in range(args.steps)]
+    launches0 = lib.aldvc_launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record()
+        for k in range(args.steps):
+            res = one_pass(tracer=tracers[k])
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = (lib.aldvc_launch_count() - launches0) / args.steps
+    if world > 1:
+        dist.barrier()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_max = float(t.item())
+    n_nodes = int(res.coords.shape[0])
+    value = world * n_nodes * args.steps / elapsed_max
+    stages = {}
+    for tr in tracers:
+        for k_, v_ in tr.stages().items():
+            stages[k_] = stages.get(k_, 0.0) + v_ / args.steps
+
+    # accuracy against the ground-truth field (interior nodes that converged)
+    coords = res.coords.cpu().numpy()
+    U = res.U.cpu().numpy()
+    U_local = res.P_local[:, 9:].cpu().numpy()
+    status_local = res.status_local.cpu().numpy()
+    truth = configs.truth_at(disp, coords)
+    status = res.status.cpu().numpy()
+    valid = res.valid.cpu().numpy()
+    gs_ = res.grid_shape
+    interior = np.zeros(gs_, dtype=bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    sel = interior.ravel() & valid & (status == 0)
+    rms_truth = float(np.sqrt(np.mean((U[sel] - truth[sel]) ** 2))) if sel.any() else float("nan")
+
+    # ---- roofline of the two heaviest stages, algorithmic work per the pass (FP32 CUDA-core bound)
+    peaks = _peaks()
+    half = tuple(int(w) // 2 for w in p.winsize)
+    S = float(np.prod([(2 * h) // p.subset_stride + 1 for h in half]))
+    sub0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
+    n_tpl = float(np.prod([2 * (int(w) // 2) + 1 for w in sub0]))
+    n_off = float(np.prod([2 * int(r) + 1 for r in p.search_radius]))
+    n_search = int(valid.sum())
+    c_voxel = 87.0 if p.interp_method == "linear" else 263.0
+    n_it = res.n_iter.cpu().numpy() if not p.use_global_step else None
+    it12 = float(getattr(res, "n_iter_local", res.n_iter).cpu().numpy().astype(np.float64).sum())
+    rl = {
+        "init_guess": {"flops": 2.0 * n_tpl * n_off * n_search, "what": "ZNCC cross term 2 n_tpl n_off per searched node"},
+        "local_icgn": {"flops": it12 * S * c_voxel, "what": f"sum(n_iter) x S x {int(c_voxel)} flop per voxel-iteration"},
+    }
+    roof = {}
+    for name, r in rl.items():
+        t_ = stages.get(name)
+        if not t_:
+            continue
+        ach = r["flops"] / t_ / 1e12
+        roof[name] = {"bound": "fp32", "achieved": ach, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                      "frac": ach / peaks["fp32_tflops"], "traffic": None, "peak_source": peaks["fp32_source"],
+                      "stage_ms": 1e3 * t_, "work": r["what"]}
+    dominant = max(roof, key=lambda k_: roof[k_]["stage_ms"]) if roof else None
+
+    # ---- plain form of the same pass
+    plain = None
+    if args.plain_steps > 0:
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ptr = [Tracer() for _ in range(args.plain_steps)]
+        e0.record()
+        for k in range(args.plain_steps):
+            res_p = one_pass(K.PLAIN, tracer=ptr[k])
+        e1.record()
+        torch.cuda.synchronize()
+        pe = e0.elapsed_time(e1) / 1e3
+        pst = {}
+        for tr in ptr:
+            for k_, v_ in tr.stages().items():
+                pst[k_] = pst.get(k_, 0.0) + v_ / args.plain_steps
+        Up = res_p.U.cpu().numpy()
+        plain = {"value": n_nodes * args.plain_steps / pe, "unit": "nodes/s", "ms_per_step": 1e3 * pe / args.plain_steps,
+                 "stages_ms": {k_: 1e3 * v_ for k_, v_ in pst.items()},
+                 "max_abs_dU_vs_batched": float(np.nanmax(np.abs(Up - U)))}
+        p.variant = K.BATCHED
+
+    # ---- end to end: host buffers through the public API, copies inside the timed region
+    f_h = f.cpu().pin_memory()
+    g_h = g.cpu().pin_memory()
+    m_h = None if mask is None else mask.cpu().pin_memory()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fd = f_h.to("cuda", non_blocking=True)
+        gd = g_h.to("cuda", non_blocking=True)
+        md = None if m_h is None else m_h.to("cuda", non_blocking=True)
+        r = run_pass(fd, gd, p, md)
+        U_host = r.U.to("cpu")
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_t = e0.elapsed_time(e1) / 1e3
+    h2d = f_h.numel() * f_h.element_size() + g_h.numel() * g_h.element_size() + (0 if m_h is None else m_h.numel())
+    d2h = U_host.numel() * U_host.element_size()
+    e2e_val = world * n_nodes * args.steps / e2e_t
+
+    # ---- CPU baseline: the FP64 oracle on a bounded node block of the same workload (rank 0, N = 1)
+    cpu = None
+    rms_oracle = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        fn = K.normalize(f).cpu().numpy()
+        gn = K.normalize(g).cpu().numpy()
+        block = node_block(res.grid_shape, args.cpu_nodes)
+        dt, nb, cres = cpu_sample(fn, gn, coords, p, block, threads)
+        cpu = {"value": nb / dt, "unit": "nodes/s", "cores": threads, "kind": "port",
+               "sample": f"{nb} nodes ({args.cpu_nodes}^3 block at the grid centre): NCC, precompute, 12-DOF"
+                         f"{' and 3-DOF ADMM passes' if p.use_global_step else ''}, FP64 oracle"}
+        ok = (cres["status"] == 0) & (status_local[block] == 0)
+        if ok.any():
+            d = U_local[block][ok] - cres["P"][ok, 9:]
+            rms_oracle = float(np.sqrt(np.mean(d * d)))
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD[cfg], "config_index": cfg, "nodes_per_step": n_nodes, "volume_shape": list(f.shape),
+                   "volume_dtype": str(f.dtype).replace("torch.", ""), "l2": "inputs larger than L2"
+                   if f.numel() * f.element_size() > 126e6 else "inputs smaller than L2 (every pass rewrites its buffers)",
+                   "parallelism": f"replica x{world}"},
+        "stages_ms": {k_: 1e3 * v_ for k_, v_ in stages.items()},
+        "accuracy": {"rms_vs_truth_vox": rms_truth, "nodes_scored": int(sel.sum()), "converged_frac": float(np.mean(status == 0)),
+                     "rms_local_vs_fp64_oracle_vox": rms_oracle},
+        "gpu_launches": int(round(launches)),
+        "roofline": roof.get(dominant),
+        "roofline_stages": roof,
+        "cpu_baseline": cpu,
+        "plain": plain,
+        "batched_over_plain": None if plain is None else value / world / plain["value"],
+        "e2e": {"value": e2e_val, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -25,6 +25,11 @@
  *                        solver/subpb2_solver.py:45 build_global_system (hex8 FEM)
  *   aldvc_nodal_gradient <- solver/global_operators.py:151 nodal_gradient (FEM)
  *   aldvc_gradients   <- io/volume_ops.py:124 _gradient_stencil7
+ *   aldvc_normalize   <- io/volume_ops.py:105 normalize_volume (whole volume)
+ *   aldvc_inpaint     <- utils/inpaint.py:35 fill_nan_grid ("spring" model, no cut mesh)
+ *   aldvc_median_test <- utils/outlier_detection.py:135 universal_median_test (no cut mesh)
+ *   aldvc_render_beads   synthetic Gaussian-bead volumes (inputs of the benchmark configurations;
+ *                        pyALDVC synthetic.py:37 generate_bead_volume is the counterpart)
  */
 #ifndef ALDVC_B200_H
 #define ALDVC_B200_H
@@ -108,6 +113,8 @@ typedef struct aldvc_hex8_mesh {
 /* ---------------------------------------------------------------- library */
 int aldvc_abi_version(void);
 const char *aldvc_last_error(void);
+/* kernels this library has launched in the process so far (a monotone counter) */
+unsigned long long aldvc_launch_count(void);
 /* name of device `device`, its SM count and compute capability; returns ALDVC_OK */
 int aldvc_device_info(int device, char *name, int name_len, int *sm_count, int *cc_major, int *cc_minor);
 
@@ -115,6 +122,31 @@ int aldvc_device_info(int device, char *name, int name_len, int *sm_count, int *
 /* 7-point central-difference gradients, zero within `border` voxels of a face */
 int aldvc_gradients(const float *f, int64_t nz, int64_t ny, int64_t nx, int32_t border, float *gx, float *gy, float *gz,
                     void *stream);
+
+/* (v - mean) / std of a whole float32 (is_uint16 == 0) or uint16 volume, FP64 statistics taken
+ * relative to `pilot` (the reference uses the centre voxel); stats (device, 2 doubles, may be NULL)
+ * receives mean and std */
+size_t aldvc_normalize_workspace_size(void);
+int aldvc_normalize(const void *vol, int32_t is_uint16, int64_t n_voxels, double pilot, float *out, double *stats,
+                    void *workspace, size_t workspace_bytes, void *stream);
+
+/* adds peak * exp(-|x - c|^2 / (2 sigma^2)) of every bead (centres (B,3) [z,y,x]) within `radius`
+ * voxels into the FP64 accumulator volume (nz, ny, nx) */
+int aldvc_render_beads(double *accum, int64_t nz, int64_t ny, int64_t nx, const double *centres_zyx, const double *peaks,
+                       int64_t n_beads, double sigma, int32_t radius, void *stream);
+
+/* ---------------------------------------------------------------- node-grid post-processing */
+/* fills the unknown nodes of the (N, ncols) FP64 field (node n = iz*ny*nx + iy*nx + ix) with the
+ * spring (discrete Laplace) solution, CG to relative residual `tol`; iters/err are device int32 */
+size_t aldvc_inpaint_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t ncols);
+int aldvc_inpaint(double *values, int64_t nz, int64_t ny, int64_t nx, int32_t ncols, const uint8_t *unknown, double tol,
+                  int32_t max_iter, void *workspace, size_t workspace_bytes, int32_t *iters, int32_t *err, void *stream);
+
+/* universal median test of an (N, ncols) field: flag (N,) = 1 for valid outliers */
+size_t aldvc_median_test_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t ncols);
+int aldvc_median_test(const double *field, int64_t nz, int64_t ny, int64_t nx, int32_t ncols, const uint8_t *valid,
+                      double threshold, double eps, uint8_t *flag, void *workspace, size_t workspace_bytes, int32_t *err,
+                      void *stream);
 
 /* ---------------------------------------------------------------- local subset solver */
 /* Per-node Hessian H (N,12,12), its Cholesky factor L (N,12,12), meanf, bottomf, n_valid, valid. */
@@ -145,14 +177,21 @@ int aldvc_ncc_map(const float *f, const float *g, int64_t nz, int64_t ny, int64_
                   int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz, const int64_t *wx0, const int64_t *wy0,
                   const int64_t *wz0, const uint8_t *t_ok, float *out, void *stream);
 
-size_t aldvc_ncc_search_workspace_size(int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz);
+/* NCC engines: TILED (shared-memory window ring, register-tiled cross term, box-filter volumes for the
+ * window statistics; templates 5..33 voxels wide) and PLAIN (one thread per offset, the reference layout) */
+#define ALDVC_NCC_TILED 0
+#define ALDVC_NCC_PLAIN 1
+
+size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz,
+                                       int32_t rx, int32_t ry, int32_t rz, int32_t engine);
 
 /* Whole single-level search: template size (2h+1) per axis, search radius r, optional integer prior
- * shift0 (N,3) [x,y,z] (NULL = 0).  disp (N,3) [x,y,z] (NaN where not ok), cc, pce (N,), clipped, ok (N,). */
+ * shift0 (N,3) [x,y,z] (NULL = 0).  disp (N,3) [x,y,z] (NaN where not ok), cc, pce (N,), clipped, ok (N,).
+ * Every engine is stream-ordered without a host round trip. */
 int aldvc_ncc_search(const float *f, const float *g, int64_t nz, int64_t ny, int64_t nx, const int64_t *coords,
                      int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz,
-                     const int64_t *shift0, void *workspace, size_t workspace_bytes, double *disp, double *cc, double *pce,
-                     uint8_t *clipped, uint8_t *ok, void *stream);
+                     const int64_t *shift0, int32_t engine, void *workspace, size_t workspace_bytes, double *disp, double *cc,
+                     double *pce, uint8_t *clipped, uint8_t *ok, void *stream);
 
 /* ---------------------------------------------------------------- global step (ADMM subproblem 2) */
 /* b = beta sum_j G_j (F1 - W)[:,:,j] + mu M (U1 - v) + alpha Kg U1, all (N,3) / (N,3,3) FP64 */

@@ -15,6 +15,8 @@ from .build import LIB
 ALDVC_OK = 0
 BATCHED = 0
 PLAIN = 1
+NCC_TILED = 0
+NCC_PLAIN = 1
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -48,6 +50,7 @@ class Hex8Mesh(ctypes.Structure):
 PROTOTYPES = {
     "aldvc_abi_version": (_i32, []),
     "aldvc_last_error": (ctypes.c_char_p, []),
+    "aldvc_launch_count": (ctypes.c_ulonglong, []),
     "aldvc_device_info": (_i32, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "aldvc_gradients": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _p, _p, _p]),
@@ -59,13 +62,20 @@ PROTOTYPES = {
     "aldvc_icgn3": (_i32, [ctypes.POINTER(Volumes), ctypes.POINTER(Subset), _p, _i64, _p, _p, _p, _p, _p, _p, _p,
                            ctypes.POINTER(IcgnParams), _p, _sz, _p, _p, _p, _p, _p]),
     "aldvc_ncc_map": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i64, _i32, _i32, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p]),
-    "aldvc_ncc_search_workspace_size": (_sz, [_i64, _i32, _i32, _i32, _i32, _i32, _i32]),
-    "aldvc_ncc_search": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i64, _i32, _i32, _i32, _i32, _i32, _i32, _p, _p, _sz, _p, _p,
+    "aldvc_ncc_search_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i32, _i32, _i32, _i32, _i32, _i32, _i32]),
+    "aldvc_ncc_search": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i64, _i32, _i32, _i32, _i32, _i32, _i32, _p, _i32, _p, _sz, _p, _p,
                                 _p, _p, _p, _p]),
     "aldvc_global_rhs": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _p, _p, _p, _p]),
     "aldvc_pcg_workspace_size": (_sz, [ctypes.POINTER(Hex8Mesh)]),
     "aldvc_pcg_hex8": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _d, _i32, _p, _sz, _p, _p, _p, _p]),
     "aldvc_nodal_gradient": (_i32, [ctypes.POINTER(Hex8Mesh), _p, _p, _p]),
+    "aldvc_normalize_workspace_size": (_sz, []),
+    "aldvc_normalize": (_i32, [_p, _i32, _i64, _d, _p, _p, _p, _sz, _p]),
+    "aldvc_render_beads": (_i32, [_p, _i64, _i64, _i64, _p, _p, _i64, _d, _i32, _p]),
+    "aldvc_inpaint_workspace_size": (_sz, [_i64, _i64, _i64, _i32]),
+    "aldvc_inpaint": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _d, _i32, _p, _sz, _p, _p, _p]),
+    "aldvc_median_test_workspace_size": (_sz, [_i64, _i64, _i64, _i32]),
+    "aldvc_median_test": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _d, _d, _p, _p, _sz, _p, _p]),
 }
 
 _lib = None

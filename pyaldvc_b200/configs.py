@@ -1,0 +1,121 @@
+"""The five benchmark configurations: seeded synthetic bead volume pairs and their solver parameters.
+
+1. 64^3 float32, 0.02 beads/voxel, sigma 1.5, peak U(0.5, 1), Gaussian noise 0.01; uniform translation
+   (1.3, -0.7, 0.4); step 8, subsets 20^3, trilinear, direct NCC +-4; local IC-GN only.
+2. 128^3 float32, same beads; 2 % uniaxial strain along z plus u_x = 0.5 sin(2 pi y / 64); step 6,
+   subsets 24^3, NCC +-8, tricubic; local IC-GN only.
+3. 256^3 uint16 (0-4095); 5 degree rotation about z plus 1 % hydrostatic strain; spherical ROI of radius
+   110; step 8, subsets 16x16x24; ADMM with beta 1e-3, 3 iterations, captured as a CUDA graph.
+5. 1024 x 1024 x 306 uint16, 0.005 beads/voxel, sigma 2, Poisson (1000 photons per unit peak) plus
+   Gaussian noise; Boussinesq indentation u_z = -10.5 a^2 / (a^2 + r^2 + d^2), a = 80, plus a 0.3 voxel
+   random-phase background; step 12, subsets 32^3, NCC +-16, tricubic, 3 ADMM iterations.
+
+Volumes up to 256^3 are rendered with NumPy (deterministic, shared with the CPU oracle); the large one
+is rendered on the device with ``aldvc_render_beads`` (FP64 accumulation, so the float32 result does not
+depend on the order of the atomic sums).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import synthetic as syn
+from .pipeline import PassParams
+
+
+def params(cfg: int, **over) -> PassParams:
+    if cfg == 1:
+        p = PassParams(winsize=(20, 20, 20), winstepsize=(8, 8, 8), search_radius=(4, 4, 4), interp_method="linear",
+                       use_global_step=False)
+    elif cfg == 2:
+        p = PassParams(winsize=(24, 24, 24), winstepsize=(6, 6, 6), search_radius=(8, 8, 8), interp_method="cubic",
+                       use_global_step=False)
+    elif cfg == 3:
+        p = PassParams(winsize=(16, 16, 24), winstepsize=(8, 8, 8), search_radius=(8, 8, 8), interp_method="cubic",
+                       beta=1e-3, mu=1e-3, admm_max_iter=3, admm_early_stop=False, graph=True)
+    elif cfg == 5:
+        p = PassParams(winsize=(32, 32, 32), winstepsize=(12, 12, 12), search_radius=(16, 16, 16), interp_method="cubic",
+                       beta=1e-3, mu=1e-3, admm_max_iter=3)
+    else:
+        raise ValueError(f"no configuration {cfg}")
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+def shape_of(cfg: int):
+    return {1: (64, 64, 64), 2: (128, 128, 128), 3: (256, 256, 256), 5: (306, 1024, 1024)}[cfg]
+
+
+def displacement(cfg: int):
+    shape = shape_of(cfg)
+    centre = tuple((s - 1) / 2 for s in shape[::-1])  # (x, y, z)
+    if cfg == 1:
+        return syn.translation((1.3, -0.7, 0.4))
+    if cfg == 2:
+        return syn.strain_z_plus_sine(0.02, 0.5, 64.0, centre)
+    if cfg == 3:
+        return syn.rotation_z_hydrostatic(5.0, 0.01, centre)
+    if cfg == 5:
+        nz, ny, nx = shape
+        return syn.indentation(10.5, 80.0, ((nx - 1) / 2, (ny - 1) / 2), 0.3, shape, seed=505)
+    raise ValueError(cfg)
+
+
+def host_pair(cfg: int, seed: int = 1000) -> syn.VolumePair:
+    """NumPy-rendered pair for configurations 1-3."""
+    shape = shape_of(cfg)
+    disp = displacement(cfg)
+    if cfg in (1, 2):
+        return syn.bead_pair(shape, density=0.02, sigma=1.5, seed=seed + cfg, disp=disp, noise=0.01)
+    if cfg == 3:
+        pair = syn.bead_pair(shape, density=0.02, sigma=1.5, seed=seed + cfg, disp=disp, noise=0.01, uint16_max=4095)
+        nz, ny, nx = shape
+        z, y, x = np.ogrid[:nz, :ny, :nx]
+        r2 = (x - (nx - 1) / 2) ** 2 + (y - (ny - 1) / 2) ** 2 + (z - (nz - 1) / 2) ** 2
+        pair.mask = (r2 <= 110.0**2).astype(np.uint8)
+        return pair
+    raise ValueError("configuration 5 is rendered on the device: use device_pair(5)")
+
+
+def device_pair(cfg: int, seed: int = 1000):
+    """(f, g) CUDA tensors of the configuration (uint16 for 3 and 5, float32 otherwise) and the field."""
+    import torch
+
+    from . import kernels as K
+
+    if cfg != 5:
+        pair = host_pair(cfg, seed)
+        f = torch.from_numpy(np.ascontiguousarray(pair.f)).cuda()
+        g = torch.from_numpy(np.ascontiguousarray(pair.g)).cuda()
+        m = None if pair.mask is None else torch.from_numpy(pair.mask).cuda()
+        return f, g, m, pair.disp
+    shape = shape_of(cfg)
+    disp = displacement(cfg)
+    centres, peaks = syn.draw_beads(shape, 0.005, seed + cfg)
+    moved = syn.displace_beads(centres, disp)
+    sigma = 2.0
+    R = int(np.ceil(4.0 * sigma))
+    vols = []
+    for k, c in enumerate((centres, moved)):
+        acc = torch.zeros(shape, dtype=torch.float64, device="cuda")
+        K.render_beads(acc, c, peaks, sigma, R)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed + cfg + 1 + k)
+        photons = 1000.0
+        v = torch.poisson(acc.clamp_min(0.0) * photons, generator=gen) / photons
+        del acc
+        v = v + 0.01 * torch.randn(shape, dtype=torch.float64, device="cuda", generator=gen)
+        vols.append(v)
+    lo = min(float(vols[0].min()), float(vols[1].min()))
+    hi = max(float(vols[0].max()), float(vols[1].max()))
+    scale = 4095.0 / max(hi - lo, 1e-12)
+    out = [torch.round((v - lo) * scale).to(torch.int32).to(torch.uint16).contiguous() for v in vols]
+    del vols
+    torch.cuda.empty_cache()
+    return out[0], out[1], None, disp
+
+
+def truth_at(disp, coords) -> np.ndarray:
+    c = np.asarray(coords, dtype=np.float64)
+    return np.column_stack(disp(c[:, 0], c[:, 1], c[:, 2]))

@@ -1,4 +1,5 @@
 // Library-level entry points: ABI version, error string, device query; the stencil-7 gradient kernel.
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -8,6 +9,9 @@
 namespace aldvc {
 
 static thread_local char g_err[512] = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -65,6 +69,8 @@ using namespace aldvc;
 extern "C" int aldvc_abi_version(void) { return ALDVC_ABI_VERSION; }
 
 extern "C" const char* aldvc_last_error(void) { return g_err; }
+
+extern "C" unsigned long long aldvc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int aldvc_device_info(int device, char* name, int name_len, int* sm, int* cc_major, int* cc_minor) {
     cudaDeviceProp p;

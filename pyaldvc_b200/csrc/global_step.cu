@@ -501,11 +501,18 @@ extern "C" int aldvc_nodal_gradient(const aldvc_hex8_mesh* mesh, const double* U
 }
 
 static int pcg_grid(int* grid_out) {
+    int* grid_out_ = grid_out;
+    static int cached = 0;  // queried once: no configuration call inside a stream capture
+    if (cached > 0) {
+        *grid_out_ = cached;
+        return ALDVC_OK;
+    }
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, PCG_THREADS, 0);
     if (e != cudaSuccess) return cuda_fail(e, "pcg: occupancy");
     if (per_sm < 1) return arg_fail("pcg: kernel does not fit on an SM");
     *grid_out = per_sm * sm_count();
+    cached = *grid_out;
     return ALDVC_OK;
 }
 
@@ -568,5 +575,6 @@ extern "C" int aldvc_pcg_hex8(const aldvc_hex8_mesh* mesh, double beta, double m
     void* args[] = {&a};
     e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
     if (e != cudaSuccess) return cuda_fail(e, "pcg: cooperative launch");
+    count_launch();
     return ALDVC_OK;
 }

@@ -19,6 +19,7 @@
 // warp composition) exactly as the reference does.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -1052,11 +1053,22 @@ template <int MODE, bool STORED, int NDOF, int THREADS>
 static int launch_batched_t(const IcgnArgs& a, int brick_cap, cudaStream_t s) {
     auto kern = icgn_batched_kernel<MODE, STORED, NDOF, THREADS>;
     const size_t smem = (size_t)brick_cap * sizeof(float);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "icgn batched: shared memory attribute");
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
-    if (e != cudaSuccess) return cuda_fail(e, "icgn batched: occupancy");
+    // attribute and occupancy are set up once per (instantiation, brick size) so that launches inside a
+    // stream capture make no configuration calls
+    static int cached_cap = -1, cached_per_sm = 0;
+    static std::mutex mu;
+    int per_sm;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (cached_cap != brick_cap) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return cuda_fail(e, "icgn batched: shared memory attribute");
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_per_sm, kern, THREADS, smem);
+            if (e != cudaSuccess) return cuda_fail(e, "icgn batched: occupancy");
+            cached_cap = brick_cap;
+        }
+        per_sm = cached_per_sm;
+    }
     if (per_sm < 1) return arg_fail("icgn batched: brick does not fit in shared memory");
     long long grid = (long long)per_sm * sm_count();
     if (grid > a.n_nodes) grid = a.n_nodes;

@@ -23,11 +23,14 @@ inline int arg_fail(const char* msg) {
     return ALDVC_ERR_ARG;
 }
 
+void count_launch();
+
 // Enqueue check after a launch: a launch error is reported, an earlier asynchronous error is left
-// for the caller's next synchronisation.
+// for the caller's next synchronisation.  Every successful check counts one kernel launch.
 inline int check_launch(const char* where) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, where);
+    count_launch();
     return ALDVC_OK;
 }
 

@@ -454,6 +454,305 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
     }
 }
 
+
+// ----------------------------------------------------------------------------- tiled engine
+// Window box sums for every template placement: separable FP32 sums of (g - c) and (g - c)^2, each
+// output a direct sum of the axis length (no running subtraction), over the whole deformed volume.
+__global__ void box_pass_kernel(const float* __restrict__ in1, const float* __restrict__ in2, float* __restrict__ out1,
+                                float* __restrict__ out2, int nz, int ny, int nx, int axis, int len, const float* pilot_at,
+                                int square_in) {
+    const float pilot = square_in ? __ldg(pilot_at) : 0.0f;
+    const int64_t n = (int64_t)nz * ny * nx;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int x = (int)(i % nx);
+    const int64_t r = i / nx;
+    const int y = (int)(r % ny), z = (int)(r / ny);
+    const int64_t stride = axis == 0 ? 1 : (axis == 1 ? (int64_t)nx : (int64_t)nx * ny);
+    const int pos = axis == 0 ? x : (axis == 1 ? y : z);
+    const int extent = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const int m = min(len, extent - pos);  // partial sums past the last placement are never read
+    float s1 = 0.0f, s2 = 0.0f;
+    for (int k = 0; k < m; ++k) {
+        if (square_in) {
+            const float v = __ldg(in1 + i + k * stride) - pilot;
+            s1 += v;
+            s2 += v * v;
+        } else {
+            s1 += __ldg(in1 + i + k * stride);
+            s2 += __ldg(in2 + i + k * stride);
+        }
+    }
+    out1[i] = s1;
+    out2[i] = s2;
+}
+
+struct TiledArgs {
+    const float* f;
+    const float* g;
+    const int64_t* coords;
+    const int64_t* wx0;
+    const int64_t* wy0;
+    const int64_t* wz0;
+    const uint8_t* t_ok;
+    const float* B1;
+    const float* B2;
+    float* out;
+    int64_t node_base, n_nodes;
+    NccGeom G;
+    int dz_slab;   // offset planes per CTA
+    int ntile;     // thread tiles along dx
+    int pitch;     // ring row pitch (floats), = 1 mod 32
+    int sxp;       // padded template row (floats, multiple of 4)
+};
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
+// One CTA per (node, slab of dz offset planes).  Thread (dzl, tile, dy) owns R consecutive dx outputs.
+// The window streams through a ring of DZ + 1 z-planes in shared memory (cp.async prefetch of the next
+// plane while the current ones are used); the template rows are fully unrolled (SX compile-time) and the
+// R window values of a row stay in registers, so each shared load feeds up to R FMAs.
+template <int SX, int R>
+__global__ void __launch_bounds__(512) ncc_tiled_kernel(TiledArgs a) {
+    extern __shared__ __align__(16) float sm[];
+    __shared__ double red[512 / 32];
+    __shared__ double s_stat[2];
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    if (node >= a.n_nodes) return;
+    const int DZ = a.dz_slab;
+    const int dz0 = blockIdx.x * DZ;
+    float* out = a.out + (int64_t)blockIdx.y * G.nmap;
+    const int tid = threadIdx.x;
+    const int dy = tid % G.vy;
+    const int rest = tid / G.vy;
+    const int tile = rest % a.ntile;
+    const int dzl = rest / a.ntile;
+    const bool worker = dzl < DZ;
+    const int dz = dz0 + dzl;
+    const int dxb = tile * R;
+
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    const int64_t wx0 = a.wx0[node], wy0 = a.wy0[node], wz0 = a.wz0[node];
+    const bool placed = x0 - G.hx >= 0 && x0 + G.hx < G.nx && y0 - G.hy >= 0 && y0 + G.hy < G.ny && z0 - G.hz >= 0 &&
+                        z0 + G.hz < G.nz && wx0 >= 0 && wx0 + G.wx <= G.nx && wy0 >= 0 && wy0 + G.wy <= G.ny && wz0 >= 0 &&
+                        wz0 + G.wz <= G.nz;
+    auto write_all = [&](float v) {
+        if (!worker || dz >= G.vz) return;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int dx = dxb + r;
+            if (dx < G.vx) out[((int64_t)dz * G.vy + dy) * G.vx + dx] = v;
+        }
+    };
+    if (!a.t_ok[node] || !placed) {
+        write_all(-2.0f);
+        return;
+    }
+    float* T = sm;                                            // [sz][sy][sxp]
+    float* ring = sm + G.sz * G.sy * a.sxp;                   // [DZ + 1][wy][pitch]
+    const int plane_f = G.wy * a.pitch;
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    // template (raw), zero padding of the rows
+    double sf = 0.0;
+    for (int i = tid; i < G.sz * G.sy * a.sxp; i += blockDim.x) {
+        const int tx = i % a.sxp, row = i / a.sxp, ty = row % G.sy, tz = row / G.sy;
+        float v = 0.0f;
+        if (tx < G.sx) {
+            v = __ldg(a.f + (z0 - G.hz + tz) * sxy + (y0 - G.hy + ty) * G.nx + (x0 - G.hx + tx));
+            sf += (double)v;
+        }
+        T[i] = v;
+    }
+    // first DZ window planes into the ring while the template statistics are reduced
+    const int nplanes = min(DZ, G.vz - dz0) + G.sz - 1;  // window planes this slab reads
+    auto load_plane = [&](int p) {
+        if (p >= nplanes) return;
+        float* dst = ring + (p % (DZ + 1)) * plane_f;
+        const float* src = a.g + (wz0 + dz0 + p) * sxy + wy0 * G.nx + wx0;
+        for (int e = tid; e < G.wy * G.wx; e += blockDim.x) {
+            const int yy = e / G.wx, xx = e - yy * G.wx;
+            cp_async4(dst + yy * a.pitch + xx, src + (int64_t)yy * G.nx + xx);
+        }
+    };
+    for (int p = 0; p < DZ; ++p) load_plane(p);
+    cp_async_commit();
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+        double v = warp_sum_d(sf);
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            s_stat[0] = t / (double)G.n_tpl;
+        }
+        __syncthreads();
+        const double mf = s_stat[0];
+        double q = 0.0;
+        for (int i = tid; i < G.sz * G.sy * a.sxp; i += blockDim.x) {
+            if (i % a.sxp < G.sx) {
+                const double d = (double)T[i] - mf;
+                q += d * d;
+                T[i] = (float)d;
+            }
+        }
+        q = warp_sum_d(q);
+        __syncthreads();
+        if (lane == 0) red[warp] = q;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            s_stat[1] = t;
+        }
+    }
+    double accd[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) accd[r] = 0.0;
+    for (int tz = 0; tz < G.sz; ++tz) {
+        cp_async_wait_all();
+        __syncthreads();  // planes tz .. tz+DZ-1 visible to all; plane tz-1's slot is free
+        load_plane(tz + DZ);
+        cp_async_commit();
+        if (worker && dz < G.vz) {
+            const float* Wp = ring + ((tz + dzl) % (DZ + 1)) * plane_f + dy * a.pitch + dxb;
+            const float* Tp = T + tz * G.sy * a.sxp;
+            float acc[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = 0.0f;
+            for (int ty = 0; ty < G.sy; ++ty) {
+                const float* wr = Wp + ty * a.pitch;
+                const float* tr = Tp + ty * a.sxp;
+                float w[R + SX - 1];
+#pragma unroll
+                for (int k = 0; k < R + SX - 1; ++k) w[k] = wr[k];
+#pragma unroll
+                for (int tx = 0; tx < SX; ++tx) {
+                    const float t = tr[tx];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) acc[r] = fmaf(t, w[tx + r], acc[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) accd[r] += (double)acc[r];
+        }
+    }
+    cp_async_wait_all();
+    if (!worker || dz >= G.vz) return;
+    const double ssf = s_stat[1];
+    if (ssf < 1e-20) {
+        write_all(-2.0f);
+        return;
+    }
+    const double n_tpl = (double)G.n_tpl;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int dx = dxb + r;
+        if (dx >= G.vx) continue;
+        const int64_t c = (wz0 + dz) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
+        const double s1 = (double)__ldg(a.B1 + c), s2 = (double)__ldg(a.B2 + c);
+        const double var = s2 - s1 * s1 / n_tpl;
+        float v = 0.0f;
+        if (!(var < 1e-20)) {
+            double q = accd[r] / sqrt(var * ssf);
+            q = q > 1.0 ? 1.0 : (q < -1.0 ? -1.0 : q);
+            v = (float)q;
+        }
+        out[((int64_t)dz * G.vy + dy) * G.vx + dx] = v;
+    }
+}
+
+struct TiledCfg {
+    int R, ntile, dz, threads, pitch, sxp;
+    size_t smem;
+};
+
+static bool tiled_supported(int sx) {
+    switch (sx) {
+        case 5: case 7: case 9: case 11: case 13: case 15: case 17: case 21: case 25: case 33: return true;
+        default: return false;
+    }
+}
+
+static bool tiled_config(const NccGeom& G, TiledCfg& c) {
+    if (!tiled_supported(G.sx)) return false;
+    const int w9 = ((G.vx + 8) / 9) * 9 - G.vx, w11 = ((G.vx + 10) / 11) * 11 - G.vx;
+    c.R = w11 <= w9 ? 11 : 9;
+    c.ntile = (G.vx + c.R - 1) / c.R;
+    c.sxp = (G.sx + 3) / 4 * 4;
+    c.pitch = G.wx + ((1 - G.wx) % 32 + 32) % 32;  // = 1 mod 32: consecutive dy rows land in distinct banks
+    const int per_plane = G.vy * c.ntile;
+    if (per_plane > 512) return false;
+    const size_t smax = (size_t)max_smem_optin() - 8192;
+    int best = 0;
+    double best_cost = 1e300;
+    const size_t tail = 64;  // the discarded tail outputs of the last tile read up to R + SX floats past the last ring row
+    for (int dz = 1; dz <= G.vz && dz * per_plane <= 512; ++dz) {
+        const size_t smem = ((size_t)G.sz * G.sy * c.sxp + (size_t)(dz + 1) * G.wy * c.pitch + tail) * sizeof(float);
+        if (smem > smax) break;
+        const int slabs = (G.vz + dz - 1) / dz;
+        // idle output planes plus the per-CTA overhead of re-reading the template and the window halo
+        const double cost = (double)slabs * dz * per_plane * (G.sz + dz - 1) / dz + 0.15 * slabs * G.n_tpl / 32.0;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = dz;
+        }
+    }
+    if (best == 0) return false;
+    c.dz = best;
+    c.threads = (best * per_plane + 31) / 32 * 32;
+    c.smem = ((size_t)G.sz * G.sy * c.sxp + (size_t)(best + 1) * G.wy * c.pitch + tail) * sizeof(float);
+    return true;
+}
+
+template <int SX, int R>
+static int launch_tiled_t(const TiledArgs& a, const TiledCfg& c, int64_t n_chunk, cudaStream_t s) {
+    auto kern = ncc_tiled_kernel<SX, R>;
+    static size_t attr = 48 * 1024;
+    if (c.smem > attr) {
+        const size_t want = (size_t)max_smem_optin() - 4096;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc tiled: shared memory attribute");
+        attr = want;
+    }
+    const unsigned slabs = (unsigned)((a.G.vz + c.dz - 1) / c.dz);
+    for (int64_t done = 0; done < n_chunk; done += 65535) {
+        TiledArgs aa = a;
+        aa.node_base = a.node_base + done;
+        aa.out = a.out + done * a.G.nmap;
+        kern<<<dim3(slabs, (unsigned)std::min<int64_t>(65535, n_chunk - done)), c.threads, c.smem, s>>>(aa);
+        const int rc = check_launch("ncc tiled");
+        if (rc) return rc;
+    }
+    return ALDVC_OK;
+}
+
+template <int SX>
+static int launch_tiled_sx(const TiledArgs& a, const TiledCfg& c, int64_t n, cudaStream_t s) {
+    return c.R == 11 ? launch_tiled_t<SX, 11>(a, c, n, s) : launch_tiled_t<SX, 9>(a, c, n, s);
+}
+
+static int launch_tiled(const TiledArgs& a, const TiledCfg& c, int64_t n, cudaStream_t s) {
+    switch (a.G.sx) {
+        case 5: return launch_tiled_sx<5>(a, c, n, s);
+        case 7: return launch_tiled_sx<7>(a, c, n, s);
+        case 9: return launch_tiled_sx<9>(a, c, n, s);
+        case 11: return launch_tiled_sx<11>(a, c, n, s);
+        case 13: return launch_tiled_sx<13>(a, c, n, s);
+        case 15: return launch_tiled_sx<15>(a, c, n, s);
+        case 17: return launch_tiled_sx<17>(a, c, n, s);
+        case 21: return launch_tiled_sx<21>(a, c, n, s);
+        case 25: return launch_tiled_sx<25>(a, c, n, s);
+        default: return launch_tiled_sx<33>(a, c, n, s);
+    }
+}
+
 static int upload_pinv() {
     static bool done = false;
     if (done) return ALDVC_OK;
@@ -504,9 +803,12 @@ static size_t tpl_smem(const NccGeom& G) { return (size_t)G.n_tpl * sizeof(float
 
 static int launch_map(const MapArgs& m, int64_t n_chunk, cudaStream_t s) {
     const size_t smem = tpl_smem(m.G);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(ncc_map_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static size_t attr_set = 48 * 1024;  // largest dynamic size already allowed (no call inside a capture)
+    if (smem > attr_set) {
+        const size_t want = (size_t)max_smem_optin() - 4096;
+        cudaError_t e = cudaFuncSetAttribute(ncc_map_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
         if (e != cudaSuccess) return cuda_fail(e, "ncc map: shared memory attribute");
+        attr_set = want;
     }
     const unsigned tiles = (unsigned)((m.G.nmap + NCC_THREADS - 1) / NCC_THREADS);
     for (int64_t done = 0; done < n_chunk; done += 65535) {
@@ -552,25 +854,33 @@ extern "C" int aldvc_ncc_map(const float* f, const float* g, int64_t nz, int64_t
     return launch_map(m, n_nodes, (cudaStream_t)stream);
 }
 
-extern "C" size_t aldvc_ncc_search_workspace_size(int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry,
-                                                  int32_t rz) {
-    const NccGeom G = make_geom(1, 1, 1, hx, hy, hz, rx, ry, rz);
+static bool use_tiled(const NccGeom& G, int32_t engine, TiledCfg& c) {
+    return engine == ALDVC_NCC_TILED && tiled_config(G, c);
+}
+
+extern "C" size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t n_nodes, int32_t hx, int32_t hy,
+                                                  int32_t hz, int32_t rx, int32_t ry, int32_t rz, int32_t engine) {
+    const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
     const int64_t n = std::max<int64_t>(n_nodes, 1);
     const int64_t chunk = search_chunk(G, n);
-    return align_up((size_t)n * 32, 256) + (size_t)chunk * G.nmap * sizeof(float);
+    size_t b = align_up((size_t)n * 32, 256) + align_up((size_t)chunk * G.nmap * sizeof(float), 256);
+    TiledCfg c;
+    if (use_tiled(G, engine, c)) b += 4 * align_up((size_t)nz * ny * nx * sizeof(float), 256);  // box sums + temporaries
+    return b;
 }
 
 extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int64_t ny, int64_t nx, const int64_t* coords,
                                 int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz, int32_t rx, int32_t ry, int32_t rz,
-                                const int64_t* shift0, void* workspace, size_t workspace_bytes, double* disp, double* cc,
-                                double* pce, uint8_t* clipped, uint8_t* ok, void* stream) {
+                                const int64_t* shift0, int32_t engine, void* workspace, size_t workspace_bytes, double* disp,
+                                double* cc, double* pce, uint8_t* clipped, uint8_t* ok, void* stream) {
     ALDVC_REQUIRE(f && g && coords && disp && cc && pce && clipped && ok, "aldvc_ncc_search: null pointer");
+    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN, "aldvc_ncc_search: unknown engine");
     const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
     int rc = check_geom(G);
     if (rc) return rc;
     ALDVC_REQUIRE(G.wx <= G.nx && G.wy <= G.ny && G.wz <= G.nz, "aldvc_ncc_search: search window larger than the volume");
     if (n_nodes <= 0) return ALDVC_OK;
-    const size_t need = aldvc_ncc_search_workspace_size(n_nodes, hx, hy, hz, rx, ry, rz);
+    const size_t need = aldvc_ncc_search_workspace_size(nz, ny, nx, n_nodes, hx, hy, hz, rx, ry, rz, engine);
     if (!workspace || workspace_bytes < need) {
         set_error("aldvc_ncc_search: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
         return ALDVC_ERR_WORKSPACE;
@@ -592,7 +902,9 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
     a.wz0 = a.wy0 + n_nodes;
     a.t_ok = (uint8_t*)(a.wz0 + n_nodes);
     a.freeb = a.t_ok + n_nodes;
+    const int64_t chunk = search_chunk(G, n_nodes);
     float* map = (float*)(w + align_up((size_t)n_nodes * 32, 256));
+    char* box = w + align_up((size_t)n_nodes * 32, 256) + align_up((size_t)chunk * G.nmap * sizeof(float), 256);
     a.map = map;
     a.disp = disp;
     a.cc = cc;
@@ -602,11 +914,54 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
     ncc_place_kernel<<<(unsigned)((n_nodes + 255) / 256), 256, 0, s>>>(a);
     rc = check_launch("ncc place");
     if (rc) return rc;
-    const int64_t chunk = search_chunk(G, n_nodes);
+    TiledCfg tc;
+    const bool tiled = use_tiled(G, engine, tc);
+    TiledArgs ta;
+    if (tiled) {
+        // window box sums of (g - c) and (g - c)^2 for every placement, c = a voxel of g near the centre
+        const size_t vb = align_up((size_t)nz * ny * nx * sizeof(float), 256);
+        float* t1 = (float*)box;
+        float* t2 = (float*)(box + vb);
+        float* b1 = (float*)(box + 2 * vb);
+        float* b2 = (float*)(box + 3 * vb);
+        const float* pilot_at = g + ((nz / 2) * ny + ny / 2) * nx + nx / 2;  // read by the kernel: no host round trip
+        const int64_t nv = nz * ny * nx;
+        const unsigned blocks = (unsigned)((nv + 255) / 256);
+        box_pass_kernel<<<blocks, 256, 0, s>>>(g, nullptr, b1, b2, (int)nz, (int)ny, (int)nx, 0, G.sx, pilot_at, 1);
+        rc = check_launch("ncc box x");
+        if (rc) return rc;
+        box_pass_kernel<<<blocks, 256, 0, s>>>(b1, b2, t1, t2, (int)nz, (int)ny, (int)nx, 1, G.sy, nullptr, 0);
+        rc = check_launch("ncc box y");
+        if (rc) return rc;
+        box_pass_kernel<<<blocks, 256, 0, s>>>(t1, t2, b1, b2, (int)nz, (int)ny, (int)nx, 2, G.sz, nullptr, 0);
+        rc = check_launch("ncc box z");
+        if (rc) return rc;
+        ta.f = f;
+        ta.g = g;
+        ta.coords = coords;
+        ta.wx0 = a.wx0;
+        ta.wy0 = a.wy0;
+        ta.wz0 = a.wz0;
+        ta.t_ok = a.t_ok;
+        ta.B1 = b1;
+        ta.B2 = b2;
+        ta.n_nodes = n_nodes;
+        ta.G = G;
+        ta.dz_slab = tc.dz;
+        ta.ntile = tc.ntile;
+        ta.pitch = tc.pitch;
+        ta.sxp = tc.sxp;
+    }
     for (int64_t start = 0; start < n_nodes; start += chunk) {
         const int64_t n = std::min(chunk, n_nodes - start);
-        MapArgs m{f, g, coords, a.wx0, a.wy0, a.wz0, a.t_ok, map, start, n_nodes, G};
-        rc = launch_map(m, n, s);
+        if (tiled) {
+            ta.node_base = start;
+            ta.out = map;
+            rc = launch_tiled(ta, tc, n, s);
+        } else {
+            MapArgs m{f, g, coords, a.wx0, a.wy0, a.wz0, a.t_ok, map, start, n_nodes, G};
+            rc = launch_map(m, n, s);
+        }
         if (rc) return rc;
         SearchArgs b = a;
         b.node_base = start;

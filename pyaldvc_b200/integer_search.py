@@ -26,9 +26,9 @@ def ncc_search_device(f_d, g_d, coords, subset, radius, shift0=None) -> dict:
     return K.ncc_search(f_d, g_d, coords, half, radius, shift0)
 
 
-def ncc_search(f, g, coords, subset, radius, shift0=None, chunk: int = 64, backend: str = "cuda") -> dict:
+def ncc_search(f, g, coords, subset, radius, shift0=None, chunk: int = 64, backend: str = "cuda", engine: int = 0) -> dict:
     """Per-node NCC search (integer_search.ncc_search :329-483); ``chunk`` and ``backend`` are accepted for
-    signature compatibility, the device chunks by its workspace."""
+    signature compatibility, the device chunks by its workspace.  ``engine`` 0 = tiled, 1 = plain."""
     import torch
 
     from .cuda_kernels import _cache
@@ -49,7 +49,7 @@ def ncc_search(f, g, coords, subset, radius, shift0=None, chunk: int = 64, backe
     sh = None if shift0 is None else np.asarray(np.round(shift0), dtype=np.int64).reshape(N, 3)
     f_d = _cache.get(f, torch.float32)
     g_d = _cache.get(g, torch.float32)
-    res = K.ncc_search(f_d, g_d, coords, (hx, hy, hz), (rx, ry, rz), sh)
+    res = K.ncc_search(f_d, g_d, coords, (hx, hy, hz), (rx, ry, rz), sh, engine)
     out["disp"] = res["disp"].cpu().numpy()
     out["cc"] = res["cc"].cpu().numpy()
     out["pce"] = res["pce"].cpu().numpy()
@@ -59,9 +59,9 @@ def ncc_search(f, g, coords, subset, radius, shift0=None, chunk: int = 64, backe
 
 
 def ncc_search_expanding(f, g, coords, subset, radius, shift0=None, auto_expand: bool = True, max_expand: int = 3,
-                         chunk: int = 64, backend: str = "cuda") -> dict:
+                         chunk: int = 64, backend: str = "cuda", engine: int = 0) -> dict:
     """``ncc_search`` plus radius doubling for clipped peaks (integer_search.ncc_search_expanding :486-524)."""
-    res = ncc_search(f, g, coords, subset, radius, shift0)
+    res = ncc_search(f, g, coords, subset, radius, shift0, engine=engine)
     res["expansions"] = 0
     res["radius"] = tuple(int(r) for r in radius)
     rad = res["radius"]
@@ -72,7 +72,7 @@ def ncc_search_expanding(f, g, coords, subset, radius, shift0=None, auto_expand:
             break
         rad = tuple(2 * r for r in rad)
         sub_shift = None if shift0 is None else np.asarray(shift0)[sel]
-        sub = ncc_search(f, g, np.asarray(coords)[sel], subset, rad, sub_shift)
+        sub = ncc_search(f, g, np.asarray(coords)[sel], subset, rad, sub_shift, engine=engine)
         if not sub["ok"].any():
             break
         idx = np.flatnonzero(sel)[sub["ok"]]

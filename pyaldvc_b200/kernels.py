@@ -16,6 +16,8 @@ from . import _lib
 
 BATCHED = _lib.BATCHED
 PLAIN = _lib.PLAIN
+NCC_TILED = _lib.NCC_TILED
+NCC_PLAIN = _lib.NCC_PLAIN
 INTERP_MODE_BY_NAME = {"linear": 0, "cubic": 1, "bspline": 2}
 
 
@@ -162,8 +164,9 @@ def ncc_map(f, g, coords, half, radius, wx0, wy0, wz0, t_ok) -> torch.Tensor:
     return out
 
 
-def ncc_search(f, g, coords, half, radius, shift0=None) -> dict:
-    """Device single-level search; returns dict of tensors disp (N,3), cc, pce, clipped, ok."""
+def ncc_search(f, g, coords, half, radius, shift0=None, engine: int = _lib.NCC_TILED) -> dict:
+    """Device single-level search; returns dict of tensors disp (N,3), cc, pce, clipped, ok.
+    ``engine``: NCC_TILED (default) or NCC_PLAIN."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
     d = coords.device
@@ -175,10 +178,10 @@ def ncc_search(f, g, coords, half, radius, shift0=None) -> dict:
     pce = torch.empty(N, dtype=torch.float64, device=d)
     clipped = torch.empty(N, dtype=torch.uint8, device=d)
     ok = torch.empty(N, dtype=torch.uint8, device=d)
-    ws = _workspace(lib().aldvc_ncc_search_workspace_size(N, hx, hy, hz, rx, ry, rz))
     nz, ny, nx = f.shape
-    _lib.check(lib().aldvc_ncc_search(_p(f), _p(g), nz, ny, nx, _p(coords), N, hx, hy, hz, rx, ry, rz, _p(sh), _p(ws),
-                                      ws.numel(), _p(disp), _p(cc), _p(pce), _p(clipped), _p(ok), stream_handle()),
+    ws = _workspace(lib().aldvc_ncc_search_workspace_size(nz, ny, nx, N, hx, hy, hz, rx, ry, rz, int(engine)))
+    _lib.check(lib().aldvc_ncc_search(_p(f), _p(g), nz, ny, nx, _p(coords), N, hx, hy, hz, rx, ry, rz, _p(sh), int(engine),
+                                      _p(ws), ws.numel(), _p(disp), _p(cc), _p(pce), _p(clipped), _p(ok), stream_handle()),
                "aldvc_ncc_search")
     return {"disp": disp, "cc": cc, "pce": pce, "clipped": clipped, "ok": ok}
 
@@ -222,3 +225,56 @@ def nodal_gradient(grid_shape, spacing, elem_active, U, gauss_order=2) -> torch.
     m = mesh_struct(grid_shape, spacing, elem_active, gauss_order)
     _lib.check(lib().aldvc_nodal_gradient(ctypes.byref(m), _p(U), _p(F), stream_handle()), "aldvc_nodal_gradient")
     return F
+
+
+# --------------------------------------------------------------------------- volumes and node-grid post-processing
+def normalize(vol: torch.Tensor, pilot: float | None = None) -> torch.Tensor:
+    """``(vol - mean) / std`` of a float32 or uint16 CUDA volume as float32 (FP64 statistics)."""
+    assert vol.is_cuda and vol.is_contiguous()
+    if vol.dtype == torch.uint16:
+        is16 = 1
+    elif vol.dtype == torch.float32:
+        is16 = 0
+    else:
+        raise TypeError("normalize: float32 or uint16 volume")
+    if pilot is None:  # the reference's pilot: the centre voxel (io/volume_ops.py:94-99)
+        nz, ny, nx = vol.shape
+        pilot = float(vol[nz // 2, ny // 2, nx // 2].item())
+    out = torch.empty(vol.shape, dtype=torch.float32, device=vol.device)
+    ws = _workspace(lib().aldvc_normalize_workspace_size())
+    _lib.check(lib().aldvc_normalize(_p(vol), is16, vol.numel(), float(pilot), _p(out), None, _p(ws), ws.numel(),
+                                     stream_handle()), "aldvc_normalize")
+    return out
+
+
+def render_beads(accum: torch.Tensor, centres_zyx, peaks, sigma: float, radius: int) -> None:
+    """Add Gaussian beads into an FP64 CUDA accumulator volume."""
+    c = dev(centres_zyx, torch.float64).reshape(-1, 3)
+    p = dev(peaks, torch.float64).reshape(-1)
+    nz, ny, nx = accum.shape
+    _lib.check(lib().aldvc_render_beads(_p(accum), nz, ny, nx, _p(c), _p(p), c.shape[0], float(sigma), int(radius),
+                                        stream_handle()), "aldvc_render_beads")
+
+
+def inpaint(values: torch.Tensor, grid_shape, unknown: torch.Tensor, tol: float = 1e-12, max_iter: int = 4000):
+    """Fill the unknown nodes of an (N, C) FP64 field in place; returns (iters, err) device int32."""
+    nz, ny, nx = (int(s) for s in grid_shape)
+    C = 1 if values.dim() == 1 else int(values.shape[1])
+    ws = _workspace(lib().aldvc_inpaint_workspace_size(nz, ny, nx, C))
+    iters = torch.zeros(1, dtype=torch.int32, device=values.device)
+    err = torch.zeros(1, dtype=torch.int32, device=values.device)
+    _lib.check(lib().aldvc_inpaint(_p(values), nz, ny, nx, C, _p(unknown), float(tol), int(max_iter), _p(ws), ws.numel(), _p(iters),
+                                   _p(err), stream_handle()), "aldvc_inpaint")
+    return iters, err
+
+
+def median_test(field: torch.Tensor, grid_shape, valid: torch.Tensor | None, threshold: float, eps: float = 0.1):
+    """Universal median test of an (N, C) FP64 field; returns (flag uint8 (N,), err)."""
+    nz, ny, nx = (int(s) for s in grid_shape)
+    C = 1 if field.dim() == 1 else int(field.shape[1])
+    flag = torch.empty(field.shape[0], dtype=torch.uint8, device=field.device)
+    err = torch.zeros(1, dtype=torch.int32, device=field.device)
+    ws = _workspace(lib().aldvc_median_test_workspace_size(nz, ny, nx, C))
+    _lib.check(lib().aldvc_median_test(_p(field), nz, ny, nx, C, _p(valid), float(threshold), float(eps), _p(flag), _p(ws),
+                                       ws.numel(), _p(err), stream_handle()), "aldvc_median_test")
+    return flag, err

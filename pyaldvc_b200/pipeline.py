@@ -1,0 +1,324 @@
+"""One full AL-DVC pass on the device (pyALDVC core/pipeline.py:255-366, sections 3-6).
+
+Every step runs in the library on CUDA tensors; the host only sequences the calls and, where the
+reference makes a data-dependent decision (NCC radius expansion, the ADMM early stop), reads a few
+scalars.  With ``admm_early_stop=False`` the ADMM loop makes no host decision at all and is
+captured once as a CUDA graph (``graph=True``).
+
+Parameter names and defaults follow ``DVCPara`` (core/config.py:36-162).
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import kernels as K
+from .mesh import build_grid_axes, grid_coords
+
+STATUS_CONVERGED = 0
+
+
+@dataclass
+class PassParams:
+    winsize: tuple = (32, 32, 32)
+    winstepsize: tuple = (16, 16, 16)
+    search_radius: tuple = (8, 8, 8)
+    init_subset: tuple | None = None  # None: min(winsize, 16) (init_disp.py:76-81)
+    interp_method: str = "cubic"
+    subset_stride: int = 1
+    icgn_tol: float = 1e-2
+    icgn_dp_tol: float = 1e-3
+    icgn_max_iter: int = 100
+    icgn_patience: int = 5
+    icgn_predictive_stop: bool = True
+    min_valid_ratio: float = 0.5
+    hessian_cond_max: float = 1e12
+    init_outlier_threshold: float = 2.0
+    local_outlier_threshold: float = 2.0
+    ncc_auto_expand: bool = True
+    ncc_max_expand: int = 3
+    use_global_step: bool = True
+    mu: float = 1e-3
+    beta: float = 1e-3
+    alpha: float = 0.0
+    admm_max_iter: int = 4
+    admm_tol: float = 1e-2
+    admm_early_stop: bool = True
+    dual_update: str = "accumulate"
+    pcg_tol: float = 1e-8
+    pcg_max_iter: int = 500
+    gauss_pt_order: int = 2
+    variant: int = K.BATCHED
+    threads: int = 0
+    brick_floats: int = 0
+    graph: bool = False
+
+
+@dataclass
+class PassResult:
+    U: torch.Tensor
+    F: torch.Tensor
+    status: torch.Tensor
+    zncc: torch.Tensor
+    n_iter: torch.Tensor
+    coords: torch.Tensor
+    grid_shape: tuple
+    valid: torch.Tensor
+    U_local: torch.Tensor | None = None
+    U0: torch.Tensor | None = None
+    admm_steps: int = 0
+    P_local: torch.Tensor | None = None  # raw 12-DOF result (before outlier filling)
+    status_local: torch.Tensor | None = None
+    n_iter_local: torch.Tensor | None = None
+
+
+class Tracer:
+    """Stage timing: CUDA events on the current stream (no synchronisation) or, with ``sync=True``,
+    wall clock after a device synchronisation.  ``stages()`` returns seconds per stage."""
+
+    def __init__(self, sync: bool = False):
+        self.sync = sync
+        self.marks: list = []
+        self._t0 = None
+
+    def start(self):
+        if self.sync:
+            torch.cuda.synchronize()
+            self._t0 = time.perf_counter()
+        else:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            self._t0 = e
+
+    def mark(self, name: str):
+        if self.sync:
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            self.marks.append((name, t - self._t0))
+            self._t0 = t
+        else:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            self.marks.append((name, self._t0, e))
+            self._t0 = e
+
+    def stages(self) -> dict:
+        out: dict = {}
+        for m in self.marks:
+            dt = m[1] if self.sync else m[1].elapsed_time(m[2]) / 1e3
+            out[m[0]] = out.get(m[0], 0.0) + dt
+        return out
+
+
+class Mesh:
+    """Node grid + reference-derived per-node data (the ``LocalContext`` of local_icgn.py:40-93)."""
+
+    def __init__(self, volume_shape, p: PassParams, voi=None):
+        x0, y0, z0 = build_grid_axes(volume_shape, p.winsize, p.winstepsize, voi)
+        self.grid_shape = (len(z0), len(y0), len(x0))
+        self.spacing = (float(x0[1] - x0[0]), float(y0[1] - y0[0]), float(z0[1] - z0[0]))
+        self.coords_np = np.round(grid_coords(x0, y0, z0)).astype(np.int64)
+        self.coords = torch.from_numpy(self.coords_np).cuda()
+        self.n = self.coords_np.shape[0]
+        self.half = tuple(int(w) // 2 for w in p.winsize)
+
+
+def _fill(values: torch.Tensor, bad: torch.Tensor, grid_shape):
+    """fill_bad_nodes / clean_initial_guess inpainting of the rows flagged in ``bad`` (all bad -> zeros)."""
+    unk = bad.to(torch.uint8).contiguous()
+    v = values.clone().contiguous()
+    v[bad] = 0.0
+    K.inpaint(v, grid_shape, unk)
+    return v, bad.all()
+
+
+def _median_flags(field: torch.Tensor, good: torch.Tensor, grid_shape, threshold):
+    if threshold <= 0:
+        return torch.zeros_like(good)
+    f, _ = K.median_test(field.contiguous(), grid_shape, good.to(torch.uint8).contiguous(), threshold)
+    # the reference runs the test only with more than 27 good nodes (local_icgn.py:469-475)
+    return (f != 0) & (good.sum() > 27)
+
+
+def _rms(a: torch.Tensor) -> torch.Tensor:
+    return torch.sqrt(torch.mean(a * a))
+
+
+def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
+             tracer: Tracer | None = None) -> PassResult:
+    """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16)."""
+    tr = tracer if tracer is not None else Tracer(sync=False)
+    tr.start()
+    f = K.normalize(f_raw) if normalize else f_raw.float().contiguous()
+    g = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
+    if p.interp_method == "bspline":
+        raise NotImplementedError("the device pass prefilters no B-spline coefficients; use cubic or linear")
+    mode = K.INTERP_MODE_BY_NAME[p.interp_method]
+    gx, gy, gz = K.gradients(f)
+    mesh = Mesh(f.shape, p)
+    m_u8 = None if mask is None else mask.to(torch.uint8).contiguous()
+    tr.mark("preprocess")
+
+    # ---------------- precompute (local_icgn.precompute_local_context :223-347)
+    H, L, meanf, bottomf, n_valid, valid = K.precompute(mesh.coords, mesh.half, f, gx, gy, gz, m_u8, p.min_valid_ratio,
+                                                        p.hessian_cond_max, p.subset_stride)
+    valid_b = valid != 0
+    if mask is not None:  # apply_mask_to_mesh (grid_mesh.py:191-253): centre in the mask, enough of the subset in it
+        c = mesh.coords
+        centre_ok = m_u8[c[:, 2], c[:, 1], c[:, 0]] != 0
+        S = float(np.prod([2 * h + 1 for h in mesh.half]))
+        node_valid = centre_ok & (n_valid.double() >= p.min_valid_ratio * S)
+        valid_b = valid_b & node_valid
+        elem_node = node_valid.reshape(mesh.grid_shape)
+        e = (elem_node[:-1, :-1, :-1] & elem_node[:-1, :-1, 1:] & elem_node[:-1, 1:, 1:] & elem_node[:-1, 1:, :-1]
+             & elem_node[1:, :-1, :-1] & elem_node[1:, :-1, 1:] & elem_node[1:, 1:, 1:] & elem_node[1:, 1:, :-1])
+        elem_active = e.reshape(-1).to(torch.uint8).contiguous()
+    else:
+        elem_active = None
+    valid_u8 = valid_b.to(torch.uint8).contiguous()
+    tr.mark("precompute")
+
+    # ---------------- section 3: initial guess (init_disp.compute_initial_guess "ncc" :110-140)
+    subset0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
+    half0 = tuple(int(w) // 2 for w in subset0)
+    rad = tuple(int(r) for r in p.search_radius)
+    act = torch.nonzero(valid_b).flatten()
+    if act.numel() == 0:
+        act = torch.arange(mesh.n, device="cuda")
+    coords_a = mesh.coords[act].contiguous()
+    engine = K.NCC_PLAIN if p.variant == K.PLAIN else K.NCC_TILED
+    res = K.ncc_search(f, g, coords_a, half0, rad, None, engine)
+    disp_a, ok_a, clipped_a = res["disp"], res["ok"] != 0, res["clipped"] != 0
+    for _ in range(p.ncc_max_expand if p.ncc_auto_expand else 0):  # integer_search.ncc_search_expanding :486-524
+        sel = clipped_a & ok_a
+        n_ok = int(ok_a.sum().item())
+        n_sel = int(sel.sum().item())
+        if n_ok == 0 or n_sel <= 0.05 * n_ok:
+            break
+        rad = tuple(2 * r for r in rad)
+        idx = torch.nonzero(sel).flatten()
+        sub = K.ncc_search(f, g, coords_a[idx].contiguous(), half0, rad, None, engine)
+        s_ok = sub["ok"] != 0
+        if not bool(s_ok.any().item()):
+            break
+        take = idx[s_ok]
+        disp_a[take] = sub["disp"][s_ok]
+        ok_a[take] = True
+        clipped_a[take] = sub["clipped"][s_ok] != 0
+    disp = torch.full((mesh.n, 3), float("nan"), dtype=torch.float64, device="cuda")
+    ok = torch.zeros(mesh.n, dtype=torch.bool, device="cuda")
+    disp[act] = disp_a
+    ok[act] = ok_a
+    # clean_initial_guess (init_disp.py:143-189)
+    bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~valid_b
+    good = ~bad
+    flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), good, mesh.grid_shape, p.init_outlier_threshold)
+    bad = bad | flag
+    U0, all_bad = _fill(disp, bad, mesh.grid_shape)
+    if bool(all_bad.item()):
+        U0.zero_()
+    tr.mark("init_guess")
+
+    # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
+    P0 = torch.zeros((mesh.n, 12), dtype=torch.float64, device="cuda")
+    P0[:, 9:] = U0
+    P, n_iter, status, zncc = K.icgn12(mesh.coords, P0, mesh.half, f, gx, gy, gz, m_u8, g, mode, L, meanf, valid_u8, p.icgn_tol,
+                                       p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, None, None, 0.0,
+                                       p.icgn_predictive_stop, None, None, p.variant, p.threads, p.brick_floats)
+    bad = status != STATUS_CONVERGED
+    flag = _median_flags(P[:, 9:].contiguous(), ~bad, mesh.grid_shape, p.local_outlier_threshold)
+    bad = bad | flag
+    UF, all_bad = _fill(P, bad, mesh.grid_shape)  # U and F inpainted together (fill_bad_nodes :492-522)
+    if bool(all_bad.item()):
+        UF.zero_()
+    U1 = UF[:, 9:].contiguous()
+    F1 = UF[:, :9].contiguous()
+    U_local = U1.clone()
+    tr.mark("local_icgn")
+
+    result = PassResult(U=U1, F=F1.reshape(-1, 3, 3), status=status, zncc=zncc, n_iter=n_iter, coords=mesh.coords,
+                        grid_shape=mesh.grid_shape, valid=valid_b, U_local=U_local, U0=U0, P_local=P, status_local=status,
+                        n_iter_local=n_iter)
+    result.tracer = tr
+    if not p.use_global_step:
+        return result
+
+    # ---------------- sections 5-6: ADMM (pipeline.py:286-352) with fixed beta
+    def global_step(U1_, F1_, W_, v_):
+        b = K.global_rhs(mesh.grid_shape, mesh.spacing, elem_active, p.beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
+        U2_, _, _ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, elem_active, p.beta, p.mu, p.alpha, b, U1_, p.pcg_tol, p.pcg_max_iter,
+                               p.gauss_pt_order)
+        F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, elem_active, U2_, p.gauss_pt_order).reshape(-1, 9)
+        F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
+        return U2_, F2_
+
+    W = torch.zeros((mesh.n, 9), dtype=torch.float64, device="cuda")
+    v = torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda")
+    U2, F2 = global_step(U1, F1, W, v)
+    W = F2 - F1
+    v = U2 - U1
+    n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
+
+    def admm_step(U2, F2, W, v):
+        # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
+        U, it3, st3, zc3 = K.icgn3(mesh.coords, U2, F2, v, mesh.half, f, gx, gy, gz, m_u8, g, mode, H, meanf, bottomf, valid_u8,
+                                   p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full,
+                                   0.0, p.icgn_predictive_stop, None, None, p.variant, p.threads, p.brick_floats)
+        bad3 = st3 != STATUS_CONVERGED
+        bad3 = bad3 | _median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold)
+        U1n = torch.where(bad3[:, None], U2, U)
+        F1n = F2
+        U2n, F2n = global_step(U1n, F1n, W, v)
+        if p.dual_update == "accumulate":
+            Wn = W + (F2n - F1n)
+            vn = v + (U2n - U1n)
+        else:
+            Wn = F2n - F1n
+            vn = U2n - U1n
+        du_g = _rms(U2n - U2)
+        return U1n, U2n, F2n, Wn, vn, du_g, st3, zc3, it3
+
+    steps = 1
+    st_last, zc_last, it_last = status, zncc, n_iter
+    U1_prev = U1
+    if p.graph and not p.admm_early_stop and p.admm_max_iter > 1:
+        # capture the whole remaining loop once, replay it (no host step inside)
+        static = {"U2": U2.clone(), "F2": F2.clone(), "W": W.clone(), "v": v.clone(), "U1": U1.clone()}
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # warm-up outside capture (allocator pools, kernel attributes)
+            admm_step(static["U2"], static["F2"], static["W"], static["v"])
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            a = (static["U2"], static["F2"], static["W"], static["v"])
+            outs = []
+            for _ in range(2, p.admm_max_iter + 1):
+                U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg = admm_step(*a)
+                outs.append((U1g, stg, zcg, itg))
+                a = (U2g, F2g, Wg, vg)
+        tr.mark("admm_capture")
+        graph.replay()
+        U2, F2 = a[0], a[1]
+        U1, st_last, zc_last, it_last = outs[-1]
+        steps = p.admm_max_iter
+        result.graph = graph  # keep the graph (and its memory) alive with the result
+    else:
+        for step in range(2, p.admm_max_iter + 1):
+            steps = step
+            U1n, U2n, F2n, W, v, du_g, st_last, zc_last, it_last = admm_step(U2, F2, W, v)
+            du_l = _rms(U1n - U1_prev)
+            U1_prev = U1n
+            U1, U2, F2 = U1n, U2n, F2n
+            if p.admm_early_stop and (float(du_g.item()) < p.admm_tol or float(du_l.item()) < p.admm_tol):
+                break
+    tr.mark("admm")
+    result.U = U2
+    result.F = F2.reshape(-1, 3, 3)
+    result.status, result.zncc, result.n_iter = st_last, zc_last, it_last
+    result.admm_steps = steps
+    return result

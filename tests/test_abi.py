@@ -52,4 +52,4 @@ def test_workspace_queries_are_host_only():
     wb = L.aldvc_icgn_workspace_size(ctypes.byref(sub), n, ctypes.byref(batched))
     wp = L.aldvc_icgn_workspace_size(ctypes.byref(sub), n, ctypes.byref(plain))
     assert wb >= 4 and wp >= n * 25 ** 3 * 4  # the plain form keeps a sample row per node in flight
-    assert L.aldvc_ncc_search_workspace_size(n, 8, 8, 8, 8, 8, 8) >= 17 ** 3 * 4
+    assert L.aldvc_ncc_search_workspace_size(128, 128, 128, n, 8, 8, 8, 8, 8, 8, 1) >= 17 ** 3 * 4

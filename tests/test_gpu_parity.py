@@ -139,20 +139,22 @@ def _check_search(res, ref_get, name):
     np.testing.assert_allclose(res["pce"][ok], ref_get("pce")[ok], rtol=1e-3, err_msg=name)
 
 
+@pytest.mark.parametrize("engine", [0, 1], ids=["tiled", "plain"])
 @pytest.mark.parametrize("name", list(SEARCHES))
-def test_ncc_search_matches_reference(golden, name):
+def test_ncc_search_matches_reference(golden, name, engine):
     from pyaldvc_b200.integer_search import ncc_search
 
     c = SEARCHES[name]
     shift = np.round(golden["U_true"]).astype(np.int64) if c["shift"] else None
-    res = ncc_search(golden["f"], golden["g"], golden["coords"], c["subset"], c["radius"], shift)
+    res = ncc_search(golden["f"], golden["g"], golden["coords"], c["subset"], c["radius"], shift, engine=engine)
     _check_search(res, lambda k: golden[f"ncc_{name}_{k}"], name)
 
 
-def test_ncc_search_expanding_matches_reference(golden):
+@pytest.mark.parametrize("engine", [0, 1], ids=["tiled", "plain"])
+def test_ncc_search_expanding_matches_reference(golden, engine):
     from pyaldvc_b200.integer_search import ncc_search_expanding
 
-    res = ncc_search_expanding(golden["f"], golden["g"], golden["coords"], (8, 8, 8), (1, 1, 1))
+    res = ncc_search_expanding(golden["f"], golden["g"], golden["coords"], (8, 8, 8), (1, 1, 1), engine=engine)
     assert res["expansions"] == int(golden["nccx_expansions"])
     _check_search(res, lambda k: golden[f"nccx_{k}"], "expanding")
 
@@ -174,3 +176,28 @@ def test_global_step_matches_reference(golden):
     U2b, info2 = solve_subpb2(system2, *args)
     assert abs(info2["iterations"] - int(golden["pcg_alpha_iters"])) <= 1
     np.testing.assert_allclose(U2b, golden["pcg_alpha_U2"], rtol=0, atol=1e-8)
+
+
+@pytest.fixture(scope="module")
+def config1_pair():
+    from pyaldvc_b200 import configs, synthetic
+    from pyaldvc_b200.mesh import build_grid_axes, grid_coords
+
+    pair = configs.host_pair(1)
+    f = synthetic.normalize_volume(pair.f)
+    g = synthetic.normalize_volume(pair.g)
+    x0, y0, z0 = build_grid_axes(f.shape, (20, 20, 20), (8, 8, 8))
+    coords = np.round(grid_coords(x0, y0, z0)).astype(np.int64)
+    return f, g, coords
+
+
+@pytest.mark.parametrize("engine", [0, 1], ids=["tiled", "plain"])
+@pytest.mark.parametrize("radius", [4, 8])
+def test_ncc_search_17cube_template_matches_oracle(oracle_mod, config1_pair, engine, radius):
+    """Default template of the pipeline (17^3, min(winsize, 16)) against the FP64 direct map of the oracle."""
+    from pyaldvc_b200.integer_search import ncc_search
+
+    f, g, coords = config1_pair
+    ref = oracle_mod.ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3)
+    res = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=engine)
+    _check_search(res, lambda k: ref[k], f"17^3 r{radius}")
