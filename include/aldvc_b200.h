@@ -207,6 +207,17 @@ int aldvc_pcg_hex8(const aldvc_hex8_mesh *mesh, double beta, double mu, double a
                    double tol, int32_t max_iter, void *workspace, size_t workspace_bytes, double *X, int32_t *iters,
                    int32_t *err, void *stream);
 
+/* aldvc_pcg_hex8 without a workspace, for callers that cannot allocate device memory (a plugin inside a
+ * host application that owns the device budget, a real-time loop that must not call cudaMalloc).  No
+ * counterpart in the reference.  Its scratch is a file-scope device array of about 28 MB that every GPU
+ * loading the library holds until exit; meshes above aldvc_pcg_hex8_noalloc_max_nodes() nodes (262144)
+ * are rejected with ALDVC_ERR_ARG.  All calls share the array: calls that overlap on the GPU race.  The
+ * first call on a device looks up the array's address; make it before any stream capture. */
+int64_t aldvc_pcg_hex8_noalloc_max_nodes(void);
+int aldvc_pcg_hex8_noalloc(const aldvc_hex8_mesh *mesh, double beta, double mu, double alpha, const double *B,
+                           const double *X0, double tol, int32_t max_iter, double *X, int32_t *iters, int32_t *err,
+                           void *stream);
+
 /* F (N,3,3) = (G_j^T u_i) / m_L on the active nodes, NaN elsewhere */
 int aldvc_nodal_gradient(const aldvc_hex8_mesh *mesh, const double *U, double *F, void *stream);
 

@@ -68,6 +68,8 @@ PROTOTYPES = {
     "aldvc_global_rhs": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _p, _p, _p, _p]),
     "aldvc_pcg_workspace_size": (_sz, [ctypes.POINTER(Hex8Mesh)]),
     "aldvc_pcg_hex8": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _d, _i32, _p, _sz, _p, _p, _p, _p]),
+    "aldvc_pcg_hex8_noalloc_max_nodes": (_i64, []),
+    "aldvc_pcg_hex8_noalloc": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _d, _i32, _p, _p, _p, _p]),
     "aldvc_nodal_gradient": (_i32, [ctypes.POINTER(Hex8Mesh), _p, _p, _p]),
     "aldvc_normalize_workspace_size": (_sz, []),
     "aldvc_normalize": (_i32, [_p, _i32, _i64, _d, _p, _p, _p, _sz, _p]),

@@ -11,6 +11,7 @@
 // the error word and returns.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -575,6 +576,109 @@ extern "C" int aldvc_pcg_hex8(const aldvc_hex8_mesh* mesh, double beta, double m
     void* args[] = {&a};
     e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
     if (e != cudaSuccess) return cuda_fail(e, "pcg: cooperative launch");
+    count_launch();
+    return ALDVC_OK;
+}
+
+// ----------------------------------------------------------------------------- PCG without allocation
+// Some callers cannot allocate device memory at all: a plugin running inside a larger imaging
+// application whose own allocator owns the device budget, or a real-time acquisition loop that must not
+// call cudaMalloc (it synchronises the device and can stall for milliseconds).  For them this variant
+// of the PCG keeps its scratch (residual, preconditioned residual, direction, A*direction, Jacobi
+// diagonal, active set, block partials, barrier words) in one file-scope device array instead of a
+// caller-provided workspace.  The caller still passes B, X0, X, iters and err.
+//
+// The array is NOALLOC_PCG_BYTES of device memory held by every GPU that loads the library, until the
+// process exits.  It bounds the mesh to NOALLOC_PCG_MAX_NODES nodes; larger meshes are rejected.
+// All calls share the array and it keeps the last call's contents: the barrier words are cleared on
+// every call and every other region is written by the kernel before it is read.  Calls whose kernels
+// overlap on the GPU (different streams without ordering, or different host threads) race on the
+// array.  The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+// with that device current); make that first call before any stream capture.
+constexpr int64_t NOALLOC_PCG_MAX_NODES = 262144;
+constexpr int NOALLOC_PCG_MAX_GRID = 4096;
+constexpr size_t NOALLOC_V3 = (size_t)NOALLOC_PCG_MAX_NODES * 3 * sizeof(double);
+constexpr size_t NOALLOC_PART = (size_t)3 * NOALLOC_PCG_MAX_GRID * 8 * sizeof(double);
+constexpr size_t NOALLOC_PCG_BYTES =
+    4 * NOALLOC_V3 + NOALLOC_PART + (size_t)NOALLOC_PCG_MAX_NODES * sizeof(double) + (size_t)NOALLOC_PCG_MAX_NODES + 256;
+
+static __device__ __align__(256) unsigned char g_pcg_scratch[NOALLOC_PCG_BYTES];
+
+static std::mutex g_pcg_scratch_mu;
+static char* g_pcg_scratch_ptr[128] = {nullptr};  // device address of the array, per device ordinal
+
+// set-up once per device, with that device current
+static int pcg_scratch_address(char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: current device");
+    if (dev < 0 || dev >= 128) return arg_fail("aldvc_pcg_hex8_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_pcg_scratch_mu);
+    if (!g_pcg_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: scratch address");
+        g_pcg_scratch_ptr[dev] = (char*)p;
+    }
+    *out = g_pcg_scratch_ptr[dev];
+    return ALDVC_OK;
+}
+
+extern "C" int64_t aldvc_pcg_hex8_noalloc_max_nodes(void) { return NOALLOC_PCG_MAX_NODES; }
+
+extern "C" int aldvc_pcg_hex8_noalloc(const aldvc_hex8_mesh* mesh, double beta, double mu, double alpha, const double* B,
+                                      const double* X0, double tol, int32_t max_iter, double* X, int32_t* iters, int32_t* err,
+                                      void* stream) {
+    ALDVC_REQUIRE(B && X0 && X && iters && err, "aldvc_pcg_hex8_noalloc: null pointer");
+    ALDVC_REQUIRE(max_iter >= 0, "aldvc_pcg_hex8_noalloc: max_iter must be >= 0");
+    Mesh m;
+    Spacing sp;
+    int rc = set_mesh(mesh, m, sp);
+    if (rc) return rc;
+    if (m.n > NOALLOC_PCG_MAX_NODES) {
+        set_error("aldvc_pcg_hex8_noalloc: mesh of %lld nodes exceeds the %lld-node limit of the built-in scratch; "
+                  "use aldvc_pcg_hex8 with a workspace",
+                  (long long)m.n, (long long)NOALLOC_PCG_MAX_NODES);
+        return ALDVC_ERR_ARG;
+    }
+    int grid = 0;
+    rc = pcg_grid(&grid);
+    if (rc) return rc;
+    if (grid > NOALLOC_PCG_MAX_GRID) grid = NOALLOC_PCG_MAX_GRID;
+    char* w = nullptr;
+    rc = pcg_scratch_address(&w);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    PcgArgs a;
+    a.m = m;
+    a.sp = sp;
+    a.sk = beta + alpha;
+    a.sm = mu;
+    a.B = B;
+    a.X0 = X0;
+    a.X = X;
+    a.R = (double*)w;
+    a.Z = (double*)(w + NOALLOC_V3);
+    a.P = (double*)(w + 2 * NOALLOC_V3);
+    a.AP = (double*)(w + 3 * NOALLOC_V3);
+    a.part = (double*)(w + 4 * NOALLOC_V3);
+    a.inv_diag = (double*)(w + 4 * NOALLOC_V3 + NOALLOC_PART);
+    a.active = (uint8_t*)(w + 4 * NOALLOC_V3 + NOALLOC_PART + (size_t)NOALLOC_PCG_MAX_NODES * sizeof(double));
+    a.bar_count = (unsigned int*)(w + 4 * NOALLOC_V3 + NOALLOC_PART + (size_t)NOALLOC_PCG_MAX_NODES * sizeof(double) +
+                                  (size_t)NOALLOC_PCG_MAX_NODES);
+    a.bar_gen = a.bar_count + 1;
+    a.tol = tol;
+    a.max_iter = max_iter;
+    a.iters = iters;
+    a.err = err;
+    // the barrier words must start at zero on every call; everything else is written before it is read
+    cudaError_t e = cudaMemsetAsync(a.bar_count, 0, 2 * sizeof(unsigned int), s);
+    if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: barrier reset");
+    e = cudaMemsetAsync(err, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: error word reset");
+    void* args[] = {&a};
+    e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
+    if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: cooperative launch");
     count_launch();
     return ALDVC_OK;
 }
