@@ -10,6 +10,8 @@
 //   the winner, quadratic sub-voxel fit -- all on the device, in node chunks through a workspace.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -497,13 +499,16 @@ struct TiledArgs {
     const uint8_t* t_ok;
     const float* B1;
     const float* B2;
+    const float* T;     // centred templates of the chunk, [node][sz][sy][sxp]
+    const double* ssf;  // their sums of squares
     float* out;
     int64_t node_base, n_nodes;
     NccGeom G;
     int dz_slab;   // offset planes per CTA
     int ntile;     // thread tiles along dx
-    int pitch;     // ring row pitch (floats), = 1 mod 32
-    int sxp;       // padded template row (floats, multiple of 4)
+    int pitch;         // ring row pitch (floats)
+    int plane_stride;  // ring plane stride (floats)
+    int sxp;           // padded template row (floats, multiple of 4)
 };
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
@@ -513,28 +518,96 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
-// One CTA per (node, slab of dz offset planes).  Thread (dzl, tile, dy) owns R consecutive dx outputs.
-// The window streams through a ring of DZ + 1 z-planes in shared memory (cp.async prefetch of the next
-// plane while the current ones are used); the template rows are fully unrolled (SX compile-time) and the
-// R window values of a row stay in registers, so each shared load feeds up to R FMAs.
+// Centred FP32 template of every node of a chunk (FP64 mean, FP64 sum of squares), rows padded to sxp floats.
+__global__ void __launch_bounds__(256) ncc_template_kernel(TiledArgs a, float* T, double* ssf) {
+    __shared__ double red[256 / 32];
+    __shared__ double s_mean;
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.x;
+    const int tid = threadIdx.x;
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    const bool placed = x0 - G.hx >= 0 && x0 + G.hx < G.nx && y0 - G.hy >= 0 && y0 + G.hy < G.ny && z0 - G.hz >= 0 &&
+                        z0 + G.hz < G.nz;
+    const int n = G.sz * G.sy * a.sxp;
+    float* dst = T + (int64_t)blockIdx.x * n;
+    if (!a.t_ok[node] || !placed) {
+        for (int i = tid; i < n; i += blockDim.x) dst[i] = 0.0f;
+        if (tid == 0) ssf[blockIdx.x] = 0.0;
+        return;
+    }
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    auto at = [&](int i) {
+        const int tx = i % a.sxp, row = i / a.sxp, ty = row % G.sy, tz = row / G.sy;
+        return __ldg(a.f + (z0 - G.hz + tz) * sxy + (y0 - G.hy + ty) * G.nx + (x0 - G.hx + tx));
+    };
+    double sf = 0.0;
+    for (int i = tid; i < n; i += blockDim.x)
+        if (i % a.sxp < G.sx) sf += (double)at(i);
+    const int lane = tid & 31, warp = tid >> 5;
+    sf = warp_sum_d(sf);
+    if (lane == 0) red[warp] = sf;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        s_mean = t / (double)G.n_tpl;
+    }
+    __syncthreads();
+    const double mf = s_mean;
+    double q = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        float v = 0.0f;
+        if (i % a.sxp < G.sx) {
+            const double d = (double)at(i) - mf;
+            q += d * d;
+            v = (float)d;
+        }
+        dst[i] = v;
+    }
+    q = warp_sum_d(q);
+    __syncthreads();
+    if (lane == 0) red[warp] = q;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        ssf[blockIdx.x] = t;
+    }
+}
+
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src));
+}
+
+// One CTA per (node, slab of DZ offset planes).  Thread (dzl, tile, dy pair) owns R consecutive dx outputs in
+// two adjacent dy rows: every window row it loads into registers serves two template rows (R * SX FMAs each),
+// so one shared load feeds about 2 * R * SX / (R + SX + SX / 2) FMAs.  Window and template stream through
+// shared memory one z-plane at a time (rings of DZ + 2 window planes and 3 template planes); cp.async keeps
+// the next planes in flight while the current ones are used (wait_group 1), so a step waits only for data
+// issued a step earlier.  Template rows are read as float4 broadcasts.  Partial sums: FP32 per template
+// plane (sy * sx terms), then FP32 across planes; the peak is settled later on FP64 re-scores.
 template <int SX, int R>
-__global__ void __launch_bounds__(512) ncc_tiled_kernel(TiledArgs a) {
+__global__ void __launch_bounds__(512, 1) ncc_tiled_kernel(TiledArgs a) {
     extern __shared__ __align__(16) float sm[];
-    __shared__ double red[512 / 32];
-    __shared__ double s_stat[2];
+    constexpr int SXP = (SX + 3) / 4 * 4;
     const NccGeom& G = a.G;
     const int64_t node = a.node_base + blockIdx.y;
     if (node >= a.n_nodes) return;
     const int DZ = a.dz_slab;
+    const int NS = DZ + 2;
     const int dz0 = blockIdx.x * DZ;
     float* out = a.out + (int64_t)blockIdx.y * G.nmap;
     const int tid = threadIdx.x;
-    const int dy = tid % G.vy;
-    const int rest = tid / G.vy;
+    const int npair = (G.vy + 1) / 2;
+    const int dyp = tid % npair;
+    const int rest = tid / npair;
     const int tile = rest % a.ntile;
     const int dzl = rest / a.ntile;
-    const bool worker = dzl < DZ;
     const int dz = dz0 + dzl;
+    const bool worker = dzl < DZ && dz < G.vz;
+    const int dy0 = 2 * dyp;
+    const bool has1 = dy0 + 1 < G.vy;
     const int dxb = tile * R;
 
     const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
@@ -542,134 +615,133 @@ __global__ void __launch_bounds__(512) ncc_tiled_kernel(TiledArgs a) {
     const bool placed = x0 - G.hx >= 0 && x0 + G.hx < G.nx && y0 - G.hy >= 0 && y0 + G.hy < G.ny && z0 - G.hz >= 0 &&
                         z0 + G.hz < G.nz && wx0 >= 0 && wx0 + G.wx <= G.nx && wy0 >= 0 && wy0 + G.wy <= G.ny && wz0 >= 0 &&
                         wz0 + G.wz <= G.nz;
+    const double ssf = a.ssf[blockIdx.y];
     auto write_all = [&](float v) {
-        if (!worker || dz >= G.vz) return;
+        if (!worker) return;
+        for (int q = 0; q < 2; ++q) {
+            const int dy = dy0 + q;
+            if (dy >= G.vy) continue;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int dx = dxb + r;
-            if (dx < G.vx) out[((int64_t)dz * G.vy + dy) * G.vx + dx] = v;
+            for (int r = 0; r < R; ++r) {
+                const int dx = dxb + r;
+                if (dx < G.vx) out[((int64_t)dz * G.vy + dy) * G.vx + dx] = v;
+            }
         }
     };
-    if (!a.t_ok[node] || !placed) {
+    if (!a.t_ok[node] || !placed || ssf < 1e-20) {
         write_all(-2.0f);
         return;
     }
-    float* T = sm;                                            // [sz][sy][sxp]
-    float* ring = sm + G.sz * G.sy * a.sxp;                   // [DZ + 1][wy][pitch]
-    const int plane_f = G.wy * a.pitch;
+    const int tplane = G.sy * SXP;
+    float* tring = sm;               // [3][sy][SXP]
+    float* ring = sm + 3 * tplane;   // [NS][plane_stride]
+    const float* Tg = a.T + (int64_t)blockIdx.y * G.sz * tplane;
     const int64_t sxy = (int64_t)G.nx * G.ny;
-    // template (raw), zero padding of the rows
-    double sf = 0.0;
-    for (int i = tid; i < G.sz * G.sy * a.sxp; i += blockDim.x) {
-        const int tx = i % a.sxp, row = i / a.sxp, ty = row % G.sy, tz = row / G.sy;
-        float v = 0.0f;
-        if (tx < G.sx) {
-            v = __ldg(a.f + (z0 - G.hz + tz) * sxy + (y0 - G.hy + ty) * G.nx + (x0 - G.hx + tx));
-            sf += (double)v;
-        }
-        T[i] = v;
-    }
-    // first DZ window planes into the ring while the template statistics are reduced
     const int nplanes = min(DZ, G.vz - dz0) + G.sz - 1;  // window planes this slab reads
-    auto load_plane = [&](int p) {
-        if (p >= nplanes) return;
-        float* dst = ring + (p % (DZ + 1)) * plane_f;
-        const float* src = a.g + (wz0 + dz0 + p) * sxy + wy0 * G.nx + wx0;
-        for (int e = tid; e < G.wy * G.wx; e += blockDim.x) {
-            const int yy = e / G.wx, xx = e - yy * G.wx;
-            cp_async4(dst + yy * a.pitch + xx, src + (int64_t)yy * G.nx + xx);
-        }
-    };
-    for (int p = 0; p < DZ; ++p) load_plane(p);
-    cp_async_commit();
-    {
-        const int lane = tid & 31, warp = tid >> 5;
-        double v = warp_sum_d(sf);
-        if (lane == 0) red[warp] = v;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-            s_stat[0] = t / (double)G.n_tpl;
-        }
-        __syncthreads();
-        const double mf = s_stat[0];
-        double q = 0.0;
-        for (int i = tid; i < G.sz * G.sy * a.sxp; i += blockDim.x) {
-            if (i % a.sxp < G.sx) {
-                const double d = (double)T[i] - mf;
-                q += d * d;
-                T[i] = (float)d;
+    auto load_planes = [&](int p, int t) {
+        if (p < nplanes) {
+            float* dst = ring + (p % NS) * a.plane_stride;
+            const float* src = a.g + (wz0 + dz0 + p) * sxy + wy0 * G.nx + wx0;
+            for (int e = tid; e < G.wy * G.wx; e += blockDim.x) {
+                const int yy = e / G.wx, xx = e - yy * G.wx;
+                cp_async4(dst + yy * a.pitch + xx, src + (int64_t)yy * G.nx + xx);
             }
         }
-        q = warp_sum_d(q);
-        __syncthreads();
-        if (lane == 0) red[warp] = q;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-            s_stat[1] = t;
+        if (t < G.sz) {
+            float* dst = tring + (t % 3) * tplane;
+            const float* src = Tg + (int64_t)t * tplane;
+            for (int e = tid; e < tplane / 4; e += blockDim.x) cp_async16(dst + 4 * e, src + 4 * e);
         }
-    }
-    double accd[R];
+    };
+    for (int p = 0; p < DZ; ++p) load_planes(p, p == 0 ? 0 : G.sz);
+    cp_async_commit();
+    load_planes(DZ, 1);
+    cp_async_commit();
+
+    float tot0[R], tot1[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) accd[r] = 0.0;
+    for (int r = 0; r < R; ++r) tot0[r] = tot1[r] = 0.0f;
     for (int tz = 0; tz < G.sz; ++tz) {
-        cp_async_wait_all();
-        __syncthreads();  // planes tz .. tz+DZ-1 visible to all; plane tz-1's slot is free
-        load_plane(tz + DZ);
+        asm volatile("cp.async.wait_group 1;\n" ::);
+        __syncthreads();  // window planes tz .. tz+DZ-1 and template plane tz landed; slots of step tz-1 are free
+        load_planes(tz + DZ + 1, tz + 2);
         cp_async_commit();
-        if (worker && dz < G.vz) {
-            const float* Wp = ring + ((tz + dzl) % (DZ + 1)) * plane_f + dy * a.pitch + dxb;
-            const float* Tp = T + tz * G.sy * a.sxp;
-            float acc[R];
+        if (worker) {
+            const float* Wp = ring + ((tz + dzl) % NS) * a.plane_stride + dy0 * a.pitch + dxb;
+            const float* Tp = tring + (tz % 3) * tplane;
+            float acc0[R], acc1[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) acc[r] = 0.0f;
-            for (int ty = 0; ty < G.sy; ++ty) {
+            for (int r = 0; r < R; ++r) acc0[r] = acc1[r] = 0.0f;
+            const int last = has1 ? G.sy : G.sy - 1;
+            for (int ty = 0; ty <= last; ++ty) {
                 const float* wr = Wp + ty * a.pitch;
-                const float* tr = Tp + ty * a.sxp;
                 float w[R + SX - 1];
 #pragma unroll
                 for (int k = 0; k < R + SX - 1; ++k) w[k] = wr[k];
+                if (ty < G.sy) {
+                    const float4* t4 = reinterpret_cast<const float4*>(Tp + ty * SXP);
 #pragma unroll
-                for (int tx = 0; tx < SX; ++tx) {
-                    const float t = tr[tx];
+                    for (int q = 0; q < SXP / 4; ++q) {
+                        const float4 tv = t4[q];
+                        const float tq[4] = {tv.x, tv.y, tv.z, tv.w};
 #pragma unroll
-                    for (int r = 0; r < R; ++r) acc[r] = fmaf(t, w[tx + r], acc[r]);
+                        for (int u = 0; u < 4; ++u) {
+                            if (4 * q + u < SX) {
+#pragma unroll
+                                for (int r = 0; r < R; ++r) acc0[r] = fmaf(tq[u], w[4 * q + u + r], acc0[r]);
+                            }
+                        }
+                    }
+                }
+                if (ty >= 1 && has1) {
+                    const float4* t4 = reinterpret_cast<const float4*>(Tp + (ty - 1) * SXP);
+#pragma unroll
+                    for (int q = 0; q < SXP / 4; ++q) {
+                        const float4 tv = t4[q];
+                        const float tq[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (4 * q + u < SX) {
+#pragma unroll
+                                for (int r = 0; r < R; ++r) acc1[r] = fmaf(tq[u], w[4 * q + u + r], acc1[r]);
+                            }
+                        }
+                    }
                 }
             }
 #pragma unroll
-            for (int r = 0; r < R; ++r) accd[r] += (double)acc[r];
+            for (int r = 0; r < R; ++r) {
+                tot0[r] += acc0[r];
+                tot1[r] += acc1[r];
+            }
         }
     }
-    cp_async_wait_all();
-    if (!worker || dz >= G.vz) return;
-    const double ssf = s_stat[1];
-    if (ssf < 1e-20) {
-        write_all(-2.0f);
-        return;
-    }
+    asm volatile("cp.async.wait_all;\n" ::);
+    if (!worker) return;
     const double n_tpl = (double)G.n_tpl;
+    for (int q = 0; q < 2; ++q) {
+        const int dy = dy0 + q;
+        if (dy >= G.vy) continue;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int dx = dxb + r;
-        if (dx >= G.vx) continue;
-        const int64_t c = (wz0 + dz) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
-        const double s1 = (double)__ldg(a.B1 + c), s2 = (double)__ldg(a.B2 + c);
-        const double var = s2 - s1 * s1 / n_tpl;
-        float v = 0.0f;
-        if (!(var < 1e-20)) {
-            double q = accd[r] / sqrt(var * ssf);
-            q = q > 1.0 ? 1.0 : (q < -1.0 ? -1.0 : q);
-            v = (float)q;
+        for (int r = 0; r < R; ++r) {
+            const int dx = dxb + r;
+            if (dx >= G.vx) continue;
+            const int64_t c = (wz0 + dz) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
+            const double s1 = (double)__ldg(a.B1 + c), s2 = (double)__ldg(a.B2 + c);
+            const double var = s2 - s1 * s1 / n_tpl;
+            float v = 0.0f;
+            if (!(var < 1e-20)) {
+                double qv = (double)(q == 0 ? tot0[r] : tot1[r]) / sqrt(var * ssf);
+                qv = qv > 1.0 ? 1.0 : (qv < -1.0 ? -1.0 : qv);
+                v = (float)qv;
+            }
+            out[((int64_t)dz * G.vy + dy) * G.vx + dx] = v;
         }
-        out[((int64_t)dz * G.vy + dy) * G.vx + dx] = v;
     }
 }
 
 struct TiledCfg {
-    int R, ntile, dz, threads, pitch, sxp;
+    int R, ntile, dz, threads, pitch, plane_stride, sxp;
     size_t smem;
 };
 
@@ -680,25 +752,64 @@ static bool tiled_supported(int sx) {
     }
 }
 
+// Shared wavefronts of one window-row load, summed over the CTA's warps and over the ring rotations,
+// for the lane layout of ncc_tiled_kernel (dy pair fastest, then tile, then dz plane).
+static long long ring_wavefronts(const NccGeom& G, const TiledCfg& c, int pitch, int pstride) {
+    const int npair = (G.vy + 1) / 2, NS = c.dz + 2;
+    const int n = c.dz * c.ntile * npair;
+    long long total = 0;
+    for (int rot = 0; rot < NS; ++rot)
+        for (int w0 = 0; w0 < n; w0 += 32) {
+            int count[32] = {0};
+            long long seen[32][32];
+            int worst = 1;
+            for (int l = w0; l < std::min(n, w0 + 32); ++l) {
+                const int dyp = l % npair, rest = l / npair, tile = rest % c.ntile, dzl = rest / c.ntile;
+                const long long addr = (long long)((rot + dzl) % NS) * pstride + 2LL * dyp * pitch + (long long)tile * c.R;
+                const int b = (int)(addr % 32);
+                bool dup = false;
+                for (int k = 0; k < count[b]; ++k) dup = dup || seen[b][k] == addr;
+                if (!dup) seen[b][count[b]++] = addr;
+                worst = std::max(worst, count[b]);
+            }
+            total += worst;
+        }
+    return total;
+}
+
+static size_t tiled_smem(const NccGeom& G, const TiledCfg& c, int dz, int plane_stride) {
+    const size_t tail = 64;  // the discarded tail outputs of the last tile read up to R + SX floats past the last row
+    return ((size_t)3 * G.sy * c.sxp + (size_t)(dz + 2) * plane_stride + tail) * sizeof(float);
+}
+
 static bool tiled_config(const NccGeom& G, TiledCfg& c) {
+    static std::mutex mu;
+    static bool have = false;
+    static NccGeom lastG;
+    static TiledCfg lastC;
+    std::lock_guard<std::mutex> lock(mu);
+    if (have && std::memcmp(&lastG, &G, sizeof(G)) == 0) {
+        c = lastC;
+        return true;
+    }
     if (!tiled_supported(G.sx)) return false;
     const int w9 = ((G.vx + 8) / 9) * 9 - G.vx, w11 = ((G.vx + 10) / 11) * 11 - G.vx;
     c.R = w11 <= w9 ? 11 : 9;
     c.ntile = (G.vx + c.R - 1) / c.R;
     c.sxp = (G.sx + 3) / 4 * 4;
-    c.pitch = G.wx + ((1 - G.wx) % 32 + 32) % 32;  // = 1 mod 32: consecutive dy rows land in distinct banks
-    const int per_plane = G.vy * c.ntile;
+    const int npair = (G.vy + 1) / 2;
+    const int per_plane = npair * c.ntile;
     if (per_plane > 512) return false;
     const size_t smax = (size_t)max_smem_optin() - 8192;
+    const int max_stride = G.wy * (G.wx + 7) + 31;
     int best = 0;
     double best_cost = 1e300;
-    const size_t tail = 64;  // the discarded tail outputs of the last tile read up to R + SX floats past the last ring row
     for (int dz = 1; dz <= G.vz && dz * per_plane <= 512; ++dz) {
-        const size_t smem = ((size_t)G.sz * G.sy * c.sxp + (size_t)(dz + 1) * G.wy * c.pitch + tail) * sizeof(float);
-        if (smem > smax) break;
+        if (tiled_smem(G, c, dz, max_stride) > smax) break;
         const int slabs = (G.vz + dz - 1) / dz;
-        // idle output planes plus the per-CTA overhead of re-reading the template and the window halo
-        const double cost = (double)slabs * dz * per_plane * (G.sz + dz - 1) / dz + 0.15 * slabs * G.n_tpl / 32.0;
+        // thread-slots per template plane (idle tail planes included) plus the per-CTA plane loads
+        const double cost = (double)slabs * dz * per_plane * (G.sy + 1) * G.sx +
+                            (double)slabs * (dz + G.sz) * G.wy * G.wx * 2.0;
         if (cost < best_cost) {
             best_cost = cost;
             best = dz;
@@ -707,8 +818,30 @@ static bool tiled_config(const NccGeom& G, TiledCfg& c) {
     if (best == 0) return false;
     c.dz = best;
     c.threads = (best * per_plane + 31) / 32 * 32;
-    c.smem = ((size_t)G.sz * G.sy * c.sxp + (size_t)(best + 1) * G.wy * c.pitch + tail) * sizeof(float);
+    // ring geometry with the fewest shared wavefronts for this lane layout
+    long long best_w = -1;
+    for (int pitch = G.wx; pitch < G.wx + 8; ++pitch)
+        for (int pad = 0; pad < 32; ++pad) {
+            const int ps = G.wy * pitch + pad;
+            const long long wv = ring_wavefronts(G, c, pitch, ps);
+            if (best_w < 0 || wv < best_w) {
+                best_w = wv;
+                c.pitch = pitch;
+                c.plane_stride = ps;
+            }
+        }
+    c.smem = tiled_smem(G, c, best, c.plane_stride);
+    if (c.smem > smax) return false;
+    lastG = G;
+    lastC = c;
+    have = true;
     return true;
+}
+
+// Template scratch of the tiled engine for a chunk of nodes: centred templates, then their sums of squares.
+static size_t tiled_tpl_bytes(const NccGeom& G, int64_t chunk) {
+    const int sxp = (G.sx + 3) / 4 * 4;
+    return align_up((size_t)chunk * G.sz * G.sy * sxp * sizeof(float), 256) + align_up((size_t)chunk * sizeof(double), 256);
 }
 
 template <int SX, int R>
@@ -722,12 +855,19 @@ static int launch_tiled_t(const TiledArgs& a, const TiledCfg& c, int64_t n_chunk
         attr = want;
     }
     const unsigned slabs = (unsigned)((a.G.vz + c.dz - 1) / c.dz);
+    const int64_t tsz = (int64_t)a.G.sz * a.G.sy * c.sxp;
     for (int64_t done = 0; done < n_chunk; done += 65535) {
+        const unsigned nb = (unsigned)std::min<int64_t>(65535, n_chunk - done);
         TiledArgs aa = a;
         aa.node_base = a.node_base + done;
         aa.out = a.out + done * a.G.nmap;
-        kern<<<dim3(slabs, (unsigned)std::min<int64_t>(65535, n_chunk - done)), c.threads, c.smem, s>>>(aa);
-        const int rc = check_launch("ncc tiled");
+        aa.T = a.T + done * tsz;
+        aa.ssf = a.ssf + done;
+        ncc_template_kernel<<<nb, 256, 0, s>>>(aa, const_cast<float*>(aa.T), const_cast<double*>(aa.ssf));
+        int rc = check_launch("ncc template");
+        if (rc) return rc;
+        kern<<<dim3(slabs, nb), c.threads, c.smem, s>>>(aa);
+        rc = check_launch("ncc tiled");
         if (rc) return rc;
     }
     return ALDVC_OK;
@@ -865,7 +1005,8 @@ extern "C" size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_
     const int64_t chunk = search_chunk(G, n);
     size_t b = align_up((size_t)n * 32, 256) + align_up((size_t)chunk * G.nmap * sizeof(float), 256);
     TiledCfg c;
-    if (use_tiled(G, engine, c)) b += 4 * align_up((size_t)nz * ny * nx * sizeof(float), 256);  // box sums + temporaries
+    if (use_tiled(G, engine, c))  // box sums + temporaries, template scratch
+        b += 4 * align_up((size_t)nz * ny * nx * sizeof(float), 256) + tiled_tpl_bytes(G, chunk);
     return b;
 }
 
@@ -945,11 +1086,15 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
         ta.t_ok = a.t_ok;
         ta.B1 = b1;
         ta.B2 = b2;
+        float* tpl = (float*)(box + 4 * vb);
+        ta.T = tpl;
+        ta.ssf = (const double*)((char*)tpl + align_up((size_t)chunk * G.sz * G.sy * tc.sxp * sizeof(float), 256));
         ta.n_nodes = n_nodes;
         ta.G = G;
         ta.dz_slab = tc.dz;
         ta.ntile = tc.ntile;
         ta.pitch = tc.pitch;
+        ta.plane_stride = tc.plane_stride;
         ta.sxp = tc.sxp;
     }
     for (int64_t start = 0; start < n_nodes; start += chunk) {
