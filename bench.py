@@ -232,6 +232,18 @@ def _host_volumes(cfg: int):
 
 
 # --------------------------------------------------------------------------- B200 arm
+def _tuned_shapes() -> list:
+    """The autotuner's choice of (threads, brick_floats) per IC-GN kernel and its timings (ms per sample launch)."""
+    from pyaldvc_b200 import autotune
+
+    rows = []
+    for k, choice in autotune._cache.items():
+        t = autotune.timings(k) or {}
+        rows.append({"ndof": k[0], "mode": k[1], "half": list(k[3]), "choice": list(choice),
+                     "ms": {f"{a}x{b}": round(v, 3) for (a, b), v in t.items()}})
+    return rows
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -416,6 +428,7 @@ def main():
         "batched_over_plain": None if plain is None else value / world / plain["value"],
         "e2e": {"value": e2e_val, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "clocks": clocks.summary(),
+        "icgn_launch_shapes": _tuned_shapes(),
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

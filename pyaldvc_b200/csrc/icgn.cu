@@ -811,6 +811,240 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
     }
 }
 
+// ----------------------------------------------------------------------------- lean persistent kernel
+// NW warps per node and no shared brick: the deformed volume is sampled through L1 at positions taken
+// relative to the node centre, so a CTA holds only its control block and up to 16 nodes run per SM.
+// While thread 0 of one CTA runs the FP64 control step, the other CTAs of the SM keep the pipes busy.
+// Voxel indices advance incrementally (no divisions in the loop); the per-thread FP32 moments are
+// reduced across the warp in FP64.
+struct LeanCtl {
+    double P[12];
+    float A[9];
+    float t[3];
+    int slow;
+    int state;
+    int64_t node;
+    float cf, cg;
+};
+
+template <int MODE, bool STORED, int NDOF, int NW>
+__global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a) {
+    constexpr int T = NW * 32;
+    constexpr int NB = Acc<NDOF>::NB;
+    constexpr int NV = 5 + 3 * NB;
+    __shared__ LeanCtl sc;
+    __shared__ double red[NW][NV];
+    __shared__ int redi[NW][3];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t sxy = (int64_t)a.nx * a.ny;
+    const int nXY = a.nX * a.nY;
+    const int S = nXY * a.nZ;
+    const int sx_ = T % a.nX, sy_ = (T / a.nX) % a.nY, sz_ = T / nXY;  // index step of T voxels
+    const int tix = tid % a.nX, tiy = (tid / a.nX) % a.nY, tiz = tid / nXY;
+    const int lo = MODE == 0 ? 0 : 1, hx_ = MODE == 0 ? a.nx - 2 : a.nx - 3, hy_ = MODE == 0 ? a.ny - 2 : a.ny - 3,
+              hz_ = MODE == 0 ? a.nz - 2 : a.nz - 3;
+    Ctl12 c12;  // live in thread 0 only
+    Ctl3 c3;
+
+    for (;;) {
+        __syncthreads();  // every thread has finished reading the previous node's control block
+        if (tid == 0) {
+            const int q = atomicAdd(a.counter, 1);
+            sc.node = q < a.n_nodes ? (int64_t)q : -1;
+            sc.state = 1;
+            if (sc.node >= 0 && node_begin<NDOF>(a, sc.node, c12, c3)) {
+                sc.state = 0;
+                const double* P = NDOF == 12 ? c12.P : c3.P;
+                for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+                sc.cf = (float)a.meanf[sc.node];
+                sc.cg = sc.cf;
+            }
+        }
+        __syncthreads();
+        const int64_t node = sc.node;
+        if (node < 0) break;
+        if (sc.state != 0) continue;
+        const int64_t xc = a.coords[3 * node], yc = a.coords[3 * node + 1], zcn = a.coords[3 * node + 2];
+        const int64_t srow = a.split_index ? a.split_index[node] : -1;
+        const uint8_t* keep = srow >= 0 ? a.split_keep + srow * a.keep_bytes : nullptr;
+        const bool inside = xc - a.hx >= 0 && xc + a.hx < a.nx && yc - a.hy >= 0 && yc + a.hy < a.ny && zcn - a.hz >= 0 &&
+                            zcn + a.hz < a.nz;
+        const int xci = (int)xc, yci = (int)yc, zci = (int)zcn;
+
+        for (int it = 1; it <= a.max_iter; ++it) {
+            if (tid == 0) {
+                const Box bb = warp_box(a, sc.P, xc, yc, zcn, 0, a.nZ, MODE);
+                sc.slow = bb.corners_in ? 0 : 1;
+                const double* P = sc.P;
+                sc.A[0] = (float)(1.0 + P[0]);
+                sc.A[1] = (float)P[1];
+                sc.A[2] = (float)P[2];
+                sc.A[3] = (float)P[3];
+                sc.A[4] = (float)(1.0 + P[4]);
+                sc.A[5] = (float)P[5];
+                sc.A[6] = (float)P[6];
+                sc.A[7] = (float)P[7];
+                sc.A[8] = (float)(1.0 + P[8]);
+                sc.t[0] = (float)P[9];
+                sc.t[1] = (float)P[10];
+                sc.t[2] = (float)P[11];
+            }
+            __syncthreads();
+            const bool slow = sc.slow != 0;
+            const float A0 = sc.A[0], A1 = sc.A[1], A2 = sc.A[2], A3 = sc.A[3], A4 = sc.A[4], A5 = sc.A[5], A6 = sc.A[6],
+                        A7 = sc.A[7], A8 = sc.A[8];
+            const float T0 = sc.t[0], T1 = sc.t[1], T2 = sc.t[2];
+            const float cf = sc.cf, cg = sc.cg;
+            Acc<NDOF> acc;
+            acc.zero();
+            int ix = tix, iy = tiy, iz = tiz;
+            for (int v = tid; v < S; v += T) {
+                const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+                const int vx = ix, vy = iy, vz = iz;
+                ix += sx_;
+                iy += sy_;
+                iz += sz_;
+                if (ix >= a.nX) {
+                    ix -= a.nX;
+                    ++iy;
+                }
+                if (iy >= a.nY) {
+                    iy -= a.nY;
+                    ++iz;
+                }
+                const int xx = xci + dx, yy = yci + dy, zz = zci + dz;
+                bool k;
+                if (keep || !inside) {
+                    k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
+                    if (k)
+                        k = keep ? kept_bit(keep, (vz * a.nY + vy) * a.nX + vx)
+                                 : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0);
+                } else {
+                    k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0;
+                }
+                if (!k) continue;
+                acc.nref += 1;
+                const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+                if (slow) {
+                    const double* P = sc.P;
+                    const double xw = (1.0 + P[0]) * dx + P[1] * dy + P[2] * dz + ((double)xc + P[9]);
+                    const double yw = P[3] * dx + (1.0 + P[4]) * dy + P[5] * dz + ((double)yc + P[10]);
+                    const double zw = P[6] * dx + P[7] * dy + (1.0 + P[8]) * dz + ((double)zcn + P[11]);
+                    if (!margin_ok(zw, yw, xw, a.nz, a.ny, a.nx)) {
+                        acc.oob = 1;
+                        continue;
+                    }
+                }
+                const int64_t o = zz * sxy + (int64_t)yy * a.nx + xx;
+                // reference-frame reads first: their latency overlaps the interpolation
+                const float fv = __ldg(a.f + o);
+                float q0, q1, q2;
+                if (STORED) {
+                    q0 = __ldg(a.gx + o);
+                    q1 = __ldg(a.gy + o);
+                    q2 = __ldg(a.gz + o);
+                } else {
+                    grad_otf(a.f, a.nz, a.ny, a.nx, zz, yy, xx, q0, q1, q2);
+                }
+                const float xr = A0 * X + A1 * Y + A2 * Z + T0;
+                const float yr = A3 * X + A4 * Y + A5 * Z + T1;
+                const float zr = A6 * X + A7 * Y + A8 * Z + T2;
+                const float fxf = floorf(xr), fyf = floorf(yr), fzf = floorf(zr);
+                const int gx_ = min(max(xci + (int)fxf, lo), hx_), gy_ = min(max(yci + (int)fyf, lo), hy_),
+                          gz_ = min(max(zci + (int)fzf, lo), hz_);
+                const float gv = sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf, yr - fyf, zr - fzf);
+                if (gv != gv) continue;  // NaN: masked out in the deformed frame
+                acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
+            }
+            {
+                float vals[NV];
+                vals[0] = acc.Sg;
+                vals[1] = acc.Sgg;
+                vals[2] = acc.Sf;
+                vals[3] = acc.Sff;
+                vals[4] = acc.Sfg;
+#pragma unroll
+                for (int k = 0; k < NB; ++k) {
+                    vals[5 + k] = acc.SD[k];
+                    vals[5 + NB + k] = acc.SDf[k];
+                    vals[5 + 2 * NB + k] = acc.SDg[k];
+                }
+#pragma unroll
+                for (int i = 0; i < NV; ++i) {
+                    double s = (double)vals[i];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                    if (lane == 0) red[warp][i] = s;
+                }
+                const int n = warp_sum_i(acc.n), nr = warp_sum_i(acc.nref);
+                const int oob = __any_sync(0xffffffffu, acc.oob != 0) ? 1 : 0;
+                if (lane == 0) {
+                    redi[warp][0] = n;
+                    redi[warp][1] = nr;
+                    redi[warp][2] = oob;
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                Moments mom;
+                double t[NV];
+                for (int i = 0; i < NV; ++i) {
+                    double s = 0.0;
+                    for (int w = 0; w < NW; ++w) s += red[w][i];
+                    t[i] = s;
+                }
+                int64_t nn = 0, nrr = 0;
+                int oo = 0;
+                for (int w = 0; w < NW; ++w) {
+                    nn += redi[w][0];
+                    nrr += redi[w][1];
+                    oo |= redi[w][2];
+                }
+                mom.n = nn;
+                mom.nref = nrr;
+                mom.oob = oo;
+                mom.Sg = t[0];
+                mom.Sgg = t[1];
+                mom.Sf = t[2];
+                mom.Sff = t[3];
+                mom.Sfg = t[4];
+                for (int k = 0; k < NB; ++k) {
+                    mom.SD[k] = t[5 + k];
+                    mom.SDf[k] = t[5 + NB + k];
+                    mom.SDg[k] = t[5 + 2 * NB + k];
+                }
+                double b[12], bf, bg, s_cc;
+                int64_t nv;
+                const int st0 = finish_moments(mom, sc.cf, sc.cg, NB, b, bf, bg, s_cc, nv);
+                int st;
+                double zc = nan("");
+                if (st0 != 0) {
+                    st = st0;
+                } else if (NDOF == 12) {
+                    st = control12(c12, b, bf, bg, s_cc, nv, a.L + node * 144, a.H ? a.H + node * 144 : nullptr, a.pattern,
+                                   a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+                } else {
+                    st = control3(c3, b, bf, bg, s_cc, nv, a.mu, a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+                }
+                if (st >= 0) {
+                    node_end<NDOF>(a, node, c12, c3, it, st, zc);
+                    sc.state = 1;
+                } else {
+                    const double* P = NDOF == 12 ? c12.P : c3.P;
+                    for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+                    sc.cg = (float)((double)sc.cg + mom.Sg / (double)mom.n);
+                    if (it == a.max_iter) {
+                        node_end<NDOF>(a, node, c12, c3, a.max_iter, ST_MAX_ITER, NDOF == 12 ? c12.zncc : c3.zncc);
+                        sc.state = 1;
+                    }
+                }
+            }
+            __syncthreads();
+            if (sc.state != 0) break;
+        }
+    }
+}
+
 // ----------------------------------------------------------------------------- plain one-node-per-block kernel
 template <int MODE, bool STORED, int NDOF>
 __global__ void __launch_bounds__(256) icgn_plain_kernel(IcgnArgs a) {
@@ -1043,8 +1277,9 @@ struct LaunchCfg {
 
 static LaunchCfg batched_cfg(const aldvc_icgn_params* prm) {
     LaunchCfg c;
+    // 32/64/128: lean kernel with 1/2/4 warps per node; 256/512: shared-brick kernel
     c.threads = prm->threads > 0 ? prm->threads : 256;
-    if (c.threads != 256 && c.threads != 512) c.threads = 256;
+    if (c.threads != 32 && c.threads != 64 && c.threads != 128 && c.threads != 256 && c.threads != 512) c.threads = 256;
     c.brick_cap = prm->brick_floats > 0 ? prm->brick_floats : 24 * 1024;
     return c;
 }
@@ -1076,9 +1311,35 @@ static int launch_batched_t(const IcgnArgs& a, int brick_cap, cudaStream_t s) {
     return check_launch("icgn batched");
 }
 
+template <int MODE, bool STORED, int NDOF, int NW>
+static int launch_lean_t(const IcgnArgs& a, cudaStream_t s) {
+    auto kern = icgn_lean_kernel<MODE, STORED, NDOF, NW>;
+    static int cached_per_sm = -1;  // queried once, outside any stream capture
+    static std::mutex mu;
+    int per_sm;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (cached_per_sm < 0) {
+            int v = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, NW * 32, 0);
+            if (e != cudaSuccess) return cuda_fail(e, "icgn lean: occupancy");
+            cached_per_sm = v;
+        }
+        per_sm = cached_per_sm;
+    }
+    if (per_sm < 1) return arg_fail("icgn lean: kernel does not fit on an SM");
+    long long grid = (long long)per_sm * sm_count();
+    if (grid > a.n_nodes) grid = a.n_nodes;
+    kern<<<(unsigned)grid, NW * 32, 0, s>>>(a);
+    return check_launch("icgn lean");
+}
+
 template <int MODE, bool STORED, int NDOF>
 static int launch_batched_m(const IcgnArgs& a, const LaunchCfg& c, cudaStream_t s) {
     switch (c.threads) {
+        case 32: return launch_lean_t<MODE, STORED, NDOF, 1>(a, s);
+        case 64: return launch_lean_t<MODE, STORED, NDOF, 2>(a, s);
+        case 128: return launch_lean_t<MODE, STORED, NDOF, 4>(a, s);
         case 512: return launch_batched_t<MODE, STORED, NDOF, 512>(a, c.brick_cap, s);
         default: return launch_batched_t<MODE, STORED, NDOF, 256>(a, c.brick_cap, s);
     }

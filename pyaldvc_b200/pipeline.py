@@ -16,6 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
+from . import autotune
 from . import kernels as K
 from .mesh import build_grid_axes, grid_coords
 
@@ -53,8 +54,9 @@ class PassParams:
     pcg_max_iter: int = 500
     gauss_pt_order: int = 2
     variant: int = K.BATCHED
-    threads: int = 0
+    threads: int = 0  # 0: chosen by the autotuner (or the library default when autotune is off)
     brick_floats: int = 0
+    autotune: bool = True
     graph: bool = False
 
 
@@ -148,6 +150,16 @@ def _rms(a: torch.Tensor) -> torch.Tensor:
     return torch.sqrt(torch.mean(a * a))
 
 
+def _launch_shape(p: PassParams, ndof: int, mode: int, mesh, mask, run) -> tuple[int, int]:
+    """(threads, brick_floats) of the batched IC-GN launches: the caller's, else the autotuner's choice for
+    this kernel and subset, timed on an evenly spread sample of this pass's nodes."""
+    if p.variant != K.BATCHED or p.threads != 0 or not p.autotune:
+        return p.threads, p.brick_floats
+    k = autotune.key(ndof, mode, True, mesh.half, p.subset_stride, mask is not None, mesh.n)
+    idx = autotune.sample_index(mesh.n)
+    return autotune.tune(k, lambda th, br: run(idx, th, br))
+
+
 def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
              tracer: Tracer | None = None) -> PassResult:
     """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16)."""
@@ -226,9 +238,15 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
     P0 = torch.zeros((mesh.n, 12), dtype=torch.float64, device="cuda")
     P0[:, 9:] = U0
-    P, n_iter, status, zncc = K.icgn12(mesh.coords, P0, mesh.half, f, gx, gy, gz, m_u8, g, mode, L, meanf, valid_u8, p.icgn_tol,
-                                       p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, None, None, 0.0,
-                                       p.icgn_predictive_stop, None, None, p.variant, p.threads, p.brick_floats)
+
+    def icgn12_on(idx, th, br):
+        c, P0_, L_, mf_, v_ = ((mesh.coords, P0, L, meanf, valid_u8) if idx is None else
+                               (mesh.coords[idx], P0[idx], L[idx], meanf[idx], valid_u8[idx]))
+        return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
+                        p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br)
+
+    th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
+    P, n_iter, status, zncc = icgn12_on(None, th12, br12)
     bad = status != STATUS_CONVERGED
     flag = _median_flags(P[:, 9:].contiguous(), ~bad, mesh.grid_shape, p.local_outlier_threshold)
     bad = bad | flag
@@ -263,11 +281,20 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     v = U2 - U1
     n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
 
+    def icgn3_on(idx, U2_, F2_, v_, th, br):
+        c, H_, mf_, bf_, ok_ = ((mesh.coords, H, meanf, bottomf, valid_u8) if idx is None else
+                                (mesh.coords[idx], H[idx], meanf[idx], bottomf[idx], valid_u8[idx]))
+        if idx is not None:
+            U2_, F2_, v_ = U2_[idx], F2_[idx], v_[idx]
+        return K.icgn3(c, U2_, F2_, v_, mesh.half, f, gx, gy, gz, m_u8, g, mode, H_, mf_, bf_, ok_, p.mu, p.icgn_tol, p.icgn_dp_tol,
+                       p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0, p.icgn_predictive_stop, None, None, p.variant,
+                       th, br)
+
+    th3, br3 = _launch_shape(p, 3, mode, mesh, m_u8, lambda idx, th, br: icgn3_on(idx, U2, F2, v, th, br))
+
     def admm_step(U2, F2, W, v):
         # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
-        U, it3, st3, zc3 = K.icgn3(mesh.coords, U2, F2, v, mesh.half, f, gx, gy, gz, m_u8, g, mode, H, meanf, bottomf, valid_u8,
-                                   p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full,
-                                   0.0, p.icgn_predictive_stop, None, None, p.variant, p.threads, p.brick_floats)
+        U, it3, st3, zc3 = icgn3_on(None, U2, F2, v, th3, br3)
         bad3 = st3 != STATUS_CONVERGED
         bad3 = bad3 | _median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold)
         U1n = torch.where(bad3[:, None], U2, U)

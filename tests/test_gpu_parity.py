@@ -67,9 +67,13 @@ def test_precompute_matches_reference(golden, ck, name):
     np.testing.assert_allclose(L[ok], Lr[ok], rtol=1e-3, atol=1e-4 * np.abs(Lr[ok]).max())
 
 
-@pytest.mark.parametrize("variant", [0, 1], ids=["batched", "plain"])
+FORMS = [(0, 0), (0, 32), (0, 64), (0, 128), (1, 0)]  # (variant, threads): brick kernel, lean kernel with 1/2/4 warps, plain
+FORM_IDS = ["brick", "lean1", "lean2", "lean4", "plain"]
+
+
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 @pytest.mark.parametrize("name", list(ICGN12))
-def test_icgn12_matches_reference(golden, ck, name, variant):
+def test_icgn12_matches_reference(golden, ck, name, form):
     c = ICGN12[name]
     pc, (gx, gy, gz), mask, kw = pre_args(golden, c["pre"])
     H, L, mf, bf, valid = _pre_outputs(golden, c["pre"])
@@ -79,15 +83,15 @@ def test_icgn12_matches_reference(golden, ck, name, variant):
     args = (golden["coords"], P0, *pc["h"], golden["f"], gx, gy, gz, mask, g, c["mode"], L, mf, bf, valid, c.get("tol", 1e-2),
             c.get("dp_tol", 1e-3), c.get("max_iter", 100), c.get("patience", 5), pc["stride"], H,
             golden[f"icgn12_{name}_pattern"], gain, c.get("predictive", True))
-    got = ck.icgn_12dof_cuda(*args, **kw, variant=variant)
+    got = ck.icgn_12dof_cuda(*args, **kw, variant=form[0], threads=form[1])
     ref = tuple(golden[f"icgn12_{name}_{k}"] for k in ("P", "n_iter", "status", "zncc"))
     assert_parity(ref, got, what=f"icgn12/{name}")
     np.testing.assert_array_equal(P0, golden["P0_special"] if c.get("special") else P0)  # P0 not mutated
 
 
-@pytest.mark.parametrize("variant", [0, 1], ids=["batched", "plain"])
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 @pytest.mark.parametrize("name", list(ICGN3))
-def test_icgn3_matches_reference(golden, ck, name, variant):
+def test_icgn3_matches_reference(golden, ck, name, form):
     c = ICGN3[name]
     pc, (gx, gy, gz), mask, kw = pre_args(golden, c["pre"])
     H, L, mf, bf, valid = _pre_outputs(golden, c["pre"])
@@ -95,7 +99,7 @@ def test_icgn3_matches_reference(golden, ck, name, variant):
     gain = STENCIL_NOISE_GAIN if c.get("noise") else 0.0
     got = ck.icgn_3dof_cuda(golden["coords"], golden["U_old"], golden["F_fixed"], golden["vdual"], *pc["h"], golden["f"], gx, gy,
                             gz, mask, g, c["mode"], H, mf, bf, valid, 1e-3, 1e-2, 1e-3, 100, 5, pc["stride"],
-                            float(golden[f"icgn3_{name}_n_full"]), gain, True, **kw, variant=variant)
+                            float(golden[f"icgn3_{name}_n_full"]), gain, True, **kw, variant=form[0], threads=form[1])
     ref = tuple(golden[f"icgn3_{name}_{k}"] for k in ("U", "n_iter", "status", "zncc"))
     assert_parity(ref, got, what=f"icgn3/{name}")
 
