@@ -178,9 +178,12 @@ int aldvc_ncc_map(const float *f, const float *g, int64_t nz, int64_t ny, int64_
                   const int64_t *wz0, const uint8_t *t_ok, float *out, void *stream);
 
 /* NCC engines: TILED (shared-memory window ring, register-tiled cross term, box-filter volumes for the
- * window statistics; templates 5..33 voxels wide) and PLAIN (one thread per offset, the reference layout) */
+ * window statistics; templates 5..33 voxels wide), PLAIN (one thread per offset, the reference layout) and
+ * FFT (cross term by 3-D FFTs of 2,3,5-smooth lengths up to 128 per axis, replacing the reference's
+ * rfftn/irfftn engine, integer_search.py:423-443; a geometry it does not take runs on TILED) */
 #define ALDVC_NCC_TILED 0
 #define ALDVC_NCC_PLAIN 1
+#define ALDVC_NCC_FFT 2
 
 size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz,
                                        int32_t rx, int32_t ry, int32_t rz, int32_t engine);

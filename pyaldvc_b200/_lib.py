@@ -17,6 +17,7 @@ BATCHED = 0
 PLAIN = 1
 NCC_TILED = 0
 NCC_PLAIN = 1
+NCC_FFT = 2
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32

@@ -223,47 +223,68 @@ __global__ void ncc_place_kernel(SearchArgs a) {
     a.freeb[n] = fb;
 }
 
-// FP64 value of one offset, the reference's arithmetic (FP64 template, float32-rounded squares).
-__device__ double rescore(const SearchArgs& a, int64_t node, const float* Tf, double mf, double ssf, int dz, int dy, int dx,
-                          double* red) {
-    const NccGeom& G = a.G;
-    const int64_t sxy = (int64_t)G.nx * G.ny;
-    const int64_t zb = a.wz0[node] + dz, yb = a.wy0[node] + dy, xb = a.wx0[node] + dx;
+// FP64 value of one offset, the reference's arithmetic (FP64 centred template, float32-rounded squares),
+// computed by one warp: template voxel (k, j, i) at tp[k tsz + j tsy + i], its window voxel at
+// wp[k wsz + j wsy + i].  Lanes stride the template in C order; the sums are reduced by shuffles in a fixed
+// order, and every lane returns the value.
+__device__ double warp_rescore(const float* tp, int64_t tsz, int64_t tsy, const float* wp, int64_t wsz, int64_t wsy,
+                               const NccGeom& G, double mf, double ssf) {
+    const int lane = threadIdx.x & 31;
     double sfg = 0.0, sg = 0.0, sgg = 0.0;
-    for (int i = threadIdx.x; i < G.n_tpl; i += blockDim.x) {
-        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
-        const float v = __ldg(a.g + (zb + k) * sxy + (yb + j) * G.nx + (xb + ii));
-        const float vv = v * v;
-        sg += (double)v;
-        sgg += (double)vv;
-        // template value in FP64: f - mean, re-read so no FP32 rounding of the centred value enters
-        const float fv = __ldg(a.f + (a.coords[3 * node + 2] - G.hz + k) * sxy + (a.coords[3 * node + 1] - G.hy + j) * G.nx +
-                               (a.coords[3 * node] - G.hx + ii));
+    int ii = lane % G.sx, j = (lane / G.sx) % G.sy, k = lane / (G.sx * G.sy);
+    const int di = 32 % G.sx, dj = (32 / G.sx) % G.sy, dk = 32 / (G.sx * G.sy);
+    for (int t = lane; t < G.n_tpl; t += 32) {
+        const float fv = tp[k * tsz + j * tsy + ii];
+        const float v = wp[k * wsz + j * wsy + ii];
         sfg += ((double)fv - mf) * (double)v;
+        sg += (double)v;
+        sgg += (double)(v * v);
+        ii += di;
+        j += dj;
+        k += dk;
+        if (ii >= G.sx) {
+            ii -= G.sx;
+            ++j;
+        }
+        if (j >= G.sy) {
+            j -= G.sy;
+            ++k;
+        }
     }
-    (void)Tf;
-    sfg = block_sum_d(sfg, red);
-    sg = block_sum_d(sg, red);
-    sgg = block_sum_d(sgg, red);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sfg += __shfl_xor_sync(0xffffffffu, sfg, o);
+        sg += __shfl_xor_sync(0xffffffffu, sg, o);
+        sgg += __shfl_xor_sync(0xffffffffu, sgg, o);
+    }
     const double var = sgg - sg * sg / (double)G.n_tpl;
     if (var < 1e-20) return 0.0;
-    double v = sfg / sqrt(var * ssf);
+    const double v = sfg / sqrt(var * ssf);
     return v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v);
 }
 
-// one CTA per node of the chunk
-__global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
+// One CTA per node of the chunk.  Two sweeps of the FP32 map: (1) maximum (first index on ties), minimum;
+// (2) candidates within NEAR_TIE of the maximum and the PCE energy.  The template (raw FP32 f) and, for the
+// sub-voxel fit, the window box around the peak are staged in shared memory when SMEM; each FP64 re-score is
+// one warp's job.
+template <bool SMEM>
+__global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) float psm[];
     __shared__ double red[NCC_THREADS / 32];
-    __shared__ float s_max;
+    __shared__ float s_best[NCC_THREADS / 32], s_mn[NCC_THREADS / 32];
+    __shared__ int s_bidx[NCC_THREADS / 32];
     __shared__ int s_cand[MAX_CAND];
+    __shared__ double s_cval[MAX_CAND];
     __shared__ int s_ncand;
     __shared__ double s_neigh[27];
+    __shared__ float s_max, s_min;
     __shared__ int s_pk;
     const NccGeom& G = a.G;
     const int64_t node = a.node_base + blockIdx.x;
     if (node >= a.n_nodes) return;
     const float* map = a.map + (int64_t)blockIdx.x * G.nmap;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NCC_THREADS / 32;
     const int64_t sxy = (int64_t)G.nx * G.ny;
     if (!a.t_ok[node]) {
         if (tid == 0) {
@@ -277,14 +298,12 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
     }
     // flat template: the map is -2 everywhere (integer_search.py:420-421)
     const bool flat = map[0] < -1.5f;
-    // FP32 maximum with the first-index tie rule; the -2 marker counts as 0
-    float best = -3.0f;
+    float best = -3.0f, mn = 3.0f;
     int bidx = 0x7fffffff;
-    float mn = 3.0f;
     for (int i = tid; i < G.nmap; i += blockDim.x) {
         float v = map[i];
         v = v < -1.0f ? 0.0f : v;
-        if (v > best || (v == best && i < bidx)) {
+        if (v > best) {  // ascending i per thread: the first index wins a tie
             best = v;
             bidx = i;
         }
@@ -299,18 +318,16 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
         }
         mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
     }
-    __shared__ float s_best[NCC_THREADS / 32], s_mn[NCC_THREADS / 32];
-    __shared__ int s_bidx[NCC_THREADS / 32];
-    if ((tid & 31) == 0) {
-        s_best[tid >> 5] = best;
-        s_bidx[tid >> 5] = bidx;
-        s_mn[tid >> 5] = mn;
+    if (lane == 0) {
+        s_best[warp] = best;
+        s_bidx[warp] = bidx;
+        s_mn[warp] = mn;
     }
     __syncthreads();
     if (tid == 0) {
         float b = s_best[0], m = s_mn[0];
         int bi = s_bidx[0];
-        for (int w = 1; w < NCC_THREADS / 32; ++w) {
+        for (int w = 1; w < NW; ++w) {
             if (s_best[w] > b || (s_best[w] == b && s_bidx[w] < bi)) {
                 b = s_best[w];
                 bi = s_bidx[w];
@@ -319,45 +336,58 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
         }
         s_max = b;
         s_pk = bi;
-        s_best[0] = m;
+        s_min = m;
         s_ncand = 0;
     }
     __syncthreads();
-    const float vmax = s_max, vmin = s_best[0];
-    // candidates within the FP32 error bound of the maximum, kept in C order
-    if (!flat) {
-        for (int i = tid; i < G.nmap; i += blockDim.x) {
-            float v = map[i];
-            v = v < -1.0f ? 0.0f : v;
-            if (v >= vmax - NEAR_TIE) {
-                const int slot = atomicAdd(&s_ncand, 1);
-                if (slot < MAX_CAND) s_cand[slot] = i;
-            }
+    const float vmax = s_max, vmin = s_min;
+    const float cmin = flat ? 0.0f : vmin;
+    // candidates within the FP32 error bound of the maximum, and the PCE energy on the min-shifted map
+    // (integer_search.py:448-452)
+    double e = 0.0;
+    for (int i = tid; i < G.nmap; i += blockDim.x) {
+        float v = map[i];
+        v = v < -1.0f ? 0.0f : v;
+        if (!flat && v >= vmax - NEAR_TIE) {
+            const int slot = atomicAdd(&s_ncand, 1);
+            if (slot < MAX_CAND) s_cand[slot] = i;
         }
+        const double dv = (double)v - (double)cmin;
+        e += dv * dv;
     }
-    __syncthreads();
-    // template statistics in FP64 (the reference's centred template, integer_search.py:73-88)
+    e = block_sum_d(e, red) / (double)G.nmap;
+    // template: raw FP32 f (staged when SMEM), FP64 mean and sum of squares (integer_search.py:73-88)
     const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    const float* fg = a.f + (z0 - G.hz) * sxy + (y0 - G.hy) * G.nx + (x0 - G.hx);
+    const int64_t tsz = SMEM ? (int64_t)G.sy * G.sx : sxy, tsy = SMEM ? G.sx : G.nx;
+    const float* tp = SMEM ? psm : fg;
     double sf = 0.0;
-    for (int i = tid; i < G.n_tpl; i += blockDim.x) {
-        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
-        sf += (double)__ldg(a.f + (z0 - G.hz + k) * sxy + (y0 - G.hy + j) * G.nx + (x0 - G.hx + ii));
+    for (int r = warp; r < G.sz * G.sy; r += NW) {
+        const int k = r / G.sy, j = r - k * G.sy;
+        for (int ii = lane; ii < G.sx; ii += 32) {
+            const float v = __ldg(fg + k * sxy + (int64_t)j * G.nx + ii);
+            if (SMEM) psm[(k * G.sy + j) * G.sx + ii] = v;
+            sf += (double)v;
+        }
     }
     sf = block_sum_d(sf, red);
     const double mf = sf / (double)G.n_tpl;
     double q = 0.0;
-    for (int i = tid; i < G.n_tpl; i += blockDim.x) {
-        const int k = i / (G.sx * G.sy), r = i - k * G.sx * G.sy, j = r / G.sx, ii = r - j * G.sx;
-        const double d = (double)__ldg(a.f + (z0 - G.hz + k) * sxy + (y0 - G.hy + j) * G.nx + (x0 - G.hx + ii)) - mf;
-        q += d * d;
+    for (int r = warp; r < G.sz * G.sy; r += NW) {
+        const int k = r / G.sy, j = r - k * G.sy;
+        for (int ii = lane; ii < G.sx; ii += 32) {
+            const double d = (double)tp[k * tsz + j * tsy + ii] - mf;
+            q += d * d;
+        }
     }
     const double ssf = block_sum_d(q, red);
     int pk = s_pk;
     double peak = (double)vmax;
+    const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
     if (!flat) {
-        // FP64 re-score of the candidates; first maximum in C order wins (np.argmax)
+        // FP64 re-score of the candidates in C order; the first maximum wins (np.argmax)
         const int nc = min(s_ncand, MAX_CAND);
-        if (tid == 0) {  // order the candidates (C order)
+        if (tid == 0) {
             for (int i = 1; i < nc; ++i) {
                 const int v = s_cand[i];
                 int j = i - 1;
@@ -369,18 +399,22 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
             }
         }
         __syncthreads();
-        double bv = -3.0;
-        int bi = pk;
-        for (int c = 0; c < nc; ++c) {
+        for (int c = warp; c < nc; c += NW) {
             const int i = s_cand[c];
             const int dz = i / (G.vy * G.vx), r = i - dz * G.vy * G.vx, dy = r / G.vx, dx = r - dy * G.vx;
-            const double v = rescore(a, node, nullptr, mf, ssf, dz, dy, dx, red);
-            if (v > bv) {
-                bv = v;
-                bi = i;
-            }
+            const float* wp = a.g + (wz0 + dz) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
+            const double v = warp_rescore(tp, tsz, tsy, wp, sxy, G.nx, G, mf, ssf);
+            if (lane == 0) s_cval[c] = v;
         }
+        __syncthreads();
         if (nc > 0) {
+            double bv = -3.0;
+            int bi = pk;
+            for (int c = 0; c < nc; ++c)
+                if (s_cval[c] > bv) {
+                    bv = s_cval[c];
+                    bi = s_cand[c];
+                }
             pk = bi;
             peak = bv;
         }
@@ -389,26 +423,32 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
         pk = 0;
     }
     const int pz = pk / (G.vy * G.vx), pr = pk - pz * G.vy * G.vx, py = pr / G.vx, px = pr - py * G.vx;
-    // PCE on the min-shifted FP32 map (integer_search.py:448-452)
-    double e = 0.0;
-    const float cmin = flat ? 0.0f : vmin;
-    for (int i = tid; i < G.nmap; i += blockDim.x) {
-        float v = map[i];
-        v = v < -1.0f ? 0.0f : v;
-        const double dv = (double)v - (double)cmin;
-        e += dv * dv;
-    }
-    e = block_sum_d(e, red) / (double)G.nmap;
     // sub-voxel refinement on FP64 neighbours (integer_search.py:467-473, 297-321)
     const bool at_border = px == 0 || px == 2 * G.rx || py == 0 || py == 2 * G.ry || pz == 0 || pz == 2 * G.rz;
     const bool interior = !at_border && G.rx > 0 && G.ry > 0 && G.rz > 0 && !flat;
     double sub[3] = {0.0, 0.0, 0.0};
     if (interior) {
-        for (int t = 0; t < 27; ++t) {
-            const int dzz = t / 9 - 1, dyy = (t / 3) % 3 - 1, dxx = t % 3 - 1;
-            const double v = (dzz == 0 && dyy == 0 && dxx == 0) ? peak
-                                                                : rescore(a, node, nullptr, mf, ssf, pz + dzz, py + dyy, px + dxx, red);
-            if (tid == 0) s_neigh[t] = v;
+        const int BX = G.sx + 2, BY = G.sy + 2, BZ = G.sz + 2;
+        const float* gb = a.g + (wz0 + pz - 1) * sxy + (wy0 + py - 1) * G.nx + (wx0 + px - 1);
+        float* box = psm + G.n_tpl;
+        if (SMEM) {
+            for (int r = warp; r < BZ * BY; r += NW) {
+                const int k = r / BY, j = r - k * BY;
+                for (int ii = lane; ii < BX; ii += 32) box[(k * BY + j) * BX + ii] = __ldg(gb + k * sxy + (int64_t)j * G.nx + ii);
+            }
+            __syncthreads();
+        }
+        for (int t = warp; t < 27; t += NW) {
+            const int dzz = t / 9, dyy = (t / 3) % 3, dxx = t % 3;  // box coordinates of the neighbour's origin
+            double v;
+            if (t == 13) {
+                v = peak;
+            } else if (SMEM) {
+                v = warp_rescore(tp, tsz, tsy, box + (dzz * BY + dyy) * BX + dxx, (int64_t)BY * BX, BX, G, mf, ssf);
+            } else {
+                v = warp_rescore(tp, tsz, tsy, gb + dzz * sxy + (int64_t)dyy * G.nx + dxx, sxy, G.nx, G, mf, ssf);
+            }
+            if (lane == 0) s_neigh[t] = v;
         }
         __syncthreads();
         if (tid == 0) {
@@ -447,15 +487,47 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_peak_kernel(SearchArgs a) {
         a.pce[node] = pce;
         a.clipped[node] = on_edge ? 1 : 0;
         if (okv) {
-            a.disp[3 * node + 0] = (double)(a.wx0[node] + px + G.hx - x0) + sub[0];
-            a.disp[3 * node + 1] = (double)(a.wy0[node] + py + G.hy - y0) + sub[1];
-            a.disp[3 * node + 2] = (double)(a.wz0[node] + pz + G.hz - z0) + sub[2];
+            a.disp[3 * node + 0] = (double)(wx0 + px + G.hx - x0) + sub[0];
+            a.disp[3 * node + 1] = (double)(wy0 + py + G.hy - y0) + sub[1];
+            a.disp[3 * node + 2] = (double)(wz0 + pz + G.hz - z0) + sub[2];
         } else {
             for (int c = 0; c < 3; ++c) a.disp[3 * node + c] = nan("");
         }
     }
 }
 
+// shared bytes of the staged peak kernel (template + neighbour box), 0 when it does not fit
+static size_t peak_smem(const NccGeom& G) {
+    const size_t b = ((size_t)G.n_tpl + (size_t)(G.sx + 2) * (G.sy + 2) * (G.sz + 2)) * sizeof(float);
+    return b <= 160 * 1024 ? b : 0;
+}
+
+static int launch_peak(const SearchArgs& b, int64_t n, cudaStream_t s) {
+    const size_t sm = peak_smem(b.G);
+    if (sm > 48 * 1024) {
+        static size_t have = 0;
+        static std::mutex mu;
+        std::lock_guard<std::mutex> lock(mu);
+        if (sm > have) {
+            cudaError_t e = cudaFuncSetAttribute(ncc_peak_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return cuda_fail(e, "ncc peak: shared memory attribute");
+            have = sm;
+        }
+    }
+    for (int64_t done = 0; done < n; done += 65535) {
+        SearchArgs bb = b;
+        bb.node_base = b.node_base + done;
+        bb.map = b.map + done * b.G.nmap;
+        const unsigned nb = (unsigned)std::min<int64_t>(65535, n - done);
+        if (sm)
+            ncc_peak_kernel<true><<<nb, NCC_THREADS, sm, s>>>(bb);
+        else
+            ncc_peak_kernel<false><<<nb, NCC_THREADS, 0, s>>>(bb);
+        const int rc = check_launch("ncc peak");
+        if (rc) return rc;
+    }
+    return ALDVC_OK;
+}
 
 // ----------------------------------------------------------------------------- tiled engine
 // Window box sums for every template placement: separable FP32 sums of (g - c) and (g - c)^2, each
@@ -893,6 +965,449 @@ static int launch_tiled(const TiledArgs& a, const TiledCfg& c, int64_t n, cudaSt
     }
 }
 
+// ----------------------------------------------------------------------------- FFT engine
+// Cross term by FFT (integer_search.py:423-443 computes it with rfftn/irfftn): C = IFFT(FFT(W) conj(FFT(T))),
+// valid offsets only, with transform lengths N >= window extent (2,3,5-smooth), so no offset wraps.
+// The window W (minus the same pilot voxel as the box sums) and the centred template T are packed into one
+// complex volume Z = W + iT, whose spectrum gives both: W^[k] = (Z^[k] + conj Z^[-k]) / 2 and
+// T^[k] = (Z^[k] - conj Z^[-k]) / 2i.  Three passes per batch of nodes, each a CTA-wide Stockham FFT in
+// shared memory (radix 2/3/4/5 stages, twiddles from a device table):
+//   1. per window z-plane: FFT along x (rows < wy), then along y; plane spectrum to scratch A.
+//   2. per (ky, -ky) row pair: FFT along z, the product W^ conj T^, inverse FFT along z; planes dz < vz to P.
+//   3. per dz plane: inverse FFT along y, then along x (rows < vy); real part / (Nx Ny Nz) is the cross term,
+//      normalised with the box-sum volumes as in the tiled engine.
+constexpr int FFT_MAX_N = 128;
+constexpr int FFT_THREADS = 256;
+
+struct FftAxis {
+    int n, stages;
+    int radix[8];
+};
+
+struct FftArgs {
+    const float* g;
+    const int64_t* coords;
+    const int64_t* wx0;
+    const int64_t* wy0;
+    const int64_t* wz0;
+    const uint8_t* t_ok;
+    const float* B1;
+    const float* B2;
+    const float* T;     // centred templates of the chunk, [node][sz][sy][sxp]
+    const double* ssf;  // their sums of squares
+    const float* pilot_at;
+    const float2* tw;   // twiddle tables: x at 0, y at FFT_MAX_N, z at 2 FFT_MAX_N
+    float2* A;          // [nb][wz][Ny][Nx]
+    float2* P;          // [nb][vz][Ny][Nx]
+    float* out;         // maps of the batch
+    int64_t node_base;  // first node of the batch
+    int64_t n_nodes;
+    int nb;
+    NccGeom G;
+    int sxp;
+    FftAxis ax, ay, az;
+    int pitch;          // shared row pitch in float2 (odd)
+};
+
+__host__ inline bool fft_axis(int n, FftAxis& a) {
+    a.n = n;
+    a.stages = 0;
+    int m = n;
+    while (m % 4 == 0) { a.radix[a.stages++] = 4; m /= 4; }
+    while (m % 2 == 0) { a.radix[a.stages++] = 2; m /= 2; }
+    while (m % 3 == 0) { a.radix[a.stages++] = 3; m /= 3; }
+    while (m % 5 == 0) { a.radix[a.stages++] = 5; m /= 5; }
+    return m == 1 && a.stages <= 8 && n <= FFT_MAX_N;
+}
+
+__host__ inline int smooth_len(int n) {
+    for (int m = n;; ++m) {
+        int k = m;
+        while (k % 2 == 0) k /= 2;
+        while (k % 3 == 0) k /= 3;
+        while (k % 5 == 0) k /= 5;
+        if (k == 1) return m;
+    }
+}
+
+__global__ void fft_twiddle_kernel(float2* tw, int nx, int ny, int nz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * FFT_MAX_N) return;
+    const int axis = i / FFT_MAX_N, k = i % FFT_MAX_N;
+    const int n = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    double s = 0.0, c = 1.0;
+    if (k < n) sincospi(-2.0 * (double)k / (double)n, &s, &c);
+    tw[i] = make_float2((float)c, (float)s);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by sgn * i
+__device__ __forceinline__ float2 cmuli(float2 a, float sgn) { return make_float2(-sgn * a.y, sgn * a.x); }
+
+// In-register R-point DFT, exponent sign sgn (-1 forward, +1 inverse).
+template <int R>
+__device__ __forceinline__ void small_dft(float2* v, float sgn) {
+    if (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if (R == 4) {
+        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]), s13 = cadd(v[1], v[3]), d13 = cmuli(csub(v[1], v[3]), sgn);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cadd(d02, d13);
+        v[3] = csub(d02, d13);
+    } else if (R == 3) {
+        const float c1 = -0.5f, s1 = 0.86602540378443864676f;  // cos, sin of 2 pi / 3
+        const float2 a = v[0], b = v[1], c = v[2];
+        const float2 t = cadd(b, c), u = cmuli(csub(b, c), sgn * s1);
+        v[0] = cadd(a, t);
+        const float2 m = make_float2(a.x + c1 * t.x, a.y + c1 * t.y);
+        v[1] = cadd(m, u);
+        v[2] = csub(m, u);
+    } else {  // R == 5
+        const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;  // cos 2pi/5, cos 4pi/5
+        const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;   // sin 2pi/5, sin 4pi/5
+        const float2 a = v[0];
+        const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const float2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+        v[0] = cadd(a, cadd(t1, t2));
+        const float2 m1 = make_float2(a.x + c1 * t1.x + c2 * t2.x, a.y + c1 * t1.y + c2 * t2.y);
+        const float2 m2 = make_float2(a.x + c2 * t1.x + c1 * t2.x, a.y + c2 * t1.y + c1 * t2.y);
+        // sgn i (s1 d1 + s2 d2) and sgn i (s2 d1 - s1 d2)
+        const float2 n1 = cmuli(make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y), sgn);
+        const float2 n2 = cmuli(make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y), sgn);
+        v[1] = cadd(m1, n1);
+        v[4] = csub(m1, n1);
+        v[2] = cadd(m2, n2);
+        v[3] = csub(m2, n2);
+    }
+}
+
+// One radix-R Stockham stage over `rows` transforms.  Butterfly b of this thread walks (row fastest, then j)
+// with incremental indices, so the loop holds no integer division; j / ns uses a multiply-high by the
+// precomputed reciprocal (exact for j, ns < 2^16).  Rows q >= split sit split_stride further (rows <= 2 split).
+template <int R>
+__device__ __forceinline__ void stockham_stage(const float2* __restrict__ d0, float2* __restrict__ d1, const float2* tw, int n,
+                                               int ns, int rows, int split, int split_stride, int row_stride, int es, float sgn) {
+    const int m = n / R;
+    const int total = rows * m;
+    const int tstep = n / (ns * R);
+    // ceil(2^32 / ns) for ns >= 2 (ns == 1 is handled apart: its reciprocal does not fit 32 bits)
+    const unsigned mag = ns > 1 ? (unsigned)((0x100000000ull + (unsigned long long)ns - 1) / (unsigned long long)ns) : 0u;
+    const int nt = blockDim.x, drow = nt % rows, dj = nt / rows;
+    int row = threadIdx.x % rows, j = threadIdx.x / rows;
+    for (int b = threadIdx.x; b < total; b += nt) {
+        const int base = row < split ? row * row_stride : split_stride + (row - split) * row_stride;
+        const int q = ns > 1 ? (int)__umulhi((unsigned)j, mag) : j;
+        const int k = j - q * ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float2 x = d0[base + (j + r * m) * es];
+            if (r > 0 && k > 0) {
+                float2 w = tw[r * k * tstep];  // r k tstep < n
+                w.y *= -sgn;                   // the table holds exp(-2 pi i k / n); sgn = +1 conjugates it
+                x = cmul(x, w);
+            }
+            v[r] = x;
+        }
+        small_dft<R>(v, sgn);
+        const int od = q * ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d1[base + (od + r * ns) * es] = v[r];
+        row += drow;
+        j += dj;
+        if (row >= rows) {
+            row -= rows;
+            ++j;
+        }
+    }
+}
+
+// `rows` independent transforms along one axis; row q starts at q * row_stride, or at
+// split_stride + (q - split) * row_stride for q >= split (rows <= 2 split), its elements es apart.
+// Ping-pongs between a and b; returns the buffer holding the result.
+__device__ float2* fft_rows(float2* a, float2* b, const float2* tw, const FftAxis& ax, int rows, int split, int split_stride,
+                            int row_stride, int es, float sgn) {
+    int ns = 1;
+    for (int s = 0; s < ax.stages; ++s) {
+        const int R = ax.radix[s];
+        if (R == 4)
+            stockham_stage<4>(a, b, tw, ax.n, ns, rows, split, split_stride, row_stride, es, sgn);
+        else if (R == 2)
+            stockham_stage<2>(a, b, tw, ax.n, ns, rows, split, split_stride, row_stride, es, sgn);
+        else if (R == 3)
+            stockham_stage<3>(a, b, tw, ax.n, ns, rows, split, split_stride, row_stride, es, sgn);
+        else
+            stockham_stage<5>(a, b, tw, ax.n, ns, rows, split, split_stride, row_stride, es, sgn);
+        __syncthreads();
+        float2* t = a;
+        a = b;
+        b = t;
+        ns *= R;
+    }
+    return a;
+}
+
+// Row-by-column sweep of an (nrows x ncols <= 128) tile, one warp per row: RB rows of loads are issued before
+// any of their stores, so each thread keeps up to 4 RB global loads in flight.
+template <int RB, typename T, typename Ld, typename St>
+__device__ __forceinline__ void copy_rows(int nrows, int ncols, Ld ld, St st) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r0 = (threadIdx.x >> 5) * RB; r0 < nrows; r0 += nw * RB) {
+        T v[RB][4];
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int r = r0 + u, c = lane + 32 * h;
+                if (r < nrows && c < ncols) v[u][h] = ld(r, c);
+            }
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int r = r0 + u, c = lane + 32 * h;
+                if (r < nrows && c < ncols) st(r, c, v[u][h]);
+            }
+    }
+}
+
+__device__ __forceinline__ bool fft_node_ok(const FftArgs& a, int64_t node) {
+    const NccGeom& G = a.G;
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    const int64_t wx0 = a.wx0[node], wy0 = a.wy0[node], wz0 = a.wz0[node];
+    const bool placed = x0 - G.hx >= 0 && x0 + G.hx < G.nx && y0 - G.hy >= 0 && y0 + G.hy < G.ny && z0 - G.hz >= 0 &&
+                        z0 + G.hz < G.nz && wx0 >= 0 && wx0 + G.wx <= G.nx && wy0 >= 0 && wy0 + G.wy <= G.ny && wz0 >= 0 &&
+                        wz0 + G.wz <= G.nz;
+    return placed && a.t_ok[node] && !(a.ssf[node - a.node_base] < 1e-20);
+}
+
+// Pass 1: grid (wz, nb).  Shared: two planes Ny x pitch float2 and the x/y twiddles.
+__global__ void __launch_bounds__(FFT_THREADS, 4) fft_pass1_kernel(FftArgs a) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const NccGeom& G = a.G;
+    const int z = blockIdx.x;
+    const int64_t node = a.node_base + blockIdx.y;
+    if (!fft_node_ok(a, node)) return;
+    const int Nx = a.ax.n, Ny = a.ay.n, pitch = a.pitch;
+    float2* b0 = fsm;
+    float2* b1 = fsm + Ny * pitch;
+    float2* twx = b1 + Ny * pitch;
+    float2* twy = twx + FFT_MAX_N;
+    for (int i = threadIdx.x; i < 2 * FFT_MAX_N; i += blockDim.x) twx[i] = a.tw[i];
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    const float pilot = __ldg(a.pilot_at);
+    const float* src = a.g + (a.wz0[node] + z) * sxy + a.wy0[node] * G.nx + a.wx0[node];
+    const float* tsrc = a.T + (int64_t)blockIdx.y * G.sz * G.sy * a.sxp + (int64_t)z * G.sy * a.sxp;
+    const bool tpl_plane = z < G.sz;
+    copy_rows<4, float2>(
+        Ny, Nx,
+        [&](int y, int x) {
+            float2 v = make_float2(0.0f, 0.0f);
+            if (y < G.wy && x < G.wx) v.x = __ldg(src + (int64_t)y * G.nx + x) - pilot;
+            if (tpl_plane && y < G.sy && x < G.sx) v.y = __ldg(tsrc + y * a.sxp + x);
+            return v;
+        },
+        [&](int y, int x, float2 v) {
+            b0[y * pitch + x] = v;
+            b1[y * pitch + x] = make_float2(0.0f, 0.0f);
+        });
+    __syncthreads();
+    float2* r = fft_rows(b0, b1, twx, a.ax, G.wy, G.wy, 0, pitch, 1, -1.0f);  // along x, rows y < wy
+    float2* o = r == b0 ? b1 : b0;
+    r = fft_rows(r, o, twy, a.ay, Nx, Nx, 0, 1, pitch, -1.0f);  // along y, every column
+    float2* dst = a.A + ((int64_t)blockIdx.y * G.wz + z) * Ny * Nx;
+    copy_rows<1, float2>(Ny, Nx, [&](int y, int x) { return r[y * pitch + x]; }, [&](int y, int x, float2 v) { dst[y * Nx + x] = v; });
+}
+
+// Pass 2: grid (2 (Ny / 2 + 1), nb).  Block (p, h) takes row ky = p and its mirror (Ny - ky) mod Ny.  A row that
+// is its own mirror (ky = 0, Ny / 2) is done whole by h = 0.  Otherwise h takes the columns
+// kx in [h cb, (h + 1) cb) of row ky and the mirrored columns (Nx - kx) mod Nx of the mirror row, stored at the
+// same local index, so Z^[-k] of a column sits in the other row at the same index.
+__global__ void __launch_bounds__(FFT_THREADS, 4) fft_pass2_kernel(FftArgs a) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    if (!fft_node_ok(a, node)) return;
+    const int Nx = a.ax.n, Ny = a.ay.n, Nz = a.az.n;
+    const int ky0 = blockIdx.x >> 1, half = blockIdx.x & 1, ky1 = (Ny - ky0) % Ny;
+    const bool self = ky1 == ky0;
+    if (self && half) return;
+    const int cb = (Nx + 1) / 2;
+    const int c0 = self ? 0 : half * cb;
+    const int ncol = self ? Nx : min(cb, Nx - c0);
+    const int cp = self ? a.pitch : (cb | 1);  // odd column pitch
+    const int nrow = self ? 1 : 2;
+    const int plane = Nz * cp;
+    float2* b0 = fsm;
+    float2* b1 = fsm + nrow * plane;
+    float2* twz = fsm + 2 * max(a.pitch, 2 * (cb | 1)) * Nz;
+    for (int i = threadIdx.x; i < FFT_MAX_N; i += blockDim.x) twz[i] = a.tw[2 * FFT_MAX_N + i];
+    const float2* A = a.A + (int64_t)blockIdx.y * G.wz * Ny * Nx;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    copy_rows<4, float2>(
+        nrow * Nz, ncol,
+        [&](int zr, int c) {
+            const int q = zr >= Nz ? 1 : 0, z = zr - q * Nz;
+            const int kx = q == 0 ? c0 + c : (Nx - c0 - c) % Nx;
+            return z < G.wz ? A[((int64_t)z * Ny + (q == 0 ? ky0 : ky1)) * Nx + kx] : make_float2(0.0f, 0.0f);
+        },
+        [&](int zr, int c, float2 v) {
+            const int q = zr >= Nz ? 1 : 0, z = zr - q * Nz;
+            b0[q * plane + z * cp + c] = v;
+        });
+    __syncthreads();
+    float2* r = fft_rows(b0, b1, twz, a.az, nrow * ncol, ncol, plane, 1, cp, -1.0f);  // along z
+    float2* o = r == b0 ? b1 : b0;
+    // product W^ conj(T^) from Z^[k] and Z^[-k]
+    for (int zr = threadIdx.x >> 5; zr < nrow * Nz; zr += nw)
+        for (int c = lane; c < ncol; c += 32) {
+            const int q = zr >= Nz ? 1 : 0, kz = zr - q * Nz;
+            const int kzm = (Nz - kz) % Nz;
+            const int qm = self ? 0 : 1 - q, cm = self ? (Nx - c) % Nx : c;
+            const float2 za = r[q * plane + kz * cp + c];
+            const float2 zb = r[qm * plane + kzm * cp + cm];
+            const float2 zbc = make_float2(zb.x, -zb.y);
+            const float2 w = make_float2(0.5f * (za.x + zbc.x), 0.5f * (za.y + zbc.y));
+            // T^ = (za - zbc) / 2i = -i (za - zbc) / 2;  conj(T^) = i conj(za - zbc) / 2
+            const float2 d = csub(za, zbc);
+            const float2 tc = make_float2(0.5f * d.y, 0.5f * d.x);  // i * conj(d) / 2 = (d.y + i d.x) / 2
+            o[q * plane + kz * cp + c] = cmul(w, tc);
+        }
+    __syncthreads();
+    float2* r2 = fft_rows(o, r, twz, a.az, nrow * ncol, ncol, plane, 1, cp, 1.0f);  // inverse along z
+    float2* P = a.P + (int64_t)blockIdx.y * G.vz * Ny * Nx;
+    for (int zr = threadIdx.x >> 5; zr < nrow * G.vz; zr += nw) {
+        const int q = zr >= G.vz ? 1 : 0, z = zr - q * G.vz;
+        float2* dst = P + ((int64_t)z * Ny + (q == 0 ? ky0 : ky1)) * Nx;
+        for (int c = lane; c < ncol; c += 32) {
+            const int kx = q == 0 ? c0 + c : (Nx - c0 - c) % Nx;
+            dst[kx] = r2[q * plane + z * cp + c];
+        }
+    }
+}
+
+// Pass 3: grid (vz, nb).  Inverse along y and x, normalisation, the map plane dz.
+__global__ void __launch_bounds__(FFT_THREADS, 4) fft_pass3_kernel(FftArgs a) {
+    extern __shared__ __align__(16) float2 fsm[];
+    const NccGeom& G = a.G;
+    const int dz = blockIdx.x;
+    const int64_t node = a.node_base + blockIdx.y;
+    float* out = a.out + (int64_t)blockIdx.y * G.nmap + (int64_t)dz * G.vy * G.vx;
+    if (!fft_node_ok(a, node)) {
+        for (int i = threadIdx.x; i < G.vy * G.vx; i += blockDim.x) out[i] = -2.0f;
+        return;
+    }
+    const int Nx = a.ax.n, Ny = a.ay.n, Nz = a.az.n, pitch = a.pitch;
+    float2* b0 = fsm;
+    float2* b1 = fsm + Ny * pitch;
+    float2* twx = b1 + Ny * pitch;
+    float2* twy = twx + FFT_MAX_N;
+    for (int i = threadIdx.x; i < 2 * FFT_MAX_N; i += blockDim.x) twx[i] = a.tw[i];
+    const float2* P = a.P + ((int64_t)blockIdx.y * G.vz + dz) * Ny * Nx;
+    copy_rows<4, float2>(Ny, Nx, [&](int y, int x) { return P[y * Nx + x]; }, [&](int y, int x, float2 v) { b0[y * pitch + x] = v; });
+    __syncthreads();
+    float2* r = fft_rows(b0, b1, twy, a.ay, Nx, Nx, 0, 1, pitch, 1.0f);  // inverse along y
+    float2* o = r == b0 ? b1 : b0;
+    r = fft_rows(r, o, twx, a.ax, G.vy, G.vy, 0, pitch, 1, 1.0f);  // inverse along x, rows dy < vy
+    const double scale = 1.0 / ((double)Nx * Ny * Nz);
+    const double ssf = a.ssf[blockIdx.y], n_tpl = (double)G.n_tpl;
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
+    const float* B1 = a.B1 + (wz0 + dz) * sxy + wy0 * G.nx + wx0;
+    const float* B2 = a.B2 + (wz0 + dz) * sxy + wy0 * G.nx + wx0;
+    copy_rows<4, float2>(
+        G.vy, G.vx, [&](int dy, int dx) { return make_float2(__ldg(B1 + (int64_t)dy * G.nx + dx), __ldg(B2 + (int64_t)dy * G.nx + dx)); },
+        [&](int dy, int dx, float2 bs) {
+            const double s1 = (double)bs.x, s2 = (double)bs.y;
+            const double var = s2 - s1 * s1 / n_tpl;
+            float v = 0.0f;
+            if (!(var < 1e-20)) {
+                double qv = (double)r[dy * pitch + dx].x * scale / sqrt(var * ssf);
+                qv = qv > 1.0 ? 1.0 : (qv < -1.0 ? -1.0 : qv);
+                v = (float)qv;
+            }
+            out[dy * G.vx + dx] = v;
+        });
+}
+
+struct FftCfg {
+    FftAxis ax, ay, az;
+    int pitch;
+    size_t smem13, smem2;  // dynamic shared bytes of passes 1/3 and 2
+    int64_t per_node;      // scratch bytes per node (A and P)
+};
+
+static bool fft_config(const NccGeom& G, FftCfg& c) {
+    if (!fft_axis(smooth_len(G.wx), c.ax) || !fft_axis(smooth_len(G.wy), c.ay) || !fft_axis(smooth_len(G.wz), c.az)) return false;
+    c.pitch = c.ax.n | 1;  // odd: rows and columns of a plane fall in distinct bank pairs
+    c.smem13 = ((size_t)2 * c.ay.n * c.pitch + 2 * FFT_MAX_N) * sizeof(float2);
+    // pass 2: two buffers of one whole row (Nz x pitch) or of two half rows (2 x Nz x (cb | 1))
+    c.smem2 = ((size_t)2 * std::max(c.pitch, 2 * (((c.ax.n + 1) / 2) | 1)) * c.az.n + FFT_MAX_N) * sizeof(float2);
+    c.per_node = ((int64_t)G.wz + G.vz) * c.ay.n * c.ax.n * (int64_t)sizeof(float2);
+    const size_t smax = (size_t)max_smem_optin() - 4096;
+    return c.smem13 <= smax && c.smem2 <= smax;
+}
+
+constexpr int64_t FFT_BATCH_BYTES = 96LL << 20;  // scratch of one batch: sized to stay in L2
+
+static int64_t fft_batch(const FftCfg& c, int64_t chunk) {
+    const int64_t b = std::min<int64_t>(chunk, FFT_BATCH_BYTES / std::max<int64_t>(c.per_node, 1));
+    return std::max<int64_t>(1, std::min<int64_t>(b, 65535));  // grid y limit
+}
+
+static int fft_set_smem(size_t s13, size_t s2) {
+    static size_t have13 = 0, have2 = 0;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (s13 > 48 * 1024 && s13 > have13) {
+        cudaError_t e = cudaFuncSetAttribute(fft_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s13);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fft_pass3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s13);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc fft: shared memory attribute");
+        have13 = s13;
+    }
+    if (s2 > 48 * 1024 && s2 > have2) {
+        cudaError_t e = cudaFuncSetAttribute(fft_pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc fft: shared memory attribute");
+        have2 = s2;
+    }
+    return ALDVC_OK;
+}
+
+// Maps of nodes [a.node_base, a.node_base + n) into a.out, in batches through the scratch.
+static int launch_fft(FftArgs a, const FftCfg& c, int64_t n, int64_t batch, cudaStream_t s) {
+    int rc = fft_set_smem(c.smem13, c.smem2);
+    if (rc) return rc;
+    const NccGeom& G = a.G;
+    float* out0 = a.out;
+    const double* ssf0 = a.ssf;
+    const float* T0 = a.T;
+    const int64_t tsz = (int64_t)G.sz * G.sy * a.sxp;
+    const int64_t base0 = a.node_base;
+    for (int64_t done = 0; done < n; done += batch) {
+        const int nb = (int)std::min<int64_t>(batch, n - done);
+        a.node_base = base0 + done;
+        a.out = out0 + done * G.nmap;
+        a.ssf = ssf0 + done;
+        a.T = T0 + done * tsz;
+        a.nb = nb;
+        fft_pass1_kernel<<<dim3(G.wz, nb), FFT_THREADS, c.smem13, s>>>(a);
+        rc = check_launch("ncc fft pass 1");
+        if (rc) return rc;
+        fft_pass2_kernel<<<dim3(2 * (c.ay.n / 2 + 1), nb), FFT_THREADS, c.smem2, s>>>(a);
+        rc = check_launch("ncc fft pass 2");
+        if (rc) return rc;
+        fft_pass3_kernel<<<dim3(G.vz, nb), FFT_THREADS, c.smem13, s>>>(a);
+        rc = check_launch("ncc fft pass 3");
+        if (rc) return rc;
+    }
+    return ALDVC_OK;
+}
+
 static int upload_pinv() {
     static bool done = false;
     if (done) return ALDVC_OK;
@@ -994,8 +1509,25 @@ extern "C" int aldvc_ncc_map(const float* f, const float* g, int64_t nz, int64_t
     return launch_map(m, n_nodes, (cudaStream_t)stream);
 }
 
+static bool use_fft(const NccGeom& G, int32_t engine, FftCfg& c) { return engine == ALDVC_NCC_FFT && fft_config(G, c); }
+
+// TILED, or FFT on a geometry the FFT engine does not take
 static bool use_tiled(const NccGeom& G, int32_t engine, TiledCfg& c) {
-    return engine == ALDVC_NCC_TILED && tiled_config(G, c);
+    FftCfg fc;
+    return (engine == ALDVC_NCC_TILED || (engine == ALDVC_NCC_FFT && !fft_config(G, fc))) && tiled_config(G, c);
+}
+
+static int launch_templates(const TiledArgs& a, int64_t n, cudaStream_t s) {
+    const int64_t tsz = (int64_t)a.G.sz * a.G.sy * a.sxp;
+    for (int64_t done = 0; done < n; done += 65535) {
+        const unsigned nb = (unsigned)std::min<int64_t>(65535, n - done);
+        TiledArgs aa = a;
+        aa.node_base = a.node_base + done;
+        ncc_template_kernel<<<nb, 256, 0, s>>>(aa, const_cast<float*>(a.T) + done * tsz, const_cast<double*>(a.ssf) + done);
+        const int rc = check_launch("ncc template");
+        if (rc) return rc;
+    }
+    return ALDVC_OK;
 }
 
 extern "C" size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t n_nodes, int32_t hx, int32_t hy,
@@ -1005,8 +1537,12 @@ extern "C" size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_
     const int64_t chunk = search_chunk(G, n);
     size_t b = align_up((size_t)n * 32, 256) + align_up((size_t)chunk * G.nmap * sizeof(float), 256);
     TiledCfg c;
-    if (use_tiled(G, engine, c))  // box sums + temporaries, template scratch
+    FftCfg fc;
+    const bool fft = use_fft(G, engine, fc);
+    if (fft || use_tiled(G, engine, c))  // box sums + temporaries, template scratch
         b += 4 * align_up((size_t)nz * ny * nx * sizeof(float), 256) + tiled_tpl_bytes(G, chunk);
+    if (fft)  // twiddles, one batch of spectra
+        b += align_up(3 * FFT_MAX_N * sizeof(float2), 256) + align_up((size_t)fft_batch(fc, chunk) * fc.per_node, 256);
     return b;
 }
 
@@ -1015,7 +1551,8 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
                                 const int64_t* shift0, int32_t engine, void* workspace, size_t workspace_bytes, double* disp,
                                 double* cc, double* pce, uint8_t* clipped, uint8_t* ok, void* stream) {
     ALDVC_REQUIRE(f && g && coords && disp && cc && pce && clipped && ok, "aldvc_ncc_search: null pointer");
-    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN, "aldvc_ncc_search: unknown engine");
+    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN || engine == ALDVC_NCC_FFT,
+                  "aldvc_ncc_search: unknown engine");
     const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
     int rc = check_geom(G);
     if (rc) return rc;
@@ -1056,9 +1593,13 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
     rc = check_launch("ncc place");
     if (rc) return rc;
     TiledCfg tc;
-    const bool tiled = use_tiled(G, engine, tc);
+    FftCfg fc;
+    const bool fft = use_fft(G, engine, fc);
+    const bool tiled = !fft && use_tiled(G, engine, tc);
+    if (fft) tc.sxp = (G.sx + 3) / 4 * 4;
     TiledArgs ta;
-    if (tiled) {
+    FftArgs fa;
+    if (tiled || fft) {
         // window box sums of (g - c) and (g - c)^2 for every placement, c = a voxel of g near the centre
         const size_t vb = align_up((size_t)nz * ny * nx * sizeof(float), 256);
         float* t1 = (float*)box;
@@ -1089,6 +1630,35 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
         float* tpl = (float*)(box + 4 * vb);
         ta.T = tpl;
         ta.ssf = (const double*)((char*)tpl + align_up((size_t)chunk * G.sz * G.sy * tc.sxp * sizeof(float), 256));
+        if (fft) {
+            ta.sxp = tc.sxp;
+            char* fw = box + 4 * vb + tiled_tpl_bytes(G, chunk);
+            float2* tw = (float2*)fw;
+            fft_twiddle_kernel<<<(3 * FFT_MAX_N + 127) / 128, 128, 0, s>>>(tw, fc.ax.n, fc.ay.n, fc.az.n);
+            rc = check_launch("ncc fft twiddles");
+            if (rc) return rc;
+            const int64_t batch = fft_batch(fc, chunk);
+            float2* scr = (float2*)(fw + align_up(3 * FFT_MAX_N * sizeof(float2), 256));
+            fa.g = g;
+            fa.coords = coords;
+            fa.wx0 = a.wx0;
+            fa.wy0 = a.wy0;
+            fa.wz0 = a.wz0;
+            fa.t_ok = a.t_ok;
+            fa.B1 = b1;
+            fa.B2 = b2;
+            fa.pilot_at = pilot_at;
+            fa.tw = tw;
+            fa.A = scr;
+            fa.P = scr + batch * (int64_t)G.wz * fc.ay.n * fc.ax.n;
+            fa.n_nodes = n_nodes;
+            fa.G = G;
+            fa.sxp = tc.sxp;
+            fa.ax = fc.ax;
+            fa.ay = fc.ay;
+            fa.az = fc.az;
+            fa.pitch = fc.pitch;
+        }
         ta.n_nodes = n_nodes;
         ta.G = G;
         ta.dz_slab = tc.dz;
@@ -1099,7 +1669,17 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
     }
     for (int64_t start = 0; start < n_nodes; start += chunk) {
         const int64_t n = std::min(chunk, n_nodes - start);
-        if (tiled) {
+        if (fft) {
+            ta.node_base = start;
+            rc = launch_templates(ta, n, s);
+            if (rc) return rc;
+            FftArgs fb = fa;
+            fb.node_base = start;
+            fb.out = map;
+            fb.T = ta.T;
+            fb.ssf = ta.ssf;
+            rc = launch_fft(fb, fc, n, fft_batch(fc, chunk), s);
+        } else if (tiled) {
             ta.node_base = start;
             ta.out = map;
             rc = launch_tiled(ta, tc, n, s);
@@ -1110,14 +1690,9 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
         if (rc) return rc;
         SearchArgs b = a;
         b.node_base = start;
-        for (int64_t done = 0; done < n; done += 65535) {
-            SearchArgs bb = b;
-            bb.node_base = start + done;
-            bb.map = map + done * G.nmap;
-            ncc_peak_kernel<<<(unsigned)std::min<int64_t>(65535, n - done), NCC_THREADS, 0, s>>>(bb);
-            rc = check_launch("ncc peak");
-            if (rc) return rc;
-        }
+        b.map = map;
+        rc = launch_peak(b, n, s);
+        if (rc) return rc;
     }
     return ALDVC_OK;
 }

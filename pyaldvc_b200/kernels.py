@@ -18,6 +18,7 @@ BATCHED = _lib.BATCHED
 PLAIN = _lib.PLAIN
 NCC_TILED = _lib.NCC_TILED
 NCC_PLAIN = _lib.NCC_PLAIN
+NCC_FFT = _lib.NCC_FFT
 INTERP_MODE_BY_NAME = {"linear": 0, "cubic": 1, "bspline": 2}
 
 
@@ -166,7 +167,7 @@ def ncc_map(f, g, coords, half, radius, wx0, wy0, wz0, t_ok) -> torch.Tensor:
 
 def ncc_search(f, g, coords, half, radius, shift0=None, engine: int = _lib.NCC_TILED) -> dict:
     """Device single-level search; returns dict of tensors disp (N,3), cc, pce, clipped, ok.
-    ``engine``: NCC_TILED (default) or NCC_PLAIN."""
+    ``engine``: NCC_TILED (default), NCC_PLAIN or NCC_FFT."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
     d = coords.device

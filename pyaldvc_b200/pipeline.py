@@ -58,6 +58,7 @@ class PassParams:
     brick_floats: int = 0
     autotune: bool = True
     graph: bool = False
+    ncc_engine: str = "auto"  # auto | tiled | fft | plain
 
 
 @dataclass
@@ -150,6 +151,23 @@ def _rms(a: torch.Tensor) -> torch.Tensor:
     return torch.sqrt(torch.mean(a * a))
 
 
+# integer_search.py:395: the reference's CPU search switches from the direct map to FFTs above this many
+# template-voxel x offset products per node
+FFT_NCC_MIN_OPS = 3e7
+
+
+def _ncc_engine(p: PassParams, half, radius) -> int:
+    """NCC engine of a search: the plain form's map kernel, or by ``p.ncc_engine``; ``auto`` takes the FFT
+    engine for searches of more than ``FFT_NCC_MIN_OPS`` multiply-adds per node, else the tiled direct engine."""
+    if p.variant == K.PLAIN or p.ncc_engine == "plain":
+        return K.NCC_PLAIN
+    if p.ncc_engine in ("tiled", "fft"):
+        return K.NCC_TILED if p.ncc_engine == "tiled" else K.NCC_FFT
+    n_tpl = np.prod([2 * int(h) + 1 for h in half])
+    n_off = np.prod([2 * int(r) + 1 for r in radius])
+    return K.NCC_FFT if n_tpl * n_off > FFT_NCC_MIN_OPS else K.NCC_TILED
+
+
 def _launch_shape(p: PassParams, ndof: int, mode: int, mesh, mask, run) -> tuple[int, int]:
     """(threads, brick_floats) of the batched IC-GN launches: the caller's, else the autotuner's choice for
     this kernel and subset, timed on an evenly spread sample of this pass's nodes."""
@@ -202,7 +220,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     if act.numel() == 0:
         act = torch.arange(mesh.n, device="cuda")
     coords_a = mesh.coords[act].contiguous()
-    engine = K.NCC_PLAIN if p.variant == K.PLAIN else K.NCC_TILED
+    engine = _ncc_engine(p, half0, rad)
     res = K.ncc_search(f, g, coords_a, half0, rad, None, engine)
     disp_a, ok_a, clipped_a = res["disp"], res["ok"] != 0, res["clipped"] != 0
     for _ in range(p.ncc_max_expand if p.ncc_auto_expand else 0):  # integer_search.ncc_search_expanding :486-524
@@ -213,7 +231,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             break
         rad = tuple(2 * r for r in rad)
         idx = torch.nonzero(sel).flatten()
-        sub = K.ncc_search(f, g, coords_a[idx].contiguous(), half0, rad, None, engine)
+        sub = K.ncc_search(f, g, coords_a[idx].contiguous(), half0, rad, None, _ncc_engine(p, half0, rad))
         s_ok = sub["ok"] != 0
         if not bool(s_ok.any().item()):
             break

@@ -143,7 +143,7 @@ def _check_search(res, ref_get, name):
     np.testing.assert_allclose(res["pce"][ok], ref_get("pce")[ok], rtol=1e-3, err_msg=name)
 
 
-@pytest.mark.parametrize("engine", [0, 1], ids=["tiled", "plain"])
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["tiled", "plain", "fft"])
 @pytest.mark.parametrize("name", list(SEARCHES))
 def test_ncc_search_matches_reference(golden, name, engine):
     from pyaldvc_b200.integer_search import ncc_search
@@ -154,7 +154,7 @@ def test_ncc_search_matches_reference(golden, name, engine):
     _check_search(res, lambda k: golden[f"ncc_{name}_{k}"], name)
 
 
-@pytest.mark.parametrize("engine", [0, 1], ids=["tiled", "plain"])
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["tiled", "plain", "fft"])
 def test_ncc_search_expanding_matches_reference(golden, engine):
     from pyaldvc_b200.integer_search import ncc_search_expanding
 
@@ -195,7 +195,7 @@ def config1_pair():
     return f, g, coords
 
 
-@pytest.mark.parametrize("engine", [0, 1], ids=["tiled", "plain"])
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["tiled", "plain", "fft"])
 @pytest.mark.parametrize("radius", [4, 8])
 def test_ncc_search_17cube_template_matches_oracle(oracle_mod, config1_pair, engine, radius):
     """Default template of the pipeline (17^3, min(winsize, 16)) against the FP64 direct map of the oracle."""
@@ -205,3 +205,30 @@ def test_ncc_search_17cube_template_matches_oracle(oracle_mod, config1_pair, eng
     ref = oracle_mod.ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3)
     res = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=engine)
     _check_search(res, lambda k: ref[k], f"17^3 r{radius}")
+
+
+@pytest.fixture(scope="module")
+def bead_pair_100():
+    from pyaldvc_b200 import synthetic as S
+
+    shape = (100, 100, 100)
+    c, pk = S.draw_beads(shape, 0.03, 21)
+    f = S.normalize_volume(S.render_beads(shape, c, pk, 1.5))
+    g = S.normalize_volume(S.render_beads(shape, S.displace_beads(c, S.translation((2.6, -5.3, 7.4))), pk, 1.5))
+    ax = np.arange(20, 81, 12)
+    zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
+    return f, g, np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1).astype(np.int64)
+
+
+@pytest.mark.parametrize("radius", [4, 16, 32])
+def test_ncc_fft_engine_matches_tiled_engine_at_large_radius(bead_pair_100, radius):
+    """The FFT engine against the tiled direct engine at the +-16 search of the 1024^2 x 306 workload, its first
+    expansion (+-32, 81-voxel windows) and a small radius: identical integer peaks, ok/clipped flags and FP64
+    re-scored cc."""
+    from pyaldvc_b200.integer_search import ncc_search
+
+    f, g, coords = bead_pair_100
+    a = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=0)
+    b = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=2)
+    assert a["ok"].sum() > 100
+    _check_search(b, lambda k: a[k], f"fft vs tiled r{radius}")
