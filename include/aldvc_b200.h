@@ -24,6 +24,8 @@
  *   aldvc_pcg_hex8    <- solver/subpb2_solver.py:77 pcg_multi over
  *                        solver/subpb2_solver.py:45 build_global_system (hex8 FEM)
  *   aldvc_nodal_gradient <- solver/global_operators.py:151 nodal_gradient (FEM)
+ *   aldvc_znssd_forward / _backward: no reference counterpart (the residual of numba_kernels.py:705-708
+ *                        with a hand-written gradient)
  *   aldvc_gradients   <- io/volume_ops.py:124 _gradient_stencil7
  *   aldvc_normalize   <- io/volume_ops.py:105 normalize_volume (whole volume)
  *   aldvc_inpaint     <- utils/inpaint.py:35 fill_nan_grid ("spring" model, no cut mesh)
@@ -223,6 +225,24 @@ int aldvc_pcg_hex8_noalloc(const aldvc_hex8_mesh *mesh, double beta, double mu, 
 
 /* F (N,3,3) = (G_j^T u_i) / m_L on the active nodes, NaN elsewhere */
 int aldvc_nodal_gradient(const aldvc_hex8_mesh *mesh, const double *U, double *F, void *stream);
+
+/* ---------------------------------------------------------------- differentiable ZNSSD residual */
+/* Cost C = sum_v r_v^2 of the residual IC-GN minimises (solver/numba_kernels.py:705-708, statistics of the
+ * dynamic valid set :586-598), per subset of (2h+1)^3 voxels around coords[s] [x,y,z] under the 12-parameter
+ * warp P[s] (F row-major, u, v, w), mode 0 linear / 1 Keys cubic / 2 B-spline (g already prefiltered).
+ * vol->mask and the gradient pointers are ignored.  stats (N,7) keeps (n_valid, mf, bf, mg, bg, sum r,
+ * sum r (g - mg)/bg) for the backward.  A subset that leaves f, has a warped voxel outside the sampler's
+ * domain, or has fewer than 27 or half of its voxels valid gets cost NaN and n_valid 0.  The reference has no
+ * ZNSSD autograd; these two entry points back pyaldvc_b200.znssd (a torch.autograd.Function). */
+int aldvc_znssd_forward(const aldvc_volumes *vol, const int64_t *coords, int64_t n, int32_t hx, int32_t hy, int32_t hz,
+                        int32_t mode, const double *P, double *cost, double *stats, void *stream);
+
+/* Backward of aldvc_znssd_forward for incoming gradients grad_cost (N,): grad_P (N,12) (NULL to skip), and
+ * grad_g, the gradient with respect to the deformed volume's voxels, ADDED into (nz,ny,nx) float32 (NULL to
+ * skip).  Interpolation weights are recomputed from P; nothing per voxel is kept from the forward. */
+int aldvc_znssd_backward(const aldvc_volumes *vol, const int64_t *coords, int64_t n, int32_t hx, int32_t hy, int32_t hz,
+                         int32_t mode, const double *P, const double *stats, const double *grad_cost, double *grad_P,
+                         float *grad_g, void *stream);
 
 #ifdef __cplusplus
 }

@@ -987,3 +987,42 @@ void orc_zncc_direct(const float *f, const float *g, int64_t nz, int64_t ny, int
         free(S2);
     }
 }
+
+/* ------------------------------------------------------------------ ZNSSD cost
+ * C = sum_v r_v^2 with the residual of _icgn_12dof_single (numba_kernels.py:705-708),
+ * r = (float(f) - meanf) / bottomf - (g - meang) / bottomg, over the valid set and with the statistics of
+ * _warp_and_sample (:586-598).  FP64; the checker of the differentiable ZNSSD kernels (their forward, and
+ * central differences for their backward).  No mask, no keep bits.  NaN where the warp leaves the
+ * admissible domain or the valid set is too small. */
+void orc_znssd(const float *f, const float *g, int64_t nz, int64_t ny, int64_t nx, const int64_t *coords, int64_t N, int hx,
+               int hy, int hz, int mode, const double *P_all, double *cost) {
+    ctx_t c;
+    make_ctx(&c, f, NULL, NULL, NULL, 0, NULL, g, nz, ny, nx, hx, hy, hz, 1, mode);
+    int64_t S = subset_count(hx, hy, hz, 1);
+#pragma omp parallel
+    {
+        double *gbuf = (double *)malloc((size_t)S * sizeof(double));
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t n = 0; n < N; ++n) {
+            const int64_t x0 = coords[3 * n], y0 = coords[3 * n + 1], z0 = coords[3 * n + 2];
+            int64_t nv;
+            double mf, bf, mg, bg;
+            cost[n] = NAN;
+            if (!warp_and_sample(&c, P_all + 12 * n, x0, y0, z0, gbuf, NULL, 0, &nv, &mf, &bf, &mg, &bg)) continue;
+            const double ibf = 1.0 / bf, ibg = 1.0 / bg;
+            double s = 0.0;
+            int64_t idx = 0;
+            for (int dz = -hz; dz <= hz; ++dz)
+                for (int dy = -hy; dy <= hy; ++dy)
+                    for (int dx = -hx; dx <= hx; ++dx, ++idx) {
+                        const double gv = gbuf[idx];
+                        if (gv != gv) continue;
+                        const double fd = (double)VF(&c.f, z0 + dz, y0 + dy, x0 + dx) - mf;
+                        const double r = fd * ibf - (gv - mg) * ibg;
+                        s += r * r;
+                    }
+            cost[n] = s;
+        }
+        free(gbuf);
+    }
+}

@@ -59,6 +59,7 @@ def lib():
         L.orc_icgn3.argtypes = [_P, _I64, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _I64, _I64, _I64, _I, _P, _P, _P,
                                 _D, _D, _D, _I, _I, _D, _D, _I, _P, _P, _I64, _P, _P, _P, _P]
         L.orc_zncc_direct.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]
+        L.orc_znssd.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _P, _P]
         _lib = L
     return _lib
 
@@ -99,6 +100,17 @@ def _split(n, split_index, split_keep):
 
 
 # --------------------------------------------------------------------------- interpolation / gradients
+def znssd(f, g, coords, P, half, mode):
+    """FP64 ZNSSD cost (N,) of the residual numba_kernels.py:705-708 per subset under warps P (N,12)."""
+    f, g = _f32(f), _f32(g)
+    coords = np.ascontiguousarray(coords, dtype=np.int64)
+    P = np.ascontiguousarray(P, dtype=np.float64).reshape(-1, 12)
+    out = np.empty(coords.shape[0])
+    hx, hy, hz = (int(h) for h in half)
+    lib().orc_znssd(_ptr(f), _ptr(g), *f.shape, _ptr(coords), coords.shape[0], hx, hy, hz, int(mode), _ptr(P), _ptr(out))
+    return out
+
+
 def sample_points(vol, zs, ys, xs, mode):
     """interp_kernels.sample_points (:139-152)."""
     vol = _f32(vol)

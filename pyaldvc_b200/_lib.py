@@ -72,6 +72,8 @@ PROTOTYPES = {
     "aldvc_pcg_hex8_noalloc_max_nodes": (_i64, []),
     "aldvc_pcg_hex8_noalloc": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _d, _i32, _p, _p, _p, _p]),
     "aldvc_nodal_gradient": (_i32, [ctypes.POINTER(Hex8Mesh), _p, _p, _p]),
+    "aldvc_znssd_forward": (_i32, [ctypes.POINTER(Volumes), _p, _i64, _i32, _i32, _i32, _i32, _p, _p, _p, _p]),
+    "aldvc_znssd_backward": (_i32, [ctypes.POINTER(Volumes), _p, _i64, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p]),
     "aldvc_normalize_workspace_size": (_sz, []),
     "aldvc_normalize": (_i32, [_p, _i32, _i64, _d, _p, _p, _p, _sz, _p]),
     "aldvc_render_beads": (_i32, [_p, _i64, _i64, _i64, _p, _p, _i64, _d, _i32, _p]),

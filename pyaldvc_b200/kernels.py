@@ -228,6 +228,41 @@ def nodal_gradient(grid_shape, spacing, elem_active, U, gauss_order=2) -> torch.
     return F
 
 
+# --------------------------------------------------------------------------- differentiable ZNSSD residual
+ZNSSD_STATS = 7
+
+
+def znssd_forward(f, g, coords, P, half, mode) -> tuple[torch.Tensor, torch.Tensor]:
+    """ZNSSD cost (N,) FP64 of every subset under its warp P (N,12) FP64, and the (N,7) statistics the
+    backward needs."""
+    coords = dev(coords, torch.int64)
+    P = dev(P, torch.float64).reshape(-1, 12)
+    n = coords.shape[0]
+    cost = torch.empty(n, dtype=torch.float64, device=P.device)
+    stats = torch.empty((n, ZNSSD_STATS), dtype=torch.float64, device=P.device)
+    vol = volumes_struct(f, None, None, None, None, g)
+    hx, hy, hz = (int(h) for h in half)
+    _lib.check(lib().aldvc_znssd_forward(ctypes.byref(vol), _p(coords), n, hx, hy, hz, int(mode), _p(P), _p(cost), _p(stats),
+                                         stream_handle()), "aldvc_znssd_forward")
+    return cost, stats
+
+
+def znssd_backward(f, g, coords, P, half, mode, stats, grad_cost, need_P=True, need_g=True):
+    """Gradients of sum_s grad_cost[s] C_s with respect to P (N,12) and to the voxels of g (nz,ny,nx) FP32."""
+    coords = dev(coords, torch.int64)
+    P = dev(P, torch.float64).reshape(-1, 12)
+    grad_cost = dev(grad_cost, torch.float64).reshape(-1).contiguous()
+    n = coords.shape[0]
+    gP = torch.empty((n, 12), dtype=torch.float64, device=P.device) if need_P else None
+    gG = torch.zeros_like(g) if need_g else None
+    vol = volumes_struct(f, None, None, None, None, g)
+    hx, hy, hz = (int(h) for h in half)
+    _lib.check(lib().aldvc_znssd_backward(ctypes.byref(vol), _p(coords), n, hx, hy, hz, int(mode), _p(P), _p(stats), _p(grad_cost),
+                                          None if gP is None else _p(gP), None if gG is None else _p(gG), stream_handle()),
+               "aldvc_znssd_backward")
+    return gP, gG
+
+
 # --------------------------------------------------------------------------- volumes and node-grid post-processing
 def normalize(vol: torch.Tensor, pilot: float | None = None) -> torch.Tensor:
     """``(vol - mean) / std`` of a float32 or uint16 CUDA volume as float32 (FP64 statistics)."""
