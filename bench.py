@@ -29,8 +29,10 @@ WORKLOAD = {
     1: "64^3 bead pair, translation, ws20/st8, trilinear, NCC +-4, local IC-GN (125 nodes)",
     2: "128^3 bead pair, 2% z strain + sine, ws24/st6, tricubic, NCC +-8, local IC-GN (4096 nodes)",
     3: "256^3 uint16 bead pair, 5 deg rotation + 1% hydrostatic, sphere ROI r110, ws16x16x24/st8, 3 ADMM (graph)",
+    4: "192^3 bead pair, 10000 random 21^3 subsets, random affine warps, ZNSSD forward + backward (P and g), tricubic",
     5: "1024x1024x306 uint16 confocal-like bead pair, Boussinesq indentation, ws32/st12, NCC +-16, tricubic, 3 ADMM",
 }
+ZNSSD_METRIC = "subsets/s ZNSSD forward+backward (torch.autograd.Function), 1 B200"
 
 
 def parse():
@@ -244,10 +246,105 @@ def _tuned_shapes() -> list:
     return rows
 
 
+def run_znssd(args):
+    """Differentiation workload: ZNSSD cost of 10,000 warped 21^3 subsets of a 192^3 bead pair and its gradient
+    with respect to the 12 warp parameters and the deformed volume, through the torch.autograd.Function.  A step
+    is one forward + backward over all subsets; value = subsets per second.  The CPU baseline is the FP64 oracle
+    forward plus a fourth-order central-difference gradient (48 more forward evaluations) on a 64-subset sample."""
+    import torch
+
+    from oracle import oracle as O
+    from pyaldvc_b200 import kernels as K
+    from pyaldvc_b200 import synthetic as S
+    from pyaldvc_b200.znssd import znssd
+
+    shape, n, h = (192, 192, 192), 10000, 10
+    c, pk = S.draw_beads(shape, 0.02, 4)
+    rng = np.random.default_rng(4)
+    f = S.render_beads(shape, c, pk, 1.5) + rng.normal(0.0, 0.01, shape).astype(np.float32)
+    g = S.render_beads(shape, S.displace_beads(c, S.translation((0.6, -0.9, 1.2))), pk, 1.5) + rng.normal(0.0, 0.01, shape).astype(np.float32)
+    f, g = S.normalize_volume(f), S.normalize_volume(g)
+    coords = rng.integers(h + 6, 192 - h - 6, size=(n, 3)).astype(np.int64)
+    P = np.zeros((n, 12))
+    P[:, :9] = rng.uniform(-0.03, 0.03, size=(n, 9))
+    P[:, 9:] = rng.uniform(-2.0, 2.0, size=(n, 3))
+    fd_, gd_ = torch.from_numpy(f).cuda(), torch.from_numpy(g).cuda()
+    cd, Pd = torch.from_numpy(coords).cuda(), torch.from_numpy(P).cuda()
+    w = torch.ones(n, dtype=torch.float64, device="cuda")
+
+    def step():
+        Pt = Pd.clone().requires_grad_(True)
+        gt = gd_.clone().requires_grad_(True)
+        cost = znssd(Pt, gt, fd_, cd, (h, h, h), "cubic")
+        (cost * w).sum().backward()
+        return cost, Pt.grad, gt.grad
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lib = K.lib()
+    l0 = lib.aldvc_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            cost, gP, gG = step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (lib.aldvc_launch_count() - l0) / args.steps
+    # accuracy on a sample: kernel gradient vs fourth-order central differences (h = 1e-3) of the FP64 oracle
+    sel = np.arange(64)
+    gps = gP.detach().cpu().numpy()[sel]
+    fd4 = np.empty((len(sel), 12))
+    t0 = time.perf_counter()
+    base = O.znssd(f, g, coords[sel], P[sel], (h, h, h), 1)
+    for k in range(12):
+        cs = []
+        for d in (1e-3, -1e-3, 2e-3, -2e-3):
+            Q = P[sel].copy()
+            Q[:, k] += d
+            cs.append(O.znssd(f, g, coords[sel], Q, (h, h, h), 1))
+        fd4[:, k] = (8.0 * (cs[0] - cs[1]) - (cs[2] - cs[3])) / 12e-3
+    cpu_s = time.perf_counter() - t0
+    rel = np.linalg.norm(gps - fd4, axis=1) / np.linalg.norm(fd4, axis=1)
+    cost_ref = base
+    cost_rel = float(np.max(np.abs(cost.detach().cpu().numpy()[sel] - cost_ref) / np.abs(cost_ref)))
+    # algorithmic work: forward samples every voxel twice (64 taps) and backward once with its gradient
+    # (64 taps x 4 accumulations) plus 64 scatter atomics; bytes = the subsets' f reads + 3 x 64 taps
+    S_ = (2 * h + 1) ** 3
+    flops = n * S_ * (2 * 2 * 64 + 2 * 4 * 64)
+    out = {
+        "metric": ZNSSD_METRIC, "value": n / (ms / 1e3), "unit": "subsets/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 interpolation, f64 residual and reductions", "data": "synthetic",
+        "config": {"workload": WORKLOAD[4], "config_index": 4, "subsets": n, "subset": [2 * h + 1] * 3,
+                   "l2": "volumes 28 MB each (inside L2); gradient volume rewritten every step"},
+        "accuracy": {"grad_P_rel_vs_fd4_max": float(rel.max()), "grad_P_rel_vs_fd4_median": float(np.median(rel)),
+                     "cost_rel_vs_fp64_oracle_max": cost_rel, "sample_subsets": len(sel)},
+        "gpu_launches": int(round(launches)),
+        "roofline": {"bound": "fp32", "achieved": flops / (ms / 1e3) / 1e12, "peak": 74.44992, "unit": "TFLOP/s",
+                     "frac": flops / (ms / 1e3) / 1e12 / 74.44992, "traffic": None,
+                     "peak_source": "nominal FP32 CUDA-core rate: 148 SMs x 128 lanes x 2 flop x 1965 MHz",
+                     "work": "interpolation FMAs: forward 2 x 64 taps, backward 64 taps x 4 sums, per voxel"},
+        "cpu_baseline": {"value": len(sel) / cpu_s, "unit": "subsets/s", "cores": O.num_threads(),
+                         "kind": "port", "sample": "64 subsets: FP64 oracle forward + 4th-order central-difference gradient"},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.impl == "reference" and args.config != 4:
         run_reference(args)
+        return
+    if args.config == 4:
+        if int(os.environ.get("RANK", "0")) == 0:
+            if args.impl == "reference":
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no differentiable ZNSSD residual"}))
+            else:
+                run_znssd(args)
         return
     import torch
     import torch.distributed as dist
