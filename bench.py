@@ -28,7 +28,7 @@ METRIC = "nodes/s full AL-DVC pass at <=0.01 vox RMS err; batched vs plain form,
 WORKLOAD = {
     1: "64^3 bead pair, translation, ws20/st8, trilinear, NCC +-4, local IC-GN (125 nodes)",
     2: "128^3 bead pair, 2% z strain + sine, ws24/st6, tricubic, NCC +-8, local IC-GN (4096 nodes)",
-    3: "256^3 uint16 bead pair, 5 deg rotation + 1% hydrostatic, sphere ROI r110, ws16x16x24/st8, 3 ADMM (graph)",
+    3: "256^3 uint16 bead pair, 5 deg rotation + 1% hydrostatic, sphere ROI r110, uneven subsets 16x16x24..32^3/st8, 3 ADMM (graph)",
     4: "192^3 bead pair, 10000 random 21^3 subsets, random affine warps, ZNSSD forward + backward (P and g), tricubic",
     5: "1024x1024x306 uint16 confocal-like bead pair, Boussinesq indentation, ws32/st12, NCC +-16, tricubic, 3 ADMM",
 }
@@ -112,44 +112,58 @@ def node_block(mesh_shape, edge: int):
     return (iz * ny * nx + iy * nx + ix).ravel()
 
 
-def cpu_sample(f, g, coords, p, block, threads: int):
+def cpu_sample(f, g, coords, p, block, threads: int, mask=None):
     """The per-node chain of the pass on the host cores for the nodes ``block`` of ``coords``: NCC search, precompute,
-    12-DOF IC-GN and (with the global step) two 3-DOF passes.  Volumes are cropped to the box the block touches.
-    Returns (seconds, n_nodes, results)."""
+    12-DOF IC-GN and (with the global step) two 3-DOF passes, with the pass's reference mask and per-node subset
+    shapes (the oracle is called once per shape, as the reference calls its kernels).  Volumes are cropped to the
+    box the block touches.  Returns (seconds, n_nodes, results)."""
     from oracle import oracle as orc
 
     orc.set_num_threads(threads)
     c = coords[block]
     half = tuple(int(w) // 2 for w in p.winsize)
+    if p.node_winsize is not None:
+        halves = np.asarray(p.node_winsize(c), dtype=np.int64) // 2
+    else:
+        halves = np.tile(np.asarray(half, dtype=np.int64), (len(c), 1))
     sub0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
     h0 = tuple(int(w) // 2 for w in sub0)
     reach = [max(h + 8, h0_ + r + 2) + 8 for h, h0_, r in zip(half, h0, p.search_radius)]
     lo = np.maximum(c.min(axis=0) - reach, 0)
     hi = np.minimum(c.max(axis=0) + reach + 1, [f.shape[2], f.shape[1], f.shape[0]])
-    fs = np.ascontiguousarray(f[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]])
-    gs = np.ascontiguousarray(g[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]])
+    crop = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+    fs = np.ascontiguousarray(f[crop])
+    gs = np.ascontiguousarray(g[crop])
+    ms = np.ones((1, 1, 1), np.uint8) if mask is None else np.ascontiguousarray(mask[crop])
     cl = (c - lo).astype(np.int64)
     mode = {"linear": 0, "cubic": 1}[p.interp_method]
+    n = cl.shape[0]
+    P = np.zeros((n, 12))
+    st = np.zeros(n, dtype=np.int8)
     t0 = time.perf_counter()
     gx, gy, gz = orc.compute_gradients(fs)
     res = orc.ncc_search(fs, gs, cl, sub0, p.search_radius)
     U0 = np.where(np.isfinite(res["disp"]), res["disp"], 0.0)
-    H, L, mf, bf, nv, valid = orc.precompute_nodes(cl, *half, fs, gx, gy, gz, np.ones((1, 1, 1), np.uint8), p.min_valid_ratio,
-                                                   p.hessian_cond_max, p.subset_stride)
-    P0 = np.zeros((cl.shape[0], 12))
-    P0[:, 9:] = U0
-    P, it, st, zc = orc.icgn_12dof_parallel(cl, P0, *half, fs, gx, gy, gz, np.ones((1, 1, 1), np.uint8), gs, mode, L, mf, bf, valid,
-                                            p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride)
-    U = P[:, 9:]
-    if p.use_global_step:
-        F = P[:, :9].reshape(-1, 3, 3)
-        v = np.zeros_like(U)
-        for _ in range(2, p.admm_max_iter + 1):
-            U, it3, st3, zc3 = orc.icgn_3dof_parallel(cl, U, F, v, *half, fs, gx, gy, gz, np.ones((1, 1, 1), np.uint8), gs, mode, H,
-                                                      mf, bf, valid, p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
-                                                      p.icgn_patience, p.subset_stride)
+    for sh in np.unique(halves, axis=0):
+        sel = np.flatnonzero((halves == sh).all(axis=1))
+        cs = cl[sel]
+        hs = tuple(int(v) for v in sh)
+        H, L, mf, bf, nv, valid = orc.precompute_nodes(cs, *hs, fs, gx, gy, gz, ms, p.min_valid_ratio, p.hessian_cond_max,
+                                                       p.subset_stride)
+        P0 = np.zeros((len(sel), 12))
+        P0[:, 9:] = U0[sel]
+        Ps, it, sts, zc = orc.icgn_12dof_parallel(cs, P0, *hs, fs, gx, gy, gz, ms, gs, mode, L, mf, bf, valid, p.icgn_tol,
+                                                  p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride)
+        P[sel], st[sel] = Ps, sts
+        if p.use_global_step:
+            U, F = Ps[:, 9:], Ps[:, :9].reshape(-1, 3, 3)
+            v = np.zeros_like(U)
+            for _ in range(2, p.admm_max_iter + 1):
+                U, it3, st3, zc3 = orc.icgn_3dof_parallel(cs, U, F, v, *hs, fs, gx, gy, gz, ms, gs, mode, H, mf, bf, valid, p.mu,
+                                                          p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience,
+                                                          p.subset_stride)
     dt = time.perf_counter() - t0
-    return dt, int(cl.shape[0]), {"P": P, "status": st, "U0": U0}
+    return dt, int(n), {"P": P, "status": st, "U0": U0}
 
 
 def run_reference(args):
@@ -164,15 +178,15 @@ def run_reference(args):
     x0, y0, z0 = mesh.build_grid_axes(shape, p.winsize, p.winstepsize)
     coords = np.round(mesh.grid_coords(x0, y0, z0)).astype(np.int64)
     grid_shape = (len(z0), len(y0), len(x0))
-    f, g = _host_volumes(args.config)
+    f, g, mask = _host_volumes(args.config)
     threads = os.cpu_count() or 1
     block = node_block(grid_shape, args.cpu_nodes)
     for _ in range(max(0, args.warmup and 1)):
-        cpu_sample(f, g, coords, p, block[:8], threads)
+        cpu_sample(f, g, coords, p, block[:8], threads, mask)
     times = []
     n = 0
     for _ in range(args.steps):
-        dt, n, _ = cpu_sample(f, g, coords, p, block, threads)
+        dt, n, _ = cpu_sample(f, g, coords, p, block, threads, mask)
         times.append(dt)
     value = n / float(np.mean(times))
     sample = f"{n} nodes ({args.cpu_nodes}^3 block at the grid centre) per step, FP64 oracle, {threads} threads"
@@ -217,20 +231,21 @@ def _normalize_np(v):
 
 
 def _host_volumes(cfg: int):
-    """Normalised host volumes of the configuration (for the CPU arm)."""
+    """Normalised host volumes of the configuration and its reference mask (for the CPU arm)."""
     from pyaldvc_b200 import configs
 
-    if cfg == 5:
+    if cfg in (3, 5):
         import torch
 
         if torch.cuda.is_available():
-            f, g, _, _ = configs.device_pair(cfg)
+            f, g, m, _ = configs.device_pair(cfg)
             from pyaldvc_b200 import kernels as K
 
-            return K.normalize(f).cpu().numpy(), K.normalize(g).cpu().numpy()
-        raise RuntimeError("configuration 5 is rendered on the device")
+            return K.normalize(f).cpu().numpy(), K.normalize(g).cpu().numpy(), None if m is None else m.cpu().numpy()
+        if cfg == 5:
+            raise RuntimeError("configuration 5 is rendered on the device")
     pair = configs.host_pair(cfg)
-    return _normalize_np(pair.f), _normalize_np(pair.g)
+    return _normalize_np(pair.f), _normalize_np(pair.g), pair.mask
 
 
 # --------------------------------------------------------------------------- B200 arm
@@ -416,10 +431,20 @@ def main():
     status = res.status.cpu().numpy()
     valid = res.valid.cpu().numpy()
     gs_ = res.grid_shape
+    # interior = every node of the 3x3x3 neighbourhood valid (the grid border and an ROI's boundary layer excluded)
+    vg = valid.reshape(gs_)
     interior = np.zeros(gs_, dtype=bool)
     interior[1:-1, 1:-1, 1:-1] = True
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                interior[1:-1, 1:-1, 1:-1] &= vg[1 + dz:gs_[0] - 1 + dz, 1 + dy:gs_[1] - 1 + dy, 1 + dx:gs_[2] - 1 + dx]
     sel = interior.ravel() & valid & (status == 0)
     rms_truth = float(np.sqrt(np.mean((U[sel] - truth[sel]) ** 2))) if sel.any() else float("nan")
+    sel_all = valid & (status == 0)
+    rms_truth_all = float(np.sqrt(np.mean((U[sel_all] - truth[sel_all]) ** 2))) if sel_all.any() else float("nan")
+    sel_l = sel_all & (status_local == 0)
+    rms_local_truth = float(np.sqrt(np.mean((U_local[sel_l] - truth[sel_l]) ** 2))) if sel_l.any() else float("nan")
 
     # ---- roofline of the two heaviest stages, algorithmic work per the pass (FP32 CUDA-core bound)
     peaks = _peaks()
@@ -497,7 +522,7 @@ def main():
         fn = K.normalize(f).cpu().numpy()
         gn = K.normalize(g).cpu().numpy()
         block = node_block(res.grid_shape, args.cpu_nodes)
-        dt, nb, cres = cpu_sample(fn, gn, coords, p, block, threads)
+        dt, nb, cres = cpu_sample(fn, gn, coords, p, block, threads, None if mask is None else mask.cpu().numpy())
         cpu = {"value": nb / dt, "unit": "nodes/s", "cores": threads, "kind": "port",
                "sample": f"{nb} nodes ({args.cpu_nodes}^3 block at the grid centre): NCC, precompute, 12-DOF"
                          f"{' and 3-DOF ADMM passes' if p.use_global_step else ''}, FP64 oracle"}
@@ -515,7 +540,8 @@ def main():
                    if f.numel() * f.element_size() > 126e6 else "inputs smaller than L2 (every pass rewrites its buffers)",
                    "parallelism": f"replica x{world}"},
         "stages_ms": {k_: 1e3 * v_ for k_, v_ in stages.items()},
-        "accuracy": {"rms_vs_truth_vox": rms_truth, "nodes_scored": int(sel.sum()), "converged_frac": float(np.mean(status == 0)),
+        "accuracy": {"rms_vs_truth_vox": rms_truth, "nodes_scored": int(sel.sum()), "converged_frac": float(np.mean(status[valid] == 0)),
+                     "rms_vs_truth_all_valid_vox": rms_truth_all, "rms_local_vs_truth_vox": rms_local_truth,
                      "rms_local_vs_fp64_oracle_vox": rms_oracle},
         "gpu_launches": int(round(launches)),
         "roofline": roof.get(dominant),

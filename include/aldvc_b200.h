@@ -77,15 +77,19 @@ typedef struct aldvc_volumes {
     int64_t nz, ny, nx;
 } aldvc_volumes;
 
-/* Subset geometry shared by every node of a call. */
+/* Subset geometry of a call: one shape for every node, or per-node (uneven, anisotropic) shapes. */
 typedef struct aldvc_subset {
-    int32_t hx, hy, hz;          /* half-widths (winsize // 2) */
+    int32_t hx, hy, hz;          /* half-widths (winsize // 2); with node_half, the largest over the nodes */
     int32_t stride;              /* sample every stride-th voxel per axis (>= 1) */
     int32_t mode;                /* 0 trilinear, 1 Keys cubic (a = -0.5), 2 cubic B-spline on prefiltered g */
     int32_t reserved;
     const int64_t *split_index;  /* (N,) row of split_keep per node, -1 = whole subset; NULL: no splitting */
     const uint8_t *split_keep;   /* (rows, keep_bytes) packed keep bits in sampling order */
     int64_t keep_bytes;
+    /* (N,3) int32 [hx, hy, hz] per node, each <= (hx, hy, hz) above; NULL: every node takes (hx, hy, hz).
+     * Not combined with split rows or the noise-corrected Hessian.  The reference calls its kernels once per
+     * subset shape; here one persistent launch takes every shape. */
+    const int32_t *node_half;
 } aldvc_subset;
 
 /* IC-GN controls (pyALDVC core/config.py:76-95 field meanings). */

@@ -33,7 +33,7 @@ class Volumes(ctypes.Structure):
 
 class Subset(ctypes.Structure):
     _fields_ = [("hx", _i32), ("hy", _i32), ("hz", _i32), ("stride", _i32), ("mode", _i32), ("reserved", _i32),
-                ("split_index", _p), ("split_keep", _p), ("keep_bytes", _i64)]
+                ("split_index", _p), ("split_keep", _p), ("keep_bytes", _i64), ("node_half", _p)]
 
 
 class IcgnParams(ctypes.Structure):

@@ -5,7 +5,8 @@
 2. 128^3 float32, same beads; 2 % uniaxial strain along z plus u_x = 0.5 sin(2 pi y / 64); step 6,
    subsets 24^3, NCC +-8, tricubic; local IC-GN only.
 3. 256^3 uint16 (0-4095); 5 degree rotation about z plus 1 % hydrostatic strain; spherical ROI of radius
-   110; step 8, subsets 16x16x24; ADMM with beta 1e-3, 3 iterations, captured as a CUDA graph.
+   110; step 8, uneven anisotropic subsets from 16x16x24 (ROI centre) to 32^3 (ROI edge), one persistent launch
+   for every shape; ADMM with beta 1e-3, 3 iterations, captured as a CUDA graph.
 5. 1024 x 1024 x 306 uint16, 0.005 beads/voxel, sigma 2, Poisson (1000 photons per unit peak) plus
    Gaussian noise; Boussinesq indentation u_z = -10.5 a^2 / (a^2 + r^2 + d^2), a = 80, plus a 0.3 voxel
    random-phase background; step 12, subsets 32^3, NCC +-16, tricubic, 3 ADMM iterations.
@@ -31,8 +32,8 @@ def params(cfg: int, **over) -> PassParams:
         p = PassParams(winsize=(24, 24, 24), winstepsize=(6, 6, 6), search_radius=(8, 8, 8), interp_method="cubic",
                        use_global_step=False)
     elif cfg == 3:
-        p = PassParams(winsize=(16, 16, 24), winstepsize=(8, 8, 8), search_radius=(8, 8, 8), interp_method="cubic",
-                       beta=1e-3, mu=1e-3, admm_max_iter=3, admm_early_stop=False, graph=True)
+        p = PassParams(winsize=(32, 32, 32), winstepsize=(8, 8, 8), search_radius=(8, 8, 8), interp_method="cubic",
+                       beta=1e-3, mu=1e-3, admm_max_iter=3, admm_early_stop=False, graph=True, node_winsize=uneven_winsize)
     elif cfg == 5:
         p = PassParams(winsize=(32, 32, 32), winstepsize=(12, 12, 12), search_radius=(16, 16, 16), interp_method="cubic",
                        beta=1e-3, mu=1e-3, admm_max_iter=3)
@@ -41,6 +42,20 @@ def params(cfg: int, **over) -> PassParams:
     for k, v in over.items():
         setattr(p, k, v)
     return p
+
+
+ROI_RADIUS = 110.0
+
+
+def uneven_winsize(coords) -> np.ndarray:
+    """Per-node window sizes of configuration 3: 16 x 16 x 24 at the centre of the spherical ROI, growing with the
+    distance r from it to 32 x 32 x 32 at r = 110 (even sizes, (x, y, z) order)."""
+    c = np.asarray(coords, dtype=np.float64)
+    centre = (np.asarray(shape_of(3)[::-1], dtype=np.float64) - 1.0) / 2.0
+    t = np.clip(np.linalg.norm(c - centre[None, :], axis=1) / ROI_RADIUS, 0.0, 1.0)
+    wxy = 2 * np.round((16.0 + 16.0 * t) / 2.0)
+    wz = 2 * np.round((24.0 + 8.0 * t) / 2.0)
+    return np.stack([wxy, wxy, wz], 1).astype(np.int64)
 
 
 def shape_of(cfg: int):
@@ -79,22 +94,24 @@ def host_pair(cfg: int, seed: int = 1000) -> syn.VolumePair:
 
 
 def device_pair(cfg: int, seed: int = 1000):
-    """(f, g) CUDA tensors of the configuration (uint16 for 3 and 5, float32 otherwise) and the field."""
+    """(f, g, mask, field): CUDA tensors of the configuration (uint16 for 3 and 5, float32 otherwise)."""
     import torch
 
     from . import kernels as K
 
-    if cfg != 5:
+    if cfg not in (3, 5):
         pair = host_pair(cfg, seed)
         f = torch.from_numpy(np.ascontiguousarray(pair.f)).cuda()
         g = torch.from_numpy(np.ascontiguousarray(pair.g)).cuda()
         m = None if pair.mask is None else torch.from_numpy(pair.mask).cuda()
         return f, g, m, pair.disp
+    # 3: beads 0.02 / voxel, sigma 1.5, Gaussian noise 0.01, spherical ROI; 5: 0.005 / voxel, sigma 2,
+    # Poisson (1000 photons per unit peak) plus Gaussian noise 0.01.  Both scaled to uint16 0-4095.
     shape = shape_of(cfg)
     disp = displacement(cfg)
-    centres, peaks = syn.draw_beads(shape, 0.005, seed + cfg)
+    density, sigma, poisson = (0.02, 1.5, False) if cfg == 3 else (0.005, 2.0, True)
+    centres, peaks = syn.draw_beads(shape, density, seed + cfg)
     moved = syn.displace_beads(centres, disp)
-    sigma = 2.0
     R = int(np.ceil(4.0 * sigma))
     vols = []
     for k, c in enumerate((centres, moved)):
@@ -102,8 +119,11 @@ def device_pair(cfg: int, seed: int = 1000):
         K.render_beads(acc, c, peaks, sigma, R)
         gen = torch.Generator(device="cuda")
         gen.manual_seed(seed + cfg + 1 + k)
-        photons = 1000.0
-        v = torch.poisson(acc.clamp_min(0.0) * photons, generator=gen) / photons
+        if poisson:
+            photons = 1000.0
+            v = torch.poisson(acc.clamp_min(0.0) * photons, generator=gen) / photons
+        else:
+            v = acc.clone()
         del acc
         v = v + 0.01 * torch.randn(shape, dtype=torch.float64, device="cuda", generator=gen)
         vols.append(v)
@@ -113,7 +133,14 @@ def device_pair(cfg: int, seed: int = 1000):
     out = [torch.round((v - lo) * scale).to(torch.int32).to(torch.uint16).contiguous() for v in vols]
     del vols
     torch.cuda.empty_cache()
-    return out[0], out[1], None, disp
+    mask = None
+    if cfg == 3:
+        nz, ny, nx = shape
+        z, y, x = (torch.arange(n, device="cuda", dtype=torch.float64) for n in (nz, ny, nx))
+        r2 = ((x[None, None, :] - (nx - 1) / 2) ** 2 + (y[None, :, None] - (ny - 1) / 2) ** 2
+              + (z[:, None, None] - (nz - 1) / 2) ** 2)
+        mask = (r2 <= ROI_RADIUS**2).to(torch.uint8).contiguous()
+    return out[0], out[1], mask, disp
 
 
 def truth_at(disp, coords) -> np.ndarray:

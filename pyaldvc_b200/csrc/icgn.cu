@@ -69,7 +69,23 @@ struct IcgnArgs {
     int* counter;       // batched work queue
     float* gbuf;        // plain: (blocks, S)
     int brick_cap;      // batched: floats of the shared brick
+    const int32_t* node_half;  // (N,3) per-node half-widths (<= hx, hy, hz), NULL: one shape
 };
+
+// Subset shape of one node: the call's, or the node's own (node_half); ok is false when a node's own shape
+// exceeds the call's maximum (the node is then invalid: buffers and bricks are sized by the maximum).
+struct Shape {
+    int hx, hy, hz, nX, nY, nZ;
+};
+
+__device__ __forceinline__ Shape node_shape(const IcgnArgs& a, int64_t node, bool& ok) {
+    ok = true;
+    if (!a.node_half) return Shape{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ};
+    const int hx = a.node_half[3 * node], hy = a.node_half[3 * node + 1], hz = a.node_half[3 * node + 2];
+    ok = hx >= 0 && hy >= 0 && hz >= 0 && hx <= a.hx && hy <= a.hy && hz <= a.hz;
+    if (!ok) return Shape{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ};
+    return Shape{hx, hy, hz, (2 * hx) / a.stride + 1, (2 * hy) / a.stride + 1, (2 * hz) / a.stride + 1};
+}
 
 // ----------------------------------------------------------------------------- per-node control state
 struct Ctl12 {
@@ -308,7 +324,7 @@ __device__ __noinline__ int control3(Ctl3& s, const double* b_in, double bottomf
 // ----------------------------------------------------------------------------- node set-up / write-back (thread 0)
 // Returns true when the node is to be iterated; otherwise its outputs are already written.
 template <int NDOF>
-__device__ __noinline__ bool node_begin(const IcgnArgs& a, int64_t node, Ctl12& c12, Ctl3& c3) {
+__device__ __noinline__ bool node_begin(const IcgnArgs& a, int64_t node, Ctl12& c12, Ctl3& c3, const Shape& sh, bool shape_ok) {
     if (NDOF == 12) {
         const double* P0 = a.P0 + node * 12;
         double* Po = a.P_out + node * 12;
@@ -322,7 +338,7 @@ __device__ __noinline__ bool node_begin(const IcgnArgs& a, int64_t node, Ctl12& 
         }
         a.n_iter[node] = 0;
         a.zncc[node] = nan("");
-        if (!a.valid[node]) {
+        if (!a.valid[node] || !shape_ok) {
             a.status[node] = ST_INVALID;
             return false;
         }
@@ -337,7 +353,7 @@ __device__ __noinline__ bool node_begin(const IcgnArgs& a, int64_t node, Ctl12& 
         c12.best_dp = 1e300;
         c12.zncc = nan("");
         c12.stall = 0;
-        c12.half_scale = (double)max(a.hx, max(a.hy, a.hz));
+        c12.half_scale = (double)max(sh.hx, max(sh.hy, sh.hz));
         return true;
     } else {
         double* Uo = a.P_out + node * 3;
@@ -356,7 +372,7 @@ __device__ __noinline__ bool node_begin(const IcgnArgs& a, int64_t node, Ctl12& 
         }
         a.n_iter[node] = 0;
         a.zncc[node] = nan("");
-        if (!a.valid[node]) {
+        if (!a.valid[node] || !shape_ok) {
             a.status[node] = ST_INVALID;
             return false;
         }
@@ -404,13 +420,14 @@ struct Box {
     bool corners_in;
 };
 
-__device__ __noinline__ Box warp_box(const IcgnArgs& a, const double* P, int64_t xc, int64_t yc, int64_t zc, int zc0, int zc1, int mode) {
+__device__ __noinline__ Box warp_box(const IcgnArgs& a, const Shape& sh, const double* P, int64_t xc, int64_t yc, int64_t zc, int zc0,
+                                     int zc1, int mode) {
     const double a00 = 1.0 + P[0], a01 = P[1], a02 = P[2], a10 = P[3], a11 = 1.0 + P[4], a12 = P[5], a20 = P[6], a21 = P[7],
                  a22 = 1.0 + P[8];
     const double tx = (double)xc + P[9], ty = (double)yc + P[10], tz = (double)zc + P[11];
-    const double Xs[2] = {(double)-a.hx, (double)(-a.hx + (a.nX - 1) * a.stride)};
-    const double Ys[2] = {(double)-a.hy, (double)(-a.hy + (a.nY - 1) * a.stride)};
-    const double Zs[2] = {(double)(-a.hz + zc0 * a.stride), (double)(-a.hz + (zc1 - 1) * a.stride)};
+    const double Xs[2] = {(double)-sh.hx, (double)(-sh.hx + (sh.nX - 1) * a.stride)};
+    const double Ys[2] = {(double)-sh.hy, (double)(-sh.hy + (sh.nY - 1) * a.stride)};
+    const double Zs[2] = {(double)(-sh.hz + zc0 * a.stride), (double)(-sh.hz + (zc1 - 1) * a.stride)};
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     bool in = true;
     for (int i = 0; i < 2; ++i)
@@ -620,7 +637,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
             sc.state = 1;
             if (sc.node >= 0) {
                 const int64_t node = sc.node;
-                if (node_begin<NDOF>(a, node, c12, c3)) {
+                if (node_begin<NDOF>(a, node, c12, c3, Shape{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ}, true)) {
                     sc.state = 0;
                     const double* P = NDOF == 12 ? c12.P : c3.P;
                     for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
@@ -654,14 +671,15 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
                 if (tid == 0) {
                     // largest chunk of subset planes whose box fits in the brick
                     int lo = zc0 + 1, hi = a.nZ, best = zc0 + 1;
-                    Box bb = warp_box(a, sc.P, xc, yc, zcn, zc0, hi, MODE);
+                    const Shape sh0{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ};
+                    Box bb = warp_box(a, sh0, sc.P, xc, yc, zcn, zc0, hi, MODE);
                     bool fits = (long long)bb.bx * bb.by * bb.bz <= a.brick_cap;
                     if (fits) {
                         best = hi;
                     } else {
                         while (lo <= hi) {
                             const int mid = (lo + hi) / 2;
-                            Box t = warp_box(a, sc.P, xc, yc, zcn, zc0, mid, MODE);
+                            Box t = warp_box(a, sh0, sc.P, xc, yc, zcn, zc0, mid, MODE);
                             if ((long long)t.bx * t.by * t.bz <= a.brick_cap) {
                                 best = mid;
                                 bb = t;
@@ -670,7 +688,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
                                 hi = mid - 1;
                             }
                         }
-                        bb = warp_box(a, sc.P, xc, yc, zcn, zc0, best, MODE);
+                        bb = warp_box(a, sh0, sc.P, xc, yc, zcn, zc0, best, MODE);
                     }
                     const bool use = (long long)bb.bx * bb.by * bb.bz <= a.brick_cap;
                     sc.use_brick = use ? 1 : 0;
@@ -827,7 +845,7 @@ struct LeanCtl {
     float cf, cg;
 };
 
-template <int MODE, bool STORED, int NDOF, int NW>
+template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN>
 __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a) {
     constexpr int T = NW * 32;
     constexpr int NB = Acc<NDOF>::NB;
@@ -837,10 +855,6 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
     __shared__ int redi[NW][3];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t sxy = (int64_t)a.nx * a.ny;
-    const int nXY = a.nX * a.nY;
-    const int S = nXY * a.nZ;
-    const int sx_ = T % a.nX, sy_ = (T / a.nX) % a.nY, sz_ = T / nXY;  // index step of T voxels
-    const int tix = tid % a.nX, tiy = (tid / a.nX) % a.nY, tiz = tid / nXY;
     const int lo = MODE == 0 ? 0 : 1, hx_ = MODE == 0 ? a.nx - 2 : a.nx - 3, hy_ = MODE == 0 ? a.ny - 2 : a.ny - 3,
               hz_ = MODE == 0 ? a.nz - 2 : a.nz - 3;
     Ctl12 c12;  // live in thread 0 only
@@ -852,7 +866,9 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
             const int q = atomicAdd(a.counter, 1);
             sc.node = q < a.n_nodes ? (int64_t)q : -1;
             sc.state = 1;
-            if (sc.node >= 0 && node_begin<NDOF>(a, sc.node, c12, c3)) {
+            bool shape_ok = true;
+            const Shape sh0 = (UNEVEN && sc.node >= 0) ? node_shape(a, sc.node, shape_ok) : Shape{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ};
+            if (sc.node >= 0 && node_begin<NDOF>(a, sc.node, c12, c3, sh0, shape_ok)) {
                 sc.state = 0;
                 const double* P = NDOF == 12 ? c12.P : c3.P;
                 for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
@@ -864,16 +880,23 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
         const int64_t node = sc.node;
         if (node < 0) break;
         if (sc.state != 0) continue;
+        // one shape per call: the kernel parameters themselves; uneven: the node's (node_begin rejected a bad one)
+        bool shape_ok = true;
+        const Shape sh = UNEVEN ? node_shape(a, node, shape_ok) : Shape{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ};
+        const int nXY = sh.nX * sh.nY;
+        const int S = nXY * sh.nZ;
+        const int sx_ = T % sh.nX, sy_ = (T / sh.nX) % sh.nY, sz_ = T / nXY;  // index step of T voxels
+        const int tix = tid % sh.nX, tiy = (tid / sh.nX) % sh.nY, tiz = tid / nXY;
         const int64_t xc = a.coords[3 * node], yc = a.coords[3 * node + 1], zcn = a.coords[3 * node + 2];
         const int64_t srow = a.split_index ? a.split_index[node] : -1;
         const uint8_t* keep = srow >= 0 ? a.split_keep + srow * a.keep_bytes : nullptr;
-        const bool inside = xc - a.hx >= 0 && xc + a.hx < a.nx && yc - a.hy >= 0 && yc + a.hy < a.ny && zcn - a.hz >= 0 &&
-                            zcn + a.hz < a.nz;
+        const bool inside = xc - sh.hx >= 0 && xc + sh.hx < a.nx && yc - sh.hy >= 0 && yc + sh.hy < a.ny && zcn - sh.hz >= 0 &&
+                            zcn + sh.hz < a.nz;
         const int xci = (int)xc, yci = (int)yc, zci = (int)zcn;
 
         for (int it = 1; it <= a.max_iter; ++it) {
             if (tid == 0) {
-                const Box bb = warp_box(a, sc.P, xc, yc, zcn, 0, a.nZ, MODE);
+                const Box bb = warp_box(a, sh, sc.P, xc, yc, zcn, 0, sh.nZ, MODE);
                 sc.slow = bb.corners_in ? 0 : 1;
                 const double* P = sc.P;
                 sc.A[0] = (float)(1.0 + P[0]);
@@ -899,17 +922,17 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
             acc.zero();
             int ix = tix, iy = tiy, iz = tiz;
             for (int v = tid; v < S; v += T) {
-                const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+                const int dx = -sh.hx + ix * a.stride, dy = -sh.hy + iy * a.stride, dz = -sh.hz + iz * a.stride;
                 const int vx = ix, vy = iy, vz = iz;
                 ix += sx_;
                 iy += sy_;
                 iz += sz_;
-                if (ix >= a.nX) {
-                    ix -= a.nX;
+                if (ix >= sh.nX) {
+                    ix -= sh.nX;
                     ++iy;
                 }
-                if (iy >= a.nY) {
-                    iy -= a.nY;
+                if (iy >= sh.nY) {
+                    iy -= sh.nY;
                     ++iz;
                 }
                 const int xx = xci + dx, yy = yci + dy, zz = zci + dz;
@@ -917,7 +940,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
                 if (keep || !inside) {
                     k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
                     if (k)
-                        k = keep ? kept_bit(keep, (vz * a.nY + vy) * a.nX + vx)
+                        k = keep ? kept_bit(keep, (vz * sh.nY + vy) * sh.nX + vx)
                                  : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0);
                 } else {
                     k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0;
@@ -1061,13 +1084,15 @@ __global__ void __launch_bounds__(256) icgn_plain_kernel(IcgnArgs a) {
     const int64_t node = a.node_base + blockIdx.x;
     if (node >= a.n_nodes) return;
     const int64_t sxy = (int64_t)a.nx * a.ny;
-    const int nXY = a.nX * a.nY;
-    const int S = nXY * a.nZ;
-    float* gbuf = a.gbuf + (int64_t)blockIdx.x * S;
+    bool shape_ok;
+    const Shape sh = node_shape(a, node, shape_ok);
+    const int nXY = sh.nX * sh.nY;
+    const int S = nXY * sh.nZ;
+    float* gbuf = a.gbuf + (int64_t)blockIdx.x * ((int64_t)a.nX * a.nY * a.nZ);  // rows sized by the largest shape
     Ctl12 c12;
     Ctl3 c3;
     if (tid == 0) {
-        sc.state = node_begin<NDOF>(a, node, c12, c3) ? 0 : 1;
+        sc.state = node_begin<NDOF>(a, node, c12, c3, sh, shape_ok) ? 0 : 1;
         if (sc.state == 0) {
             const double* P = NDOF == 12 ? c12.P : c3.P;
             for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
@@ -1081,13 +1106,13 @@ __global__ void __launch_bounds__(256) icgn_plain_kernel(IcgnArgs a) {
     const int64_t xc = a.coords[3 * node], yc = a.coords[3 * node + 1], zcn = a.coords[3 * node + 2];
     const int64_t srow = a.split_index ? a.split_index[node] : -1;
     const uint8_t* keep = srow >= 0 ? a.split_keep + srow * a.keep_bytes : nullptr;
-    const bool inside = xc - a.hx >= 0 && xc + a.hx < a.nx && yc - a.hy >= 0 && yc + a.hy < a.ny && zcn - a.hz >= 0 &&
-                        zcn + a.hz < a.nz;
+    const bool inside = xc - sh.hx >= 0 && xc + sh.hx < a.nx && yc - sh.hy >= 0 && yc + sh.hy < a.ny && zcn - sh.hz >= 0 &&
+                        zcn + sh.hz < a.nz;
     __syncthreads();
 
     for (int it = 1; it <= a.max_iter; ++it) {
         if (tid == 0) {
-            const Box bb = warp_box(a, sc.P, xc, yc, zcn, 0, a.nZ, MODE);
+            const Box bb = warp_box(a, sh, sc.P, xc, yc, zcn, 0, sh.nZ, MODE);
             sc.slow = bb.corners_in ? 0 : 1;
             const double* P = sc.P;
             sc.A[0] = (float)(1.0 + P[0]);
@@ -1111,8 +1136,8 @@ __global__ void __launch_bounds__(256) icgn_plain_kernel(IcgnArgs a) {
         const float cf = sc.cf;
         for (int v = tid; v < S; v += THREADS) {
             const int iz = v / nXY, rem = v - iz * nXY;
-            const int iy = rem / a.nX, ix = rem - iy * a.nX;
-            const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+            const int iy = rem / sh.nX, ix = rem - iy * sh.nX;
+            const int dx = -sh.hx + ix * a.stride, dy = -sh.hy + iy * a.stride, dz = -sh.hz + iz * a.stride;
             const int64_t xx = xc + dx, yy = yc + dy, zz = zcn + dz;
             bool k;
             if (keep || !inside) {
@@ -1188,8 +1213,8 @@ __global__ void __launch_bounds__(256) icgn_plain_kernel(IcgnArgs a) {
             const float gv = gbuf[v];
             if (gv != gv) continue;
             const int iz = v / nXY, rem = v - iz * nXY;
-            const int iy = rem / a.nX, ix = rem - iy * a.nX;
-            const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+            const int iy = rem / sh.nX, ix = rem - iy * sh.nX;
+            const int dx = -sh.hx + ix * a.stride, dy = -sh.hy + iy * a.stride, dz = -sh.hz + iz * a.stride;
             const int64_t o = (zcn + dz) * sxy + (yc + dy) * a.nx + (xc + dx);
             const float fd = __ldg(a.f + o) - mfd;
             const float gd = gv - mgd;
@@ -1311,9 +1336,9 @@ static int launch_batched_t(const IcgnArgs& a, int brick_cap, cudaStream_t s) {
     return check_launch("icgn batched");
 }
 
-template <int MODE, bool STORED, int NDOF, int NW>
+template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN = false>
 static int launch_lean_t(const IcgnArgs& a, cudaStream_t s) {
-    auto kern = icgn_lean_kernel<MODE, STORED, NDOF, NW>;
+    auto kern = icgn_lean_kernel<MODE, STORED, NDOF, NW, UNEVEN>;
     static int cached_per_sm = -1;  // queried once, outside any stream capture
     static std::mutex mu;
     int per_sm;
@@ -1336,6 +1361,8 @@ static int launch_lean_t(const IcgnArgs& a, cudaStream_t s) {
 
 template <int MODE, bool STORED, int NDOF>
 static int launch_batched_m(const IcgnArgs& a, const LaunchCfg& c, cudaStream_t s) {
+    // per-node shapes run on the lean kernel with 4 warps per node (the brick kernel stages one shape per call)
+    if (a.node_half) return launch_lean_t<MODE, STORED, NDOF, 4, true>(a, s);
     switch (c.threads) {
         case 32: return launch_lean_t<MODE, STORED, NDOF, 1>(a, s);
         case 64: return launch_lean_t<MODE, STORED, NDOF, 2>(a, s);
@@ -1402,6 +1429,9 @@ static int fill_common(IcgnArgs& a, const aldvc_volumes* vol, const aldvc_subset
     a.split_index = sub->split_index;
     a.split_keep = sub->split_keep;
     a.keep_bytes = sub->keep_bytes;
+    ALDVC_REQUIRE(!(sub->node_half && sub->split_index), "icgn: per-node shapes do not combine with split rows");
+    ALDVC_REQUIRE(!(sub->node_half && prm->noise_gain > 0.0), "icgn: per-node shapes do not combine with the noise correction");
+    a.node_half = sub->node_half;
     a.coords = coords;
     a.n_nodes = n;
     a.tol = prm->tol;

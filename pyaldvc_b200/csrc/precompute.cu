@@ -33,6 +33,7 @@ struct PreArgs {
     double* bottomf;
     int64_t* n_valid;
     uint8_t* valid;
+    const int32_t* node_half;  // (N,3) per-node half-widths, NULL: (hx, hy, hz) for every node
 };
 
 // (i,k) pair index of the gradient products gg: 00 01 02 11 12 22
@@ -67,15 +68,23 @@ __global__ void __launch_bounds__(PRE_THREADS) precompute_kernel(PreArgs a) {
     __shared__ double tot[PRE_NSUM];
 
     const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    // this node's subset shape; a per-node shape beyond the call's maximum is rejected like an outside subset
+    int hx = a.hx, hy = a.hy, hz = a.hz;
+    bool shape_ok = true;
+    if (a.node_half) {
+        hx = a.node_half[3 * node];
+        hy = a.node_half[3 * node + 1];
+        hz = a.node_half[3 * node + 2];
+        shape_ok = hx >= 0 && hy >= 0 && hz >= 0 && hx <= a.hx && hy <= a.hy && hz <= a.hz;
+    }
     const int64_t r = a.split_index ? a.split_index[node] : -1;
     const bool use_keep = r >= 0;
     const uint8_t* keep = use_keep ? a.split_keep + r * a.keep_bytes : nullptr;
     double* H = a.H + node * 144;
     double* L = a.L + node * 144;
 
-    const bool inside = x0 - a.hx >= 0 && x0 + a.hx < a.nx && y0 - a.hy >= 0 && y0 + a.hy < a.ny && z0 - a.hz >= 0 &&
-                        z0 + a.hz < a.nz;
-    if (!use_keep && !inside) {
+    const bool inside = x0 - hx >= 0 && x0 + hx < a.nx && y0 - hy >= 0 && y0 + hy < a.ny && z0 - hz >= 0 && z0 + hz < a.nz;
+    if ((!use_keep && !inside) || !shape_ok) {
         for (int i = tid; i < 144; i += PRE_THREADS) {
             H[i] = 0.0;
             L[i] = 0.0;
@@ -99,14 +108,14 @@ __global__ void __launch_bounds__(PRE_THREADS) precompute_kernel(PreArgs a) {
     for (int i = 0; i < PRE_NSUM; ++i) acc[i] = 0.0f;
     int n = 0;
 
-    const int nX = (2 * a.hx) / a.stride + 1, nY = (2 * a.hy) / a.stride + 1, nZ = (2 * a.hz) / a.stride + 1;
+    const int nX = (2 * hx) / a.stride + 1, nY = (2 * hy) / a.stride + 1, nZ = (2 * hz) / a.stride + 1;
     const int S = nX * nY * nZ;
     // mixed-radix step of PRE_THREADS voxels through (iz, iy, ix)
     const int st_z = PRE_THREADS / (nX * nY), rem = PRE_THREADS % (nX * nY);
     const int st_y = rem / nX, st_x = rem % nX;
     int ix = tid % nX, iy = (tid / nX) % nY, iz = tid / (nX * nY);
     for (int v = tid; v < S; v += PRE_THREADS) {
-        const int dx = -a.hx + ix * a.stride, dy = -a.hy + iy * a.stride, dz = -a.hz + iz * a.stride;
+        const int dx = -hx + ix * a.stride, dy = -hy + iy * a.stride, dz = -hz + iz * a.stride;
         const int64_t xx = x0 + dx, yy = y0 + dy, zz = z0 + dz;
         bool k;
         if (use_keep) {
@@ -174,7 +183,7 @@ __global__ void __launch_bounds__(PRE_THREADS) precompute_kernel(PreArgs a) {
         for (int q = 0; q < 12; ++q) Hl[p * 12 + q] = tot[gg_index(comp(p), comp(q)) * 10 + xx_index(coord(p), coord(q))];
     for (int i = 0; i < 144; ++i) H[i] = Hl[i];
     a.n_valid[node] = nv;
-    const int64_t total = subset_count(a.hx, a.hy, a.hz, a.stride);
+    const int64_t total = subset_count(hx, hy, hz, a.stride);
     double Ll[144];
     for (int i = 0; i < 144; ++i) Ll[i] = 0.0;
     bool ok = !(nv < 27 || (double)nv < a.min_valid_ratio * (double)total);
@@ -218,11 +227,12 @@ extern "C" int aldvc_precompute(const aldvc_volumes* vol, const aldvc_subset* su
     const bool stored = vol->gx && vol->gy && vol->gz;
     ALDVC_REQUIRE(stored || (!vol->gx && !vol->gy && !vol->gz), "aldvc_precompute: give all three gradients or none");
     ALDVC_REQUIRE(!sub->split_index || (sub->split_keep && sub->keep_bytes > 0), "aldvc_precompute: split rows missing");
+    ALDVC_REQUIRE(!(sub->node_half && sub->split_index), "aldvc_precompute: per-node shapes do not combine with split rows");
     if (n_nodes <= 0) return ALDVC_OK;
     ALDVC_REQUIRE(n_nodes < (1LL << 31), "aldvc_precompute: too many nodes");
     PreArgs a{vol->f, vol->gx, vol->gy, vol->gz, vol->mask, (int)vol->nz, (int)vol->ny, (int)vol->nx, sub->hx, sub->hy, sub->hz,
               sub->stride, sub->split_index, sub->split_keep, sub->keep_bytes, coords, n_nodes, min_valid_ratio, cond_max,
-              H_all, L_all, meanf, bottomf, n_valid, valid};
+              H_all, L_all, meanf, bottomf, n_valid, valid, sub->node_half};
     cudaStream_t s = (cudaStream_t)stream;
     if (stored)
         precompute_kernel<true><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);

@@ -54,12 +54,15 @@ def volumes_struct(f, gx, gy, gz, mask, g) -> _lib.Volumes:
                         None if g is None else g.data_ptr(), nz, ny, nx)
 
 
-def subset_struct(half, stride, mode, split_index=None, split_keep=None) -> _lib.Subset:
+def subset_struct(half, stride, mode, split_index=None, split_keep=None, node_half=None) -> _lib.Subset:
+    """``half`` (hx, hy, hz); with ``node_half`` ((N,3) int32 CUDA tensor of per-node half-widths) ``half`` must be
+    their maximum."""
     hx, hy, hz = (int(h) for h in half)
+    nh = None if node_half is None else node_half.data_ptr()
     if split_index is not None and split_keep is not None:
         return _lib.Subset(hx, hy, hz, int(stride), int(mode), 0, split_index.data_ptr(), split_keep.data_ptr(),
-                           int(split_keep.shape[1]))
-    return _lib.Subset(hx, hy, hz, int(stride), int(mode), 0, None, None, 0)
+                           int(split_keep.shape[1]), nh)
+    return _lib.Subset(hx, hy, hz, int(stride), int(mode), 0, None, None, 0, nh)
 
 
 # --------------------------------------------------------------------------- preprocessing
@@ -74,8 +77,10 @@ def gradients(f: torch.Tensor, border: int = 3):
 
 
 # --------------------------------------------------------------------------- local solver
-def precompute(coords, half, f, gx, gy, gz, mask, min_valid_ratio, cond_max, stride=1, split_index=None, split_keep=None):
-    """Device ``precompute_nodes``: returns (H (N,12,12), L (N,12,12), meanf, bottomf, n_valid, valid) tensors."""
+def precompute(coords, half, f, gx, gy, gz, mask, min_valid_ratio, cond_max, stride=1, split_index=None, split_keep=None,
+               node_half=None):
+    """Device ``precompute_nodes``: returns (H (N,12,12), L (N,12,12), meanf, bottomf, n_valid, valid) tensors.
+    ``node_half``: optional (N,3) per-node half-widths (uneven subsets; ``half`` is then their maximum)."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
     d = coords.device
@@ -86,7 +91,8 @@ def precompute(coords, half, f, gx, gy, gz, mask, min_valid_ratio, cond_max, str
     nv = torch.empty(N, dtype=torch.int64, device=d)
     valid = torch.empty(N, dtype=torch.uint8, device=d)
     vol = volumes_struct(f, gx, gy, gz, mask, None)
-    sub = subset_struct(half, stride, 0, split_index, split_keep)
+    nh = None if node_half is None else dev(node_half, torch.int32)
+    sub = subset_struct(half, stride, 0, split_index, split_keep, nh)
     _lib.check(lib().aldvc_precompute(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, float(min_valid_ratio),
                                       float(cond_max), _p(H), _p(L), _p(mf), _p(bf), _p(nv), _p(valid), stream_handle()),
                "aldvc_precompute")
@@ -101,8 +107,9 @@ def icgn_params(tol, dp_tol, max_iter, patience, noise_gain=0.0, predictive=True
 
 def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol, dp_tol, max_iter, patience, stride=1, H=None,
            pattern=None, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED, threads=0,
-           brick_floats=0):
-    """Device 12-DOF IC-GN; returns (P (N,12), n_iter, status, zncc) tensors."""
+           brick_floats=0, node_half=None):
+    """Device 12-DOF IC-GN; returns (P (N,12), n_iter, status, zncc) tensors.  ``node_half``: optional (N,3)
+    per-node half-widths (``half`` is then their maximum)."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
     d = coords.device
@@ -112,7 +119,8 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
     status = torch.empty(N, dtype=torch.int8, device=d)
     zncc = torch.empty(N, dtype=torch.float64, device=d)
     vol = volumes_struct(f, gx, gy, gz, mask, g)
-    sub = subset_struct(half, stride, mode, split_index, split_keep)
+    nh = None if node_half is None else dev(node_half, torch.int32)
+    sub = subset_struct(half, stride, mode, split_index, split_keep, nh)
     prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats)
     ws_n = lib().aldvc_icgn_workspace_size(ctypes.byref(sub), N, ctypes.byref(prm))
     ws = _workspace(ws_n)
@@ -127,7 +135,7 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
 
 def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, meanf, bottomf, valid, mu, tol, dp_tol, max_iter,
           patience, stride=1, n_full=0.0, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED,
-          threads=0, brick_floats=0):
+          threads=0, brick_floats=0, node_half=None):
     """Device 3-DOF IC-GN (ADMM subproblem 1); returns (U (N,3), n_iter, status, zncc) tensors."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
@@ -140,7 +148,8 @@ def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, 
     status = torch.empty(N, dtype=torch.int8, device=d)
     zncc = torch.empty(N, dtype=torch.float64, device=d)
     vol = volumes_struct(f, gx, gy, gz, mask, g)
-    sub = subset_struct(half, stride, mode, split_index, split_keep)
+    nh = None if node_half is None else dev(node_half, torch.int32)
+    sub = subset_struct(half, stride, mode, split_index, split_keep, nh)
     prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats, mu, n_full)
     ws = _workspace(lib().aldvc_icgn_workspace_size(ctypes.byref(sub), N, ctypes.byref(prm)))
     _lib.check(lib().aldvc_icgn3(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, _p(U_old), _p(F_fixed), _p(vdual), _p(H),

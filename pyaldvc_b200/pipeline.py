@@ -59,6 +59,9 @@ class PassParams:
     autotune: bool = True
     graph: bool = False
     ncc_engine: str = "auto"  # auto | tiled | fft | plain
+    # uneven subsets: coords (N,3) [x, y, z] -> (N,3) even window sizes per node, each <= winsize (which then
+    # sets the mesh border and the maximum shape); every shape runs in the same persistent launches
+    node_winsize: object = None
 
 
 @dataclass
@@ -171,11 +174,29 @@ def _ncc_engine(p: PassParams, half, radius) -> int:
 def _launch_shape(p: PassParams, ndof: int, mode: int, mesh, mask, run) -> tuple[int, int]:
     """(threads, brick_floats) of the batched IC-GN launches: the caller's, else the autotuner's choice for
     this kernel and subset, timed on an evenly spread sample of this pass's nodes."""
-    if p.variant != K.BATCHED or p.threads != 0 or not p.autotune:
-        return p.threads, p.brick_floats
+    if p.variant != K.BATCHED or p.threads != 0 or not p.autotune or p.node_winsize is not None:
+        return p.threads, p.brick_floats  # per-node shapes always run the lean kernel
     k = autotune.key(ndof, mode, True, mesh.half, p.subset_stride, mask is not None, mesh.n)
     idx = autotune.sample_index(mesh.n)
     return autotune.tune(k, lambda th, br: run(idx, th, br))
+
+
+# captured ADMM loops, keyed by problem shape and parameters (the oldest is dropped beyond the limit)
+ADMM_GRAPH_CACHE = 2
+_ADMM_GRAPHS: dict = {}
+
+
+def _graph_key(p: PassParams, mesh, mode, th3, br3, n_full, tensors) -> tuple:
+    shapes = tuple((k, None if t is None else (tuple(t.shape), str(t.dtype))) for k, t in sorted(tensors.items()))
+    prm = (p.beta, p.mu, p.alpha, p.pcg_tol, p.pcg_max_iter, p.gauss_pt_order, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
+           p.icgn_patience, p.icgn_predictive_stop, p.admm_max_iter, p.dual_update, p.local_outlier_threshold, p.subset_stride,
+           p.variant)
+    return (mesh.grid_shape, tuple(mesh.half), tuple(mesh.spacing), mode, th3, br3, n_full, prm, shapes)
+
+
+def clear_graphs() -> None:
+    """Release every captured ADMM loop (and the device memory its static tensors hold)."""
+    _ADMM_GRAPHS.clear()
 
 
 def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
@@ -194,13 +215,23 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     tr.mark("preprocess")
 
     # ---------------- precompute (local_icgn.precompute_local_context :223-347)
+    node_half = None
+    if p.node_winsize is not None:
+        ws = np.asarray(p.node_winsize(mesh.coords.cpu().numpy()), dtype=np.int64).reshape(-1, 3)
+        hs = ws // 2
+        if (hs > np.asarray(mesh.half)[None, :]).any():
+            raise ValueError("node_winsize exceeds winsize")
+        node_half = torch.from_numpy(hs.astype(np.int32)).cuda()
     H, L, meanf, bottomf, n_valid, valid = K.precompute(mesh.coords, mesh.half, f, gx, gy, gz, m_u8, p.min_valid_ratio,
-                                                        p.hessian_cond_max, p.subset_stride)
+                                                        p.hessian_cond_max, p.subset_stride, None, None, node_half)
     valid_b = valid != 0
     if mask is not None:  # apply_mask_to_mesh (grid_mesh.py:191-253): centre in the mask, enough of the subset in it
         c = mesh.coords
         centre_ok = m_u8[c[:, 2], c[:, 1], c[:, 0]] != 0
-        S = float(np.prod([2 * h + 1 for h in mesh.half]))
+        if node_half is None:
+            S = float(np.prod([2 * h + 1 for h in mesh.half]))
+        else:
+            S = (2 * node_half.double() + 1).prod(dim=1)
         node_valid = centre_ok & (n_valid.double() >= p.min_valid_ratio * S)
         valid_b = valid_b & node_valid
         elem_node = node_valid.reshape(mesh.grid_shape)
@@ -260,8 +291,10 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     def icgn12_on(idx, th, br):
         c, P0_, L_, mf_, v_ = ((mesh.coords, P0, L, meanf, valid_u8) if idx is None else
                                (mesh.coords[idx], P0[idx], L[idx], meanf[idx], valid_u8[idx]))
+        nh = node_half if (node_half is None or idx is None) else node_half[idx]
         return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
-                        p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br)
+                        p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
+                        node_half=nh)
 
     th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
     P, n_iter, status, zncc = icgn12_on(None, th12, br12)
@@ -284,78 +317,100 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         return result
 
     # ---------------- sections 5-6: ADMM (pipeline.py:286-352) with fixed beta
-    def global_step(U1_, F1_, W_, v_):
-        b = K.global_rhs(mesh.grid_shape, mesh.spacing, elem_active, p.beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
-        U2_, _, _ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, elem_active, p.beta, p.mu, p.alpha, b, U1_, p.pcg_tol, p.pcg_max_iter,
-                               p.gauss_pt_order)
-        F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, elem_active, U2_, p.gauss_pt_order).reshape(-1, 9)
-        F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
-        return U2_, F2_
+    n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
+    # every tensor the ADMM loop reads; a captured loop reads static copies of them
+    T = {"f": f, "g": g, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
+         "coords": mesh.coords, "elem": elem_active, "node_half": node_half}
 
+    def make_steps(T):
+        def global_step(U1_, F1_, W_, v_):
+            b = K.global_rhs(mesh.grid_shape, mesh.spacing, T["elem"], p.beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
+            U2_, _, _ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, T["elem"], p.beta, p.mu, p.alpha, b, U1_, p.pcg_tol,
+                                   p.pcg_max_iter, p.gauss_pt_order)
+            F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, T["elem"], U2_, p.gauss_pt_order).reshape(-1, 9)
+            F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
+            return U2_, F2_
+
+        def icgn3_on(idx, U2_, F2_, v_, th, br):
+            keys = ("coords", "H", "meanf", "bottomf", "valid")
+            c, H_, mf_, bf_, ok_ = (T[k] if idx is None else T[k][idx] for k in keys)
+            if idx is not None:
+                U2_, F2_, v_ = U2_[idx], F2_[idx], v_[idx]
+            nh = T["node_half"] if (T["node_half"] is None or idx is None) else T["node_half"][idx]
+            return K.icgn3(c, U2_, F2_, v_, mesh.half, T["f"], T["gx"], T["gy"], T["gz"], T["m"], T["g"], mode, H_, mf_, bf_, ok_,
+                           p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0,
+                           p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh)
+
+        def admm_step(U2, F2, W, v, th3, br3):
+            # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
+            U, it3, st3, zc3 = icgn3_on(None, U2, F2, v, th3, br3)
+            bad3 = st3 != STATUS_CONVERGED
+            bad3 = bad3 | _median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold)
+            U1n = torch.where(bad3[:, None], U2, U)
+            F1n = F2
+            U2n, F2n = global_step(U1n, F1n, W, v)
+            if p.dual_update == "accumulate":
+                Wn = W + (F2n - F1n)
+                vn = v + (U2n - U1n)
+            else:
+                Wn = F2n - F1n
+                vn = U2n - U1n
+            du_g = _rms(U2n - U2)
+            return U1n, U2n, F2n, Wn, vn, du_g, st3, zc3, it3
+
+        return global_step, icgn3_on, admm_step
+
+    global_step, icgn3_on, admm_step = make_steps(T)
     W = torch.zeros((mesh.n, 9), dtype=torch.float64, device="cuda")
     v = torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda")
     U2, F2 = global_step(U1, F1, W, v)
     W = F2 - F1
     v = U2 - U1
-    n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
-
-    def icgn3_on(idx, U2_, F2_, v_, th, br):
-        c, H_, mf_, bf_, ok_ = ((mesh.coords, H, meanf, bottomf, valid_u8) if idx is None else
-                                (mesh.coords[idx], H[idx], meanf[idx], bottomf[idx], valid_u8[idx]))
-        if idx is not None:
-            U2_, F2_, v_ = U2_[idx], F2_[idx], v_[idx]
-        return K.icgn3(c, U2_, F2_, v_, mesh.half, f, gx, gy, gz, m_u8, g, mode, H_, mf_, bf_, ok_, p.mu, p.icgn_tol, p.icgn_dp_tol,
-                       p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0, p.icgn_predictive_stop, None, None, p.variant,
-                       th, br)
-
     th3, br3 = _launch_shape(p, 3, mode, mesh, m_u8, lambda idx, th, br: icgn3_on(idx, U2, F2, v, th, br))
-
-    def admm_step(U2, F2, W, v):
-        # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
-        U, it3, st3, zc3 = icgn3_on(None, U2, F2, v, th3, br3)
-        bad3 = st3 != STATUS_CONVERGED
-        bad3 = bad3 | _median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold)
-        U1n = torch.where(bad3[:, None], U2, U)
-        F1n = F2
-        U2n, F2n = global_step(U1n, F1n, W, v)
-        if p.dual_update == "accumulate":
-            Wn = W + (F2n - F1n)
-            vn = v + (U2n - U1n)
-        else:
-            Wn = F2n - F1n
-            vn = U2n - U1n
-        du_g = _rms(U2n - U2)
-        return U1n, U2n, F2n, Wn, vn, du_g, st3, zc3, it3
 
     steps = 1
     st_last, zc_last, it_last = status, zncc, n_iter
     U1_prev = U1
     if p.graph and not p.admm_early_stop and p.admm_max_iter > 1:
-        # capture the whole remaining loop once, replay it (no host step inside)
-        static = {"U2": U2.clone(), "F2": F2.clone(), "W": W.clone(), "v": v.clone(), "U1": U1.clone()}
-        side = torch.cuda.Stream()
-        side.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(side):  # warm-up outside capture (allocator pools, kernel attributes)
-            admm_step(static["U2"], static["F2"], static["W"], static["v"])
-        torch.cuda.current_stream().wait_stream(side)
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
-            a = (static["U2"], static["F2"], static["W"], static["v"])
-            outs = []
-            for _ in range(2, p.admm_max_iter + 1):
-                U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg = admm_step(*a)
-                outs.append((U1g, stg, zcg, itg))
-                a = (U2g, F2g, Wg, vg)
-        tr.mark("admm_capture")
-        graph.replay()
-        U2, F2 = a[0], a[1]
-        U1, st_last, zc_last, it_last = outs[-1]
+        # the remaining loop as one CUDA graph, captured on the first pass of this problem shape and replayed
+        # by every later one after its inputs are copied into the graph's static tensors (no host step inside)
+        state = {"U2": U2, "F2": F2, "W": W, "v": v}
+        key = _graph_key(p, mesh, mode, th3, br3, n_full, {**T, **state})
+        entry = _ADMM_GRAPHS.get(key)
+        if entry is None:
+            static = {k: (None if t is None else t.clone()) for k, t in {**T, **state}.items()}
+            _, _, admm_static = make_steps(static)
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):  # warm-up outside capture (allocator pools, kernel attributes)
+                admm_static(static["U2"], static["F2"], static["W"], static["v"], th3, br3)
+            torch.cuda.current_stream().wait_stream(side)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                a = (static["U2"], static["F2"], static["W"], static["v"])
+                outs = []
+                for _ in range(2, p.admm_max_iter + 1):
+                    U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg = admm_static(*a, th3, br3)
+                    outs.append((U1g, stg, zcg, itg))
+                    a = (U2g, F2g, Wg, vg)
+            entry = {"graph": graph, "static": static, "final": a, "outs": outs[-1]}
+            _ADMM_GRAPHS[key] = entry
+            while len(_ADMM_GRAPHS) > ADMM_GRAPH_CACHE:
+                _ADMM_GRAPHS.pop(next(iter(_ADMM_GRAPHS)))
+            tr.mark("admm_capture")
+        else:
+            for k, t in {**T, **state}.items():
+                if t is not None:
+                    entry["static"][k].copy_(t)
+        entry["graph"].replay()
+        # the graph's outputs are overwritten by its next replay: the result keeps copies
+        U2, F2 = entry["final"][0].clone(), entry["final"][1].clone()
+        U1, st_last, zc_last, it_last = (t.clone() for t in entry["outs"])
         steps = p.admm_max_iter
-        result.graph = graph  # keep the graph (and its memory) alive with the result
     else:
         for step in range(2, p.admm_max_iter + 1):
             steps = step
-            U1n, U2n, F2n, W, v, du_g, st_last, zc_last, it_last = admm_step(U2, F2, W, v)
+            U1n, U2n, F2n, W, v, du_g, st_last, zc_last, it_last = admm_step(U2, F2, W, v, th3, br3)
             du_l = _rms(U1n - U1_prev)
             U1_prev = U1n
             U1, U2, F2 = U1n, U2n, F2n
