@@ -2,8 +2,8 @@
 // ZNSSD normalisation of the reference subset (pyALDVC numba_kernels._precompute_one :326-418).
 //
 // One CTA per node.  H[(i,j),(k,l)] = sum g_i g_k X_j X_l with X = (X, Y, Z, 1) has only 6 x 10 = 60
-// distinct sums (Kronecker structure of the steepest-descent images), accumulated per thread in FP32
-// over <= S/256 voxels, reduced across the warp in FP32 and across warps in FP64.  Sum f and sum f^2
+// distinct sums (Kronecker structure of the steepest-descent images), accumulated per thread in compensated
+// (Kahan) FP32 over <= S/256 voxels, then reduced across the warp and across warps in FP64.  Sum f and sum f^2
 // are taken relative to the centre voxel so the variance does not cancel for offset intensities.
 #include "common.cuh"
 #include "internal.cuh"
@@ -57,8 +57,16 @@ __device__ __forceinline__ int xx_index(int j, int l) {
     return base[j] + (l - j);
 }
 
+// Kahan step: s + x with the rounding error carried in c (the compensated total is s - c)
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
 template <bool STORED>
-__global__ void __launch_bounds__(PRE_THREADS) precompute_kernel(PreArgs a) {
+__global__ void __launch_bounds__(PRE_THREADS, 2) precompute_kernel(PreArgs a) {
     const int64_t node = blockIdx.x;
     if (node >= a.n_nodes) return;
     const int tid = threadIdx.x;
@@ -103,65 +111,70 @@ __global__ void __launch_bounds__(PRE_THREADS) precompute_kernel(PreArgs a) {
     const int64_t cz = clampi(z0, a.nz - 1), cy = clampi(y0, a.ny - 1), cx = clampi(x0, a.nx - 1);
     const float pilot = __ldg(a.f + cz * sxy + cy * a.nx + cx);
 
-    float acc[PRE_NSUM];
-#pragma unroll
-    for (int i = 0; i < PRE_NSUM; ++i) acc[i] = 0.0f;
     int n = 0;
-
     const int nX = (2 * hx) / a.stride + 1, nY = (2 * hy) / a.stride + 1, nZ = (2 * hz) / a.stride + 1;
     const int S = nX * nY * nZ;
     // mixed-radix step of PRE_THREADS voxels through (iz, iy, ix)
     const int st_z = PRE_THREADS / (nX * nY), rem = PRE_THREADS % (nX * nY);
     const int st_y = rem / nX, st_x = rem % nX;
-    int ix = tid % nX, iy = (tid / nX) % nY, iz = tid / (nX * nY);
-    for (int v = tid; v < S; v += PRE_THREADS) {
-        const int dx = -hx + ix * a.stride, dy = -hy + iy * a.stride, dz = -hz + iz * a.stride;
-        const int64_t xx = x0 + dx, yy = y0 + dy, zz = z0 + dz;
-        bool k;
-        if (use_keep) {
-            k = kept_bit(keep, v) && xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
-        } else {
-            k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0;
-        }
-        if (k) {
-            const int64_t o = zz * sxy + yy * a.nx + xx;
-            const float fv = __ldg(a.f + o) - pilot;
-            float g0, g1, g2;
-            if (STORED) {
-                g0 = __ldg(a.gx + o);
-                g1 = __ldg(a.gy + o);
-                g2 = __ldg(a.gz + o);
+    // Compensated (Kahan) FP32 sums.  The 62 moments are swept in two halves of 31 (gradient products 00 01 02
+    // with sum f, then 11 12 22 with sum f^2) so that sum and compensation of a half fit the registers the plain
+    // sums took; each thread's corrected totals are reduced in FP64.
+#pragma unroll 1
+    for (int part = 0; part < 2; ++part) {
+        float sum[31], cmp[31];
+#pragma unroll
+        for (int i = 0; i < 31; ++i) sum[i] = cmp[i] = 0.0f;
+        int ix = tid % nX, iy = (tid / nX) % nY, iz = tid / (nX * nY);
+        for (int v = tid; v < S; v += PRE_THREADS) {
+            const int dx = -hx + ix * a.stride, dy = -hy + iy * a.stride, dz = -hz + iz * a.stride;
+            const int64_t xx = x0 + dx, yy = y0 + dy, zz = z0 + dz;
+            bool k;
+            if (use_keep) {
+                k = kept_bit(keep, v) && xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
             } else {
-                grad_otf(a.f, a.nz, a.ny, a.nx, (int)zz, (int)yy, (int)xx, g0, g1, g2);
+                k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + yy * a.nx + xx) != 0;
             }
-            const float X = (float)dx, Y = (float)dy, Z = (float)dz;
-            const float gg[6] = {g0 * g0, g0 * g1, g0 * g2, g1 * g1, g1 * g2, g2 * g2};
-            const float xq[10] = {X * X, X * Y, X * Z, X, Y * Y, Y * Z, Y, Z * Z, Z, 1.0f};
+            if (k) {
+                const int64_t o = zz * sxy + yy * a.nx + xx;
+                const float fv = __ldg(a.f + o) - pilot;
+                float g0, g1, g2;
+                if (STORED) {
+                    g0 = __ldg(a.gx + o);
+                    g1 = __ldg(a.gy + o);
+                    g2 = __ldg(a.gz + o);
+                } else {
+                    grad_otf(a.f, a.nz, a.ny, a.nx, (int)zz, (int)yy, (int)xx, g0, g1, g2);
+                }
+                const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+                // this part's gradient products: (00, 01, 02) or (11, 12, 22)
+                const float ga = part == 0 ? g0 : g1, gb = part == 0 ? g1 : g2;
+                const float gg[3] = {ga * ga, ga * gb, part == 0 ? g0 * g2 : g2 * g2};
+                const float xq[10] = {X * X, X * Y, X * Z, X, Y * Y, Y * Z, Y, Z * Z, Z, 1.0f};
 #pragma unroll
-            for (int p = 0; p < 6; ++p)
+                for (int p = 0; p < 3; ++p)
 #pragma unroll
-                for (int q = 0; q < 10; ++q) acc[p * 10 + q] += gg[p] * xq[q];
-            acc[60] += fv;
-            acc[61] += fv * fv;
-            ++n;
+                    for (int q = 0; q < 10; ++q) kahan_add(sum[p * 10 + q], cmp[p * 10 + q], gg[p] * xq[q]);
+                kahan_add(sum[30], cmp[30], part == 0 ? fv : fv * fv);
+                if (part == 0) ++n;
+            }
+            ix += st_x;
+            if (ix >= nX) {
+                ix -= nX;
+                ++iy;
+            }
+            iy += st_y;
+            if (iy >= nY) {
+                iy -= nY;
+                ++iz;
+            }
+            iz += st_z;
         }
-        ix += st_x;
-        if (ix >= nX) {
-            ix -= nX;
-            ++iy;
-        }
-        iy += st_y;
-        if (iy >= nY) {
-            iy -= nY;
-            ++iz;
-        }
-        iz += st_z;
-    }
-    // FP32 within the warp, FP64 across warps (fixed order: deterministic)
 #pragma unroll
-    for (int i = 0; i < PRE_NSUM; ++i) {
-        const float s = warp_sum(acc[i]);
-        if (lane == 0) red[warp][i] = (double)s;
+        for (int i = 0; i < 31; ++i) {
+            const double t = warp_sum_d((double)sum[i] - (double)cmp[i]);
+            if (lane == 0) red[warp][i < 30 ? 30 * part + i : 60 + part] = t;
+        }
     }
     n = warp_sum_i(n);
     if (lane == 0) red_n[warp] = n;
