@@ -219,6 +219,80 @@ def _peaks() -> dict:
             "fp32_source": f"nominal FP32 CUDA-core rate: {props.multi_processor_count} SMs x 128 lanes x 2 flop x {mhz:.0f} MHz"}
 
 
+def _smooth_len(n: int) -> int:
+    m = int(n)
+    while True:
+        k = m
+        for q in (2, 3, 5):
+            while k % q == 0:
+                k //= q
+        if k == 1:
+            return m
+        m += 1
+
+
+def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
+    """Roofline of every timed kernel of one pass: algorithmic work of the pass for that kernel (bytes it must move,
+    or FP32 flops) over its summed device time.  Work per unit:
+      fft_pass1  window + template in, spectrum planes out: (wz wy wx + sz sy sxp) 4 B + wz Ny Nx 8 B per node
+      fft_pass2  spectrum planes in, product planes out: (wz + vz) Ny Nx 8 B per node
+      fft_pass3  product planes in, box sums in, map out: vz Ny Nx 8 B + 3 n_off 4 B per node
+      ncc_peak   two sweeps of the FP32 map: 2 n_off 4 B per node
+      ncc_template  template in, centred template out: (n_tpl + sz sy sxp) 4 B per node
+      box_pass   16 B per voxel per launch
+      ncc_tiled / ncc_map  2 n_tpl n_off flop per node (direct cross term)
+      precompute 162 S flop per node; icgn12_* 263 (cubic) / 87 (linear) flop per voxel-iteration, icgn3_* 239 / 63."""
+    nvox = float(np.prod(vol_shape))
+    byte_work, flop_work = {}, {}
+    for n, half, rad, engine in getattr(res, "ncc_calls", []):
+        s_ = [2 * int(h) + 1 for h in half]
+        v_ = [2 * int(r) + 1 for r in rad]
+        w_ = [a + b - 1 for a, b in zip(s_, v_)]
+        N = [_smooth_len(w) for w in w_]
+        sxp = (s_[0] + 3) // 4 * 4
+        n_tpl, n_off = float(np.prod(s_)), float(np.prod(v_))
+        plane = N[0] * N[1] * 8.0  # Nx Ny complex
+        if engine == 2:
+            byte_work["fft_pass1"] = byte_work.get("fft_pass1", 0.0) + n * ((w_[0] * w_[1] * w_[2] + s_[2] * s_[1] * sxp) * 4.0 + w_[2] * plane)
+            byte_work["fft_pass2"] = byte_work.get("fft_pass2", 0.0) + n * (w_[2] + v_[2]) * plane
+            byte_work["fft_pass3"] = byte_work.get("fft_pass3", 0.0) + n * (v_[2] * plane + 3.0 * n_off * 4.0)
+        if engine in (0, 2):
+            byte_work["ncc_template"] = byte_work.get("ncc_template", 0.0) + n * (n_tpl + s_[2] * s_[1] * sxp) * 4.0
+        if engine == 0:
+            flop_work["ncc_tiled"] = flop_work.get("ncc_tiled", 0.0) + n * 2.0 * n_tpl * n_off
+        if engine == 1:
+            flop_work["ncc_map"] = flop_work.get("ncc_map", 0.0) + n * 2.0 * n_tpl * n_off
+        byte_work["ncc_peak"] = byte_work.get("ncc_peak", 0.0) + n * 2.0 * n_off * 4.0
+    if "box_pass" in ktimes:
+        byte_work["box_pass"] = ktimes["box_pass"][1] * 16.0 * nvox
+    half = [int(w) // 2 for w in p.winsize]
+    if getattr(res, "node_half", None) is not None:
+        S_node = ((2 * res.node_half.double() + 1).prod(dim=1)).cpu().numpy()
+    else:
+        S_node = np.full(res.coords.shape[0], float(np.prod([(2 * h) // p.subset_stride + 1 for h in half])))
+    c12, c3 = (87.0, 63.0) if p.interp_method == "linear" else (263.0, 239.0)
+    flop_work["precompute"] = 162.0 * float(S_node.sum())
+    it12 = getattr(res, "n_iter_local", res.n_iter).cpu().numpy().astype(np.float64)
+    it3 = sum((t.cpu().numpy().astype(np.float64) for t in getattr(res, "icgn3_iters", [])), np.zeros_like(it12))
+    for form in ("lean", "batched", "plain"):
+        flop_work[f"icgn12_{form}"] = c12 * float((it12 * S_node).sum())
+        flop_work[f"icgn3_{form}"] = c3 * float((it3 * S_node).sum())
+    total_ms = sum(ms for ms, _ in ktimes.values())
+    out = {}
+    for name, (ms, launches) in ktimes.items():
+        row = {"ms": ms, "launches": launches, "ms_share": ms / total_ms if total_ms else None}
+        if name in byte_work and peaks.get("hbm_gbs"):
+            ach = byte_work[name] / (ms / 1e3) / 1e9
+            row.update({"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                        "traffic": None, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"})
+        elif name in flop_work:
+            ach = flop_work[name] / (ms / 1e3) / 1e12
+            row.update({"bound": "fp32", "achieved": ach, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                        "frac": ach / peaks["fp32_tflops"], "traffic": None, "peak_source": peaks["fp32_source"]})
+        out[name] = row
+    return out
+
+
 def _normalize_np(v):
     a = np.asarray(v, dtype=np.float64)
     nz, ny, nx = a.shape
@@ -446,31 +520,15 @@ def main():
     sel_l = sel_all & (status_local == 0)
     rms_local_truth = float(np.sqrt(np.mean((U_local[sel_l] - truth[sel_l]) ** 2))) if sel_l.any() else float("nan")
 
-    # ---- roofline of the two heaviest stages, algorithmic work per the pass (FP32 CUDA-core bound)
+    # ---- per-kernel roofline: one more pass with the library's CUDA-event kernel timing on
     peaks = _peaks()
-    half = tuple(int(w) // 2 for w in p.winsize)
-    S = float(np.prod([(2 * h) // p.subset_stride + 1 for h in half]))
-    sub0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
-    n_tpl = float(np.prod([2 * (int(w) // 2) + 1 for w in sub0]))
-    n_off = float(np.prod([2 * int(r) + 1 for r in p.search_radius]))
-    n_search = int(valid.sum())
-    c_voxel = 87.0 if p.interp_method == "linear" else 263.0
-    n_it = res.n_iter.cpu().numpy() if not p.use_global_step else None
-    it12 = float(getattr(res, "n_iter_local", res.n_iter).cpu().numpy().astype(np.float64).sum())
-    rl = {
-        "init_guess": {"flops": 2.0 * n_tpl * n_off * n_search, "what": "ZNCC cross term 2 n_tpl n_off per searched node"},
-        "local_icgn": {"flops": it12 * S * c_voxel, "what": f"sum(n_iter) x S x {int(c_voxel)} flop per voxel-iteration"},
-    }
-    roof = {}
-    for name, r in rl.items():
-        t_ = stages.get(name)
-        if not t_:
-            continue
-        ach = r["flops"] / t_ / 1e12
-        roof[name] = {"bound": "fp32", "achieved": ach, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
-                      "frac": ach / peaks["fp32_tflops"], "traffic": None, "peak_source": peaks["fp32_source"],
-                      "stage_ms": 1e3 * t_, "work": r["what"]}
-    dominant = max(roof, key=lambda k_: roof[k_]["stage_ms"]) if roof else None
+    K.kernel_timing(True)
+    r_t = one_pass()
+    torch.cuda.synchronize()
+    ktimes = K.kernel_timing_read()
+    K.kernel_timing(False)
+    roof = _kernel_roofline(ktimes, r_t, p, f.shape, peaks)
+    dominant = max(roof, key=lambda k_: roof[k_]["ms"]) if roof else None
 
     # ---- plain form of the same pass
     plain = None
@@ -544,8 +602,8 @@ def main():
                      "rms_vs_truth_all_valid_vox": rms_truth_all, "rms_local_vs_truth_vox": rms_local_truth,
                      "rms_local_vs_fp64_oracle_vox": rms_oracle},
         "gpu_launches": int(round(launches)),
-        "roofline": roof.get(dominant),
-        "roofline_stages": roof,
+        "roofline": None if dominant is None else {k_: v_ for k_, v_ in roof[dominant].items() if k_ != "ms_share"} | {"kernel": dominant},
+        "roofline_kernels": roof,
         "cpu_baseline": cpu,
         "plain": plain,
         "batched_over_plain": None if plain is None else value / world / plain["value"],

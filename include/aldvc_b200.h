@@ -121,6 +121,14 @@ int aldvc_abi_version(void);
 const char *aldvc_last_error(void);
 /* kernels this library has launched in the process so far (a monotone counter) */
 unsigned long long aldvc_launch_count(void);
+
+/* Kernel timing for callers that measure a region (no reference counterpart): while enabled, the library
+ * records CUDA events on the launch stream around each launch of its main kernels (none on a stream under
+ * capture).  aldvc_kernel_timing(1) clears the records and starts, (0) clears and stops.  _read waits for
+ * the recorded events and writes, per kernel name in first-launch order, the total device milliseconds and
+ * the launch count (names: max_entries rows of name_len bytes); returns the number of distinct kernels. */
+int aldvc_kernel_timing(int enable);
+int aldvc_kernel_timing_read(int32_t max_entries, char *names, int32_t name_len, double *ms, int64_t *launches);
 /* name of device `device`, its SM count and compute capability; returns ALDVC_OK */
 int aldvc_device_info(int device, char *name, int name_len, int *sm_count, int *cc_major, int *cc_minor);
 
@@ -190,6 +198,9 @@ int aldvc_ncc_map(const float *f, const float *g, int64_t nz, int64_t ny, int64_
 #define ALDVC_NCC_TILED 0
 #define ALDVC_NCC_PLAIN 1
 #define ALDVC_NCC_FFT 2
+/* the FFT engine with its shared-memory Stockham transforms for every box (the in-register transforms of cubic
+ * boxes of length 36, 40, 48, 50, 54, 60 or 64 turned off): a comparison form */
+#define ALDVC_NCC_FFT_STOCKHAM 3
 
 size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz,
                                        int32_t rx, int32_t ry, int32_t rz, int32_t engine);

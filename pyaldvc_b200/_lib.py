@@ -18,6 +18,7 @@ PLAIN = 1
 NCC_TILED = 0
 NCC_PLAIN = 1
 NCC_FFT = 2
+NCC_FFT_STOCKHAM = 3
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -52,6 +53,8 @@ PROTOTYPES = {
     "aldvc_abi_version": (_i32, []),
     "aldvc_last_error": (ctypes.c_char_p, []),
     "aldvc_launch_count": (ctypes.c_ulonglong, []),
+    "aldvc_kernel_timing": (_i32, [_i32]),
+    "aldvc_kernel_timing_read": (_i32, [_i32, _p, _i32, _p, _p]),
     "aldvc_device_info": (_i32, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "aldvc_gradients": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _p, _p, _p]),

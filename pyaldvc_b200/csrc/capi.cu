@@ -2,6 +2,8 @@
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <vector>
+#include <algorithm>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -62,9 +64,89 @@ __global__ void gradients_kernel(const float* __restrict__ f, int nz, int ny, in
     gz[o] = comb(sxy);
 }
 
+// ---- kernel timing (off by default)
+static std::mutex g_tmu;
+static std::atomic<bool> g_timing{false};
+struct TRec {
+    const char* name;
+    cudaEvent_t a, b;
+};
+static std::vector<TRec> g_trecs;
+
+KTimer::KTimer(const char* n, cudaStream_t st) : name(n), s(st) {
+    if (!g_timing.load(std::memory_order_relaxed)) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+    if (cudaEventCreate(&a) != cudaSuccess) {
+        a = nullptr;
+        return;
+    }
+    cudaEventRecord(a, s);
+}
+
+KTimer::~KTimer() {
+    if (!a) return;
+    cudaEvent_t b;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return;
+    }
+    cudaEventRecord(b, s);
+    std::lock_guard<std::mutex> lock(g_tmu);
+    g_trecs.push_back({name, a, b});
+}
+
+static void clear_timing() {
+    for (auto& r : g_trecs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_trecs.clear();
+}
+
 }  // namespace aldvc
 
 using namespace aldvc;
+
+extern "C" int aldvc_kernel_timing(int enable) {
+    std::lock_guard<std::mutex> lock(g_tmu);
+    clear_timing();
+    g_timing.store(enable != 0);
+    return ALDVC_OK;
+}
+
+extern "C" int aldvc_kernel_timing_read(int32_t max_entries, char* names, int32_t name_len, double* ms, int64_t* launches) {
+    ALDVC_REQUIRE(max_entries >= 0 && (max_entries == 0 || (names && name_len > 1 && ms && launches)),
+                  "aldvc_kernel_timing_read: bad output buffers");
+    std::lock_guard<std::mutex> lock(g_tmu);
+    std::vector<const char*> keys;
+    std::vector<double> tot;
+    std::vector<int64_t> cnt;
+    for (auto& r : g_trecs) {
+        cudaError_t e = cudaEventSynchronize(r.b);
+        if (e != cudaSuccess) return cuda_fail(e, "aldvc_kernel_timing_read");
+        float t = 0.0f;
+        e = cudaEventElapsedTime(&t, r.a, r.b);
+        if (e != cudaSuccess) return cuda_fail(e, "aldvc_kernel_timing_read");
+        size_t k = 0;
+        while (k < keys.size() && std::strcmp(keys[k], r.name) != 0) ++k;
+        if (k == keys.size()) {
+            keys.push_back(r.name);
+            tot.push_back(0.0);
+            cnt.push_back(0);
+        }
+        tot[k] += (double)t;
+        cnt[k] += 1;
+    }
+    const int n = (int)std::min<size_t>(keys.size(), (size_t)max_entries);
+    for (int i = 0; i < n; ++i) {
+        std::strncpy(names + (size_t)i * name_len, keys[i], (size_t)name_len - 1);
+        names[(size_t)i * name_len + name_len - 1] = 0;
+        ms[i] = tot[i];
+        launches[i] = cnt[i];
+    }
+    return (int)keys.size();
+}
 
 extern "C" int aldvc_abi_version(void) { return ALDVC_ABI_VERSION; }
 

@@ -485,7 +485,10 @@ extern "C" int aldvc_global_rhs(const aldvc_hex8_mesh* mesh, double beta, double
     int rc = set_mesh(mesh, m, sp);
     if (rc) return rc;
     RhsArgs a{m, sp, beta, mu, alpha, U1, F1, W, v, b};
-    rhs_kernel<<<(unsigned)((m.n + 255) / 256), 256, 0, s>>>(a);
+    {
+        KTimer kt_("global_rhs", s);
+        rhs_kernel<<<(unsigned)((m.n + 255) / 256), 256, 0, s>>>(a);
+    }
     return check_launch("aldvc_global_rhs");
 }
 
@@ -497,7 +500,10 @@ extern "C" int aldvc_nodal_gradient(const aldvc_hex8_mesh* mesh, const double* U
     int rc = set_mesh(mesh, m, sp);
     if (rc) return rc;
     GradArgs a{m, sp, U, F};
-    grad_kernel<<<(unsigned)((m.n + 255) / 256), 256, 0, s>>>(a);
+    {
+        KTimer kt_("nodal_gradient", s);
+        grad_kernel<<<(unsigned)((m.n + 255) / 256), 256, 0, s>>>(a);
+    }
     return check_launch("aldvc_nodal_gradient");
 }
 
@@ -574,7 +580,10 @@ extern "C" int aldvc_pcg_hex8(const aldvc_hex8_mesh* mesh, double beta, double m
     e = cudaMemsetAsync(err, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "pcg: error word reset");
     void* args[] = {&a};
-    e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
+    {
+        KTimer kt_("pcg_hex8", s);
+        e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "pcg: cooperative launch");
     count_launch();
     return ALDVC_OK;

@@ -1332,7 +1332,10 @@ static int launch_batched_t(const IcgnArgs& a, int brick_cap, cudaStream_t s) {
     if (per_sm < 1) return arg_fail("icgn batched: brick does not fit in shared memory");
     long long grid = (long long)per_sm * sm_count();
     if (grid > a.n_nodes) grid = a.n_nodes;
-    kern<<<(unsigned)grid, THREADS, smem, s>>>(a);
+    {
+        KTimer kt_(NDOF == 12 ? "icgn12_batched" : "icgn3_batched", s);
+        kern<<<(unsigned)grid, THREADS, smem, s>>>(a);
+    }
     return check_launch("icgn batched");
 }
 
@@ -1355,7 +1358,10 @@ static int launch_lean_t(const IcgnArgs& a, cudaStream_t s) {
     if (per_sm < 1) return arg_fail("icgn lean: kernel does not fit on an SM");
     long long grid = (long long)per_sm * sm_count();
     if (grid > a.n_nodes) grid = a.n_nodes;
-    kern<<<(unsigned)grid, NW * 32, 0, s>>>(a);
+    {
+        KTimer kt_(NDOF == 12 ? "icgn12_lean" : "icgn3_lean", s);
+        kern<<<(unsigned)grid, NW * 32, 0, s>>>(a);
+    }
     return check_launch("icgn lean");
 }
 
@@ -1377,7 +1383,10 @@ static int launch_plain_m(IcgnArgs a, cudaStream_t s) {
     for (int64_t start = 0; start < a.n_nodes; start += PLAIN_CHUNK) {
         a.node_base = start;
         const int64_t n = std::min<int64_t>(PLAIN_CHUNK, a.n_nodes - start);
-        icgn_plain_kernel<MODE, STORED, NDOF><<<(unsigned)n, 256, 0, s>>>(a);
+        {
+            KTimer kt_(NDOF == 12 ? "icgn12_plain" : "icgn3_plain", s);
+            icgn_plain_kernel<MODE, STORED, NDOF><<<(unsigned)n, 256, 0, s>>>(a);
+        }
         const int rc = check_launch("icgn plain");
         if (rc) return rc;
     }

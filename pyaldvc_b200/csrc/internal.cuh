@@ -37,6 +37,16 @@ inline int check_launch(const char* where) {
 int sm_count();
 int max_smem_optin();
 
+// Device time of one launch (CUDA events on its stream, around the launch) while kernel timing is on
+// (aldvc_kernel_timing); nothing is recorded otherwise, nor on a stream under capture.
+struct KTimer {
+    const char* name;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr;
+    KTimer(const char* n, cudaStream_t st);
+    ~KTimer();
+};
+
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace aldvc

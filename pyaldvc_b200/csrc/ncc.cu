@@ -14,6 +14,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "fft_reg.cuh"
 #include "internal.cuh"
 
 namespace aldvc {
@@ -520,9 +521,15 @@ static int launch_peak(const SearchArgs& b, int64_t n, cudaStream_t s) {
         bb.map = b.map + done * b.G.nmap;
         const unsigned nb = (unsigned)std::min<int64_t>(65535, n - done);
         if (sm)
-            ncc_peak_kernel<true><<<nb, NCC_THREADS, sm, s>>>(bb);
+            {
+                KTimer kt_("ncc_peak", s);
+                ncc_peak_kernel<true><<<nb, NCC_THREADS, sm, s>>>(bb);
+            }
         else
-            ncc_peak_kernel<false><<<nb, NCC_THREADS, 0, s>>>(bb);
+            {
+                KTimer kt_("ncc_peak", s);
+                ncc_peak_kernel<false><<<nb, NCC_THREADS, 0, s>>>(bb);
+            }
         const int rc = check_launch("ncc peak");
         if (rc) return rc;
     }
@@ -935,10 +942,16 @@ static int launch_tiled_t(const TiledArgs& a, const TiledCfg& c, int64_t n_chunk
         aa.out = a.out + done * a.G.nmap;
         aa.T = a.T + done * tsz;
         aa.ssf = a.ssf + done;
-        ncc_template_kernel<<<nb, 256, 0, s>>>(aa, const_cast<float*>(aa.T), const_cast<double*>(aa.ssf));
+        {
+            KTimer kt_("ncc_template", s);
+            ncc_template_kernel<<<nb, 256, 0, s>>>(aa, const_cast<float*>(aa.T), const_cast<double*>(aa.ssf));
+        }
         int rc = check_launch("ncc template");
         if (rc) return rc;
-        kern<<<dim3(slabs, nb), c.threads, c.smem, s>>>(aa);
+        {
+            KTimer kt_("ncc_tiled", s);
+            kern<<<dim3(slabs, nb), c.threads, c.smem, s>>>(aa);
+        }
         rc = check_launch("ncc tiled");
         if (rc) return rc;
     }
@@ -1154,6 +1167,28 @@ __device__ float2* fft_rows(float2* a, float2* b, const float2* tw, const FftAxi
 
 // Row-by-column sweep of an (nrows x ncols <= 128) tile, one warp per row: RB rows of loads are issued before
 // any of their stores, so each thread keeps up to 4 RB global loads in flight.
+// Sweep of an (nrows x ncols) tile by linear index (every lane busy whatever ncols is); the row of index i is
+// (i + 0.5) / ncols in FP32, exact for i < 2^22.  RB indices per thread are loaded before any is stored.
+template <int RB, typename T, typename Ld, typename St>
+__device__ __forceinline__ void sweep_lin(int nrows, int ncols, Ld ld, St st) {
+    const int total = nrows * ncols;
+    const float inv = 1.0f / (float)ncols;
+    for (int i0 = threadIdx.x; i0 < total; i0 += RB * blockDim.x) {
+        T v[RB];
+        int rr[RB], cc[RB];
+#pragma unroll
+        for (int u = 0; u < RB; ++u) {
+            const int i = i0 + u * blockDim.x;
+            rr[u] = (int)(((float)i + 0.5f) * inv);
+            cc[u] = i - rr[u] * ncols;
+            if (i < total) v[u] = ld(rr[u], cc[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+            if (i0 + u * (int)blockDim.x < total) st(rr[u], cc[u], v[u]);
+    }
+}
+
 template <int RB, typename T, typename Ld, typename St>
 __device__ __forceinline__ void copy_rows(int nrows, int ncols, Ld ld, St st) {
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1335,15 +1370,253 @@ __global__ void __launch_bounds__(FFT_THREADS, 4) fft_pass3_kernel(FftArgs a) {
         });
 }
 
+// ---- cubic boxes (Nx = Ny = Nz = N, a length with an in-register transform): the same three passes, each line
+// transformed by one thread in registers (fft_line), shared memory only to turn lines between axes.
+// Planes per CTA: as many as keep its shared tile near 70 KB (3 CTAs per SM), at most 256 / N.
+template <int N>
+__host__ __device__ constexpr int fftr_planes() {
+    constexpr int by_smem = 70000 / (N * (N | 1) * 8);
+    constexpr int by_threads = 256 / N;
+    return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
+}
+
+// Pass 1: thread (plane, y) reads its window row straight into registers, transforms along x, parks the row in
+// shared memory; then thread (plane, x) transforms the column along y and the planes go out coalesced.
+template <int N>
+__global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass1_kernel(FftArgs a) {
+    constexpr int P = fftr_planes<N>();
+    constexpr int PITCH = N | 1;
+    extern __shared__ __align__(16) float2 fsm[];  // [P][N][PITCH]
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    if (!fft_node_ok(a, node)) return;
+    const int z0 = blockIdx.x * P;
+    const int np = min(P, G.wz - z0);
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    const float pilot = __ldg(a.pilot_at);
+    const int t = threadIdx.x;
+    const int pl = t / N, yx = t - pl * N;  // row y in the x phase, column x in the y phase
+    if (pl < np) {
+        const int z = z0 + pl, y = yx;
+        float2 v[N];
+        const float* wrow = a.g + (a.wz0[node] + z) * sxy + (a.wy0[node] + y) * G.nx + a.wx0[node];
+        const float* trow = a.T + (int64_t)blockIdx.y * G.sz * G.sy * a.sxp + ((int64_t)z * G.sy + y) * a.sxp;
+        const bool wy_in = y < G.wy, ty_in = z < G.sz && y < G.sy;
+#pragma unroll
+        for (int x = 0; x < N; ++x) {
+            v[x].x = (wy_in && x < G.wx) ? __ldg(wrow + x) - pilot : 0.0f;
+            v[x].y = (ty_in && x < G.sx) ? __ldg(trow + x) : 0.0f;
+        }
+        if (wy_in) fft_line<N, -1>(v);  // rows past the window are zero and stay zero
+        float2* row = fsm + (pl * N + y) * PITCH;
+#pragma unroll
+        for (int x = 0; x < N; ++x) row[x] = v[x];
+    }
+    __syncthreads();
+    if (pl < np) {
+        float2* col = fsm + pl * N * PITCH + yx;
+        float2 v[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) v[k] = col[k * PITCH];
+        fft_line<N, -1>(v);
+#pragma unroll
+        for (int k = 0; k < N; ++k) col[k * PITCH] = v[k];
+    }
+    __syncthreads();
+    float2* dst = a.A + ((int64_t)blockIdx.y * G.wz + z0) * N * N;
+    sweep_lin<2, float2>(np * N, N, [&](int r, int x) { return fsm[r * PITCH + x]; },
+                         [&](int r, int x, float2 v) { dst[(int64_t)r * N + x] = v; });
+}
+
+// One CTA per (ky, -ky) row pair: thread (q, c) holds the z-line of column c of its row in registers.
+template <int N>
+__global__ void __launch_bounds__(2 * N) fftr_pass2_kernel(FftArgs a) {
+    constexpr int PITCH = N | 1;
+    extern __shared__ __align__(16) float2 fsm[];  // the two rows' spectra [2][N][PITCH]
+    auto S = [&](int q, int k, int c) -> float2& { return fsm[(q * N + k) * PITCH + c]; };
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    if (!fft_node_ok(a, node)) return;
+    const int ky0 = blockIdx.x, ky1 = (N - ky0) % N;
+    const bool self = ky0 == ky1;
+    const int t = threadIdx.x, q = t / N, c = t - q * N;
+    const bool active = !(self && q == 1);
+    const int ky = q == 0 ? ky0 : ky1;
+    float2 v[N];
+    if (active) {
+        const float2* col = a.A + (int64_t)blockIdx.y * G.wz * N * N + ky * N + c;
+#pragma unroll
+        for (int z = 0; z < N; ++z) v[z] = z < G.wz ? col[(int64_t)z * N * N] : make_float2(0.0f, 0.0f);
+        fft_line<N, -1>(v);
+#pragma unroll
+        for (int k = 0; k < N; ++k) S(q, k, c) = v[k];
+    }
+    __syncthreads();
+    if (!active) return;
+    const int qm = self ? 0 : 1 - q, cm = (N - c) % N;
+#pragma unroll
+    for (int kz = 0; kz < N; ++kz) {
+        const float2 za = v[kz];
+        const float2 zb = S(qm, (N - kz) % N, cm);
+        const float2 zbc = make_float2(zb.x, -zb.y);
+        const float2 w = make_float2(0.5f * (za.x + zbc.x), 0.5f * (za.y + zbc.y));
+        const float2 d = make_float2(za.x - zbc.x, za.y - zbc.y);
+        const float2 tc = make_float2(0.5f * d.y, 0.5f * d.x);  // conj(T^) = i conj(za - zbc) / 2
+        v[kz] = fr_mul(w, tc);
+    }
+    fft_line<N, 1>(v);
+    float2* dst = a.P + (int64_t)blockIdx.y * G.vz * N * N + ky * N + c;
+#pragma unroll
+    for (int dz = 0; dz < N; ++dz)
+        if (dz < G.vz) dst[(int64_t)dz * N * N] = v[dz];
+}
+
+// Pass 3: thread (plane, x) reads its y-column of the product straight into registers (coalesced across
+// threads) and inverts along y; thread (plane, dy < vy) inverts the row along x; the normalised map rows go out.
+template <int N>
+__global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArgs a) {
+    constexpr int P = fftr_planes<N>();
+    constexpr int PITCH = N | 1;
+    extern __shared__ __align__(16) float2 fsm[];  // [P][N][PITCH]
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    const int dz0 = blockIdx.x * P;
+    const int np = min(P, G.vz - dz0);
+    float* out = a.out + (int64_t)blockIdx.y * G.nmap + (int64_t)dz0 * G.vy * G.vx;
+    if (!fft_node_ok(a, node)) {
+        for (int i = threadIdx.x; i < np * G.vy * G.vx; i += blockDim.x) out[i] = -2.0f;
+        return;
+    }
+    const int t = threadIdx.x;
+    const int pl = t / N, yx = t - pl * N;
+    if (pl < np) {  // inverse along y, every column
+        const float2* colg = a.P + ((int64_t)blockIdx.y * G.vz + dz0 + pl) * N * N + yx;
+        float2 v[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) v[k] = colg[k * N];
+        fft_line<N, 1>(v);
+        float2* col = fsm + pl * N * PITCH + yx;
+#pragma unroll
+        for (int k = 0; k < N; ++k) col[k * PITCH] = v[k];
+    }
+    __syncthreads();
+    if (pl < np && yx < G.vy) {  // inverse along x, rows dy < vy
+        float2* row = fsm + (pl * N + yx) * PITCH;
+        float2 v[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) v[k] = row[k];
+        fft_line<N, 1>(v);
+#pragma unroll
+        for (int k = 0; k < N; ++k) row[k] = v[k];
+    }
+    __syncthreads();
+    const double scale = 1.0 / ((double)N * N * N);
+    const double ssf = a.ssf[blockIdx.y], n_tpl = (double)G.n_tpl;
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
+    // window variance in FP64 (it cancels), the normalisation itself in FP32: the map is FP32, and the peak is
+    // settled on FP64 re-scores
+    const float fscale = (float)scale;
+    const double inv_n = 1.0 / n_tpl;
+    sweep_lin<4, float2>(
+        np * G.vy, G.vx,
+        [&](int r, int dx) {
+            const int p_ = (int)(((float)r + 0.5f) / (float)G.vy), dy = r - p_ * G.vy;
+            const int64_t o = (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
+            return make_float2(__ldg(a.B1 + o), __ldg(a.B2 + o));
+        },
+        [&](int r, int dx, float2 bs) {
+            const int p_ = (int)(((float)r + 0.5f) / (float)G.vy), dy = r - p_ * G.vy;
+            const double s1 = (double)bs.x;
+            const double var = (double)bs.y - s1 * s1 * inv_n;
+            float v = 0.0f;
+            if (!(var < 1e-20)) {
+                v = fsm[(p_ * N + dy) * PITCH + dx].x * fscale * rsqrtf((float)(var * ssf));
+                v = fminf(1.0f, fmaxf(-1.0f, v));
+            }
+            out[(int64_t)p_ * G.vy * G.vx + dy * G.vx + dx] = v;
+        });
+}
+
+// twiddles of the in-register transforms, once per device (before any capture: the first FFT search does it)
+static int fftr_upload() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "ncc fft: device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && done[dev]) return ALDVC_OK;
+    float2 h[FFTR_TOTAL];
+    for (int i = 0; i < FFTR_NSIZES; ++i) {
+        const int n = FFTR_SIZES[i], o = fftr_offset(n);
+        for (int k = 0; k < n; ++k) {
+            const double ang = -2.0 * 3.14159265358979323846 * (double)k / (double)n;
+            h[o + k] = make_float2((float)cos(ang), (float)sin(ang));
+        }
+    }
+    e = cudaMemcpyToSymbol(c_fftr_tw, h, sizeof(h));
+    if (e != cudaSuccess) return cuda_fail(e, "ncc fft: twiddle upload");
+    if (dev < 64) done[dev] = true;
+    return ALDVC_OK;
+}
+
+template <int N>
+static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
+    constexpr int P = fftr_planes<N>();
+    constexpr size_t SM = (size_t)P * N * (N | 1) * sizeof(float2);
+    constexpr size_t SM2 = (size_t)2 * N * (N | 1) * sizeof(float2);
+    static bool attr = false;  // set once, outside any capture (the first search of this length)
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(fftr_pass1_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fftr_pass3_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fftr_pass2_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM2);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc fft: shared memory attribute");
+        attr = true;
+    }
+    const NccGeom& G = a.G;
+    {
+        KTimer kt_("fft_pass1", s);
+        fftr_pass1_kernel<N><<<dim3((G.wz + P - 1) / P, nb), P * N, SM, s>>>(a);
+    }
+    int rc = check_launch("ncc fft pass 1");
+    if (rc) return rc;
+    {
+        KTimer kt_("fft_pass2", s);
+        fftr_pass2_kernel<N><<<dim3(N / 2 + 1, nb), 2 * N, SM2, s>>>(a);
+    }
+    rc = check_launch("ncc fft pass 2");
+    if (rc) return rc;
+    {
+        KTimer kt_("fft_pass3", s);
+        fftr_pass3_kernel<N><<<dim3((G.vz + P - 1) / P, nb), P * N, SM, s>>>(a);
+    }
+    return check_launch("ncc fft pass 3");
+}
+
+static int launch_fftr_n(int n, FftArgs& a, int nb, cudaStream_t s) {
+    switch (n) {
+        case 36: return launch_fftr<36>(a, nb, s);
+        case 40: return launch_fftr<40>(a, nb, s);
+        case 48: return launch_fftr<48>(a, nb, s);
+        case 50: return launch_fftr<50>(a, nb, s);
+        case 54: return launch_fftr<54>(a, nb, s);
+        case 60: return launch_fftr<60>(a, nb, s);
+        default: return launch_fftr<64>(a, nb, s);
+    }
+}
+
 struct FftCfg {
     FftAxis ax, ay, az;
+    bool reg;  // cubic box of a length with an in-register transform (fftr passes)
     int pitch;
     size_t smem13, smem2;  // dynamic shared bytes of passes 1/3 and 2
     int64_t per_node;      // scratch bytes per node (A and P)
 };
 
-static bool fft_config(const NccGeom& G, FftCfg& c) {
+static bool fft_config(const NccGeom& G, FftCfg& c, bool engine_reg = true) {
     if (!fft_axis(smooth_len(G.wx), c.ax) || !fft_axis(smooth_len(G.wy), c.ay) || !fft_axis(smooth_len(G.wz), c.az)) return false;
+    c.reg = engine_reg && c.ax.n == c.ay.n && c.ax.n == c.az.n && fftr_supported(c.ax.n);
     c.pitch = c.ax.n | 1;  // odd: rows and columns of a plane fall in distinct bank pairs
     c.smem13 = ((size_t)2 * c.ay.n * c.pitch + 2 * FFT_MAX_N) * sizeof(float2);
     // pass 2: two buffers of one whole row (Nz x pitch) or of two half rows (2 x Nz x (cb | 1))
@@ -1395,13 +1668,27 @@ static int launch_fft(FftArgs a, const FftCfg& c, int64_t n, int64_t batch, cuda
         a.ssf = ssf0 + done;
         a.T = T0 + done * tsz;
         a.nb = nb;
-        fft_pass1_kernel<<<dim3(G.wz, nb), FFT_THREADS, c.smem13, s>>>(a);
+        if (c.reg) {
+            rc = launch_fftr_n(c.ax.n, a, nb, s);
+            if (rc) return rc;
+            continue;
+        }
+        {
+            KTimer kt_("fft_pass1", s);
+            fft_pass1_kernel<<<dim3(G.wz, nb), FFT_THREADS, c.smem13, s>>>(a);
+        }
         rc = check_launch("ncc fft pass 1");
         if (rc) return rc;
-        fft_pass2_kernel<<<dim3(2 * (c.ay.n / 2 + 1), nb), FFT_THREADS, c.smem2, s>>>(a);
+        {
+            KTimer kt_("fft_pass2", s);
+            fft_pass2_kernel<<<dim3(2 * (c.ay.n / 2 + 1), nb), FFT_THREADS, c.smem2, s>>>(a);
+        }
         rc = check_launch("ncc fft pass 2");
         if (rc) return rc;
-        fft_pass3_kernel<<<dim3(G.vz, nb), FFT_THREADS, c.smem13, s>>>(a);
+        {
+            KTimer kt_("fft_pass3", s);
+            fft_pass3_kernel<<<dim3(G.vz, nb), FFT_THREADS, c.smem13, s>>>(a);
+        }
         rc = check_launch("ncc fft pass 3");
         if (rc) return rc;
     }
@@ -1471,7 +1758,10 @@ static int launch_map(const MapArgs& m, int64_t n_chunk, cudaStream_t s) {
         mm.node_base = m.node_base + done;
         mm.out = m.out + done * m.G.nmap;
         const unsigned ny = (unsigned)std::min<int64_t>(65535, n_chunk - done);
-        ncc_map_kernel<<<dim3(tiles, ny), NCC_THREADS, smem, s>>>(mm);
+        {
+            KTimer kt_("ncc_map", s);
+            ncc_map_kernel<<<dim3(tiles, ny), NCC_THREADS, smem, s>>>(mm);
+        }
         const int rc = check_launch("ncc map");
         if (rc) return rc;
     }
@@ -1509,12 +1799,15 @@ extern "C" int aldvc_ncc_map(const float* f, const float* g, int64_t nz, int64_t
     return launch_map(m, n_nodes, (cudaStream_t)stream);
 }
 
-static bool use_fft(const NccGeom& G, int32_t engine, FftCfg& c) { return engine == ALDVC_NCC_FFT && fft_config(G, c); }
+static bool use_fft(const NccGeom& G, int32_t engine, FftCfg& c) {
+    return (engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM) && fft_config(G, c, engine == ALDVC_NCC_FFT);
+}
 
 // TILED, or FFT on a geometry the FFT engine does not take
 static bool use_tiled(const NccGeom& G, int32_t engine, TiledCfg& c) {
     FftCfg fc;
-    return (engine == ALDVC_NCC_TILED || (engine == ALDVC_NCC_FFT && !fft_config(G, fc))) && tiled_config(G, c);
+    const bool fft = engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM;
+    return (engine == ALDVC_NCC_TILED || (fft && !fft_config(G, fc))) && tiled_config(G, c);
 }
 
 static int launch_templates(const TiledArgs& a, int64_t n, cudaStream_t s) {
@@ -1523,7 +1816,10 @@ static int launch_templates(const TiledArgs& a, int64_t n, cudaStream_t s) {
         const unsigned nb = (unsigned)std::min<int64_t>(65535, n - done);
         TiledArgs aa = a;
         aa.node_base = a.node_base + done;
-        ncc_template_kernel<<<nb, 256, 0, s>>>(aa, const_cast<float*>(a.T) + done * tsz, const_cast<double*>(a.ssf) + done);
+        {
+            KTimer kt_("ncc_template", s);
+            ncc_template_kernel<<<nb, 256, 0, s>>>(aa, const_cast<float*>(a.T) + done * tsz, const_cast<double*>(a.ssf) + done);
+        }
         const int rc = check_launch("ncc template");
         if (rc) return rc;
     }
@@ -1551,7 +1847,7 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
                                 const int64_t* shift0, int32_t engine, void* workspace, size_t workspace_bytes, double* disp,
                                 double* cc, double* pce, uint8_t* clipped, uint8_t* ok, void* stream) {
     ALDVC_REQUIRE(f && g && coords && disp && cc && pce && clipped && ok, "aldvc_ncc_search: null pointer");
-    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN || engine == ALDVC_NCC_FFT,
+    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN || engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM,
                   "aldvc_ncc_search: unknown engine");
     const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
     int rc = check_geom(G);
@@ -1609,13 +1905,22 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
         const float* pilot_at = g + ((nz / 2) * ny + ny / 2) * nx + nx / 2;  // read by the kernel: no host round trip
         const int64_t nv = nz * ny * nx;
         const unsigned blocks = (unsigned)((nv + 255) / 256);
-        box_pass_kernel<<<blocks, 256, 0, s>>>(g, nullptr, b1, b2, (int)nz, (int)ny, (int)nx, 0, G.sx, pilot_at, 1);
+        {
+            KTimer kt_("box_pass", s);
+            box_pass_kernel<<<blocks, 256, 0, s>>>(g, nullptr, b1, b2, (int)nz, (int)ny, (int)nx, 0, G.sx, pilot_at, 1);
+        }
         rc = check_launch("ncc box x");
         if (rc) return rc;
-        box_pass_kernel<<<blocks, 256, 0, s>>>(b1, b2, t1, t2, (int)nz, (int)ny, (int)nx, 1, G.sy, nullptr, 0);
+        {
+            KTimer kt_("box_pass", s);
+            box_pass_kernel<<<blocks, 256, 0, s>>>(b1, b2, t1, t2, (int)nz, (int)ny, (int)nx, 1, G.sy, nullptr, 0);
+        }
         rc = check_launch("ncc box y");
         if (rc) return rc;
-        box_pass_kernel<<<blocks, 256, 0, s>>>(t1, t2, b1, b2, (int)nz, (int)ny, (int)nx, 2, G.sz, nullptr, 0);
+        {
+            KTimer kt_("box_pass", s);
+            box_pass_kernel<<<blocks, 256, 0, s>>>(t1, t2, b1, b2, (int)nz, (int)ny, (int)nx, 2, G.sz, nullptr, 0);
+        }
         rc = check_launch("ncc box z");
         if (rc) return rc;
         ta.f = f;
@@ -1631,6 +1936,10 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
         ta.T = tpl;
         ta.ssf = (const double*)((char*)tpl + align_up((size_t)chunk * G.sz * G.sy * tc.sxp * sizeof(float), 256));
         if (fft) {
+            if (fc.reg) {
+                rc = fftr_upload();
+                if (rc) return rc;
+            }
             ta.sxp = tc.sxp;
             char* fw = box + 4 * vb + tiled_tpl_bytes(G, chunk);
             float2* tw = (float2*)fw;

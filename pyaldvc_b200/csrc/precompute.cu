@@ -248,8 +248,14 @@ extern "C" int aldvc_precompute(const aldvc_volumes* vol, const aldvc_subset* su
               H_all, L_all, meanf, bottomf, n_valid, valid, sub->node_half};
     cudaStream_t s = (cudaStream_t)stream;
     if (stored)
-        precompute_kernel<true><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("precompute", s);
+            precompute_kernel<true><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);
+        }
     else
-        precompute_kernel<false><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("precompute", s);
+            precompute_kernel<false><<<(unsigned)n_nodes, PRE_THREADS, 0, s>>>(a);
+        }
     return check_launch("aldvc_precompute");
 }

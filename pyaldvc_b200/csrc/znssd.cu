@@ -375,11 +375,20 @@ extern "C" int aldvc_znssd_forward(const aldvc_volumes* vol, const int64_t* coor
     a.stats = stats;
     cudaStream_t s = (cudaStream_t)stream;
     if (mode == 0)
-        znssd_forward_kernel<0><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("znssd_forward", s);
+            znssd_forward_kernel<0><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        }
     else if (mode == 1)
-        znssd_forward_kernel<1><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("znssd_forward", s);
+            znssd_forward_kernel<1><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        }
     else
-        znssd_forward_kernel<2><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("znssd_forward", s);
+            znssd_forward_kernel<2><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        }
     return check_launch("znssd forward");
 }
 
@@ -397,10 +406,19 @@ extern "C" int aldvc_znssd_backward(const aldvc_volumes* vol, const int64_t* coo
     a.gG = grad_g;
     cudaStream_t s = (cudaStream_t)stream;
     if (mode == 0)
-        znssd_backward_kernel<0><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("znssd_backward", s);
+            znssd_backward_kernel<0><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        }
     else if (mode == 1)
-        znssd_backward_kernel<1><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("znssd_backward", s);
+            znssd_backward_kernel<1><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        }
     else
-        znssd_backward_kernel<2><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        {
+            KTimer kt_("znssd_backward", s);
+            znssd_backward_kernel<2><<<(unsigned)n, ZN_THREADS, 0, s>>>(a);
+        }
     return check_launch("znssd backward");
 }

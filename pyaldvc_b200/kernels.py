@@ -19,6 +19,7 @@ PLAIN = _lib.PLAIN
 NCC_TILED = _lib.NCC_TILED
 NCC_PLAIN = _lib.NCC_PLAIN
 NCC_FFT = _lib.NCC_FFT
+NCC_FFT_STOCKHAM = _lib.NCC_FFT_STOCKHAM
 INTERP_MODE_BY_NAME = {"linear": 0, "cubic": 1, "bspline": 2}
 
 
@@ -235,6 +236,28 @@ def nodal_gradient(grid_shape, spacing, elem_active, U, gauss_order=2) -> torch.
     m = mesh_struct(grid_shape, spacing, elem_active, gauss_order)
     _lib.check(lib().aldvc_nodal_gradient(ctypes.byref(m), _p(U), _p(F), stream_handle()), "aldvc_nodal_gradient")
     return F
+
+
+# --------------------------------------------------------------------------- kernel timing
+def kernel_timing(enable: bool) -> None:
+    """Start (clearing earlier records) or stop the library's per-launch CUDA-event timing of its main kernels."""
+    _lib.check(lib().aldvc_kernel_timing(1 if enable else 0), "aldvc_kernel_timing")
+
+
+def kernel_timing_read(max_entries: int = 64) -> dict:
+    """{kernel name: (total device ms, launches)} of the launches recorded since timing started."""
+    name_len = 48
+    names = ctypes.create_string_buffer(max_entries * name_len)
+    ms = (ctypes.c_double * max_entries)()
+    cnt = (ctypes.c_int64 * max_entries)()
+    n = lib().aldvc_kernel_timing_read(max_entries, names, name_len, ms, cnt)
+    if n < 0:
+        _lib.check(n, "aldvc_kernel_timing_read")
+    out = {}
+    for i in range(min(n, max_entries)):
+        nm = names.raw[i * name_len:(i + 1) * name_len].split(b"\0", 1)[0].decode()
+        out[nm] = (float(ms[i]), int(cnt[i]))
+    return out
 
 
 # --------------------------------------------------------------------------- differentiable ZNSSD residual

@@ -252,6 +252,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         act = torch.arange(mesh.n, device="cuda")
     coords_a = mesh.coords[act].contiguous()
     engine = _ncc_engine(p, half0, rad)
+    ncc_calls = [(int(coords_a.shape[0]), half0, rad, engine)]
     res = K.ncc_search(f, g, coords_a, half0, rad, None, engine)
     disp_a, ok_a, clipped_a = res["disp"], res["ok"] != 0, res["clipped"] != 0
     for _ in range(p.ncc_max_expand if p.ncc_auto_expand else 0):  # integer_search.ncc_search_expanding :486-524
@@ -262,6 +263,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             break
         rad = tuple(2 * r for r in rad)
         idx = torch.nonzero(sel).flatten()
+        ncc_calls.append((int(idx.shape[0]), half0, rad, _ncc_engine(p, half0, rad)))
         sub = K.ncc_search(f, g, coords_a[idx].contiguous(), half0, rad, None, _ncc_engine(p, half0, rad))
         s_ok = sub["ok"] != 0
         if not bool(s_ok.any().item()):
@@ -313,6 +315,9 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                         grid_shape=mesh.grid_shape, valid=valid_b, U_local=U_local, U0=U0, P_local=P, status_local=status,
                         n_iter_local=n_iter)
     result.tracer = tr
+    result.ncc_calls = ncc_calls  # (nodes, half, radius, engine) of every integer search of the pass
+    result.node_half = node_half
+    result.icgn3_iters = []  # n_iter tensors of every 3-DOF pass
     if not p.use_global_step:
         return result
 
@@ -393,7 +398,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                     U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg = admm_static(*a, th3, br3)
                     outs.append((U1g, stg, zcg, itg))
                     a = (U2g, F2g, Wg, vg)
-            entry = {"graph": graph, "static": static, "final": a, "outs": outs[-1]}
+            entry = {"graph": graph, "static": static, "final": a, "outs": outs[-1], "iters": [o[3] for o in outs]}
             _ADMM_GRAPHS[key] = entry
             while len(_ADMM_GRAPHS) > ADMM_GRAPH_CACHE:
                 _ADMM_GRAPHS.pop(next(iter(_ADMM_GRAPHS)))
@@ -406,11 +411,13 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         # the graph's outputs are overwritten by its next replay: the result keeps copies
         U2, F2 = entry["final"][0].clone(), entry["final"][1].clone()
         U1, st_last, zc_last, it_last = (t.clone() for t in entry["outs"])
+        result.icgn3_iters = [t.clone() for t in entry["iters"]]
         steps = p.admm_max_iter
     else:
         for step in range(2, p.admm_max_iter + 1):
             steps = step
             U1n, U2n, F2n, W, v, du_g, st_last, zc_last, it_last = admm_step(U2, F2, W, v, th3, br3)
+            result.icgn3_iters.append(it_last)
             du_l = _rms(U1n - U1_prev)
             U1_prev = U1n
             U1, U2, F2 = U1n, U2n, F2n

@@ -220,15 +220,17 @@ def bead_pair_100():
     return f, g, np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1).astype(np.int64)
 
 
-@pytest.mark.parametrize("radius", [4, 16, 32])
-def test_ncc_fft_engine_matches_tiled_engine_at_large_radius(bead_pair_100, radius):
-    """The FFT engine against the tiled direct engine at the +-16 search of the 1024^2 x 306 workload, its first
-    expansion (+-32, 81-voxel windows) and a small radius: identical integer peaks, ok/clipped flags and FP64
-    re-scored cc."""
+@pytest.mark.parametrize("engine", [2, 3], ids=["fft", "fft_stockham"])
+@pytest.mark.parametrize("radius", [4, 8, 16, 32])
+def test_ncc_fft_engine_matches_tiled_engine_at_large_radius(bead_pair_100, radius, engine):
+    """The FFT engine (in-register transforms where the box is cubic with a compiled length -- 36 at +-8, 50 at
+    +-16 -- and Stockham transforms elsewhere; engine 3 forces Stockham everywhere) against the tiled direct engine
+    at the +-16 search of the 1024^2 x 306 workload, its first expansion (+-32, 81-voxel windows) and small radii:
+    identical integer peaks, ok/clipped flags and FP64 re-scored cc."""
     from pyaldvc_b200.integer_search import ncc_search
 
     f, g, coords = bead_pair_100
     a = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=0)
-    b = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=2)
+    b = ncc_search(f, g, coords, (16, 16, 16), (radius,) * 3, engine=engine)
     assert a["ok"].sum() > 100
     _check_search(b, lambda k: a[k], f"fft vs tiled r{radius}")
