@@ -10,6 +10,7 @@
 //   the winner, quadratic sub-voxel fit -- all on the device, in node chunks through a workspace.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -1626,10 +1627,19 @@ static bool fft_config(const NccGeom& G, FftCfg& c, bool engine_reg = true) {
     return c.smem13 <= smax && c.smem2 <= smax;
 }
 
-constexpr int64_t FFT_BATCH_BYTES = 96LL << 20;  // scratch of one batch: sized to stay in L2
+// scratch of one batch (spectra A and P); ALDVC_FFT_BATCH_MB overrides it (a tuning knob, read once)
+constexpr int64_t FFT_BATCH_BYTES = 1LL << 30;  // larger batches fill the GPU better (measured up to 1.5 GB)
+static int64_t fft_batch_bytes() {
+    static const int64_t b = [] {
+        const char* e = std::getenv("ALDVC_FFT_BATCH_MB");
+        const long v = e ? std::atol(e) : 0;
+        return v > 0 ? (int64_t)v << 20 : FFT_BATCH_BYTES;
+    }();
+    return b;
+}
 
 static int64_t fft_batch(const FftCfg& c, int64_t chunk) {
-    const int64_t b = std::min<int64_t>(chunk, FFT_BATCH_BYTES / std::max<int64_t>(c.per_node, 1));
+    const int64_t b = std::min<int64_t>(chunk, fft_batch_bytes() / std::max<int64_t>(c.per_node, 1));
     return std::max<int64_t>(1, std::min<int64_t>(b, 65535));  // grid y limit
 }
 
@@ -1777,7 +1787,7 @@ static int check_geom(const NccGeom& G) {
 
 static int64_t search_chunk(const NccGeom& G, int64_t n) {
     const int64_t per = (int64_t)G.nmap * 4;
-    int64_t c = (256LL << 20) / std::max<int64_t>(per, 1);
+    int64_t c = (512LL << 20) / std::max<int64_t>(per, 1);  // maps of one chunk: 512 MB
     c = std::max<int64_t>(1, std::min<int64_t>(c, n));
     return c;
 }
