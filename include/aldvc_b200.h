@@ -28,6 +28,11 @@
  *                        with a hand-written gradient)
  *   aldvc_gradients   <- io/volume_ops.py:124 _gradient_stencil7
  *   aldvc_normalize   <- io/volume_ops.py:105 normalize_volume (whole volume)
+ *   aldvc_sep_filter  <- io/volume_ops.py:215 prefilter_bspline (scipy spline_filter, order 3,
+ *                        mirror) and :200 presmooth_volume (scipy gaussian_filter, nearest),
+ *                        one axis per call
+ *   aldvc_mask_fill   <- io/volume_ops.py:225 prepare_deformed (masked voxels -> NaN) and the
+ *                        NCC input of core/pipeline.py:260-262 (masked voxels -> 0)
  *   aldvc_inpaint     <- utils/inpaint.py:35 fill_nan_grid ("spring" model, no cut mesh)
  *   aldvc_median_test <- utils/outlier_detection.py:135 universal_median_test (no cut mesh)
  *   aldvc_render_beads   synthetic Gaussian-bead volumes (inputs of the benchmark configurations;
@@ -143,6 +148,18 @@ int aldvc_gradients(const float *f, int64_t nz, int64_t ny, int64_t nx, int32_t 
 size_t aldvc_normalize_workspace_size(void);
 int aldvc_normalize(const void *vol, int32_t is_uint16, int64_t n_voxels, double pilot, float *out, double *stats,
                     void *workspace, size_t workspace_bytes, void *stream);
+
+/* One axis (0 = x, 1 = y, 2 = z) of a symmetric FIR over a float32 volume:
+ *   out[k] = w[0] s[k] + sum_{j=1..half_taps} w[j] (s[k-j] + s[k+j])
+ * FP64 products and sums in that order (no fused multiply-add), rounded to float32.  boundary 0 = mirror
+ * (period 2n - 2; a line of one sample is copied), 1 = nearest.  weights: HOST array of half_taps + 1
+ * doubles, half_taps <= 63.  in != out; nz, ny <= 65535.  The cubic B-spline prefilter is the three axes
+ * z, y, x in turn with w[j] = sqrt(3) (sqrt(3) - 2)^j, half_taps 32, mirror. */
+int aldvc_sep_filter(const float *in, float *out, int64_t nz, int64_t ny, int64_t nx, int32_t axis, const double *weights,
+                     int32_t half_taps, int32_t boundary, void *stream);
+
+/* vol[i] = value wherever mask[i] == 0 (mask: uint8, same voxel count) */
+int aldvc_mask_fill(float *vol, const uint8_t *mask, int64_t n_voxels, float value, void *stream);
 
 /* adds peak * exp(-|x - c|^2 / (2 sigma^2)) of every bead (centres (B,3) [z,y,x]) within `radius`
  * voxels into the FP64 accumulator volume (nz, ny, nx) */

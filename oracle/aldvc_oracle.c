@@ -1026,3 +1026,46 @@ void orc_znssd(const float *f, const float *g, int64_t nz, int64_t ny, int64_t n
         free(gbuf);
     }
 }
+
+/* ---------------------------------------------------------------- separable volume filters
+ * The two whole-volume filters the reference runs before the local step, both scipy.ndimage calls
+ * (scipy >= 1.10 per the reference's pyproject; 1.18.1 here), restated as one symmetric FIR along
+ * one axis with FP64 accumulation and float32 output per axis:
+ *   io/volume_ops.py:215-222 prefilter_bspline = spline_filter(order 3, mode "mirror"): the inverse of
+ *     the cubic B-spline sampling filter (z + 4 + 1/z) / 6 on the mirror-symmetric extension of each line,
+ *     whose impulse response is sqrt(3) z^|j|, z = sqrt(3) - 2 (Unser, Aldroubi & Eden, IEEE TSP 1993);
+ *     |z|^33 < 2e-19, so 32 taps each side reach FP64 resolution;
+ *   io/volume_ops.py:200-212 presmooth_volume = gaussian_filter(mode "nearest"): the normalised Gaussian
+ *     of radius int(4 sigma + 0.5), edge samples repeated.
+ * out[k] = w[0] s[k] + sum_{j=1..J} w[j] (s[k-j] + s[k+j]) in that order, no fused multiply-add. */
+static inline int64_t reflect_index(int64_t k, int64_t n, int boundary) {
+    if (boundary == 1) return k < 0 ? 0 : (k >= n ? n - 1 : k); /* nearest */
+    if (n == 1) return 0;
+    const int64_t p = 2 * n - 2; /* mirror: period 2n - 2, edge samples not repeated */
+    k %= p;
+    if (k < 0) k += p;
+    return k < n ? k : p - k;
+}
+
+void orc_sep_filter(const float *in, float *out, int64_t nz, int64_t ny, int64_t nx, int axis, const double *w, int J,
+                    int boundary) {
+    const int64_t n = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const int64_t stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
+    const int64_t total = nz * ny * nx;
+    if (boundary == 0 && n == 1) { /* a mirrored line of one sample is its own coefficient */
+        memcpy(out, in, (size_t)total * sizeof(float));
+        return;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < total; ++i) {
+        const int64_t k = (i / stride) % n;
+        const float *line = in + (i - k * stride);
+        double acc = w[0] * (double)line[k * stride];
+        for (int j = 1; j <= J; ++j) {
+            const double a = (double)line[reflect_index(k - j, n, boundary) * stride];
+            const double b = (double)line[reflect_index(k + j, n, boundary) * stride];
+            acc = acc + w[j] * (a + b);
+        }
+        out[i] = (float)acc;
+    }
+}

@@ -60,6 +60,7 @@ def lib():
                                 _D, _D, _D, _I, _I, _D, _D, _I, _P, _P, _I64, _P, _P, _P, _P]
         L.orc_zncc_direct.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]
         L.orc_znssd.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _P, _P]
+        L.orc_sep_filter.argtypes = [_P, _P, _I64, _I64, _I64, _I, _P, _I, _I]
         _lib = L
     return _lib
 
@@ -108,6 +109,54 @@ def znssd(f, g, coords, P, half, mode):
     out = np.empty(coords.shape[0])
     hx, hy, hz = (int(h) for h in half)
     lib().orc_znssd(_ptr(f), _ptr(g), *f.shape, _ptr(coords), coords.shape[0], hx, hy, hz, int(mode), _ptr(P), _ptr(out))
+    return out
+
+
+BSPLINE_POLE = np.sqrt(3.0) - 2.0
+BSPLINE_HALF_TAPS = 32
+
+
+def bspline_weights() -> np.ndarray:
+    """Taps sqrt(3) z^j, j = 0..32, of the cubic B-spline prefilter (the inverse of (z + 4 + 1/z) / 6)."""
+    return np.sqrt(3.0) * BSPLINE_POLE ** np.arange(BSPLINE_HALF_TAPS + 1)
+
+
+def gaussian_weights(sigma: float) -> np.ndarray:
+    """Taps j = 0..r, r = int(4 sigma + 0.5), of the normalised Gaussian (scipy.ndimage.gaussian_filter, truncate 4)."""
+    r = int(4.0 * float(sigma) + 0.5)
+    x = np.arange(-r, r + 1)
+    phi = np.exp(-0.5 / (float(sigma) * float(sigma)) * x**2)
+    phi = phi / phi.sum()
+    return np.ascontiguousarray(phi[r:])
+
+
+def sep_filter(vol, axis, w, boundary):
+    """One axis (0 = x, 1 = y, 2 = z) of a symmetric FIR, FP64 sums, float32 out; boundary 0 mirror, 1 nearest."""
+    v = _f32(vol)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    out = np.empty_like(v)
+    nz, ny, nx = v.shape
+    lib().orc_sep_filter(_ptr(v), _ptr(out), nz, ny, nx, int(axis), _ptr(w), len(w) - 1, int(boundary))
+    return out
+
+
+def prefilter_bspline(vol):
+    """io/volume_ops.py:215-222: cubic B-spline coefficients, mirror boundary.  Axes z, y, x in turn, each rounded
+    to float32, the order in which scipy.ndimage filters array axes 0, 1, 2."""
+    out = _f32(vol)
+    for axis in (2, 1, 0):
+        out = sep_filter(out, axis, bspline_weights(), 0)
+    return out
+
+
+def presmooth_volume(vol, sigma):
+    """io/volume_ops.py:200-212: Gaussian smoothing with edge repeat (axes z, y, x in turn), identity when
+    sigma <= 0."""
+    if sigma is None or sigma <= 0:
+        return _f32(vol)
+    out = _f32(vol)
+    for axis in (2, 1, 0):
+        out = sep_filter(out, axis, gaussian_weights(sigma), 1)
     return out
 
 

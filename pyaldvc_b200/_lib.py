@@ -79,6 +79,8 @@ PROTOTYPES = {
     "aldvc_znssd_backward": (_i32, [ctypes.POINTER(Volumes), _p, _i64, _i32, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p]),
     "aldvc_normalize_workspace_size": (_sz, []),
     "aldvc_normalize": (_i32, [_p, _i32, _i64, _d, _p, _p, _p, _sz, _p]),
+    "aldvc_sep_filter": (_i32, [_p, _p, _i64, _i64, _i64, _i32, _p, _i32, _i32, _p]),
+    "aldvc_mask_fill": (_i32, [_p, _p, _i64, ctypes.c_float, _p]),
     "aldvc_render_beads": (_i32, [_p, _i64, _i64, _i64, _p, _p, _i64, _d, _i32, _p]),
     "aldvc_inpaint_workspace_size": (_sz, [_i64, _i64, _i64, _i32]),
     "aldvc_inpaint": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _d, _i32, _p, _sz, _p, _p, _p]),

@@ -1,5 +1,6 @@
-// Volume preprocessing on the device: whole-volume normalisation (pyALDVC io/volume_ops.py:52-121) and the
-// Gaussian-bead renderer of the synthetic volume pairs.
+// Volume preprocessing on the device: whole-volume normalisation (pyALDVC io/volume_ops.py:52-121), the separable
+// filters run before the local step (B-spline prefilter io/volume_ops.py:215-222, Gaussian presmoothing :200-212),
+// the deformed-frame mask fill (:225-244) and the Gaussian-bead renderer of the synthetic volume pairs.
 #include <algorithm>
 
 #include "common.cuh"
@@ -87,6 +88,89 @@ __global__ void render_beads_kernel(double* acc, int nz, int ny, int nx, const d
     }
 }
 
+// ----------------------------------------------------------------------------- separable symmetric filter
+// out[k] = w[0] s[k] + sum_{j=1..J} w[j] (s[k-j] + s[k+j]) along one axis, FP64 products and sums in that order
+// (no contraction into fused multiply-adds), float32 out.  Boundary 0 "mirror" (period 2n - 2, edge sample not
+// repeated), 1 "nearest" (edge sample repeated).  The B-spline prefilter is this filter with w[j] = sqrt(3) z^j,
+// z = sqrt(3) - 2, J = 32, mirror; the Gaussian presmoothing is the normalised Gaussian with nearest.
+//
+// A CTA filters a tile of SEP_COLS lines x SEP_LEN outputs; the tile's samples, halo included, are staged once in
+// shared memory, so every input is read from HBM about (SEP_LEN + 2J) / SEP_LEN times and every output written
+// once.  For the x axis lanes run along the line (rows of the tile contiguous); for y and z lanes run across 32
+// neighbouring x columns, so every global access is a 128-byte row.
+constexpr int SEP_MAX_HALF = 63;
+constexpr int SEP_COLS = 32;
+constexpr int SEP_LEN = 192;
+constexpr int SEP_THREADS = 256;
+constexpr int SEP_SMEM_FLOATS = (SEP_LEN + 2 * SEP_MAX_HALF) * SEP_COLS;  // 40,704 bytes
+
+struct SepTaps {
+    double w[SEP_MAX_HALF + 1];
+};
+
+__device__ __forceinline__ int64_t sep_reflect(int64_t k, int64_t n, int boundary) {
+    if (boundary == 1) return k < 0 ? 0 : (k >= n ? n - 1 : k);
+    if (n == 1) return 0;
+    const int64_t p = 2 * n - 2;
+    k %= p;
+    if (k < 0) k += p;
+    return k < n ? k : p - k;
+}
+
+__device__ __forceinline__ float sep_apply(const float* t, int step, const SepTaps& w, int J) {
+    double acc = __dmul_rn(w.w[0], (double)t[0]);
+    for (int j = 1; j <= J; ++j) acc = __dadd_rn(acc, __dmul_rn(w.w[j], __dadd_rn((double)t[-j * step], (double)t[j * step])));
+    return (float)acc;
+}
+
+// filter axis x: tile rows are 32 consecutive y of one z plane
+__global__ void __launch_bounds__(SEP_THREADS) sep_filter_x_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                                   int nz, int ny, int nx, SepTaps w, int J, int boundary) {
+    __shared__ float tile[SEP_SMEM_FLOATS];
+    const int A = SEP_LEN + 2 * J;
+    const int x0 = blockIdx.x * SEP_LEN, y0 = blockIdx.y * SEP_COLS, z = blockIdx.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = warp; r < SEP_COLS; r += SEP_THREADS / 32) {
+        const int y = y0 + r;
+        if (y >= ny) break;
+        const float* row = in + ((int64_t)z * ny + y) * nx;
+        for (int a = lane; a < A; a += 32) tile[r * A + a] = __ldg(row + sep_reflect((int64_t)x0 - J + a, nx, boundary));
+    }
+    __syncthreads();
+    for (int r = warp; r < SEP_COLS; r += SEP_THREADS / 32) {
+        const int y = y0 + r;
+        if (y >= ny) break;
+        float* orow = out + ((int64_t)z * ny + y) * nx;
+        for (int o = lane; o < SEP_LEN && x0 + o < nx; o += 32) orow[x0 + o] = sep_apply(tile + r * A + o + J, 1, w, J);
+    }
+}
+
+// filter axis y (AXIS 1) or z (AXIS 2): tile columns are 32 consecutive x
+template <int AXIS>
+__global__ void __launch_bounds__(SEP_THREADS) sep_filter_yz_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                                    int nz, int ny, int nx, SepTaps w, int J, int boundary) {
+    __shared__ float tile[SEP_SMEM_FLOATS];
+    const int A = SEP_LEN + 2 * J;
+    const int n = AXIS == 1 ? ny : nz;
+    const int64_t stride = AXIS == 1 ? (int64_t)nx : (int64_t)nx * ny;
+    const int x0 = blockIdx.x * SEP_COLS, k0 = blockIdx.y * SEP_LEN;
+    const int64_t base = AXIS == 1 ? (int64_t)blockIdx.z * ny * nx : (int64_t)blockIdx.z * nx;  // plane z, or row y
+    const int c = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const bool col_ok = x0 + c < nx;
+    for (int a = ty; a < A; a += SEP_THREADS / 32)
+        tile[a * SEP_COLS + c] = col_ok ? __ldg(in + base + sep_reflect((int64_t)k0 - J + a, n, boundary) * stride + x0 + c) : 0.0f;
+    __syncthreads();
+    if (!col_ok) return;
+    for (int o = ty; o < SEP_LEN && k0 + o < n; o += SEP_THREADS / 32)
+        out[base + (int64_t)(k0 + o) * stride + x0 + c] = sep_apply(tile + (o + J) * SEP_COLS + c, SEP_COLS, w, J);
+}
+
+// deformed-frame mask (io/volume_ops.py:238-243 and the NCC input of core/pipeline.py:260-262): value where mask == 0
+__global__ void mask_fill_kernel(float* __restrict__ v, const uint8_t* __restrict__ mask, int64_t n, float value) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (mask[i] == 0) v[i] = value;
+}
+
 }  // namespace aldvc
 
 using namespace aldvc;
@@ -125,4 +209,43 @@ extern "C" int aldvc_render_beads(double* accum, int64_t nz, int64_t ny, int64_t
     render_beads_kernel<<<(unsigned)n_beads, 256, 0, (cudaStream_t)stream>>>(accum, (int)nz, (int)ny, (int)nx, centres_zyx, peaks,
                                                                                n_beads, 1.0 / (2.0 * sigma * sigma), radius);
     return check_launch("aldvc_render_beads");
+}
+
+extern "C" int aldvc_sep_filter(const float* in, float* out, int64_t nz, int64_t ny, int64_t nx, int32_t axis, const double* weights,
+                                int32_t half_taps, int32_t boundary, void* stream) {
+    ALDVC_REQUIRE(in && out && weights, "aldvc_sep_filter: null pointer");
+    ALDVC_REQUIRE(in != out, "aldvc_sep_filter: in and out must be different buffers");
+    ALDVC_REQUIRE(axis >= 0 && axis <= 2, "aldvc_sep_filter: axis must be 0 (x), 1 (y) or 2 (z)");
+    ALDVC_REQUIRE(half_taps >= 0 && half_taps <= SEP_MAX_HALF, "aldvc_sep_filter: half_taps must be in [0, 63]");
+    ALDVC_REQUIRE(boundary == 0 || boundary == 1, "aldvc_sep_filter: boundary must be 0 (mirror) or 1 (nearest)");
+    ALDVC_REQUIRE(nz > 0 && ny > 0 && nx > 0 && nz <= 65535 && ny <= 65535 && nx < (1 << 30), "aldvc_sep_filter: shape");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    if (boundary == 0 && n == 1) {  // a mirrored line of one sample is its own coefficient
+        cudaError_t e = cudaMemcpyAsync(out, in, (size_t)(nz * ny * nx) * sizeof(float), cudaMemcpyDeviceToDevice, s);
+        return e == cudaSuccess ? ALDVC_OK : cuda_fail(e, "aldvc_sep_filter: copy");
+    }
+    SepTaps w{};
+    for (int j = 0; j <= half_taps; ++j) w.w[j] = weights[j];
+    const int Z = (int)nz, Y = (int)ny, X = (int)nx;
+    KTimer kt_("sep_filter", s);
+    if (axis == 0) {
+        dim3 grid((unsigned)((nx + SEP_LEN - 1) / SEP_LEN), (unsigned)((ny + SEP_COLS - 1) / SEP_COLS), (unsigned)nz);
+        sep_filter_x_kernel<<<grid, SEP_THREADS, 0, s>>>(in, out, Z, Y, X, w, half_taps, boundary);
+    } else if (axis == 1) {
+        dim3 grid((unsigned)((nx + SEP_COLS - 1) / SEP_COLS), (unsigned)((ny + SEP_LEN - 1) / SEP_LEN), (unsigned)nz);
+        sep_filter_yz_kernel<1><<<grid, SEP_THREADS, 0, s>>>(in, out, Z, Y, X, w, half_taps, boundary);
+    } else {
+        dim3 grid((unsigned)((nx + SEP_COLS - 1) / SEP_COLS), (unsigned)((nz + SEP_LEN - 1) / SEP_LEN), (unsigned)ny);
+        sep_filter_yz_kernel<2><<<grid, SEP_THREADS, 0, s>>>(in, out, Z, Y, X, w, half_taps, boundary);
+    }
+    return check_launch("aldvc_sep_filter");
+}
+
+extern "C" int aldvc_mask_fill(float* vol, const uint8_t* mask, int64_t n_voxels, float value, void* stream) {
+    ALDVC_REQUIRE(vol && mask, "aldvc_mask_fill: null pointer");
+    if (n_voxels <= 0) return ALDVC_OK;
+    const int64_t blocks = std::min<int64_t>((n_voxels + 255) / 256, 148 * 16);
+    mask_fill_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vol, mask, n_voxels, value);
+    return check_launch("aldvc_mask_fill");
 }

@@ -315,6 +315,68 @@ def normalize(vol: torch.Tensor, pilot: float | None = None) -> torch.Tensor:
     return out
 
 
+BOUNDARY_MIRROR, BOUNDARY_NEAREST = 0, 1
+BSPLINE_HALF_TAPS = 32
+
+
+def bspline_taps() -> np.ndarray:
+    """Taps sqrt(3) z^j (j = 0..32, z = sqrt(3) - 2) of the cubic B-spline prefilter: the impulse response of the
+    inverse of the sampling filter (z + 4 + 1/z) / 6; |z|^33 < 2e-19, so the tail is below FP64 resolution."""
+    return np.sqrt(3.0) * (np.sqrt(3.0) - 2.0) ** np.arange(BSPLINE_HALF_TAPS + 1)
+
+
+def gaussian_taps(sigma: float) -> np.ndarray:
+    """Taps j = 0..r of the normalised Gaussian of scipy.ndimage.gaussian_filter (radius r = int(4 sigma + 0.5))."""
+    r = int(4.0 * float(sigma) + 0.5)
+    x = np.arange(-r, r + 1)
+    phi = np.exp(-0.5 / (float(sigma) * float(sigma)) * x**2)
+    phi = phi / phi.sum()
+    return np.ascontiguousarray(phi[r:])
+
+
+def sep_filter(vol: torch.Tensor, axis: int, taps, boundary: int, out: torch.Tensor | None = None) -> torch.Tensor:
+    """One axis (0 = x, 1 = y, 2 = z) of the symmetric FIR ``aldvc_sep_filter`` over a float32 CUDA volume."""
+    vol = dev(vol, torch.float32)
+    w = np.ascontiguousarray(taps, dtype=np.float64)
+    if len(w) - 1 > 63:
+        raise ValueError("sep_filter: at most 63 taps each side (Gaussian sigma <= 15.6)")
+    if out is None:
+        out = torch.empty_like(vol)
+    nz, ny, nx = vol.shape
+    _lib.check(lib().aldvc_sep_filter(_p(vol), _p(out), nz, ny, nx, int(axis), w.ctypes.data_as(ctypes.c_void_p), len(w) - 1,
+                                      int(boundary), stream_handle()), "aldvc_sep_filter")
+    return out
+
+
+def _three_axes(vol: torch.Tensor, taps, boundary: int) -> torch.Tensor:
+    # axes z, y, x in turn, each rounded to float32: the order of scipy.ndimage's separable filters
+    a = sep_filter(vol, 2, taps, boundary)
+    b = sep_filter(a, 1, taps, boundary)
+    return sep_filter(b, 0, taps, boundary, out=a)
+
+
+def bspline_prefilter(vol: torch.Tensor) -> torch.Tensor:
+    """Cubic B-spline coefficients of a float32 CUDA volume, mirror boundary (io/volume_ops.py:215-222)."""
+    return _three_axes(vol, bspline_taps(), BOUNDARY_MIRROR)
+
+
+def gaussian_presmooth(vol: torch.Tensor, sigma: float) -> torch.Tensor:
+    """Gaussian smoothing with edge repeat (io/volume_ops.py:200-212); a float32 copy when sigma <= 0."""
+    if sigma is None or sigma <= 0:
+        return dev(vol, torch.float32).clone()
+    return _three_axes(vol, gaussian_taps(sigma), BOUNDARY_NEAREST)
+
+
+def mask_fill(vol: torch.Tensor, mask: torch.Tensor, value: float) -> torch.Tensor:
+    """In place: ``vol[mask == 0] = value`` (float32 volume, uint8/bool mask of the same shape)."""
+    assert vol.is_cuda and vol.is_contiguous() and vol.dtype == torch.float32
+    m = dev(mask.to(torch.uint8) if mask.dtype == torch.bool else mask, torch.uint8)
+    if m.numel() != vol.numel():
+        raise ValueError(f"mask_fill: mask shape {tuple(m.shape)} != volume shape {tuple(vol.shape)}")
+    _lib.check(lib().aldvc_mask_fill(_p(vol), _p(m), vol.numel(), float(value), stream_handle()), "aldvc_mask_fill")
+    return vol
+
+
 def render_beads(accum: torch.Tensor, centres_zyx, peaks, sigma: float, radius: int) -> None:
     """Add Gaussian beads into an FP64 CUDA accumulator volume."""
     c = dev(centres_zyx, torch.float64).reshape(-1, 3)

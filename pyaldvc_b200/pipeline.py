@@ -62,6 +62,7 @@ class PassParams:
     # uneven subsets: coords (N,3) [x, y, z] -> (N,3) even window sizes per node, each <= winsize (which then
     # sets the mesh border and the maximum shape); every shape runs in the same persistent launches
     node_winsize: object = None
+    prefilter_sigma: float = 0.0  # Gaussian pre-smoothing of both volumes after normalisation (0 = off)
 
 
 @dataclass
@@ -200,15 +201,25 @@ def clear_graphs() -> None:
 
 
 def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
-             tracer: Tracer | None = None) -> PassResult:
-    """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16)."""
+             tracer: Tracer | None = None, g_mask: torch.Tensor | None = None) -> PassResult:
+    """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16).  ``mask``: reference-frame
+    material mask; ``g_mask``: deformed-frame mask (False voxels are excluded from every correlation)."""
     tr = tracer if tracer is not None else Tracer(sync=False)
     tr.start()
     f = K.normalize(f_raw) if normalize else f_raw.float().contiguous()
     g = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
-    if p.interp_method == "bspline":
-        raise NotImplementedError("the device pass prefilters no B-spline coefficients; use cubic or linear")
+    if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:197, 257
+        f = K.gaussian_presmooth(f, p.prefilter_sigma)
+        g = K.gaussian_presmooth(g, p.prefilter_sigma)
     mode = K.INTERP_MODE_BY_NAME[p.interp_method]
+    # the array the interpolation samples, and the NCC input (core/pipeline.py:258-262, io/volume_ops.py:225-244)
+    g_prep = K.bspline_prefilter(g) if p.interp_method == "bspline" else g
+    if g_mask is not None:
+        gm = g_mask.to(torch.uint8).contiguous()
+        if g_prep is g:
+            g_prep = g.clone()
+        K.mask_fill(g_prep, gm, float("nan"))
+        g = K.mask_fill(g.clone(), gm, 0.0)
     gx, gy, gz = K.gradients(f)
     mesh = Mesh(f.shape, p)
     m_u8 = None if mask is None else mask.to(torch.uint8).contiguous()
@@ -294,7 +305,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         c, P0_, L_, mf_, v_ = ((mesh.coords, P0, L, meanf, valid_u8) if idx is None else
                                (mesh.coords[idx], P0[idx], L[idx], meanf[idx], valid_u8[idx]))
         nh = node_half if (node_half is None or idx is None) else node_half[idx]
-        return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
+        return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g_prep, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
                         p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
                         node_half=nh)
 
@@ -324,7 +335,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     # ---------------- sections 5-6: ADMM (pipeline.py:286-352) with fixed beta
     n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
     # every tensor the ADMM loop reads; a captured loop reads static copies of them
-    T = {"f": f, "g": g, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
+    T = {"f": f, "g": g_prep, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
          "coords": mesh.coords, "elem": elem_active, "node_half": node_half}
 
     def make_steps(T):

@@ -26,7 +26,7 @@ os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
 
 from al_dvc.core.config import dvcpara_default  # noqa: E402
 from al_dvc.core.data_structures import P_from_UF  # noqa: E402
-from al_dvc.io.volume_ops import compute_gradients, normalize_volume, prefilter_bspline  # noqa: E402
+from al_dvc.io.volume_ops import compute_gradients, normalize_volume, prefilter_bspline, presmooth_volume  # noqa: E402
 from al_dvc.mesh.grid_mesh import build_grid_axes as ref_grid_axes  # noqa: E402
 from al_dvc.mesh.grid_mesh import mesh_setup  # noqa: E402
 from al_dvc.solver import integer_search as ris  # noqa: E402
@@ -250,5 +250,21 @@ def main():
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+def volume_ops_fixtures():
+    """The reference's whole-volume filters on a bead volume whose x lines are longer than one device tile (197)
+    and whose z lines are short (10), plus a 5 x 3 x 2 volume of lines of 1, 2, 3 and 5 samples."""
+    shape = (10, 17, 197)
+    pair = syn.bead_pair(shape, density=0.03, sigma=1.5, seed=21, disp=syn.translation((0.0, 0.0, 0.0)), noise=0.01)
+    v = normalize_volume(pair.f)
+    small = np.random.default_rng(22).normal(0.0, 1.0, (5, 3, 2)).astype(np.float32)
+    out = {"vol": v, "bspline": prefilter_bspline(v), "gauss_0.8": presmooth_volume(v, 0.8),
+           "gauss_2.0": presmooth_volume(v, 2.0), "small": small, "small_bspline": prefilter_bspline(small),
+           "small_gauss_1.0": presmooth_volume(small, 1.0)}
+    path = os.path.join(HERE, "golden_volume_ops.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 if __name__ == "__main__":
     main()
+    volume_ops_fixtures()
