@@ -265,6 +265,38 @@ __device__ double warp_rescore(const float* tp, int64_t tsz, int64_t tsy, const 
     return v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v);
 }
 
+// warp_rescore over a template staged contiguously in shared memory, with the (k, j, i) coordinates of every
+// template voxel packed in kji[t] (k << 20 | j << 10 | i): the loads of successive voxels do not wait on one
+// another's index arithmetic, so a lane keeps several window loads in flight.  Same per-lane order and reduction
+// as warp_rescore, hence the same value.  GLOBAL: the window is in global memory (read through the
+// non-coherent path); otherwise in shared memory.
+template <bool GLOBAL>
+__device__ double warp_rescore_tab(const float* tp, const uint32_t* kji, const float* wp, int64_t wsz, int64_t wsy, int n_tpl,
+                                   double mf, double ssf) {
+    const int lane = threadIdx.x & 31;
+    double sfg = 0.0, sg = 0.0, sgg = 0.0;
+#pragma unroll 4
+    for (int t = lane; t < n_tpl; t += 32) {
+        const uint32_t c = kji[t];
+        const float fv = tp[t];
+        const int64_t o = (int64_t)(c >> 20) * wsz + (int64_t)((c >> 10) & 1023u) * wsy + (int64_t)(c & 1023u);
+        const float v = GLOBAL ? __ldg(wp + o) : wp[o];
+        sfg += ((double)fv - mf) * (double)v;
+        sg += (double)v;
+        sgg += (double)(v * v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sfg += __shfl_xor_sync(0xffffffffu, sfg, o);
+        sg += __shfl_xor_sync(0xffffffffu, sg, o);
+        sgg += __shfl_xor_sync(0xffffffffu, sgg, o);
+    }
+    const double var = sgg - sg * sg / (double)n_tpl;
+    if (var < 1e-20) return 0.0;
+    const double v = sfg / sqrt(var * ssf);
+    return v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v);
+}
+
 // One CTA per node of the chunk.  Two sweeps of the FP32 map: (1) maximum (first index on ties), minimum;
 // (2) candidates within NEAR_TIE of the maximum and the PCE energy.  The template (raw FP32 f) and, for the
 // sub-voxel fit, the window box around the peak are staged in shared memory when SMEM; each FP64 re-score is
@@ -279,6 +311,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     __shared__ double s_cval[MAX_CAND];
     __shared__ int s_ncand;
     __shared__ double s_neigh[27];
+    __shared__ double s_coef[10];
     __shared__ float s_max, s_min;
     __shared__ int s_pk;
     const NccGeom& G = a.G;
@@ -302,14 +335,21 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     const bool flat = map[0] < -1.5f;
     float best = -3.0f, mn = 3.0f;
     int bidx = 0x7fffffff;
-    for (int i = tid; i < G.nmap; i += blockDim.x) {
-        float v = map[i];
-        v = v < -1.0f ? 0.0f : v;
-        if (v > best) {  // ascending i per thread: the first index wins a tie
-            best = v;
-            bidx = i;
+    // four loads in flight per thread, then the compares in ascending i (the first index wins a tie)
+    for (int i0 = tid; i0 < G.nmap; i0 += 4 * NCC_THREADS) {
+        float vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) vv[u] = i0 + u * NCC_THREADS < G.nmap ? map[i0 + u * NCC_THREADS] : -3.0f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * NCC_THREADS >= G.nmap) break;
+            const float v = vv[u] < -1.0f ? 0.0f : vv[u];
+            if (v > best) {
+                best = v;
+                bidx = i0 + u * NCC_THREADS;
+            }
+            mn = fminf(mn, v);
         }
-        mn = fminf(mn, v);
     }
     for (int o = 16; o > 0; o >>= 1) {
         const float ob = __shfl_xor_sync(0xffffffffu, best, o);
@@ -347,15 +387,22 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     // candidates within the FP32 error bound of the maximum, and the PCE energy on the min-shifted map
     // (integer_search.py:448-452)
     double e = 0.0;
-    for (int i = tid; i < G.nmap; i += blockDim.x) {
-        float v = map[i];
-        v = v < -1.0f ? 0.0f : v;
-        if (!flat && v >= vmax - NEAR_TIE) {
-            const int slot = atomicAdd(&s_ncand, 1);
-            if (slot < MAX_CAND) s_cand[slot] = i;
+    for (int i0 = tid; i0 < G.nmap; i0 += 4 * NCC_THREADS) {
+        float vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) vv[u] = i0 + u * NCC_THREADS < G.nmap ? map[i0 + u * NCC_THREADS] : 0.0f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * NCC_THREADS;
+            if (i >= G.nmap) break;
+            const float v = vv[u] < -1.0f ? 0.0f : vv[u];
+            if (!flat && v >= vmax - NEAR_TIE) {
+                const int slot = atomicAdd(&s_ncand, 1);
+                if (slot < MAX_CAND) s_cand[slot] = i;
+            }
+            const double dv = (double)v - (double)cmin;
+            e += dv * dv;
         }
-        const double dv = (double)v - (double)cmin;
-        e += dv * dv;
     }
     e = block_sum_d(e, red) / (double)G.nmap;
     // template: raw FP32 f (staged when SMEM), FP64 mean and sum of squares (integer_search.py:73-88)
@@ -363,12 +410,18 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     const float* fg = a.f + (z0 - G.hz) * sxy + (y0 - G.hy) * G.nx + (x0 - G.hx);
     const int64_t tsz = SMEM ? (int64_t)G.sy * G.sx : sxy, tsy = SMEM ? G.sx : G.nx;
     const float* tp = SMEM ? psm : fg;
+    // shared layout: template (n_tpl floats), neighbour box ((sx+2)(sy+2)(sz+2) floats), packed template
+    // coordinates (n_tpl words)
+    uint32_t* kji = reinterpret_cast<uint32_t*>(psm + G.n_tpl + (G.sx + 2) * (G.sy + 2) * (G.sz + 2));
     double sf = 0.0;
     for (int r = warp; r < G.sz * G.sy; r += NW) {
         const int k = r / G.sy, j = r - k * G.sy;
         for (int ii = lane; ii < G.sx; ii += 32) {
             const float v = __ldg(fg + k * sxy + (int64_t)j * G.nx + ii);
-            if (SMEM) psm[(k * G.sy + j) * G.sx + ii] = v;
+            if (SMEM) {
+                psm[(k * G.sy + j) * G.sx + ii] = v;
+                kji[(k * G.sy + j) * G.sx + ii] = ((uint32_t)k << 20) | ((uint32_t)j << 10) | (uint32_t)ii;
+            }
             sf += (double)v;
         }
     }
@@ -405,7 +458,8 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             const int i = s_cand[c];
             const int dz = i / (G.vy * G.vx), r = i - dz * G.vy * G.vx, dy = r / G.vx, dx = r - dy * G.vx;
             const float* wp = a.g + (wz0 + dz) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
-            const double v = warp_rescore(tp, tsz, tsy, wp, sxy, G.nx, G, mf, ssf);
+            const double v = SMEM ? warp_rescore_tab<true>(tp, kji, wp, sxy, G.nx, G.n_tpl, mf, ssf)
+                                  : warp_rescore(tp, tsz, tsy, wp, sxy, G.nx, G, mf, ssf);
             if (lane == 0) s_cval[c] = v;
         }
         __syncthreads();
@@ -446,20 +500,22 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             if (t == 13) {
                 v = peak;
             } else if (SMEM) {
-                v = warp_rescore(tp, tsz, tsy, box + (dzz * BY + dyy) * BX + dxx, (int64_t)BY * BX, BX, G, mf, ssf);
+                v = warp_rescore_tab<false>(tp, kji, box + (dzz * BY + dyy) * BX + dxx, (int64_t)BY * BX, BX, G.n_tpl, mf, ssf);
             } else {
                 v = warp_rescore(tp, tsz, tsy, gb + dzz * sxy + (int64_t)dyy * G.nx + dxx, sxy, G.nx, G, mf, ssf);
             }
             if (lane == 0) s_neigh[t] = v;
         }
         __syncthreads();
+        if (tid < 10) {  // one coefficient per thread, the same sum order as a serial loop
+            double s = 0.0;
+            for (int t = 0; t < 27; ++t) s += c_pinv[tid * 27 + t] * s_neigh[t];
+            s_coef[tid] = s;
+        }
+        __syncthreads();
         if (tid == 0) {
             double coef[10];
-            for (int r = 0; r < 10; ++r) {
-                double s = 0.0;
-                for (int t = 0; t < 27; ++t) s += c_pinv[r * 27 + t] * s_neigh[t];
-                coef[r] = s;
-            }
+            for (int r = 0; r < 10; ++r) coef[r] = s_coef[r];
             double H[3][3] = {{2 * coef[7], coef[4], coef[5]}, {coef[4], 2 * coef[8], coef[6]}, {coef[5], coef[6], 2 * coef[9]}};
             double Hi[3][3];
             const double det = inv3(H, Hi);
@@ -498,9 +554,11 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     }
 }
 
-// shared bytes of the staged peak kernel (template + neighbour box), 0 when it does not fit
+// shared bytes of the staged peak kernel (template, neighbour box, packed template coordinates), 0 when it does
+// not fit or a template side does not fit the 10-bit coordinate fields
 static size_t peak_smem(const NccGeom& G) {
-    const size_t b = ((size_t)G.n_tpl + (size_t)(G.sx + 2) * (G.sy + 2) * (G.sz + 2)) * sizeof(float);
+    if (G.sx >= 1024 || G.sy >= 1024 || G.sz >= 1024) return 0;
+    const size_t b = ((size_t)2 * G.n_tpl + (size_t)(G.sx + 2) * (G.sy + 2) * (G.sz + 2)) * sizeof(float);
     return b <= 160 * 1024 ? b : 0;
 }
 

@@ -32,8 +32,13 @@ def main(argv=None) -> None:
     n, h, r = args.size, args.half, args.radius
     shape = (n, n, n)
     c, pk = S.draw_beads(shape, 0.03, 5)
-    f = torch.from_numpy(S.render_beads(shape, c, pk, 1.5)).cuda()
-    g = torch.from_numpy(S.render_beads(shape, S.displace_beads(c, S.translation((1.3, -2.4, 3.1))), pk, 1.5)).cuda()
+    vols = []
+    for cc in (c, S.displace_beads(c, S.translation((1.3, -2.4, 3.1)))):  # rendered on the device (FP64 sums)
+        acc = torch.zeros(shape, dtype=torch.float64, device="cuda")
+        K.render_beads(acc, cc, pk, 1.5, 6)
+        vols.append(acc.float().contiguous())
+        del acc
+    f, g = vols
     m = h + r + 2
     ax = np.arange(m, n - m, 12)
     zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
