@@ -31,6 +31,11 @@
  *   aldvc_sep_filter  <- io/volume_ops.py:215 prefilter_bspline (scipy spline_filter, order 3,
  *                        mirror) and :200 presmooth_volume (scipy gaussian_filter, nearest),
  *                        one axis per call
+ *   aldvc_volume_stats / aldvc_normalize_voi <- io/volume_ops.py:74 voi_mean_std,
+ *                        :105 normalize_volume with a VOI box
+ *   aldvc_block_downsample <- solver/integer_search.py:235 block_downsample
+ *   aldvc_phase_correlation <- solver/integer_search.py:247 phase_correlation_shift (after the
+ *                        VOI crop and the block downsampling, which the caller does)
  *   aldvc_mask_fill   <- io/volume_ops.py:225 prepare_deformed (masked voxels -> NaN) and the
  *                        NCC input of core/pipeline.py:260-262 (masked voxels -> 0)
  *   aldvc_inpaint     <- utils/inpaint.py:35 fill_nan_grid ("spring" model, no cut mesh)
@@ -157,6 +162,28 @@ int aldvc_normalize(const void *vol, int32_t is_uint16, int64_t n_voxels, double
  * z, y, x in turn with w[j] = sqrt(3) (sqrt(3) - 2)^j, half_taps 32, mirror. */
 int aldvc_sep_filter(const float *in, float *out, int64_t nz, int64_t ny, int64_t nx, int32_t axis, const double *weights,
                      int32_t half_taps, int32_t boundary, void *stream);
+
+/* Mean and population standard deviation (device stats[2], FP64) of the float32 (is_uint16 == 0) or uint16
+ * volume over the box[6] = {z0, z1, y0, y1, x0, x1} (host array, half-open; NULL = whole volume), moments
+ * taken relative to `pilot` (the reference uses the box's centre voxel). */
+size_t aldvc_stats_workspace_size(void);
+int aldvc_volume_stats(const void *vol, int32_t is_uint16, int64_t nz, int64_t ny, int64_t nx, const int64_t *box, double pilot,
+                       double *stats, void *workspace, size_t workspace_bytes, void *stream);
+/* aldvc_volume_stats over the box, then (v - mean) / std over the WHOLE volume into out (std < 1e-12 -> 1) */
+int aldvc_normalize_voi(const void *vol, int32_t is_uint16, int64_t nz, int64_t ny, int64_t nx, const int64_t *box, double pilot,
+                        float *out, double *stats, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Block means of factor^3 voxels (FP64 sums, float32 out); out is (nz/factor, ny/factor, nx/factor), the
+ * trailing voxels of each axis dropped. */
+int aldvc_block_downsample(const float *in, int64_t nz, int64_t ny, int64_t nx, int32_t factor, float *out, void *stream);
+
+/* Phase correlation of two equal-shape float32 volumes (each axis <= 1024): both centred on their mean and
+ * multiplied by a separable Hann window, cross-power spectrum G conj(F) / |G conj(F)|, inverse transform; peak
+ * (device int64) receives the flat C-order index of the first maximum of its real part.  The shift along an
+ * axis of length n is the peak coordinate p, or p - n when p > n / 2.  Transforms are direct FP64 DFTs. */
+size_t aldvc_phase_correlation_workspace_size(int64_t nz, int64_t ny, int64_t nx);
+int aldvc_phase_correlation(const float *fs, const float *gs, int64_t nz, int64_t ny, int64_t nx, int64_t *peak, void *workspace,
+                            size_t workspace_bytes, void *stream);
 
 /* vol[i] = value wherever mask[i] == 0 (mask: uint8, same voxel count) */
 int aldvc_mask_fill(float *vol, const uint8_t *mask, int64_t n_voxels, float value, void *stream);

@@ -160,6 +160,47 @@ def presmooth_volume(vol, sigma):
     return out
 
 
+def block_downsample(vol, factor):
+    """integer_search.py:235-244: block means of factor^3 voxels (trailing voxels dropped), FP64 sums, float32."""
+    v = np.asarray(vol, dtype=np.float32)
+    if factor <= 1:
+        return v.copy()
+    nz, ny, nx = (s // factor * factor for s in v.shape)
+    b = v[:nz, :ny, :nx].astype(np.float64).reshape(nz // factor, factor, ny // factor, factor, nx // factor, factor)
+    return (b.sum(axis=(1, 3, 5)) / float(factor**3)).astype(np.float32)
+
+
+def phase_correlation_shift(f, g, max_dim=128):
+    """integer_search.py:247-291 without a VOI: block means until no axis exceeds max_dim, centring and a separable
+    Hann window in float32, then the cross-power spectrum and its inverse in complex128; the first maximum,
+    wrapped to (-n/2, n/2] and scaled back, as (dx, dy, dz)."""
+    import math
+
+    f = np.asarray(f, dtype=np.float32)
+    g = np.asarray(g, dtype=np.float32)
+    factor = max(1, int(math.ceil(max(f.shape) / max_dim)))
+    fs, gs = block_downsample(f, factor), block_downsample(g, factor)
+    fs = fs - np.float32(fs.astype(np.float64).mean())
+    gs = gs - np.float32(gs.astype(np.float64).mean())
+    win = np.ones(fs.shape, dtype=np.float32)
+    for ax, n in enumerate(fs.shape):
+        shape = [1, 1, 1]
+        shape[ax] = n
+        win = win * np.hanning(n).astype(np.float32).reshape(shape)
+    Ff = np.fft.fftn((fs * win).astype(np.float64))
+    Fg = np.fft.fftn((gs * win).astype(np.float64))
+    R = Fg * np.conj(Ff)
+    mag = np.abs(R)
+    R = R / np.where(mag > 1e-12, mag, 1.0)
+    r = np.real(np.fft.ifftn(R))
+    shift = np.array(np.unravel_index(int(np.argmax(r)), r.shape), dtype=np.float64)
+    for ax, n in enumerate(r.shape):
+        if shift[ax] > n // 2:
+            shift[ax] -= n
+    dz, dy, dx = shift * factor
+    return np.array([dx, dy, dz], dtype=np.float64)
+
+
 def sample_points(vol, zs, ys, xs, mode):
     """interp_kernels.sample_points (:139-152)."""
     vol = _f32(vol)

@@ -39,6 +39,10 @@ def params(cfg: int, **over) -> PassParams:
                        beta=1e-3, mu=1e-3, admm_max_iter=3)
     else:
         raise ValueError(f"no configuration {cfg}")
+    # every configuration seeds IC-GN from one full-resolution NCC search of the stated radius, with no global
+    # phase-correlation pre-shift (the reference's defaults are the pyramid search and the pre-shift)
+    p.init_guess_method = "ncc"
+    p.global_shift = False
     for k, v in over.items():
         setattr(p, k, v)
     return p

@@ -315,6 +315,86 @@ def normalize(vol: torch.Tensor, pilot: float | None = None) -> torch.Tensor:
     return out
 
 
+def _vol_kind(vol: torch.Tensor) -> int:
+    if vol.dtype == torch.uint16:
+        return 1
+    if vol.dtype == torch.float32:
+        return 0
+    raise TypeError("float32 or uint16 volume expected")
+
+
+def _box(box):
+    if box is None:
+        return None
+    b = (ctypes.c_int64 * 6)(*(int(v) for v in box))
+    return ctypes.cast(b, ctypes.c_void_p), b  # keep the array alive with the pointer
+
+
+def _box_pilot(vol: torch.Tensor, box) -> float:
+    """The reference's pilot value: the centre voxel of the box (io/volume_ops.py:86)."""
+    nz, ny, nx = vol.shape
+    z0, z1, y0, y1, x0, x1 = box if box is not None else (0, nz, 0, ny, 0, nx)
+    return float(vol[(z0 + z1) // 2, (y0 + y1) // 2, (x0 + x1) // 2].item())
+
+
+def volume_stats(vol: torch.Tensor, box=None, pilot: float | None = None) -> torch.Tensor:
+    """(mean, population std) FP64 device tensor of a float32/uint16 CUDA volume over ``box`` =
+    (z0, z1, y0, y1, x0, x1) half-open (None: whole volume)."""
+    assert vol.is_cuda and vol.is_contiguous()
+    kind = _vol_kind(vol)
+    if pilot is None:
+        pilot = _box_pilot(vol, box)
+    stats = torch.empty(2, dtype=torch.float64, device=vol.device)
+    ws = _workspace(lib().aldvc_stats_workspace_size())
+    bp = _box(box)
+    nz, ny, nx = vol.shape
+    _lib.check(lib().aldvc_volume_stats(_p(vol), kind, nz, ny, nx, None if bp is None else bp[0], float(pilot), _p(stats), _p(ws),
+                                        ws.numel(), stream_handle()), "aldvc_volume_stats")
+    return stats
+
+
+def normalize_voi(vol: torch.Tensor, box, pilot: float | None = None):
+    """(v - mean) / std of the whole volume with the statistics of ``box``; returns (float32 volume, stats)."""
+    assert vol.is_cuda and vol.is_contiguous()
+    kind = _vol_kind(vol)
+    if pilot is None:
+        pilot = _box_pilot(vol, box)
+    out = torch.empty(vol.shape, dtype=torch.float32, device=vol.device)
+    stats = torch.empty(2, dtype=torch.float64, device=vol.device)
+    ws = _workspace(lib().aldvc_stats_workspace_size())
+    bp = _box(box)
+    nz, ny, nx = vol.shape
+    _lib.check(lib().aldvc_normalize_voi(_p(vol), kind, nz, ny, nx, None if bp is None else bp[0], float(pilot), _p(out), _p(stats),
+                                         _p(ws), ws.numel(), stream_handle()), "aldvc_normalize_voi")
+    return out, stats
+
+
+def block_downsample(vol: torch.Tensor, factor: int) -> torch.Tensor:
+    """Block means of ``factor``^3 voxels (trailing voxels dropped); ``factor <= 1`` returns a float32 copy."""
+    vol = dev(vol, torch.float32)
+    if factor <= 1:
+        return vol.clone()
+    nz, ny, nx = vol.shape
+    out = torch.empty((nz // factor, ny // factor, nx // factor), dtype=torch.float32, device=vol.device)
+    _lib.check(lib().aldvc_block_downsample(_p(vol), nz, ny, nx, int(factor), _p(out), stream_handle()), "aldvc_block_downsample")
+    return out
+
+
+def phase_correlation_peak(fs: torch.Tensor, gs: torch.Tensor) -> tuple:
+    """(pz, py, px): the first maximum of the phase-correlation surface of two equal-shape float32 CUDA volumes."""
+    fs = dev(fs, torch.float32)
+    gs = dev(gs, torch.float32)
+    if fs.shape != gs.shape:
+        raise ValueError("phase correlation: the volumes differ in shape")
+    nz, ny, nx = fs.shape
+    ws = _workspace(lib().aldvc_phase_correlation_workspace_size(nz, ny, nx))
+    peak = torch.empty(1, dtype=torch.int64, device=fs.device)
+    _lib.check(lib().aldvc_phase_correlation(_p(fs), _p(gs), nz, ny, nx, _p(peak), _p(ws), ws.numel(), stream_handle()),
+               "aldvc_phase_correlation")
+    i = int(peak.item())
+    return i // (ny * nx), (i // nx) % ny, i % nx
+
+
 BOUNDARY_MIRROR, BOUNDARY_NEAREST = 0, 1
 BSPLINE_HALF_TAPS = 32
 

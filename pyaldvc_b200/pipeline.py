@@ -17,6 +17,7 @@ import numpy as np
 import torch
 
 from . import autotune
+from . import integer_search as IS
 from . import kernels as K
 from .mesh import build_grid_axes, grid_coords
 
@@ -63,6 +64,13 @@ class PassParams:
     # sets the mesh border and the maximum shape); every shape runs in the same persistent launches
     node_winsize: object = None
     prefilter_sigma: float = 0.0  # Gaussian pre-smoothing of both volumes after normalisation (0 = off)
+    # initial guess (core/config.py:61-71): "pyramid" (coarse-to-fine NCC), "ncc" (one full-resolution search)
+    # or "zero"; an optional global phase-correlation pre-shift
+    init_guess_method: str = "pyramid"
+    global_shift: bool = True
+    pyramid_levels: int = 0  # 0: automatic
+    pyramid_fine_radius: int = 2
+    init_min_pce: float = 0.0
 
 
 @dataclass
@@ -236,6 +244,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     H, L, meanf, bottomf, n_valid, valid = K.precompute(mesh.coords, mesh.half, f, gx, gy, gz, m_u8, p.min_valid_ratio,
                                                         p.hessian_cond_max, p.subset_stride, None, None, node_half)
     valid_b = valid != 0
+    node_valid = torch.ones(mesh.n, dtype=torch.bool, device="cuda")  # apply_mask_to_mesh's node_valid (all without a mask)
     if mask is not None:  # apply_mask_to_mesh (grid_mesh.py:191-253): centre in the mask, enough of the subset in it
         c = mesh.coords
         centre_ok = m_u8[c[:, 2], c[:, 1], c[:, 0]] != 0
@@ -254,47 +263,54 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     valid_u8 = valid_b.to(torch.uint8).contiguous()
     tr.mark("precompute")
 
-    # ---------------- section 3: initial guess (init_disp.compute_initial_guess "ncc" :110-140)
+    # ---------------- section 3: initial guess (init_disp.compute_initial_guess :53-140, clean_initial_guess :143-189)
     subset0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
     half0 = tuple(int(w) // 2 for w in subset0)
     rad = tuple(int(r) for r in p.search_radius)
-    act = torch.nonzero(valid_b).flatten()
-    if act.numel() == 0:
-        act = torch.arange(mesh.n, device="cuda")
-    coords_a = mesh.coords[act].contiguous()
-    engine = _ncc_engine(p, half0, rad)
-    ncc_calls = [(int(coords_a.shape[0]), half0, rad, engine)]
-    res = K.ncc_search(f, g, coords_a, half0, rad, None, engine)
-    disp_a, ok_a, clipped_a = res["disp"], res["ok"] != 0, res["clipped"] != 0
-    for _ in range(p.ncc_max_expand if p.ncc_auto_expand else 0):  # integer_search.ncc_search_expanding :486-524
-        sel = clipped_a & ok_a
-        n_ok = int(ok_a.sum().item())
-        n_sel = int(sel.sum().item())
-        if n_ok == 0 or n_sel <= 0.05 * n_ok:
-            break
-        rad = tuple(2 * r for r in rad)
-        idx = torch.nonzero(sel).flatten()
-        ncc_calls.append((int(idx.shape[0]), half0, rad, _ncc_engine(p, half0, rad)))
-        sub = K.ncc_search(f, g, coords_a[idx].contiguous(), half0, rad, None, _ncc_engine(p, half0, rad))
-        s_ok = sub["ok"] != 0
-        if not bool(s_ok.any().item()):
-            break
-        take = idx[s_ok]
-        disp_a[take] = sub["disp"][s_ok]
-        ok_a[take] = True
-        clipped_a[take] = sub["clipped"][s_ok] != 0
-    disp = torch.full((mesh.n, 3), float("nan"), dtype=torch.float64, device="cuda")
-    ok = torch.zeros(mesh.n, dtype=torch.bool, device="cuda")
-    disp[act] = disp_a
-    ok[act] = ok_a
-    # clean_initial_guess (init_disp.py:143-189)
-    bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~valid_b
-    good = ~bad
-    flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), good, mesh.grid_shape, p.init_outlier_threshold)
-    bad = bad | flag
-    U0, all_bad = _fill(disp, bad, mesh.grid_shape)
-    if bool(all_bad.item()):
-        U0.zero_()
+    ncc_calls: list = []
+    engine_of = lambda h, r: _ncc_engine(p, h, r)  # noqa: E731
+    if p.init_guess_method not in ("pyramid", "ncc", "zero", "previous"):
+        raise ValueError(f"unknown init_guess_method {p.init_guess_method!r}")
+    if p.init_guess_method == "zero":
+        U0 = torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda")
+        init_info = {"method": "zero"}
+    else:
+        shift = IS.phase_correlation_shift_device(f, g) if p.global_shift else None
+        if p.init_guess_method in ("pyramid", "previous"):  # "previous" has no earlier frame here: the reference falls back
+            info = IS.pyramid_search_device(f, g, mesh.coords, mesh.grid_shape, subset0, rad, p.pyramid_levels, shift,
+                                            p.init_outlier_threshold, p.ncc_auto_expand, p.ncc_max_expand, p.pyramid_fine_radius,
+                                            node_valid, engine_of, ncc_calls)
+            disp, ok, pce = info["disp"], info.get("ok"), info.get("pce")
+            if ok is None:
+                ok = torch.ones(mesh.n, dtype=torch.bool, device="cuda")
+            init_info = {"method": "pyramid", "levels": info["levels"], "per_level": info["per_level"],
+                         "expansions": info["expansions"]}
+        else:
+            act = torch.nonzero(node_valid).flatten()
+            if act.numel() == 0:
+                act = torch.arange(mesh.n, device="cuda")
+            sh0 = None
+            if shift is not None:
+                sh0 = torch.as_tensor(np.round(shift).astype(np.int64), device="cuda")[None, :].expand(act.numel(), 3).contiguous()
+            res = IS.ncc_search_expanding_device(f, g, mesh.coords[act].contiguous(), half0, rad, sh0, p.ncc_auto_expand,
+                                                 p.ncc_max_expand, engine_of, ncc_calls)
+            disp = torch.full((mesh.n, 3), float("nan"), dtype=torch.float64, device="cuda")
+            ok = torch.zeros(mesh.n, dtype=torch.bool, device="cuda")
+            pce = torch.full((mesh.n,), float("nan"), dtype=torch.float64, device="cuda")
+            disp[act] = res["disp"]
+            ok[act] = res["ok"]
+            pce[act] = res["pce"]
+            init_info = {"method": "ncc", "radius": res["radius"], "expansions": res["expansions"]}
+        init_info["global_shift"] = shift
+        bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~node_valid
+        if p.init_min_pce > 0 and pce is not None:
+            bad = bad | (torch.isfinite(pce) & (pce < p.init_min_pce))
+        flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), ~bad, mesh.grid_shape, p.init_outlier_threshold)
+        bad = bad | flag
+        U0, all_bad = _fill(disp, bad, mesh.grid_shape)
+        if bool(all_bad.item()):
+            U0.zero_()
+        init_info["n_bad"] = int(bad.sum().item())
     tr.mark("init_guess")
 
     # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
@@ -327,6 +343,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                         n_iter_local=n_iter)
     result.tracer = tr
     result.ncc_calls = ncc_calls  # (nodes, half, radius, engine) of every integer search of the pass
+    result.init_info = init_info
     result.node_half = node_half
     result.icgn3_iters = []  # n_iter tensors of every 3-DOF pass
     if not p.use_global_step:

@@ -38,6 +38,9 @@ from al_dvc.solver.uncertainty import STENCIL_NOISE_GAIN, noise_hessian_pattern 
 
 from pyaldvc_b200 import synthetic as syn  # noqa: E402
 
+sys.path.insert(0, HERE)
+import init_guess_inputs as IG  # noqa: E402
+
 SHAPE = (32, 34, 36)  # (nz, ny, nx), non-cubic on purpose
 F_TRUE = np.array([[0.015, 0.004, 0.0], [0.003, -0.01, 0.002], [0.0, -0.002, 0.012]])
 T_TRUE = (1.3, -0.7, 0.4)
@@ -265,6 +268,60 @@ def volume_ops_fixtures():
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+def init_guess_fixtures():
+    """The reference's initial-guess pipeline around the NCC kernel: block_downsample, phase_correlation_shift,
+    universal_median_test, fill_nan_grid, auto_pyramid_levels and pyramid_search (numba backend)."""
+    from al_dvc.utils.inpaint import fill_nan_grid
+    from al_dvc.utils.outlier_detection import universal_median_test
+
+    out = {}
+    rng = np.random.default_rng(31)
+    v = rng.normal(0.0, 2.0, (20, 22, 26)).astype(np.float32)
+    out["bd_vol"] = v
+    for fac in (2, 3, 4):
+        out[f"bd_{fac}"] = ris.block_downsample(v, fac)
+
+    # phase correlation: a bead pair under a translation, at max_dim 128 (factor 1) and 24 (factor 4)
+    pair = IG.raw_pc_pair()
+    pf, pg = normalize_volume(pair.f), normalize_volume(pair.g)
+    out.update(pc_sha_f=IG.sha(pf), pc_sha_g=IG.sha(pg), pc_shift=ris.phase_correlation_shift(pf, pg),
+               pc_shift_md24=ris.phase_correlation_shift(pf, pg, None, 24))
+
+    # median test and inpainting on a 7 x 8 x 9 vector field with outliers and holes
+    gs = (7, 8, 9)
+    zz, yy, xx = np.meshgrid(*(np.arange(n, dtype=np.float64) for n in gs), indexing="ij")
+    field = np.stack([0.3 * xx + 0.1 * yy, -0.2 * zz + 0.05 * xx * yy / 8, 0.5 + 0.02 * zz * zz], -1)
+    field += rng.normal(0.0, 0.02, field.shape)
+    field[2, 3, 4] += (3.0, -2.0, 1.0)
+    field[5, 1, 7] += (0.0, 4.0, 0.0)
+    field[0, 0, 0] += (-2.5, 0.0, 0.0)
+    valid = rng.random(gs) > 0.15
+    out.update(mt_field=field, mt_valid=valid, mt_flag=universal_median_test(field, valid, 2.0))
+    holes = field[..., 0].copy()
+    holes[~valid] = np.nan
+    out.update(fill_in=holes, fill_out=fill_nan_grid(holes))
+
+    # pyramid search: 96^3 pair, translation plus a small shear, nodes every 10 voxels, 16^3 template, +-12
+    pair = IG.raw_py_pair()
+    yf, yg = normalize_volume(pair.f), normalize_volume(pair.g)
+    x0, y0, z0 = ref_grid_axes(dvcpara_default().voi, IG.PY_SHAPE, (20, 20, 20), (10, 10, 10))
+    pm = mesh_setup(x0, y0, z0)
+    coords = np.round(pm.coordinates).astype(np.int64)
+    shift = ris.phase_correlation_shift(yf, yg)
+    levels = ris.auto_pyramid_levels(IG.PY_SHAPE, IG.PY_SUBSET, IG.PY_RADIUS, f=yf)
+    info = ris.pyramid_search(yf, yg, coords, pm.grid_shape, IG.PY_SUBSET, IG.PY_RADIUS, 0, global_shift=shift, backend="numba")
+    out.update(py_sha_f=IG.sha(yf), py_sha_g=IG.sha(yg), py_coords=coords, py_grid=np.array(pm.grid_shape), py_shift=shift,
+               py_levels=levels, py_disp=info["disp"], py_ok=info["ok"], py_cc=info["cc"], py_pce=info["pce"],
+               py_clipped=info["clipped"], py_expansions=info["expansions"],
+               py_level_nok=np.array([d["n_ok"] for d in info["per_level"]]),
+               py_level_radius=np.array([d["radius"] for d in info["per_level"]]),
+               py_level_subset=np.array([d["subset"] for d in info["per_level"]]))
+    path = os.path.join(HERE, "golden_init_guess.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB); pyramid levels {levels}, shift {shift}")
+
+
 if __name__ == "__main__":
     main()
     volume_ops_fixtures()
+    init_guess_fixtures()
