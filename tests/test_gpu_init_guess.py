@@ -3,9 +3,10 @@
 utils/inpaint.py:35) and the oracle.
 
 Parity bar: integer results (phase-correlation shifts, pyramid levels, per-level radii, subsets and peak counts,
-expansions, ok flags, median-test flags) identical; the pyramid's sub-voxel displacements within 1e-6 voxel (the
-levels' NCC values are FP64 on both sides; the inpainting between levels is a CG solve to 1e-12 here and a direct
-solve in the reference); block means within one float32 step of the reference's float32 sums.
+expansions, ok flags, median-test flags) identical; the pyramid's sub-voxel displacements within 1e-6 voxel and its
+peak values within 1e-9 (FP64 re-scores on both sides; the inpainting between levels is a CG solve to 1e-12 here
+and a direct solve in the reference); PCE within 1e-5 relative (map energy from the FP32 map); block means within
+one float32 step of the reference's float32 sums.
 """
 
 from __future__ import annotations
@@ -121,30 +122,36 @@ def test_pyramid_search_matches_reference(ig):
     np.testing.assert_allclose(info["disp"], ig["py_disp"], rtol=0, atol=1e-6)
     ok = ig["py_ok"]
     np.testing.assert_allclose(info["cc"][ok], ig["py_cc"][ok], rtol=0, atol=1e-9)
-    np.testing.assert_allclose(info["pce"][ok], ig["py_pce"][ok], rtol=1e-7)
+    # PCE divides by the energy of the whole map, summed over the FP32 map here and the FP64 map in the reference
+    np.testing.assert_allclose(info["pce"][ok], ig["py_pce"][ok], rtol=1e-5)
 
 
-@pytest.mark.parametrize("method,shift", [("pyramid", True), ("ncc", True), ("zero", False)])
-def test_pass_initial_guess_methods(method, shift):
-    """A full pass on the 96^3 affine pair seeded by each initial-guess method recovers the field."""
+def test_pass_initial_guess_methods():
+    """Full passes on the 96^3 affine pair (translation (5.4, -7.2, 9.7) plus shear) seeded by the pyramid search
+    and by one full-resolution NCC search, both with the global pre-shift: every node that converges from both
+    seeds reaches the same solution (within IC-GN's stopping tolerance), within 0.02 voxel RMS of the truth.  Nodes within about 10 voxels of a face
+    leave the volume under the translation (status 2) whatever the seed.  A zero seed runs to completion."""
     import torch
 
     from pyaldvc_b200.pipeline import PassParams, run_pass
 
     pair = IG.raw_py_pair()
     f, g = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (pair.f, pair.g))
-    radius = (12, 12, 12) if method != "zero" else (4, 4, 4)
-    p = PassParams(winsize=(20, 20, 20), winstepsize=(10, 10, 10), search_radius=radius, init_guess_method=method,
-                   global_shift=shift, use_global_step=False, autotune=False)
-    res = run_pass(f, g, p)
-    assert res.init_info["method"] == method
-    U = res.U.cpu().numpy()
-    truth = np.column_stack(pair.disp(*(res.coords.cpu().numpy().astype(float).T)))
-    ok = res.status.cpu().numpy() == 0
-    if method == "zero":  # a 10-voxel translation is beyond IC-GN's reach from zero: only check that it ran
-        assert np.isfinite(U).all()
-        return
-    assert ok.mean() > 0.9
-    assert np.sqrt(np.mean((U[ok] - truth[ok]) ** 2)) < 0.02
-    if method == "pyramid":
-        assert res.init_info["levels"] >= 1
+    out = {}
+    for method in ("pyramid", "ncc", "zero"):
+        p = PassParams(winsize=(20, 20, 20), winstepsize=(10, 10, 10), search_radius=(12, 12, 12), init_guess_method=method,
+                       global_shift=method != "zero", use_global_step=False, autotune=False)
+        res = run_pass(f, g, p)
+        assert res.init_info["method"] == method
+        out[method] = res
+    assert out["pyramid"].init_info["levels"] >= 1
+    coords = out["ncc"].coords.cpu().numpy().astype(float)
+    truth = np.column_stack(pair.disp(*coords.T))
+    ok = (out["pyramid"].status.cpu().numpy() == 0) & (out["ncc"].status.cpu().numpy() == 0)
+    assert ok.mean() > 0.6
+    Up, Un = (out[m].U.cpu().numpy() for m in ("pyramid", "ncc"))
+    # IC-GN stops once its update falls below dp_tol = 1e-3: runs from two seeds end within a few such steps
+    np.testing.assert_allclose(Up[ok], Un[ok], rtol=0, atol=5e-3)
+    assert np.mean(np.abs(Up[ok] - Un[ok]) < 1e-3) > 0.99
+    assert np.sqrt(np.mean((Up[ok] - truth[ok]) ** 2)) < 0.02
+    assert np.isfinite(out["zero"].U.cpu().numpy()).all()
