@@ -36,6 +36,12 @@
  *   aldvc_block_downsample <- solver/integer_search.py:235 block_downsample
  *   aldvc_phase_correlation <- solver/integer_search.py:247 phase_correlation_shift (after the
  *                        VOI crop and the block downsampling, which the caller does)
+ *   aldvc_gradient_plane_fit <- strain/gradient_methods.py:151 gradient_plane_fit (no cut mesh)
+ *   aldvc_gradient_fd <- strain/gradient_methods.py:231 gradient_fd (no cut mesh)
+ *   aldvc_grid_smooth <- utils/grid_interp.py:54 smooth_grid_field
+ *   aldvc_strain_measures <- strain/strain_types.py:19-114 (strain_tensor, principal_strains,
+ *                        von_mises_strain, max_shear_strain, volumetric_strain,
+ *                        det_deformation_gradient, polar_rotation_deg)
  *   aldvc_mask_fill   <- io/volume_ops.py:225 prepare_deformed (masked voxels -> NaN) and the
  *                        NCC input of core/pipeline.py:260-262 (masked voxels -> 0)
  *   aldvc_inpaint     <- utils/inpaint.py:35 fill_nan_grid ("spring" model, no cut mesh)
@@ -192,6 +198,25 @@ int aldvc_mask_fill(float *vol, const uint8_t *mask, int64_t n_voxels, float val
  * voxels into the FP64 accumulator volume (nz, ny, nx) */
 int aldvc_render_beads(double *accum, int64_t nz, int64_t ny, int64_t nx, const double *centres_zyx, const double *peaks,
                        int64_t n_beads, double sigma, int32_t radius, void *stream);
+
+/* ---------------------------------------------------------------- strain on the node grid (FP64) */
+/* Displacement gradient F (N, 9) row-major, F[c][j] = du_c/dx_j in units of the node spacing (hx, hy, hz), of the
+ * (N, 3) field U on the (nz, ny, nx) grid; valid (N,) uint8 or NULL (non-finite U is invalid too).  Invalid
+ * nodes get NaN.  complete (N,) = the stencil was whole. */
+int aldvc_gradient_plane_fit(const double *U, const uint8_t *valid, int64_t nz, int64_t ny, int64_t nx, double hx, double hy,
+                             double hz, int32_t rx, int32_t ry, int32_t rz, double *F, uint8_t *complete, void *stream);
+int aldvc_gradient_fd(const double *U, const uint8_t *valid, int64_t nz, int64_t ny, int64_t nx, double hx, double hy, double hz,
+                      double *F, uint8_t *complete, void *stream);
+/* Normalised Gaussian smoothing of an (nz, ny, nx) FP64 grid field: taps weights[0..half_taps] (HOST array),
+ * edge repeat, NaN / invalid nodes neither give nor take weight and come back NaN. */
+size_t aldvc_grid_smooth_workspace_size(int64_t nz, int64_t ny, int64_t nx);
+int aldvc_grid_smooth(const double *field, const uint8_t *valid, int64_t nz, int64_t ny, int64_t nx, const double *weights,
+                      int32_t half_taps, double *out, void *workspace, size_t workspace_bytes, void *stream);
+/* Strain of every node from its gradient H (N, 9): E (N, 9) of type 0 infinitesimal, 1 Green-Lagrange,
+ * 2 Euler-Almansi, 3 Hencky; principal strains (N, 3) descending; maximum shear, von Mises, volumetric
+ * strain, det(I + H) and the polar rotation angle in degrees (N each).  NaN in, NaN out. */
+int aldvc_strain_measures(const double *H, int64_t n_nodes, int32_t strain_type, double *E, double *principal, double *max_shear,
+                          double *von_mises, double *volumetric, double *det_F, double *rotation_deg, void *stream);
 
 /* ---------------------------------------------------------------- node-grid post-processing */
 /* fills the unknown nodes of the (N, ncols) FP64 field (node n = iz*ny*nx + iy*nx + ix) with the

@@ -395,6 +395,78 @@ def phase_correlation_peak(fs: torch.Tensor, gs: torch.Tensor) -> tuple:
     return i // (ny * nx), (i // nx) % ny, i % nx
 
 
+# --------------------------------------------------------------------------- strain on the node grid
+STRAIN_TYPES = {"infinitesimal": 0, "green_lagrange": 1, "euler_almansi": 2, "hencky": 3}
+
+
+def _grid_args(grid_shape):
+    nz, ny, nx = (int(s) for s in grid_shape)
+    return nz, ny, nx
+
+
+def gradient_plane_fit(U, grid_shape, spacing, halfwidth, valid=None):
+    """(F (N, 3, 3), complete (N,) bool) of the FP64 (N, 3) field on the node grid (plane fit)."""
+    U = dev(U, torch.float64).reshape(-1, 3).contiguous()
+    N = U.shape[0]
+    v = None if valid is None else dev(valid.to(torch.uint8) if isinstance(valid, torch.Tensor) else np.asarray(valid, np.uint8),
+                                       torch.uint8).reshape(N)
+    F = torch.empty((N, 3, 3), dtype=torch.float64, device=U.device)
+    comp = torch.empty(N, dtype=torch.uint8, device=U.device)
+    rx, ry, rz = (int(r) for r in halfwidth)
+    hx, hy, hz = (float(h) for h in spacing)
+    _lib.check(lib().aldvc_gradient_plane_fit(_p(U), _p(v), *_grid_args(grid_shape), hx, hy, hz, rx, ry, rz, _p(F), _p(comp),
+                                              stream_handle()), "aldvc_gradient_plane_fit")
+    return F, comp != 0
+
+
+def gradient_fd(U, grid_shape, spacing, valid=None):
+    """(F (N, 3, 3), complete (N,) bool) of the FP64 (N, 3) field by central / one-sided differences."""
+    U = dev(U, torch.float64).reshape(-1, 3).contiguous()
+    N = U.shape[0]
+    v = None if valid is None else dev(valid.to(torch.uint8) if isinstance(valid, torch.Tensor) else np.asarray(valid, np.uint8),
+                                       torch.uint8).reshape(N)
+    F = torch.empty((N, 3, 3), dtype=torch.float64, device=U.device)
+    comp = torch.empty(N, dtype=torch.uint8, device=U.device)
+    hx, hy, hz = (float(h) for h in spacing)
+    _lib.check(lib().aldvc_gradient_fd(_p(U), _p(v), *_grid_args(grid_shape), hx, hy, hz, _p(F), _p(comp), stream_handle()),
+               "aldvc_gradient_fd")
+    return F, comp != 0
+
+
+def grid_smooth(field, grid_shape, sigma: float, valid=None) -> torch.Tensor:
+    """Normalised Gaussian smoothing (sigma in nodes) of an FP64 grid field (N,); NaN / invalid nodes -> NaN."""
+    x = dev(field, torch.float64).reshape(-1).contiguous()
+    N = x.shape[0]
+    v = None if valid is None else dev(valid.to(torch.uint8) if isinstance(valid, torch.Tensor) else np.asarray(valid, np.uint8),
+                                       torch.uint8).reshape(N)
+    w = gaussian_taps(sigma)
+    if len(w) - 1 > 63:
+        raise ValueError("grid_smooth: sigma too large (at most 63 taps each side)")
+    out = torch.empty_like(x)
+    nz, ny, nx = _grid_args(grid_shape)
+    ws = _workspace(lib().aldvc_grid_smooth_workspace_size(nz, ny, nx))
+    _lib.check(lib().aldvc_grid_smooth(_p(x), _p(v), nz, ny, nx, w.ctypes.data_as(ctypes.c_void_p), len(w) - 1, _p(out), _p(ws),
+                                       ws.numel(), stream_handle()), "aldvc_grid_smooth")
+    return out
+
+
+def strain_measures(H, strain_type: str) -> dict:
+    """Every strain measure of the physical gradients H (N, 3, 3): E, principal, max_shear, von_mises, volumetric,
+    det_F, rotation_deg (FP64 CUDA tensors)."""
+    H = dev(H, torch.float64).reshape(-1, 9).contiguous()
+    N = H.shape[0]
+    d = H.device
+    out = {"E": torch.empty((N, 3, 3), dtype=torch.float64, device=d), "principal": torch.empty((N, 3), dtype=torch.float64, device=d)}
+    for k in ("max_shear", "von_mises", "volumetric", "det_F", "rotation_deg"):
+        out[k] = torch.empty(N, dtype=torch.float64, device=d)
+    if strain_type not in STRAIN_TYPES:
+        raise ValueError(f"unknown strain_type {strain_type!r}")
+    _lib.check(lib().aldvc_strain_measures(_p(H), N, STRAIN_TYPES[strain_type], _p(out["E"]), _p(out["principal"]),
+                                           _p(out["max_shear"]), _p(out["von_mises"]), _p(out["volumetric"]), _p(out["det_F"]),
+                                           _p(out["rotation_deg"]), stream_handle()), "aldvc_strain_measures")
+    return out
+
+
 BOUNDARY_MIRROR, BOUNDARY_NEAREST = 0, 1
 BSPLINE_HALF_TAPS = 32
 

@@ -321,7 +321,56 @@ def init_guess_fixtures():
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB); pyramid levels {levels}, shift {shift}")
 
 
+def strain_fixtures():
+    """The reference's strain module (strain/compute_strain.py, gradient_methods.py, strain_types.py) on a smooth
+    nonlinear displacement over a 9 x 10 x 11 node grid with invalid nodes."""
+    from al_dvc.strain.compute_strain import compute_strain
+    from al_dvc.strain.gradient_methods import gradient_fd, gradient_plane_fit
+
+    rng = np.random.default_rng(41)
+    x0, y0, z0 = np.arange(11) * 6.0 + 10, np.arange(10) * 5.0 + 10, np.arange(9) * 7.0 + 10
+    sm = mesh_setup(x0, y0, z0)
+    N = sm.n_nodes
+    X, Y, Z = (sm.coordinates[:, k] for k in range(3))
+    U = np.column_stack([0.02 * X + 0.004 * Y - 3e-4 * X * Z + 0.3 * np.sin(Y / 17.0),
+                         -0.015 * Y + 0.01 * Z + 2e-4 * X * X,
+                         0.03 * Z - 0.02 * X + 0.1 * np.cos(X / 23.0) * np.sin(Z / 31.0)])
+    U += rng.normal(0.0, 1e-3, U.shape)
+    valid = rng.random(N) > 0.1
+    valid[[0, 57, 300]] = False
+    F_direct = rng.normal(0.0, 0.02, (N, 3, 3))
+    sm.node_valid = valid
+    out = {"st_x0": x0, "st_y0": y0, "st_z0": z0, "st_U": U, "st_valid": valid, "st_F_direct": F_direct,
+           "st_boundary": sm.boundary_nodes}
+    grid = sm.grid_shape
+    Ug = U.reshape(grid + (3,)).copy()
+    for hw in ((1, 1, 1), (2, 1, 1)):
+        F, c = gradient_plane_fit(Ug, sm.spacing, hw, valid.reshape(grid))
+        out[f"pf_{hw[0]}{hw[1]}{hw[2]}_F"], out[f"pf_{hw[0]}{hw[1]}{hw[2]}_complete"] = F, c
+    F, c = gradient_fd(Ug, sm.spacing, valid.reshape(grid))
+    out["fd_F"], out["fd_complete"] = F, c
+    keys = ("disp_u", "disp_v", "disp_w", "F", "exx", "eyy", "ezz", "exy", "exz", "eyz", "principal", "max_shear",
+            "von_mises", "volumetric", "det_F", "rotation_deg", "strain_valid")
+    cases = {
+        "inf_pf": dict(strain_type="infinitesimal", strain_method="plane_fit"),
+        "gl_fd": dict(strain_type="green_lagrange", strain_method="fd"),
+        "ea_pf2": dict(strain_type="euler_almansi", strain_method="plane_fit", strain_plane_fit_halfwidth=(2, 1, 1)),
+        "he_direct": dict(strain_type="hencky", strain_method="direct", voxel_size=(0.5, 0.7, 1.3)),
+        "inf_smooth": dict(strain_type="infinitesimal", strain_method="plane_fit", disp_smoothing=0.8, strain_smoothing=1.1,
+                           strain_edge_trim=False),
+    }
+    for name, kw in cases.items():
+        para = dvcpara_default(**kw)
+        r = compute_strain(sm, para, U, F_direct=F_direct)
+        for k in keys:
+            out[f"cs_{name}_{k}"] = np.asarray(getattr(r, k))
+    path = os.path.join(HERE, "golden_strain.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 if __name__ == "__main__":
     main()
     volume_ops_fixtures()
     init_guess_fixtures()
+    strain_fixtures()
