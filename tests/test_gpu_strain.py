@@ -84,17 +84,18 @@ def test_compute_strain_matches_reference(sg, name):
 
 def test_strain_measures_of_known_deformations():
     """Closed forms: a rotation by 30 degrees about z has zero Green-Lagrange strain, det 1 and a 30 degree polar
-    angle; a reflection keeps det -1 and the rotation part of its polar factor; a uniaxial stretch 1.1 gives
+    angle; a reflected stretch keeps its negative det and the rotation of its polar factor; a uniaxial stretch 1.1 gives
     Hencky log(1.1) and Green-Lagrange (1.21 - 1) / 2."""
     from pyaldvc_b200 import strain as S
 
     t = np.radians(30.0)
     R = np.array([[np.cos(t), -np.sin(t), 0.0], [np.sin(t), np.cos(t), 0.0], [0.0, 0.0, 1.0]])
-    Hs = np.stack([R - np.eye(3), np.diag([0.1, 0.0, 0.0]), np.diag([1.0, 1.0, -1.0]) @ R - np.eye(3)])
+    # the reflected case has distinct stretches: with equal ones the rotation part of a reflection is not unique
+    Hs = np.stack([R - np.eye(3), np.diag([0.1, 0.0, 0.0]), np.diag([1.0, 1.0, -1.0]) @ R @ np.diag([1.1, 1.0, 0.9]) - np.eye(3)])
     gl = S.strain_tensor(Hs, "green_lagrange")
     np.testing.assert_allclose(gl[0], 0.0, atol=1e-15)
     np.testing.assert_allclose(gl[1], np.diag([0.105, 0.0, 0.0]), atol=1e-15)
     np.testing.assert_allclose(S.strain_tensor(Hs[1:2], "hencky")[0], np.diag([np.log(1.1), 0.0, 0.0]), atol=1e-15)
-    np.testing.assert_allclose(S.det_deformation_gradient(Hs), [1.0, 1.1, -1.0], atol=1e-15)
+    np.testing.assert_allclose(S.det_deformation_gradient(Hs), [1.0, 1.1, -0.99], atol=1e-15)
     np.testing.assert_allclose(S.polar_rotation_deg(Hs), [30.0, 0.0, 30.0], atol=1e-12)  # the reference gives 30 too
     np.testing.assert_allclose(S.principal_strains(np.stack([np.diag([0.1, -0.2, 0.3])]))[0], [0.3, 0.1, -0.2], atol=1e-15)
