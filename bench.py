@@ -200,6 +200,9 @@ def run_reference(args):
     }), flush=True)
 
 
+HBM_FALLBACK_GBS = 6650.0
+
+
 def _peaks() -> dict:
     """Peaks for the roofline.  The hot kernels are FP32 CUDA-core bound; the measured-peaks file holds HBM and
     bf16 tensor figures only, so the FP32 peak is the nominal rate of the device (SMs x 128 FP32 lanes x 2 x max clock)."""
@@ -214,8 +217,12 @@ def _peaks() -> dict:
             mp = json.load(fh)
         mhz = float(mp.get("sm_max_mhz", mhz))
         hbm = mp.get("hbm_gbs")
+    hbm_source = "measured (MEASURED_PEAKS.json hbm_gbs)"
+    if hbm is None:  # no measured-peaks file on this box: the earlier copy-bandwidth measurement of this GPU pool
+        hbm = HBM_FALLBACK_GBS
+        hbm_source = "fallback: 6650 GB/s, an earlier STREAM-style copy measurement on B200s of this pool"
     fp32 = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
-    return {"fp32_tflops": fp32, "hbm_gbs": hbm,
+    return {"fp32_tflops": fp32, "hbm_gbs": hbm, "hbm_source": hbm_source,
             "fp32_source": f"nominal FP32 CUDA-core rate: {props.multi_processor_count} SMs x 128 lanes x 2 flop x {mhz:.0f} MHz"}
 
 
@@ -284,7 +291,7 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
         if name in byte_work and peaks.get("hbm_gbs"):
             ach = byte_work[name] / (ms / 1e3) / 1e9
             row.update({"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
-                        "traffic": None, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"})
+                        "traffic": None, "peak_source": peaks["hbm_source"]})
         elif name in flop_work:
             ach = flop_work[name] / (ms / 1e3) / 1e12
             row.update({"bound": "fp32", "achieved": ach, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
