@@ -627,6 +627,79 @@ __global__ void box_pass_kernel(const float* __restrict__ in1, const float* __re
     out2[i] = s2;
 }
 
+// The same box sums from shared-memory tiles: a CTA stages 32 lines x (BOX_TL + len - 1) samples once, so every
+// voxel is read from HBM about (BOX_TL + len - 1) / BOX_TL times instead of len times from L2.  Each output is the
+// same sequential sum as box_pass_kernel (samples past the volume end staged as zeros, which add nothing).
+constexpr int BOX_TL = 128;
+constexpr int BOX_MAX_LEN = 64;
+constexpr int BOX_A = BOX_TL + BOX_MAX_LEN - 1;
+
+// x axis, from g: s1 = sum (g - c), s2 = sum (g - c)^2; tile rows are 32 consecutive y of one z plane
+__global__ void __launch_bounds__(256) box_tile_x_kernel(const float* __restrict__ in, float* __restrict__ out1, float* __restrict__ out2,
+                                                        int ny, int nx, int len, const float* pilot_at) {
+    __shared__ float tile[32 * BOX_A];
+    const float pilot = __ldg(pilot_at);
+    const int A = BOX_TL + len - 1;
+    const int x0 = blockIdx.x * BOX_TL, y0 = blockIdx.y * 32, z = blockIdx.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = warp; r < 32; r += 8) {
+        const int y = y0 + r;
+        if (y >= ny) break;
+        const float* row = in + ((int64_t)z * ny + y) * nx;
+        for (int a = lane; a < A; a += 32) tile[r * A + a] = x0 + a < nx ? __ldg(row + x0 + a) - pilot : 0.0f;
+    }
+    __syncthreads();
+    for (int r = warp; r < 32; r += 8) {
+        const int y = y0 + r;
+        if (y >= ny) break;
+        const int64_t ro = ((int64_t)z * ny + y) * nx;
+        for (int o = lane; o < BOX_TL && x0 + o < nx; o += 32) {
+            const float* t = tile + r * A + o;
+            float s1 = 0.0f, s2 = 0.0f;
+            for (int k = 0; k < len; ++k) {
+                const float v = t[k];
+                s1 += v;
+                s2 = __fmaf_rn(v, v, s2);
+            }
+            out1[ro + x0 + o] = s1;
+            out2[ro + x0 + o] = s2;
+        }
+    }
+}
+
+// y (AXIS 1) or z (AXIS 2) axis, summing the two partial-sum volumes of the previous pass; tile columns are 32 x
+template <int AXIS>
+__global__ void __launch_bounds__(256) box_tile_yz_kernel(const float* __restrict__ in1, const float* __restrict__ in2,
+                                                         float* __restrict__ out1, float* __restrict__ out2, int nz, int ny, int nx,
+                                                         int len) {
+    __shared__ float t1[BOX_A * 32], t2[BOX_A * 32];
+    const int A = BOX_TL + len - 1;
+    const int n = AXIS == 1 ? ny : nz;
+    const int64_t stride = AXIS == 1 ? (int64_t)nx : (int64_t)nx * ny;
+    const int x0 = blockIdx.x * 32, k0 = blockIdx.y * BOX_TL;
+    const int64_t base = AXIS == 1 ? (int64_t)blockIdx.z * ny * nx : (int64_t)blockIdx.z * nx;  // plane z, or row y
+    const int c = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const bool col_ok = x0 + c < nx;
+    for (int a = ty; a < A; a += 8) {
+        const bool in = col_ok && k0 + a < n;
+        const int64_t o = base + (int64_t)(k0 + a) * stride + x0 + c;
+        t1[a * 32 + c] = in ? __ldg(in1 + o) : 0.0f;
+        t2[a * 32 + c] = in ? __ldg(in2 + o) : 0.0f;
+    }
+    __syncthreads();
+    if (!col_ok) return;
+    for (int o = ty; o < BOX_TL && k0 + o < n; o += 8) {
+        float s1 = 0.0f, s2 = 0.0f;
+        for (int k = 0; k < len; ++k) {
+            s1 += t1[(o + k) * 32 + c];
+            s2 += t2[(o + k) * 32 + c];
+        }
+        const int64_t q = base + (int64_t)(k0 + o) * stride + x0 + c;
+        out1[q] = s1;
+        out2[q] = s2;
+    }
+}
+
 struct TiledArgs {
     const float* f;
     const float* g;
@@ -1973,21 +2046,35 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
         const float* pilot_at = g + ((nz / 2) * ny + ny / 2) * nx + nx / 2;  // read by the kernel: no host round trip
         const int64_t nv = nz * ny * nx;
         const unsigned blocks = (unsigned)((nv + 255) / 256);
+        // tiled passes while the window and the grid fit their limits, else one thread per output
+        const bool tiles = G.sx <= BOX_MAX_LEN && G.sy <= BOX_MAX_LEN && G.sz <= BOX_MAX_LEN && nz <= 65535 && ny <= 65535;
+        const unsigned gx_t = (unsigned)((nx + BOX_TL - 1) / BOX_TL), gy_32 = (unsigned)((ny + 31) / 32), gx_32 = (unsigned)((nx + 31) / 32);
         {
             KTimer kt_("box_pass", s);
-            box_pass_kernel<<<blocks, 256, 0, s>>>(g, nullptr, b1, b2, (int)nz, (int)ny, (int)nx, 0, G.sx, pilot_at, 1);
+            if (tiles)
+                box_tile_x_kernel<<<dim3(gx_t, gy_32, (unsigned)nz), 256, 0, s>>>(g, b1, b2, (int)ny, (int)nx, G.sx, pilot_at);
+            else
+                box_pass_kernel<<<blocks, 256, 0, s>>>(g, nullptr, b1, b2, (int)nz, (int)ny, (int)nx, 0, G.sx, pilot_at, 1);
         }
         rc = check_launch("ncc box x");
         if (rc) return rc;
         {
             KTimer kt_("box_pass", s);
-            box_pass_kernel<<<blocks, 256, 0, s>>>(b1, b2, t1, t2, (int)nz, (int)ny, (int)nx, 1, G.sy, nullptr, 0);
+            if (tiles)
+                box_tile_yz_kernel<1><<<dim3(gx_32, (unsigned)((ny + BOX_TL - 1) / BOX_TL), (unsigned)nz), 256, 0, s>>>(
+                    b1, b2, t1, t2, (int)nz, (int)ny, (int)nx, G.sy);
+            else
+                box_pass_kernel<<<blocks, 256, 0, s>>>(b1, b2, t1, t2, (int)nz, (int)ny, (int)nx, 1, G.sy, nullptr, 0);
         }
         rc = check_launch("ncc box y");
         if (rc) return rc;
         {
             KTimer kt_("box_pass", s);
-            box_pass_kernel<<<blocks, 256, 0, s>>>(t1, t2, b1, b2, (int)nz, (int)ny, (int)nx, 2, G.sz, nullptr, 0);
+            if (tiles)
+                box_tile_yz_kernel<2><<<dim3(gx_32, (unsigned)((nz + BOX_TL - 1) / BOX_TL), (unsigned)ny), 256, 0, s>>>(
+                    t1, t2, b1, b2, (int)nz, (int)ny, (int)nx, G.sz);
+            else
+                box_pass_kernel<<<blocks, 256, 0, s>>>(t1, t2, b1, b2, (int)nz, (int)ny, (int)nx, 2, G.sz, nullptr, 0);
         }
         rc = check_launch("ncc box z");
         if (rc) return rc;
