@@ -17,9 +17,10 @@ import numpy as np
 import torch
 
 from . import autotune
+from . import beta_tuning as BT
 from . import integer_search as IS
 from . import kernels as K
-from .mesh import build_grid_axes, grid_coords
+from .mesh import build_grid_axes, grid_coords, surface_nodes
 
 STATUS_CONVERGED = 0
 
@@ -45,7 +46,9 @@ class PassParams:
     ncc_max_expand: int = 3
     use_global_step: bool = True
     mu: float = 1e-3
-    beta: float = 1e-3
+    beta: float | None = 1e-3  # None: tuned per pass over beta_range (solver/beta_tuning.py)
+    beta_range: tuple = BT.DEFAULT_BETA_RANGE
+    beta_criterion: str = "matlab"
     alpha: float = 0.0
     admm_max_iter: int = 4
     admm_tol: float = 1e-2
@@ -195,9 +198,9 @@ ADMM_GRAPH_CACHE = 2
 _ADMM_GRAPHS: dict = {}
 
 
-def _graph_key(p: PassParams, mesh, mode, th3, br3, n_full, tensors) -> tuple:
+def _graph_key(p: PassParams, mesh, mode, th3, br3, n_full, tensors, beta) -> tuple:
     shapes = tuple((k, None if t is None else (tuple(t.shape), str(t.dtype))) for k, t in sorted(tensors.items()))
-    prm = (p.beta, p.mu, p.alpha, p.pcg_tol, p.pcg_max_iter, p.gauss_pt_order, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
+    prm = (beta, p.mu, p.alpha, p.pcg_tol, p.pcg_max_iter, p.gauss_pt_order, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
            p.icgn_patience, p.icgn_predictive_stop, p.admm_max_iter, p.dual_update, p.local_outlier_threshold, p.subset_stride,
            p.variant)
     return (mesh.grid_shape, tuple(mesh.half), tuple(mesh.spacing), mode, th3, br3, n_full, prm, shapes)
@@ -349,7 +352,16 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     if not p.use_global_step:
         return result
 
-    # ---------------- sections 5-6: ADMM (pipeline.py:286-352) with fixed beta
+    # ---------------- sections 5-6: ADMM (pipeline.py:286-352), beta fixed or tuned (pipeline.py:288-298)
+    beta = p.beta
+    result.beta_sweep = None
+    if beta is None:
+        exclude = bad.clone()
+        exclude[torch.from_numpy(surface_nodes(mesh.grid_shape)).cuda()] = True
+        beta, result.beta_sweep = BT.auto_tune_beta_device(mesh.grid_shape, mesh.spacing, elem_active, p.mu, p.alpha, U1, F1, exclude,
+                                                           p.winstepsize, p.beta_range, p.beta_criterion, p.pcg_tol, p.pcg_max_iter,
+                                                           p.gauss_pt_order)
+    result.beta = beta
     n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
     # every tensor the ADMM loop reads; a captured loop reads static copies of them
     T = {"f": f, "g": g_prep, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
@@ -357,8 +369,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
 
     def make_steps(T):
         def global_step(U1_, F1_, W_, v_):
-            b = K.global_rhs(mesh.grid_shape, mesh.spacing, T["elem"], p.beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
-            U2_, _, _ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, T["elem"], p.beta, p.mu, p.alpha, b, U1_, p.pcg_tol,
+            b = K.global_rhs(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
+            U2_, _, _ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, b, U1_, p.pcg_tol,
                                    p.pcg_max_iter, p.gauss_pt_order)
             F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, T["elem"], U2_, p.gauss_pt_order).reshape(-1, 9)
             F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
@@ -408,7 +420,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         # the remaining loop as one CUDA graph, captured on the first pass of this problem shape and replayed
         # by every later one after its inputs are copied into the graph's static tensors (no host step inside)
         state = {"U2": U2, "F2": F2, "W": W, "v": v}
-        key = _graph_key(p, mesh, mode, th3, br3, n_full, {**T, **state})
+        key = _graph_key(p, mesh, mode, th3, br3, n_full, {**T, **state}, beta)
         entry = _ADMM_GRAPHS.get(key)
         if entry is None:
             static = {k: (None if t is None else t.clone()) for k, t in {**T, **state}.items()}

@@ -369,8 +369,45 @@ def strain_fixtures():
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+def beta_fixtures():
+    """The reference's beta auto-tune (solver/beta_tuning.py) on a 6 x 5 x 4 hex mesh with three invalid nodes, a
+    smooth field plus noise, boundary nodes excluded, both scoring criteria."""
+    from al_dvc.solver.beta_tuning import auto_tune_beta
+
+    gm = mesh_setup(np.arange(6) * 6.0, np.arange(5) * 7.0, np.arange(4) * 5.0)
+    nn = gm.n_nodes
+    node_valid = np.ones(nn, dtype=bool)
+    node_valid[[7, 8, 33]] = False
+    elems = gm.elements.copy()
+    bad = ~node_valid[elems].all(axis=1)
+    elems[bad, :] = -1
+    gm.elements = elems
+    gm.node_valid = node_valid
+    ops = build_fem_operators(gm, 2)
+    rng = np.random.default_rng(51)
+    X, Y, Z = (gm.coordinates[:, k] for k in range(3))
+    U1 = np.column_stack([0.02 * X - 0.01 * Y, 0.015 * Z + 0.3 * np.sin(X / 9.0), -0.01 * X + 0.02 * Z]) + rng.normal(0, 0.05, (nn, 3))
+    F1 = np.tile(np.array([[0.02, -0.01, 0.0], [0.0, 0.0, 0.015], [-0.01, 0.0, 0.02]]), (nn, 1, 1)) + rng.normal(0, 0.01, (nn, 3, 3))
+    exclude = np.zeros(nn, dtype=bool)
+    exclude[gm.boundary_nodes] = True
+    exclude[[20, 21]] = True
+    out = {"bt_U1": U1, "bt_F1": F1, "bt_exclude": exclude, "bt_elem_active": ~bad, "bt_grid": np.array(gm.grid_shape),
+           "bt_spacing": np.array(gm.spacing)}
+    for crit in ("matlab", "normalized"):
+        para = dvcpara_default(winstepsize=(6, 6, 6), beta_criterion=crit, global_solver="pcg", pcg_tol=1e-10)
+        beta, info = auto_tune_beta(ops, para, 1e-3, U1, F1, exclude)
+        for k in ("betas", "err1", "err2", "score", "k_best"):
+            out[f"bt_{crit}_{k}"] = np.asarray(info[k])
+        out[f"bt_{crit}_beta"] = beta
+    path = os.path.join(HERE, "golden_beta.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB): betas {out['bt_matlab_betas']}, k {out['bt_matlab_k_best']}, "
+          f"{out['bt_normalized_k_best']}, beta {out['bt_normalized_beta']}")
+
+
 if __name__ == "__main__":
     main()
     volume_ops_fixtures()
     init_guess_fixtures()
     strain_fixtures()
+    beta_fixtures()
