@@ -248,7 +248,9 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
       ncc_template  template in, centred template out: (n_tpl + sz sy sxp) 4 B per node
       box_pass   16 B per voxel per launch
       ncc_tiled / ncc_map  2 n_tpl n_off flop per node (direct cross term)
-      precompute 162 S flop per node; icgn12_* 263 (cubic) / 87 (linear) flop per voxel-iteration, icgn3_* 239 / 63."""
+      precompute 162 S flop per node (per-node form); separable grid form: 16 B per voxel + its two intermediate sum
+                 volumes written and read (80 B per voxel row and node column, 304 B per plane and node)
+      icgn12_* 263 (cubic) / 87 (linear) flop per voxel-iteration, icgn3_* 239 / 63."""
     nvox = float(np.prod(vol_shape))
     byte_work, flop_work = {}, {}
     for n, half, rad, engine in getattr(res, "ncc_calls", []):
@@ -278,7 +280,14 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
     else:
         S_node = np.full(res.coords.shape[0], float(np.prod([(2 * h) // p.subset_stride + 1 for h in half])))
     c12, c3 = (87.0, 63.0) if p.interp_method == "linear" else (263.0, 239.0)
-    flop_work["precompute"] = 162.0 * float(S_node.sum())
+    if getattr(res, "precompute_form", "per_node") == "grid":
+        # separable form: f, gx, gy, gz read once (16 B / voxel), the x pass's 20 FP32 row sums per (z, y, node column)
+        # written and read, the y pass's 38 FP64 sums per (z, node row, node column) written and read
+        gz_, gy_, gx_ = res.grid_shape
+        nz_, ny_ = vol_shape[0], vol_shape[1]
+        byte_work["precompute"] = 16.0 * nvox + 2 * 80.0 * nz_ * ny_ * gx_ + 2 * 304.0 * nz_ * gy_ * gx_
+    else:
+        flop_work["precompute"] = 162.0 * float(S_node.sum())
     it12 = getattr(res, "n_iter_local", res.n_iter).cpu().numpy().astype(np.float64)
     it3 = sum((t.cpu().numpy().astype(np.float64) for t in getattr(res, "icgn3_iters", [])), np.zeros_like(it12))
     for form in ("lean", "batched", "plain"):

@@ -11,6 +11,7 @@
  *
  * Reference interfaces replaced (pyALDVC v1.2.1, src/al_dvc/...):
  *   aldvc_precompute  <- solver/cuda_kernels.py:1635 precompute_nodes_cuda
+ *   aldvc_precompute_grid <- the same on a tensor node grid, separable moment sums
  *                        (contract of solver/numba_kernels.py:499 precompute_nodes)
  *   aldvc_icgn12      <- solver/cuda_kernels.py:1397 icgn_12dof_cuda
  *                        (contract of solver/numba_kernels.py:1211 icgn_12dof_parallel)
@@ -236,6 +237,16 @@ int aldvc_median_test(const double *field, int64_t nz, int64_t ny, int64_t nx, i
 int aldvc_precompute(const aldvc_volumes *vol, const aldvc_subset *sub, const int64_t *coords, int64_t n_nodes,
                      double min_valid_ratio, double cond_max, double *H_all, double *L_all, double *meanf, double *bottomf,
                      int64_t *n_valid, uint8_t *valid, void *stream);
+
+/* aldvc_precompute on a tensor grid of nodes: node n = (iz * ngy + iy) * ngx + ix sits at (xs[ix], ys[iy], zs[iz])
+ * (device int64 arrays).  For volumes with stored gradients and no mask, split rows or per-node shapes, stride 1:
+ * the moments are summed separably (each voxel row once per node column instead of once per node).  Same outputs
+ * and validity rules as aldvc_precompute; workspace of aldvc_precompute_grid_workspace_size bytes.  nx <= 8192. */
+size_t aldvc_precompute_grid_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t ngx, int64_t ngy);
+int aldvc_precompute_grid(const aldvc_volumes *vol, const aldvc_subset *sub, const int64_t *xs, int64_t ngx, const int64_t *ys,
+                          int64_t ngy, const int64_t *zs, int64_t ngz, double min_valid_ratio, double cond_max, double *H_all,
+                          double *L_all, double *meanf, double *bottomf, int64_t *n_valid, uint8_t *valid, void *workspace,
+                          size_t workspace_bytes, void *stream);
 
 /* bytes of workspace aldvc_icgn12/aldvc_icgn3 need for `n_nodes` nodes with these params */
 size_t aldvc_icgn_workspace_size(const aldvc_subset *sub, int64_t n_nodes, const aldvc_icgn_params *prm);

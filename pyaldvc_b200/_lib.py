@@ -58,6 +58,9 @@ PROTOTYPES = {
     "aldvc_device_info": (_i32, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "aldvc_gradients": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _p, _p, _p]),
+    "aldvc_precompute_grid_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64]),
+    "aldvc_precompute_grid": (_i32, [ctypes.POINTER(Volumes), ctypes.POINTER(Subset), _p, _i64, _p, _i64, _p, _i64, _d, _d, _p, _p, _p,
+                                     _p, _p, _p, _p, _sz, _p]),
     "aldvc_precompute": (_i32, [ctypes.POINTER(Volumes), ctypes.POINTER(Subset), _p, _i64, _d, _d, _p, _p, _p, _p, _p, _p,
                                 _p]),
     "aldvc_icgn_workspace_size": (_sz, [ctypes.POINTER(Subset), _i64, ctypes.POINTER(IcgnParams)]),

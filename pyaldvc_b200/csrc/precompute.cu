@@ -249,6 +249,204 @@ __global__ void __launch_bounds__(PRE_THREADS, 2) precompute_kernel(PreArgs a) {
     a.valid[node] = ok ? 1 : 0;
 }
 
+// ----------------------------------------------------------------------------- node grids, separable form
+// On a tensor grid of nodes (x centres xs, y centres ys, z centres zs) with no mask, no split rows, one subset
+// shape, stride 1 and stored gradients, every node's 60 Hessian moments sum g_a g_b X^i Y^j Z^k (i + j + k <= 2)
+// factor along the axes: pass x sums each product against 1, X, X^2 along the node's x window for every voxel row
+// (z, y) (FP32 with Kahan compensation, 33 terms for a 32-voxel subset), pass y sums those rows against 1, Y, Y^2
+// for every plane z (FP64), pass z against 1, Z, Z^2 (FP64), so the subset is swept once per row instead of once
+// per node.  Sum f and sum f^2 follow the same path relative to the row, plane and node centre voxels, shifted
+// exactly in FP64 between the passes, so they are taken relative to the node's centre voxel as in precompute_kernel.
+constexpr int PG_X = 20;  // per row and node column: 6 products x (1, X, X^2), sum (f - c), sum (f - c)^2
+constexpr int PG_Y = 38;  // per plane and node: 6 products x (1, X, X^2, Y, XY, Y^2), f sums
+
+struct PreGridArgs {
+    const float* f;
+    const float* gx;
+    const float* gy;
+    const float* gz;
+    int nz, ny, nx;
+    int hx, hy, hz;
+    const int64_t* xs;
+    const int64_t* ys;
+    const int64_t* zs;
+    int ngx, ngy, ngz;
+    float* Mx;   // [PG_X][nz][ny][ngx]
+    double* My;  // [PG_Y][nz][ngy][ngx]
+    double min_valid_ratio, cond_max;
+    double* H;
+    double* L;
+    double* meanf;
+    double* bottomf;
+    int64_t* n_valid;
+    uint8_t* valid;
+};
+
+// pass x: one CTA per voxel row (z, y), the row of f, gx, gy, gz staged in shared memory, one thread per node column
+__global__ void __launch_bounds__(128) pregrid_x_kernel(PreGridArgs a) {
+    extern __shared__ float prow[];  // [4][nx]: f, gx, gy, gz
+    const int y = blockIdx.x, z = blockIdx.y;
+    const int64_t ro = ((int64_t)z * a.ny + y) * a.nx;
+    for (int x = threadIdx.x; x < a.nx; x += blockDim.x) {
+        prow[x] = __ldg(a.f + ro + x);
+        prow[a.nx + x] = __ldg(a.gx + ro + x);
+        prow[2 * a.nx + x] = __ldg(a.gy + ro + x);
+        prow[3 * a.nx + x] = __ldg(a.gz + ro + x);
+    }
+    __syncthreads();
+    const int64_t plane = (int64_t)a.nz * a.ny * a.ngx, oi = ((int64_t)z * a.ny + y) * a.ngx;
+    for (int c = threadIdx.x; c < a.ngx; c += blockDim.x) {
+        const int64_t xc = a.xs[c];
+        float sum[PG_X], cmp[PG_X];
+#pragma unroll
+        for (int k = 0; k < PG_X; ++k) sum[k] = cmp[k] = 0.0f;
+        if (xc - a.hx >= 0 && xc + a.hx < a.nx) {  // a column past the volume edge belongs to invalid nodes only
+            const float cf = prow[xc];
+            for (int d = -a.hx; d <= a.hx; ++d) {
+                const int x = (int)xc + d;
+                const float g0 = prow[a.nx + x], g1 = prow[2 * a.nx + x], g2 = prow[3 * a.nx + x];
+                const float X = (float)d, X2 = X * X, fv = prow[x] - cf;
+                const float gg[6] = {g0 * g0, g0 * g1, g0 * g2, g1 * g1, g1 * g2, g2 * g2};
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    kahan_add(sum[3 * q], cmp[3 * q], gg[q]);
+                    kahan_add(sum[3 * q + 1], cmp[3 * q + 1], gg[q] * X);
+                    kahan_add(sum[3 * q + 2], cmp[3 * q + 2], gg[q] * X2);
+                }
+                kahan_add(sum[18], cmp[18], fv);
+                kahan_add(sum[19], cmp[19], fv * fv);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PG_X; ++k) a.Mx[k * plane + oi + c] = sum[k] - cmp[k];
+    }
+}
+
+// pass y: one thread per (z, node row, node column), FP64
+__global__ void __launch_bounds__(128) pregrid_y_kernel(PreGridArgs a) {
+    const int64_t n = (int64_t)a.nz * a.ngy * a.ngx;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = (int)(i % a.ngx), r = (int)((i / a.ngx) % a.ngy), z = (int)(i / ((int64_t)a.ngx * a.ngy));
+    const int64_t yc = a.ys[r], xc = a.xs[c];
+    double acc[PG_Y];
+#pragma unroll
+    for (int k = 0; k < PG_Y; ++k) acc[k] = 0.0;
+    const int64_t xplane = (int64_t)a.nz * a.ny * a.ngx, yplane = (int64_t)a.nz * a.ngy * a.ngx;
+    if (yc - a.hy >= 0 && yc + a.hy < a.ny && xc - a.hx >= 0 && xc + a.hx < a.nx) {
+        const int64_t sxy = (int64_t)a.nx * a.ny;
+        const double c2 = (double)__ldg(a.f + z * sxy + yc * a.nx + xc);  // this plane's centre voxel
+        const double nx_w = (double)(2 * a.hx + 1);
+        for (int d = -a.hy; d <= a.hy; ++d) {
+            const int64_t y = yc + d;
+            const int64_t o = ((int64_t)z * a.ny + y) * a.ngx + c;
+            const double Y = (double)d, Y2 = Y * Y;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const double m0 = a.Mx[(3 * q) * xplane + o], m1 = a.Mx[(3 * q + 1) * xplane + o], m2 = a.Mx[(3 * q + 2) * xplane + o];
+                acc[6 * q + 0] += m0;      // 1
+                acc[6 * q + 1] += m1;      // X
+                acc[6 * q + 2] += m2;      // X^2
+                acc[6 * q + 3] += m0 * Y;  // Y
+                acc[6 * q + 4] += m1 * Y;  // XY
+                acc[6 * q + 5] += m0 * Y2; // Y^2
+            }
+            // the row's sums are relative to its centre voxel cr: shift them to c2
+            const double cr = (double)__ldg(a.f + z * sxy + y * a.nx + xc), s = cr - c2;
+            const double a0 = a.Mx[18 * xplane + o], a1 = a.Mx[19 * xplane + o];
+            acc[36] += a0 + nx_w * s;
+            acc[37] += a1 + 2.0 * s * a0 + nx_w * s * s;
+        }
+    }
+    const int64_t oo = ((int64_t)z * a.ngy + r) * a.ngx + c;
+#pragma unroll
+    for (int k = 0; k < PG_Y; ++k) a.My[k * yplane + oo] = acc[k];
+}
+
+// pass z and the per-node finish of precompute_kernel: one thread per node
+__global__ void __launch_bounds__(64) pregrid_z_kernel(PreGridArgs a) {
+    const int64_t n_nodes = (int64_t)a.ngz * a.ngy * a.ngx;
+    const int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (node >= n_nodes) return;
+    const int c = (int)(node % a.ngx), r = (int)((node / a.ngx) % a.ngy), t = (int)(node / ((int64_t)a.ngx * a.ngy));
+    const int64_t xc = a.xs[c], yc = a.ys[r], zc = a.zs[t];
+    double* H = a.H + node * 144;
+    double* L = a.L + node * 144;
+    const bool inside = xc - a.hx >= 0 && xc + a.hx < a.nx && yc - a.hy >= 0 && yc + a.hy < a.ny && zc - a.hz >= 0 && zc + a.hz < a.nz;
+    if (!inside) {
+        for (int i = 0; i < 144; ++i) H[i] = L[i] = 0.0;
+        a.meanf[node] = 0.0;
+        a.bottomf[node] = 1.0;
+        a.n_valid[node] = 0;
+        a.valid[node] = 0;
+        return;
+    }
+    const int64_t sxy = (int64_t)a.nx * a.ny, yplane = (int64_t)a.nz * a.ngy * a.ngx;
+    const double p = (double)__ldg(a.f + zc * sxy + yc * a.nx + xc);  // the node's centre voxel
+    const double nxy = (double)(2 * a.hx + 1) * (2 * a.hy + 1);
+    double tot[PRE_NSUM];
+    for (int k = 0; k < PRE_NSUM; ++k) tot[k] = 0.0;
+    for (int d = -a.hz; d <= a.hz; ++d) {
+        const int64_t z = zc + d;
+        const int64_t o = (z * a.ngy + r) * a.ngx + c;
+        const double Z = (double)d, Z2 = Z * Z;
+        for (int q = 0; q < 6; ++q) {
+            const double* m = a.My + (6 * q) * yplane + o;
+            const double m1 = m[0], mX = m[yplane], mXX = m[2 * yplane], mY = m[3 * yplane], mXY = m[4 * yplane], mYY = m[5 * yplane];
+            double* tq = tot + 10 * q;  // XX XY XZ X YY YZ Y ZZ Z 1
+            tq[0] += mXX;
+            tq[1] += mXY;
+            tq[2] += mX * Z;
+            tq[3] += mX;
+            tq[4] += mYY;
+            tq[5] += mY * Z;
+            tq[6] += mY;
+            tq[7] += m1 * Z2;
+            tq[8] += m1 * Z;
+            tq[9] += m1;
+        }
+        const double cz = (double)__ldg(a.f + z * sxy + yc * a.nx + xc), s = cz - p;
+        const double b0 = a.My[36 * yplane + o], b1 = a.My[37 * yplane + o];
+        tot[60] += b0 + nxy * s;
+        tot[61] += b1 + 2.0 * s * b0 + nxy * s * s;
+    }
+    const int64_t nv = subset_count(a.hx, a.hy, a.hz, 1);
+    auto comp = [](int a_) { return a_ < 9 ? a_ / 3 : a_ - 9; };
+    auto coord = [](int a_) { return a_ < 9 ? a_ % 3 : 3; };
+    double Hl[144], Ll[144];
+    for (int pp = 0; pp < 12; ++pp)
+        for (int qq = 0; qq < 12; ++qq) Hl[pp * 12 + qq] = tot[gg_index(comp(pp), comp(qq)) * 10 + xx_index(coord(pp), coord(qq))];
+    for (int i = 0; i < 144; ++i) {
+        H[i] = Hl[i];
+        Ll[i] = 0.0;
+    }
+    a.n_valid[node] = nv;
+    bool ok = !(nv < 27 || (double)nv < a.min_valid_ratio * (double)nv);
+    double meanf = 0.0, bottomf = 1.0;
+    if (ok) {
+        const double m_rel = tot[60] / (double)nv;
+        meanf = p + m_rel;
+        double ssf = tot[61] - (double)nv * m_rel * m_rel;
+        if (ssf < 0.0) ssf = 0.0;
+        bottomf = sqrt(ssf > 1e-30 ? ssf : 1e-30);
+        if (bottomf < 1e-10) ok = false;
+        if (ok) ok = chol12(Hl, Ll);
+        if (ok) {
+            double dmin = Ll[0], dmax = Ll[0];
+            for (int i = 1; i < 12; ++i) {
+                const double dd = Ll[i * 12 + i];
+                dmin = dd < dmin ? dd : dmin;
+                dmax = dd > dmax ? dd : dmax;
+            }
+            if (dmin <= 0.0 || (dmax / dmin) * (dmax / dmin) > a.cond_max) ok = false;
+        }
+    }
+    for (int i = 0; i < 144; ++i) L[i] = Ll[i];
+    a.meanf[node] = meanf;
+    a.bottomf[node] = bottomf;
+    a.valid[node] = ok ? 1 : 0;
+}
+
 }  // namespace aldvc
 
 using namespace aldvc;
@@ -290,4 +488,46 @@ extern "C" int aldvc_precompute(const aldvc_volumes* vol, const aldvc_subset* su
             precompute_kernel<false><<<(unsigned)n_nodes, PRE_THREADS, KAH, s>>>(a);
         }
     return check_launch("aldvc_precompute");
+}
+
+extern "C" size_t aldvc_precompute_grid_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t ngx, int64_t ngy) {
+    return (size_t)PG_X * nz * ny * ngx * sizeof(float) + 256 + (size_t)PG_Y * nz * ngy * ngx * sizeof(double);
+}
+
+extern "C" int aldvc_precompute_grid(const aldvc_volumes* vol, const aldvc_subset* sub, const int64_t* xs, int64_t ngx, const int64_t* ys,
+                                     int64_t ngy, const int64_t* zs, int64_t ngz, double min_valid_ratio, double cond_max, double* H_all,
+                                     double* L_all, double* meanf, double* bottomf, int64_t* n_valid, uint8_t* valid, void* workspace,
+                                     size_t workspace_bytes, void* stream) {
+    ALDVC_REQUIRE(vol && sub, "aldvc_precompute_grid: null descriptor");
+    ALDVC_REQUIRE(vol->f && vol->gx && vol->gy && vol->gz && xs && ys && zs && H_all && L_all && meanf && bottomf && n_valid && valid &&
+                      workspace,
+                  "aldvc_precompute_grid: null pointer (the gradients must be stored)");
+    ALDVC_REQUIRE(!vol->mask && !sub->split_index && !sub->node_half && sub->stride == 1,
+                  "aldvc_precompute_grid: masks, split rows, per-node shapes and strides take aldvc_precompute");
+    ALDVC_REQUIRE(sub->hx >= 0 && sub->hy >= 0 && sub->hz >= 0, "aldvc_precompute_grid: bad subset");
+    ALDVC_REQUIRE(vol->nz > 0 && vol->ny > 0 && vol->nx > 0 && vol->nz <= 65535 && vol->ny <= 65535 && vol->nx <= 8192,
+                  "aldvc_precompute_grid: volume shape (nz, ny <= 65535, nx <= 8192)");
+    ALDVC_REQUIRE(ngx > 0 && ngy > 0 && ngz > 0 && ngx * ngy * ngz < (1LL << 31), "aldvc_precompute_grid: node grid");
+    ALDVC_REQUIRE(workspace_bytes >= aldvc_precompute_grid_workspace_size(vol->nz, vol->ny, vol->nx, ngx, ngy),
+                  "aldvc_precompute_grid: workspace");
+    const size_t xbytes = (size_t)PG_X * vol->nz * vol->ny * ngx * sizeof(float);
+    PreGridArgs a{vol->f, vol->gx, vol->gy, vol->gz, (int)vol->nz, (int)vol->ny, (int)vol->nx, sub->hx, sub->hy, sub->hz, xs, ys, zs,
+                  (int)ngx, (int)ngy, (int)ngz, (float*)workspace, (double*)((char*)workspace + align_up(xbytes, 256)), min_valid_ratio,
+                  cond_max, H_all, L_all, meanf, bottomf, n_valid, valid};
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t row_smem = (size_t)4 * vol->nx * sizeof(float);
+    static int attr = 0;  // largest dynamic shared size set so far (the first call sets it, outside any capture)
+    if (row_smem > 48 * 1024 && (int)row_smem > attr) {
+        cudaError_t e = cudaFuncSetAttribute(pregrid_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem);
+        if (e != cudaSuccess) return cuda_fail(e, "aldvc_precompute_grid: shared memory attribute");
+        attr = (int)row_smem;
+    }
+    const int64_t ny_planes = (int64_t)vol->nz * ngy * ngx, nodes = ngz * ngy * ngx;
+    {
+        KTimer kt_("precompute", s);
+        pregrid_x_kernel<<<dim3((unsigned)vol->ny, (unsigned)vol->nz), 128, row_smem, s>>>(a);
+        pregrid_y_kernel<<<(unsigned)((ny_planes + 127) / 128), 128, 0, s>>>(a);
+        pregrid_z_kernel<<<(unsigned)((nodes + 63) / 64), 64, 0, s>>>(a);
+    }
+    return check_launch("aldvc_precompute_grid");
 }

@@ -100,6 +100,29 @@ def precompute(coords, half, f, gx, gy, gz, mask, min_valid_ratio, cond_max, str
     return H, L, mf, bf, nv, valid
 
 
+def precompute_grid(xs, ys, zs, half, f, gx, gy, gz, min_valid_ratio, cond_max):
+    """``precompute`` for the nodes of the tensor grid xs x ys x zs (node (iz * ny + iy) * nx + ix), separable sums;
+    stored gradients, no mask, stride 1.  Same outputs as ``precompute``."""
+    xs, ys, zs = (dev(np.asarray(a, dtype=np.int64) if not isinstance(a, torch.Tensor) else a, torch.int64).reshape(-1)
+                  for a in (xs, ys, zs))
+    N = xs.numel() * ys.numel() * zs.numel()
+    d = f.device
+    H = torch.empty((N, 12, 12), dtype=torch.float64, device=d)
+    L = torch.empty((N, 12, 12), dtype=torch.float64, device=d)
+    mf = torch.empty(N, dtype=torch.float64, device=d)
+    bf = torch.empty(N, dtype=torch.float64, device=d)
+    nv = torch.empty(N, dtype=torch.int64, device=d)
+    valid = torch.empty(N, dtype=torch.uint8, device=d)
+    vol = volumes_struct(f, gx, gy, gz, None, None)
+    sub = subset_struct(half, 1, 0, None, None, None)
+    nz, ny, nx = f.shape
+    ws = _workspace(lib().aldvc_precompute_grid_workspace_size(nz, ny, nx, xs.numel(), ys.numel()))
+    _lib.check(lib().aldvc_precompute_grid(ctypes.byref(vol), ctypes.byref(sub), _p(xs), xs.numel(), _p(ys), ys.numel(), _p(zs),
+                                           zs.numel(), float(min_valid_ratio), float(cond_max), _p(H), _p(L), _p(mf), _p(bf), _p(nv),
+                                           _p(valid), _p(ws), ws.numel(), stream_handle()), "aldvc_precompute_grid")
+    return H, L, mf, bf, nv, valid
+
+
 def icgn_params(tol, dp_tol, max_iter, patience, noise_gain=0.0, predictive=True, variant=BATCHED, threads=0, brick_floats=0,
                 mu=0.0, n_full=0.0) -> _lib.IcgnParams:
     return _lib.IcgnParams(float(tol), float(dp_tol), int(max_iter), int(patience), float(noise_gain), int(bool(predictive)),

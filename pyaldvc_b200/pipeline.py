@@ -140,6 +140,7 @@ class Mesh:
         self.grid_shape = (len(z0), len(y0), len(x0))
         self.spacing = (float(x0[1] - x0[0]), float(y0[1] - y0[0]), float(z0[1] - z0[0]))
         self.coords_np = np.round(grid_coords(x0, y0, z0)).astype(np.int64)
+        self.axes = tuple(np.round(np.asarray(a, dtype=np.float64)).astype(np.int64) for a in (x0, y0, z0))  # xs, ys, zs
         self.coords = torch.from_numpy(self.coords_np).cuda()
         self.n = self.coords_np.shape[0]
         self.half = tuple(int(w) // 2 for w in p.winsize)
@@ -244,8 +245,16 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         if (hs > np.asarray(mesh.half)[None, :]).any():
             raise ValueError("node_winsize exceeds winsize")
         node_half = torch.from_numpy(hs.astype(np.int32)).cuda()
-    H, L, meanf, bottomf, n_valid, valid = K.precompute(mesh.coords, mesh.half, f, gx, gy, gz, m_u8, p.min_valid_ratio,
-                                                        p.hessian_cond_max, p.subset_stride, None, None, node_half)
+    nz_, ny_, nx_ = f.shape
+    if mask is None and node_half is None and p.subset_stride == 1 and p.variant == K.BATCHED and nx_ <= 8192 and ny_ <= 65535:
+        # a tensor grid of nodes with one subset shape: separable moment sums (the batched form)
+        H, L, meanf, bottomf, n_valid, valid = K.precompute_grid(*mesh.axes, mesh.half, f, gx, gy, gz, p.min_valid_ratio,
+                                                                 p.hessian_cond_max)
+        precompute_form = "grid"
+    else:
+        precompute_form = "per_node"
+        H, L, meanf, bottomf, n_valid, valid = K.precompute(mesh.coords, mesh.half, f, gx, gy, gz, m_u8, p.min_valid_ratio,
+                                                            p.hessian_cond_max, p.subset_stride, None, None, node_half)
     valid_b = valid != 0
     node_valid = torch.ones(mesh.n, dtype=torch.bool, device="cuda")  # apply_mask_to_mesh's node_valid (all without a mask)
     if mask is not None:  # apply_mask_to_mesh (grid_mesh.py:191-253): centre in the mask, enough of the subset in it
@@ -347,6 +356,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     result.tracer = tr
     result.ncc_calls = ncc_calls  # (nodes, half, radius, engine) of every integer search of the pass
     result.init_info = init_info
+    result.precompute_form = precompute_form
     result.node_half = node_half
     result.icgn3_iters = []  # n_iter tensors of every 3-DOF pass
     if not p.use_global_step:
