@@ -3,7 +3,7 @@
 Each function takes a host NumPy volume (and then returns a host array, the reference's contract) or a CUDA
 tensor (and then returns a CUDA tensor, the pipeline's fast path):
 
-  normalize_volume   io/volume_ops.py:105-121   (whole volume; a VOI box is not supported here)
+  normalize_volume   io/volume_ops.py:74-121    (whole volume or a VOI box)
   compute_gradients  io/volume_ops.py:177-197   7-point stencil, zero 3-voxel border
   presmooth_volume   io/volume_ops.py:200-212   Gaussian, edge repeat, per-axis float32 rounding
   prefilter_bspline  io/volume_ops.py:215-222   cubic B-spline coefficients, mirror boundary
@@ -33,18 +33,36 @@ def _back(t: torch.Tensor, keep_device: bool):
     return t if keep_device else t.cpu().numpy()
 
 
+def _voi_box(shape, voi):
+    """(z0, z1, y0, y1, x0, x1) half-open bounds of the clamped VOI (io/volume_ops.py:40-49); ``voi`` has the
+    reference VOIRange's ``clamp(shape).slices``."""
+    sz, sy, sx = voi.clamp(tuple(shape)).slices
+    z0, z1, _ = sz.indices(shape[0])
+    y0, y1, _ = sy.indices(shape[1])
+    x0, x1, _ = sx.indices(shape[2])
+    if z1 <= z0 or y1 <= y0 or x1 <= x0:
+        raise ValueError("VOI is empty after clamping to the volume.")
+    return z0, z1, y0, y1, x0, x1
+
+
 def normalize_volume(vol, voi=None):
-    """``(vol - mean) / std`` over the whole volume, FP64 statistics, float32 result (std < 1e-12 -> 1)."""
-    if voi is not None:
-        raise NotImplementedError("normalize_volume: statistics over a VOI box are not computed on the device")
+    """``(vol - mean) / std`` with the FP64 mean and population std of the (clamped) VOI, or of the whole volume, taken
+    relative to the VOI's centre voxel; float32 result, std < 1e-12 taken as 1 (io/volume_ops.py:74-121)."""
     if isinstance(vol, torch.Tensor):
         t = vol.contiguous() if vol.dtype in (torch.float32, torch.uint16) else vol.float().contiguous()
-        return K.normalize(K.dev(t, t.dtype))
-    arr = np.asarray(vol)
-    if arr.ndim != 3:
-        raise ValueError(f"Expected a 3-D volume, got shape {arr.shape}.")
-    t = torch.from_numpy(np.ascontiguousarray(arr if arr.dtype == np.uint16 else arr.astype(np.float32))).cuda()
-    return K.normalize(t).cpu().numpy()
+        t = K.dev(t, t.dtype)
+        keep = True
+    else:
+        arr = np.asarray(vol)
+        if arr.ndim != 3:
+            raise ValueError(f"Expected a 3-D volume, got shape {arr.shape}.")
+        t = torch.from_numpy(np.ascontiguousarray(arr if arr.dtype == np.uint16 else arr.astype(np.float32))).cuda()
+        keep = False
+    if voi is None:
+        out = K.normalize(t)
+    else:
+        out, _ = K.normalize_voi(t, _voi_box(tuple(t.shape), voi))
+    return _back(out, keep)
 
 
 def compute_gradients(f):

@@ -260,7 +260,13 @@ def volume_ops_fixtures():
     pair = syn.bead_pair(shape, density=0.03, sigma=1.5, seed=21, disp=syn.translation((0.0, 0.0, 0.0)), noise=0.01)
     v = normalize_volume(pair.f)
     small = np.random.default_rng(22).normal(0.0, 1.0, (5, 3, 2)).astype(np.float32)
-    out = {"vol": v, "bspline": prefilter_bspline(v), "gauss_0.8": presmooth_volume(v, 0.8),
+    from al_dvc.core.data_structures import VOIRange
+
+    raw = np.random.default_rng(23).integers(0, 4096, (12, 20, 45)).astype(np.uint16)
+    raw[3:9, 5:15, 10:30] += 200  # a brighter block, so the VOI statistics differ from the whole volume's
+    out = {"norm_raw": raw, "norm_whole": normalize_volume(raw),
+           "norm_voi": normalize_volume(raw, VOIRange(x=(8, 33), y=(4, 16), z=(2, 10))),
+           "vol": v, "bspline": prefilter_bspline(v), "gauss_0.8": presmooth_volume(v, 0.8),
            "gauss_2.0": presmooth_volume(v, 2.0), "small": small, "small_bspline": prefilter_bspline(small),
            "small_gauss_1.0": presmooth_volume(small, 1.0)}
     path = os.path.join(HERE, "golden_volume_ops.npz")

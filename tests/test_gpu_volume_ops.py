@@ -156,3 +156,38 @@ def test_pass_with_deformed_mask(config1_device):
     assert far.any() and (~far).any()
     np.testing.assert_array_equal(slab.U.cpu().numpy()[far], base.U.cpu().numpy()[far])
     assert np.isfinite(slab.U.cpu().numpy()).all()
+
+
+class _Voi:
+    """Inclusive (lo, hi) index ranges with the reference VOIRange's clamp / slices (core/data_structures.py:87-130)."""
+
+    def __init__(self, x, y, z):
+        self.x, self.y, self.z = x, y, z
+
+    def clamp(self, shape):
+        nz, ny, nx = shape
+
+        def one(r, n):
+            lo, hi = int(r[0]), int(r[1])
+            hi = n - 1 if hi < 0 else hi
+            lo = max(0, min(lo, n - 1))
+            return lo, max(lo, min(hi, n - 1))
+
+        return _Voi(one(self.x, nx), one(self.y, ny), one(self.z, nz))
+
+    @property
+    def slices(self):
+        return slice(self.z[0], self.z[1] + 1), slice(self.y[0], self.y[1] + 1), slice(self.x[0], self.x[1] + 1)
+
+
+def test_normalize_volume_whole_and_voi_match_reference(vg):
+    """normalize_volume (io/volume_ops.py:105-121) of a uint16 volume, whole and over a VOI box: within one float32
+    step of the reference (FP64 statistics on both sides, summed in another order), almost all bit-identical."""
+    from pyaldvc_b200 import volume_ops as VO
+
+    raw = vg["norm_raw"]
+    for got, ref in ((VO.normalize_volume(raw), vg["norm_whole"]),
+                     (VO.normalize_volume(raw, _Voi((8, 33), (4, 16), (2, 10))), vg["norm_voi"]))):
+        np.testing.assert_allclose(got, ref, rtol=0, atol=np.spacing(np.abs(ref).max()))
+        assert np.mean(got == ref) > 0.999
+    assert not np.allclose(vg["norm_whole"], vg["norm_voi"])  # the VOI statistics differ from the whole volume's
