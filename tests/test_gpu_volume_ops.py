@@ -187,7 +187,7 @@ def test_normalize_volume_whole_and_voi_match_reference(vg):
 
     raw = vg["norm_raw"]
     for got, ref in ((VO.normalize_volume(raw), vg["norm_whole"]),
-                     (VO.normalize_volume(raw, _Voi((8, 33), (4, 16), (2, 10))), vg["norm_voi"]))):
+                     (VO.normalize_volume(raw, _Voi((8, 33), (4, 16), (2, 10))), vg["norm_voi"])):
         np.testing.assert_allclose(got, ref, rtol=0, atol=np.spacing(np.abs(ref).max()))
         assert np.mean(got == ref) > 0.999
     assert not np.allclose(vg["norm_whole"], vg["norm_voi"])  # the VOI statistics differ from the whole volume's
