@@ -312,6 +312,8 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     __shared__ int s_ncand;
     __shared__ double s_neigh[27];
     __shared__ double s_coef[10];
+    __shared__ double s_nb[9][9];               // per (dz, dy) pair: sum (f - mf) g, sum g, sum g^2 for dx = 0, 1, 2
+    __shared__ double s_p8[NCC_THREADS / 32][9];  // the warps' partials of pair 8
     __shared__ float s_max, s_min;
     __shared__ int s_pk;
     const NccGeom& G = a.G;
@@ -494,17 +496,82 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             }
             __syncthreads();
         }
-        for (int t = warp; t < 27; t += NW) {
-            const int dzz = t / 9, dyy = (t / 3) % 3, dxx = t % 3;  // box coordinates of the neighbour's origin
-            double v;
-            if (t == 13) {
-                v = peak;
-            } else if (SMEM) {
-                v = warp_rescore_tab<false>(tp, kji, box + (dzz * BY + dyy) * BX + dxx, (int64_t)BY * BX, BX, G.n_tpl, mf, ssf);
-            } else {
-                v = warp_rescore(tp, tsz, tsy, gb + dzz * sxy + (int64_t)dyy * G.nx + dxx, sxy, G.nx, G, mf, ssf);
+        if (SMEM) {
+            // the 26 neighbours by (dz, dy) box row pairs: a lane walks whole template rows once and slides a three-
+            // sample window along the box row, feeding the three dx neighbours of its pair at once.  Warp w < 8 takes
+            // pair w over all template rows; pair 8 is split over the warps by row and its partials summed in order.
+            static_assert(NCC_THREADS == 256, "one warp per (dz, dy) pair 0..7");
+            const int rows = G.sz * G.sy;
+            auto pair_rows = [&](int pr, int r0, int rstep, double acc[9]) {
+                const int dzz = pr / 3, dyy = pr % 3;
+                for (int r = r0; r < rows; r += rstep) {
+                    const int k = r / G.sy, j = r - k * G.sy;
+                    const float* trow = tp + (int64_t)r * G.sx;
+                    const float* brow = box + ((k + dzz) * BY + (j + dyy)) * BX;
+                    float b0 = brow[0], b1 = brow[1];
+                    for (int i = 0; i < G.sx; ++i) {
+                        const float b2 = brow[i + 2];
+                        const double tf = (double)trow[i] - mf;
+                        acc[0] += tf * (double)b0;
+                        acc[1] += tf * (double)b1;
+                        acc[2] += tf * (double)b2;
+                        acc[3] += (double)b0;
+                        acc[4] += (double)b1;
+                        acc[5] += (double)b2;
+                        acc[6] += (double)(b0 * b0);
+                        acc[7] += (double)(b1 * b1);
+                        acc[8] += (double)(b2 * b2);
+                        b0 = b1;
+                        b1 = b2;
+                    }
+                }
+            };
+            double acc[9];
+            if (warp < 8) {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+                pair_rows(warp, lane, 32, acc);
+#pragma unroll
+                for (int q = 0; q < 9; ++q) acc[q] = warp_sum_d(acc[q]);
+                if (lane == 0)
+                    for (int q = 0; q < 9; ++q) s_nb[warp][q] = acc[q];
             }
-            if (lane == 0) s_neigh[t] = v;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+            pair_rows(8, warp * 32 + lane, 32 * NW, acc);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[q] = warp_sum_d(acc[q]);
+            if (lane == 0)
+                for (int q = 0; q < 9; ++q) s_p8[warp][q] = acc[q];
+            __syncthreads();
+            if (tid < 9) {
+                double t8 = 0.0;
+                for (int w = 0; w < NW; ++w) t8 += s_p8[w][tid];
+                s_nb[8][tid] = t8;
+            }
+            __syncthreads();
+            if (tid < 27) {
+                const int pr = tid / 3, dxx = tid % 3;
+                double v = peak;
+                if (tid != 13) {
+                    const double sfg = s_nb[pr][dxx], sg = s_nb[pr][3 + dxx], sgg = s_nb[pr][6 + dxx];
+                    const double var = sgg - sg * sg / (double)G.n_tpl;
+                    if (var < 1e-20) {
+                        v = 0.0;
+                    } else {
+                        v = sfg / sqrt(var * ssf);
+                        v = v > 1.0 ? 1.0 : (v < -1.0 ? -1.0 : v);
+                    }
+                }
+                s_neigh[tid] = v;
+            }
+        } else {
+            for (int t = warp; t < 27; t += NW) {
+                const int dzz = t / 9, dyy = (t / 3) % 3, dxx = t % 3;  // box coordinates of the neighbour's origin
+                const double v = t == 13 ? peak
+                                         : warp_rescore(tp, tsz, tsy, gb + dzz * sxy + (int64_t)dyy * G.nx + dxx, sxy, G.nx, G, mf, ssf);
+                if (lane == 0) s_neigh[t] = v;
+            }
         }
         __syncthreads();
         if (tid < 10) {  // one coefficient per thread, the same sum order as a serial loop
