@@ -26,6 +26,9 @@ constexpr int MAX_CAND = 64;
 
 __constant__ double c_pinv[10 * 27];  // pseudo-inverse of the 27-point quadratic design (integer_search.py:210-227)
 
+// hint that a line is read soon: fetched into L2 without occupying a register
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 struct NccGeom {
     int nz, ny, nx;
     int hx, hy, hz, rx, ry, rz;
@@ -333,6 +336,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         }
         return;
     }
+    for (int i = tid * 32; i < G.nmap; i += NCC_THREADS * 32) prefetch_l2(map + i);  // the whole map towards L2
     // flat template: the map is -2 everywhere (integer_search.py:420-421)
     const bool flat = map[0] < -1.5f;
     float best = -3.0f, mn = 3.0f;
@@ -1736,6 +1740,15 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArg
     }
     const int t = threadIdx.x;
     const int pl = t / N, yx = t - pl * N;
+    {  // the box sums of these planes are read last: start them towards L2 while the transforms run
+        const int64_t sxy = (int64_t)G.nx * G.ny, wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
+        const int nch = (G.vx + 31) / 32, per_row = 2 * nch;
+        for (int i = t; i < np * G.vy * per_row; i += blockDim.x) {
+            const int r = i / per_row, rem = i - r * per_row, p_ = r / G.vy, dy = r - p_ * G.vy;
+            const float* b = (rem & 1) ? a.B2 : a.B1;
+            prefetch_l2(b + (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + wx0 + 32 * (rem >> 1));
+        }
+    }
     if (pl < np) {  // inverse along y, every column
         const float2* colg = a.P + ((int64_t)blockIdx.y * G.vz + dz0 + pl) * N * N + yx;
         float2 v[N];
