@@ -239,9 +239,10 @@ int aldvc_precompute(const aldvc_volumes *vol, const aldvc_subset *sub, const in
                      int64_t *n_valid, uint8_t *valid, void *stream);
 
 /* aldvc_precompute on a tensor grid of nodes: node n = (iz * ngy + iy) * ngx + ix sits at (xs[ix], ys[iy], zs[iz])
- * (device int64 arrays).  For volumes with stored gradients and no mask, split rows or per-node shapes, stride 1:
- * the moments are summed separably (each voxel row once per node column instead of once per node).  Same outputs
- * and validity rules as aldvc_precompute; workspace of aldvc_precompute_grid_workspace_size bytes.  nx <= 8192. */
+ * (device int64 arrays).  For volumes with stored gradients, an optional mask, no split rows or per-node shapes,
+ * stride 1: the moments are summed separably (each voxel row once per node column instead of once per node).  Same
+ * outputs and validity rules as aldvc_precompute; workspace of aldvc_precompute_grid_workspace_size bytes.
+ * nx <= 8192. */
 size_t aldvc_precompute_grid_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t ngx, int64_t ngy);
 int aldvc_precompute_grid(const aldvc_volumes *vol, const aldvc_subset *sub, const int64_t *xs, int64_t ngx, const int64_t *ys,
                           int64_t ngy, const int64_t *zs, int64_t ngz, double min_valid_ratio, double cond_max, double *H_all,

@@ -250,21 +250,22 @@ __global__ void __launch_bounds__(PRE_THREADS, 2) precompute_kernel(PreArgs a) {
 }
 
 // ----------------------------------------------------------------------------- node grids, separable form
-// On a tensor grid of nodes (x centres xs, y centres ys, z centres zs) with no mask, no split rows, one subset
-// shape, stride 1 and stored gradients, every node's 60 Hessian moments sum g_a g_b X^i Y^j Z^k (i + j + k <= 2)
+// On a tensor grid of nodes (x centres xs, y centres ys, z centres zs) with no split rows, one subset shape,
+// stride 1 and stored gradients (a mask allowed: its voxels drop out of every sum and the count), every node's 60 Hessian moments sum g_a g_b X^i Y^j Z^k (i + j + k <= 2)
 // factor along the axes: pass x sums each product against 1, X, X^2 along the node's x window for every voxel row
 // (z, y) (FP32 with Kahan compensation, 33 terms for a 32-voxel subset), pass y sums those rows against 1, Y, Y^2
 // for every plane z (FP64), pass z against 1, Z, Z^2 (FP64), so the subset is swept once per row instead of once
 // per node.  Sum f and sum f^2 follow the same path relative to the row, plane and node centre voxels, shifted
 // exactly in FP64 between the passes, so they are taken relative to the node's centre voxel as in precompute_kernel.
-constexpr int PG_X = 20;  // per row and node column: 6 products x (1, X, X^2), sum (f - c), sum (f - c)^2
-constexpr int PG_Y = 38;  // per plane and node: 6 products x (1, X, X^2, Y, XY, Y^2), f sums
+constexpr int PG_X = 21;  // per row and node column: 6 products x (1, X, X^2), sum (f - c), sum (f - c)^2, voxel count
+constexpr int PG_Y = 39;  // per plane and node: 6 products x (1, X, X^2, Y, XY, Y^2), f sums, voxel count
 
 struct PreGridArgs {
     const float* f;
     const float* gx;
     const float* gy;
     const float* gz;
+    const uint8_t* mask;  // NULL: every voxel
     int nz, ny, nx;
     int hx, hy, hz;
     const int64_t* xs;
@@ -282,9 +283,10 @@ struct PreGridArgs {
     uint8_t* valid;
 };
 
-// pass x: one CTA per voxel row (z, y), the row of f, gx, gy, gz staged in shared memory, one thread per node column
+// pass x: one CTA per voxel row (z, y), the row of f, gx, gy, gz (and the mask) staged in shared memory, one thread
+// per node column; voxels outside the mask add nothing and are not counted
 __global__ void __launch_bounds__(128) pregrid_x_kernel(PreGridArgs a) {
-    extern __shared__ float prow[];  // [4][nx]: f, gx, gy, gz
+    extern __shared__ float prow[];  // [5][nx]: f, gx, gy, gz, mask (0 / 1)
     const int y = blockIdx.x, z = blockIdx.y;
     const int64_t ro = ((int64_t)z * a.ny + y) * a.nx;
     for (int x = threadIdx.x; x < a.nx; x += blockDim.x) {
@@ -292,18 +294,22 @@ __global__ void __launch_bounds__(128) pregrid_x_kernel(PreGridArgs a) {
         prow[a.nx + x] = __ldg(a.gx + ro + x);
         prow[2 * a.nx + x] = __ldg(a.gy + ro + x);
         prow[3 * a.nx + x] = __ldg(a.gz + ro + x);
+        prow[4 * a.nx + x] = (a.mask == nullptr || __ldg(a.mask + ro + x) != 0) ? 1.0f : 0.0f;
     }
     __syncthreads();
     const int64_t plane = (int64_t)a.nz * a.ny * a.ngx, oi = ((int64_t)z * a.ny + y) * a.ngx;
     for (int c = threadIdx.x; c < a.ngx; c += blockDim.x) {
         const int64_t xc = a.xs[c];
-        float sum[PG_X], cmp[PG_X];
+        float sum[PG_X - 1], cmp[PG_X - 1];
 #pragma unroll
-        for (int k = 0; k < PG_X; ++k) sum[k] = cmp[k] = 0.0f;
+        for (int k = 0; k < PG_X - 1; ++k) sum[k] = cmp[k] = 0.0f;
+        int count = 0;
         if (xc - a.hx >= 0 && xc + a.hx < a.nx) {  // a column past the volume edge belongs to invalid nodes only
             const float cf = prow[xc];
             for (int d = -a.hx; d <= a.hx; ++d) {
                 const int x = (int)xc + d;
+                if (prow[4 * a.nx + x] == 0.0f) continue;
+                ++count;
                 const float g0 = prow[a.nx + x], g1 = prow[2 * a.nx + x], g2 = prow[3 * a.nx + x];
                 const float X = (float)d, X2 = X * X, fv = prow[x] - cf;
                 const float gg[6] = {g0 * g0, g0 * g1, g0 * g2, g1 * g1, g1 * g2, g2 * g2};
@@ -318,7 +324,8 @@ __global__ void __launch_bounds__(128) pregrid_x_kernel(PreGridArgs a) {
             }
         }
 #pragma unroll
-        for (int k = 0; k < PG_X; ++k) a.Mx[k * plane + oi + c] = sum[k] - cmp[k];
+        for (int k = 0; k < PG_X - 1; ++k) a.Mx[k * plane + oi + c] = sum[k] - cmp[k];
+        a.Mx[20 * plane + oi + c] = (float)count;
     }
 }
 
@@ -336,7 +343,6 @@ __global__ void __launch_bounds__(128) pregrid_y_kernel(PreGridArgs a) {
     if (yc - a.hy >= 0 && yc + a.hy < a.ny && xc - a.hx >= 0 && xc + a.hx < a.nx) {
         const int64_t sxy = (int64_t)a.nx * a.ny;
         const double c2 = (double)__ldg(a.f + z * sxy + yc * a.nx + xc);  // this plane's centre voxel
-        const double nx_w = (double)(2 * a.hx + 1);
         for (int d = -a.hy; d <= a.hy; ++d) {
             const int64_t y = yc + d;
             const int64_t o = ((int64_t)z * a.ny + y) * a.ngx + c;
@@ -353,9 +359,10 @@ __global__ void __launch_bounds__(128) pregrid_y_kernel(PreGridArgs a) {
             }
             // the row's sums are relative to its centre voxel cr: shift them to c2
             const double cr = (double)__ldg(a.f + z * sxy + y * a.nx + xc), s = cr - c2;
-            const double a0 = a.Mx[18 * xplane + o], a1 = a.Mx[19 * xplane + o];
-            acc[36] += a0 + nx_w * s;
-            acc[37] += a1 + 2.0 * s * a0 + nx_w * s * s;
+            const double a0 = a.Mx[18 * xplane + o], a1 = a.Mx[19 * xplane + o], cnt = a.Mx[20 * xplane + o];
+            acc[36] += a0 + cnt * s;
+            acc[37] += a1 + 2.0 * s * a0 + cnt * s * s;
+            acc[38] += cnt;
         }
     }
     const int64_t oo = ((int64_t)z * a.ngy + r) * a.ngx + c;
@@ -383,8 +390,7 @@ __global__ void __launch_bounds__(64) pregrid_z_kernel(PreGridArgs a) {
     }
     const int64_t sxy = (int64_t)a.nx * a.ny, yplane = (int64_t)a.nz * a.ngy * a.ngx;
     const double p = (double)__ldg(a.f + zc * sxy + yc * a.nx + xc);  // the node's centre voxel
-    const double nxy = (double)(2 * a.hx + 1) * (2 * a.hy + 1);
-    double tot[PRE_NSUM];
+    double tot[PRE_NSUM], nvd = 0.0;
     for (int k = 0; k < PRE_NSUM; ++k) tot[k] = 0.0;
     for (int d = -a.hz; d <= a.hz; ++d) {
         const int64_t z = zc + d;
@@ -406,11 +412,12 @@ __global__ void __launch_bounds__(64) pregrid_z_kernel(PreGridArgs a) {
             tq[9] += m1;
         }
         const double cz = (double)__ldg(a.f + z * sxy + yc * a.nx + xc), s = cz - p;
-        const double b0 = a.My[36 * yplane + o], b1 = a.My[37 * yplane + o];
-        tot[60] += b0 + nxy * s;
-        tot[61] += b1 + 2.0 * s * b0 + nxy * s * s;
+        const double b0 = a.My[36 * yplane + o], b1 = a.My[37 * yplane + o], cnt = a.My[38 * yplane + o];
+        tot[60] += b0 + cnt * s;
+        tot[61] += b1 + 2.0 * s * b0 + cnt * s * s;
+        nvd += cnt;
     }
-    const int64_t nv = subset_count(a.hx, a.hy, a.hz, 1);
+    const int64_t nv = (int64_t)nvd, total = subset_count(a.hx, a.hy, a.hz, 1);
     auto comp = [](int a_) { return a_ < 9 ? a_ / 3 : a_ - 9; };
     auto coord = [](int a_) { return a_ < 9 ? a_ % 3 : 3; };
     double Hl[144], Ll[144];
@@ -421,7 +428,7 @@ __global__ void __launch_bounds__(64) pregrid_z_kernel(PreGridArgs a) {
         Ll[i] = 0.0;
     }
     a.n_valid[node] = nv;
-    bool ok = !(nv < 27 || (double)nv < a.min_valid_ratio * (double)nv);
+    bool ok = !(nv < 27 || (double)nv < a.min_valid_ratio * (double)total);
     double meanf = 0.0, bottomf = 1.0;
     if (ok) {
         const double m_rel = tot[60] / (double)nv;
@@ -502,8 +509,8 @@ extern "C" int aldvc_precompute_grid(const aldvc_volumes* vol, const aldvc_subse
     ALDVC_REQUIRE(vol->f && vol->gx && vol->gy && vol->gz && xs && ys && zs && H_all && L_all && meanf && bottomf && n_valid && valid &&
                       workspace,
                   "aldvc_precompute_grid: null pointer (the gradients must be stored)");
-    ALDVC_REQUIRE(!vol->mask && !sub->split_index && !sub->node_half && sub->stride == 1,
-                  "aldvc_precompute_grid: masks, split rows, per-node shapes and strides take aldvc_precompute");
+    ALDVC_REQUIRE(!sub->split_index && !sub->node_half && sub->stride == 1,
+                  "aldvc_precompute_grid: split rows, per-node shapes and strides take aldvc_precompute");
     ALDVC_REQUIRE(sub->hx >= 0 && sub->hy >= 0 && sub->hz >= 0, "aldvc_precompute_grid: bad subset");
     ALDVC_REQUIRE(vol->nz > 0 && vol->ny > 0 && vol->nx > 0 && vol->nz <= 65535 && vol->ny <= 65535 && vol->nx <= 8192,
                   "aldvc_precompute_grid: volume shape (nz, ny <= 65535, nx <= 8192)");
@@ -511,11 +518,11 @@ extern "C" int aldvc_precompute_grid(const aldvc_volumes* vol, const aldvc_subse
     ALDVC_REQUIRE(workspace_bytes >= aldvc_precompute_grid_workspace_size(vol->nz, vol->ny, vol->nx, ngx, ngy),
                   "aldvc_precompute_grid: workspace");
     const size_t xbytes = (size_t)PG_X * vol->nz * vol->ny * ngx * sizeof(float);
-    PreGridArgs a{vol->f, vol->gx, vol->gy, vol->gz, (int)vol->nz, (int)vol->ny, (int)vol->nx, sub->hx, sub->hy, sub->hz, xs, ys, zs,
+    PreGridArgs a{vol->f, vol->gx, vol->gy, vol->gz, vol->mask, (int)vol->nz, (int)vol->ny, (int)vol->nx, sub->hx, sub->hy, sub->hz, xs, ys, zs,
                   (int)ngx, (int)ngy, (int)ngz, (float*)workspace, (double*)((char*)workspace + align_up(xbytes, 256)), min_valid_ratio,
                   cond_max, H_all, L_all, meanf, bottomf, n_valid, valid};
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t row_smem = (size_t)4 * vol->nx * sizeof(float);
+    const size_t row_smem = (size_t)5 * vol->nx * sizeof(float);
     static int attr = 0;  // largest dynamic shared size set so far (the first call sets it, outside any capture)
     if (row_smem > 48 * 1024 && (int)row_smem > attr) {
         cudaError_t e = cudaFuncSetAttribute(pregrid_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem);

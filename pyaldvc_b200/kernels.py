@@ -100,9 +100,9 @@ def precompute(coords, half, f, gx, gy, gz, mask, min_valid_ratio, cond_max, str
     return H, L, mf, bf, nv, valid
 
 
-def precompute_grid(xs, ys, zs, half, f, gx, gy, gz, min_valid_ratio, cond_max):
+def precompute_grid(xs, ys, zs, half, f, gx, gy, gz, min_valid_ratio, cond_max, mask=None):
     """``precompute`` for the nodes of the tensor grid xs x ys x zs (node (iz * ny + iy) * nx + ix), separable sums;
-    stored gradients, no mask, stride 1.  Same outputs as ``precompute``."""
+    stored gradients, optional uint8 mask, stride 1.  Same outputs as ``precompute``."""
     xs, ys, zs = (dev(np.asarray(a, dtype=np.int64) if not isinstance(a, torch.Tensor) else a, torch.int64).reshape(-1)
                   for a in (xs, ys, zs))
     N = xs.numel() * ys.numel() * zs.numel()
@@ -113,7 +113,8 @@ def precompute_grid(xs, ys, zs, half, f, gx, gy, gz, min_valid_ratio, cond_max):
     bf = torch.empty(N, dtype=torch.float64, device=d)
     nv = torch.empty(N, dtype=torch.int64, device=d)
     valid = torch.empty(N, dtype=torch.uint8, device=d)
-    vol = volumes_struct(f, gx, gy, gz, None, None)
+    m = None if mask is None else dev(mask, torch.uint8)
+    vol = volumes_struct(f, gx, gy, gz, m, None)
     sub = subset_struct(half, 1, 0, None, None, None)
     nz, ny, nx = f.shape
     ws = _workspace(lib().aldvc_precompute_grid_workspace_size(nz, ny, nx, xs.numel(), ys.numel()))

@@ -246,10 +246,10 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             raise ValueError("node_winsize exceeds winsize")
         node_half = torch.from_numpy(hs.astype(np.int32)).cuda()
     nz_, ny_, nx_ = f.shape
-    if mask is None and node_half is None and p.subset_stride == 1 and p.variant == K.BATCHED and nx_ <= 8192 and ny_ <= 65535:
+    if node_half is None and p.subset_stride == 1 and p.variant == K.BATCHED and nx_ <= 8192 and ny_ <= 65535:
         # a tensor grid of nodes with one subset shape: separable moment sums (the batched form)
         H, L, meanf, bottomf, n_valid, valid = K.precompute_grid(*mesh.axes, mesh.half, f, gx, gy, gz, p.min_valid_ratio,
-                                                                 p.hessian_cond_max)
+                                                                 p.hessian_cond_max, m_u8)
         precompute_form = "grid"
     else:
         precompute_form = "per_node"
