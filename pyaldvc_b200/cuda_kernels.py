@@ -158,14 +158,35 @@ def _chunks(n: int, chunk: int):
         yield start, min(n, start + chunk)
 
 
+def _tensor_grid(coords):
+    """(xs, ys, zs) when the (N, 3) [x, y, z] node coordinates are the tensor grid of those axes in mesh order (x
+    fastest, then y, then z), else None."""
+    c = np.asarray(coords)
+    if c.ndim != 2 or c.shape[1] != 3 or c.shape[0] == 0:
+        return None
+    xs, ys, zs = (np.unique(c[:, k]) for k in range(3))
+    if len(xs) * len(ys) * len(zs) != c.shape[0]:
+        return None
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    if not (np.array_equal(c[:, 0], X.ravel()) and np.array_equal(c[:, 1], Y.ravel()) and np.array_equal(c[:, 2], Z.ravel())):
+        return None
+    return tuple(np.ascontiguousarray(a, dtype=np.int64) for a in (xs, ys, zs))
+
+
 # --------------------------------------------------------------------------- kernels
 def precompute_nodes_cuda(coords, hx, hy, hz, f, gx, gy, gz, mask, min_valid_ratio, cond_max, stride=1, split_index=None,
                           split_keep=None, chunk: int = CHUNK_NODES):
-    """Same contract as ``numba_kernels.precompute_nodes`` (:499-509), on the B200."""
+    """Same contract as ``numba_kernels.precompute_nodes`` (:499-509), on the B200.  Nodes that form a tensor grid (a
+    mesh) with stored gradients, stride 1 and no split rows take the separable form (``aldvc_precompute_grid``)."""
     K = _require()
     vols = _volumes(f, gx, gy, gz, mask)
     si, sk = _split(split_index, split_keep)
-    H, L, mf, bf, nv, valid = K.precompute(coords, (hx, hy, hz), *vols[:5], min_valid_ratio, cond_max, stride, si, sk)
+    axes = _tensor_grid(coords) if (si is None and int(stride) == 1 and vols[1] is not None and np.shape(f)[2] <= 8192) else None
+    if axes is not None:  # the nodes of a tensor grid (a mesh): separable moment sums
+        H, L, mf, bf, nv, valid = K.precompute_grid(*axes, (hx, hy, hz), vols[0], vols[1], vols[2], vols[3], min_valid_ratio,
+                                                    cond_max, vols[4])
+    else:
+        H, L, mf, bf, nv, valid = K.precompute(coords, (hx, hy, hz), *vols[:5], min_valid_ratio, cond_max, stride, si, sk)
     return (H.cpu().numpy(), L.cpu().numpy(), mf.cpu().numpy(), bf.cpu().numpy(), nv.cpu().numpy(),
             valid.cpu().numpy().astype(bool))
 
