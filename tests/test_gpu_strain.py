@@ -1,7 +1,7 @@
 """GPU: strain on the node grid against the reference's own outputs (tests/golden/golden_strain.npz, made by
 tests/golden/make_golden.py from strain/compute_strain.py, gradient_methods.py and strain_types.py).
 
-Parity bar: strains within 1e-5, here held to 1e-9 absolute: both sides are FP64 (the
+Parity bar: strains within 1e-5 (the target), here held to 1e-9 absolute: both sides are FP64 (the
 reference solves its plane-fit normal equations with LAPACK and its 3 x 3 eigen and singular value problems with
 numpy, the device with partial-pivoting elimination and Jacobi sweeps); NaN patterns, ``complete`` and
 ``strain_valid`` flags identical.
