@@ -26,6 +26,52 @@ constexpr int MAX_CAND = 64;
 
 __constant__ double c_pinv[10 * 27];  // pseudo-inverse of the 27-point quadratic design (integer_search.py:210-227)
 
+// Sweep of an (nrows x ncols) tile by linear index (every lane busy whatever ncols is); the row of index i is
+// (i + 0.5) / ncols in FP32, exact for i < 2^22.  RB indices per thread are loaded before any is stored.
+template <int RB, typename T, typename Ld, typename St>
+__device__ __forceinline__ void sweep_lin(int nrows, int ncols, Ld ld, St st) {
+    const int total = nrows * ncols;
+    const float inv = 1.0f / (float)ncols;
+    for (int i0 = threadIdx.x; i0 < total; i0 += RB * blockDim.x) {
+        T v[RB];
+        int rr[RB], cc[RB];
+#pragma unroll
+        for (int u = 0; u < RB; ++u) {
+            const int i = i0 + u * blockDim.x;
+            rr[u] = (int)(((float)i + 0.5f) * inv);
+            cc[u] = i - rr[u] * ncols;
+            if (i < total) v[u] = ld(rr[u], cc[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+            if (i0 + u * (int)blockDim.x < total) st(rr[u], cc[u], v[u]);
+    }
+}
+
+// Row-by-column sweep of an (nrows x ncols <= 128) tile, one warp per row: RB rows of loads are issued before
+// any of their stores, so each thread keeps up to 4 RB global loads in flight.
+template <int RB, typename T, typename Ld, typename St>
+__device__ __forceinline__ void copy_rows(int nrows, int ncols, Ld ld, St st) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r0 = (threadIdx.x >> 5) * RB; r0 < nrows; r0 += nw * RB) {
+        T v[RB][4];
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int r = r0 + u, c = lane + 32 * h;
+                if (r < nrows && c < ncols) v[u][h] = ld(r, c);
+            }
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int r = r0 + u, c = lane + 32 * h;
+                if (r < nrows && c < ncols) st(r, c, v[u][h]);
+            }
+    }
+}
+
 // hint that a line is read soon: fetched into L2 without occupying a register
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
@@ -278,7 +324,7 @@ __device__ double warp_rescore_tab(const float* tp, const uint32_t* kji, const f
                                    double mf, double ssf) {
     const int lane = threadIdx.x & 31;
     double sfg = 0.0, sg = 0.0, sgg = 0.0;
-#pragma unroll 4
+#pragma unroll 8
     for (int t = lane; t < n_tpl; t += 32) {
         const uint32_t c = kji[t];
         const float fv = tp[t];
@@ -337,17 +383,49 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         return;
     }
     for (int i = tid * 32; i < G.nmap; i += NCC_THREADS * 32) prefetch_l2(map + i);  // the whole map towards L2
+    // the template first: its loads do not depend on the map, so their latency overlaps the map sweeps'
+    // template: raw FP32 f (staged when SMEM), FP64 mean and sum of squares (integer_search.py:73-88)
+    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
+    const float* fg = a.f + (z0 - G.hz) * sxy + (y0 - G.hy) * G.nx + (x0 - G.hx);
+    const int64_t tsz = SMEM ? (int64_t)G.sy * G.sx : sxy, tsy = SMEM ? G.sx : G.nx;
+    const float* tp = SMEM ? psm : fg;
+    // shared layout: template (n_tpl floats), neighbour box ((sx+2)(sy+2)(sz+2) floats), packed template
+    // coordinates (n_tpl words)
+    uint32_t* kji = reinterpret_cast<uint32_t*>(psm + G.n_tpl + (G.sx + 2) * (G.sy + 2) * (G.sz + 2));
+    double sf = 0.0;
+    for (int r = warp; r < G.sz * G.sy; r += NW) {
+        const int k = r / G.sy, j = r - k * G.sy;
+        for (int ii = lane; ii < G.sx; ii += 32) {
+            const float v = __ldg(fg + k * sxy + (int64_t)j * G.nx + ii);
+            if (SMEM) {
+                psm[(k * G.sy + j) * G.sx + ii] = v;
+                kji[(k * G.sy + j) * G.sx + ii] = ((uint32_t)k << 20) | ((uint32_t)j << 10) | (uint32_t)ii;
+            }
+            sf += (double)v;
+        }
+    }
+    sf = block_sum_d(sf, red);
+    const double mf = sf / (double)G.n_tpl;
+    double q = 0.0;
+    for (int r = warp; r < G.sz * G.sy; r += NW) {
+        const int k = r / G.sy, j = r - k * G.sy;
+        for (int ii = lane; ii < G.sx; ii += 32) {
+            const double d = (double)tp[k * tsz + j * tsy + ii] - mf;
+            q += d * d;
+        }
+    }
+    const double ssf = block_sum_d(q, red);
     // flat template: the map is -2 everywhere (integer_search.py:420-421)
     const bool flat = map[0] < -1.5f;
     float best = -3.0f, mn = 3.0f;
     int bidx = 0x7fffffff;
-    // four loads in flight per thread, then the compares in ascending i (the first index wins a tie)
-    for (int i0 = tid; i0 < G.nmap; i0 += 4 * NCC_THREADS) {
-        float vv[4];
+    // eight loads in flight per thread, then the compares in ascending i (the first index wins a tie)
+    for (int i0 = tid; i0 < G.nmap; i0 += 8 * NCC_THREADS) {
+        float vv[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) vv[u] = i0 + u * NCC_THREADS < G.nmap ? map[i0 + u * NCC_THREADS] : -3.0f;
+        for (int u = 0; u < 8; ++u) vv[u] = i0 + u * NCC_THREADS < G.nmap ? map[i0 + u * NCC_THREADS] : -3.0f;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
             if (i0 + u * NCC_THREADS >= G.nmap) break;
             const float v = vv[u] < -1.0f ? 0.0f : vv[u];
             if (v > best) {
@@ -393,12 +471,12 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     // candidates within the FP32 error bound of the maximum, and the PCE energy on the min-shifted map
     // (integer_search.py:448-452)
     double e = 0.0;
-    for (int i0 = tid; i0 < G.nmap; i0 += 4 * NCC_THREADS) {
-        float vv[4];
+    for (int i0 = tid; i0 < G.nmap; i0 += 8 * NCC_THREADS) {
+        float vv[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) vv[u] = i0 + u * NCC_THREADS < G.nmap ? map[i0 + u * NCC_THREADS] : 0.0f;
+        for (int u = 0; u < 8; ++u) vv[u] = i0 + u * NCC_THREADS < G.nmap ? map[i0 + u * NCC_THREADS] : 0.0f;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
             const int i = i0 + u * NCC_THREADS;
             if (i >= G.nmap) break;
             const float v = vv[u] < -1.0f ? 0.0f : vv[u];
@@ -411,37 +489,6 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         }
     }
     e = block_sum_d(e, red) / (double)G.nmap;
-    // template: raw FP32 f (staged when SMEM), FP64 mean and sum of squares (integer_search.py:73-88)
-    const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
-    const float* fg = a.f + (z0 - G.hz) * sxy + (y0 - G.hy) * G.nx + (x0 - G.hx);
-    const int64_t tsz = SMEM ? (int64_t)G.sy * G.sx : sxy, tsy = SMEM ? G.sx : G.nx;
-    const float* tp = SMEM ? psm : fg;
-    // shared layout: template (n_tpl floats), neighbour box ((sx+2)(sy+2)(sz+2) floats), packed template
-    // coordinates (n_tpl words)
-    uint32_t* kji = reinterpret_cast<uint32_t*>(psm + G.n_tpl + (G.sx + 2) * (G.sy + 2) * (G.sz + 2));
-    double sf = 0.0;
-    for (int r = warp; r < G.sz * G.sy; r += NW) {
-        const int k = r / G.sy, j = r - k * G.sy;
-        for (int ii = lane; ii < G.sx; ii += 32) {
-            const float v = __ldg(fg + k * sxy + (int64_t)j * G.nx + ii);
-            if (SMEM) {
-                psm[(k * G.sy + j) * G.sx + ii] = v;
-                kji[(k * G.sy + j) * G.sx + ii] = ((uint32_t)k << 20) | ((uint32_t)j << 10) | (uint32_t)ii;
-            }
-            sf += (double)v;
-        }
-    }
-    sf = block_sum_d(sf, red);
-    const double mf = sf / (double)G.n_tpl;
-    double q = 0.0;
-    for (int r = warp; r < G.sz * G.sy; r += NW) {
-        const int k = r / G.sy, j = r - k * G.sy;
-        for (int ii = lane; ii < G.sx; ii += 32) {
-            const double d = (double)tp[k * tsz + j * tsy + ii] - mf;
-            q += d * d;
-        }
-    }
-    const double ssf = block_sum_d(q, red);
     int pk = s_pk;
     double peak = (double)vmax;
     const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
@@ -494,10 +541,12 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         const float* gb = a.g + (wz0 + pz - 1) * sxy + (wy0 + py - 1) * G.nx + (wx0 + px - 1);
         float* box = psm + G.n_tpl;
         if (SMEM) {
-            for (int r = warp; r < BZ * BY; r += NW) {
-                const int k = r / BY, j = r - k * BY;
-                for (int ii = lane; ii < BX; ii += 32) box[(k * BY + j) * BX + ii] = __ldg(gb + k * sxy + (int64_t)j * G.nx + ii);
-            }
+            sweep_lin<8, float>(BZ * BY, BX,
+                                [&](int r, int ii) {
+                                    const int k = r / BY, j = r - k * BY;
+                                    return __ldg(gb + k * sxy + (int64_t)j * G.nx + ii);
+                                },
+                                [&](int r, int ii, float v) { box[r * BX + ii] = v; });
             __syncthreads();
         }
         if (SMEM) {
@@ -1366,52 +1415,6 @@ __device__ float2* fft_rows(float2* a, float2* b, const float2* tw, const FftAxi
         ns *= R;
     }
     return a;
-}
-
-// Row-by-column sweep of an (nrows x ncols <= 128) tile, one warp per row: RB rows of loads are issued before
-// any of their stores, so each thread keeps up to 4 RB global loads in flight.
-// Sweep of an (nrows x ncols) tile by linear index (every lane busy whatever ncols is); the row of index i is
-// (i + 0.5) / ncols in FP32, exact for i < 2^22.  RB indices per thread are loaded before any is stored.
-template <int RB, typename T, typename Ld, typename St>
-__device__ __forceinline__ void sweep_lin(int nrows, int ncols, Ld ld, St st) {
-    const int total = nrows * ncols;
-    const float inv = 1.0f / (float)ncols;
-    for (int i0 = threadIdx.x; i0 < total; i0 += RB * blockDim.x) {
-        T v[RB];
-        int rr[RB], cc[RB];
-#pragma unroll
-        for (int u = 0; u < RB; ++u) {
-            const int i = i0 + u * blockDim.x;
-            rr[u] = (int)(((float)i + 0.5f) * inv);
-            cc[u] = i - rr[u] * ncols;
-            if (i < total) v[u] = ld(rr[u], cc[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < RB; ++u)
-            if (i0 + u * (int)blockDim.x < total) st(rr[u], cc[u], v[u]);
-    }
-}
-
-template <int RB, typename T, typename Ld, typename St>
-__device__ __forceinline__ void copy_rows(int nrows, int ncols, Ld ld, St st) {
-    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int r0 = (threadIdx.x >> 5) * RB; r0 < nrows; r0 += nw * RB) {
-        T v[RB][4];
-#pragma unroll
-        for (int u = 0; u < RB; ++u)
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const int r = r0 + u, c = lane + 32 * h;
-                if (r < nrows && c < ncols) v[u][h] = ld(r, c);
-            }
-#pragma unroll
-        for (int u = 0; u < RB; ++u)
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const int r = r0 + u, c = lane + 32 * h;
-                if (r < nrows && c < ncols) st(r, c, v[u][h]);
-            }
-    }
 }
 
 __device__ __forceinline__ bool fft_node_ok(const FftArgs& a, int64_t node) {
