@@ -492,7 +492,14 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     int pk = s_pk;
     double peak = (double)vmax;
     const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
-    if (!flat) {
+    // one candidate at an interior offset (the common case): its FP64 score is the centre of the 27-neighbourhood,
+    // taken from the staged box below instead of a separate pass over the window in global memory
+    bool centre_from_box = false;
+    if (!flat && SMEM && min(s_ncand, MAX_CAND) == 1 && G.rx > 0 && G.ry > 0 && G.rz > 0) {
+        const int qz = pk / (G.vy * G.vx), qr = pk - qz * G.vy * G.vx, qy = qr / G.vx, qx = qr - qy * G.vx;
+        centre_from_box = qx > 0 && qx < 2 * G.rx && qy > 0 && qy < 2 * G.ry && qz > 0 && qz < 2 * G.rz;
+    }
+    if (!flat && !centre_from_box) {
         // FP64 re-score of the candidates in C order; the first maximum wins (np.argmax)
         const int nc = min(s_ncand, MAX_CAND);
         if (tid == 0) {
@@ -527,7 +534,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             pk = bi;
             peak = bv;
         }
-    } else {
+    } else if (flat) {
         peak = 0.0;
         pk = 0;
     }
@@ -606,7 +613,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             if (tid < 27) {
                 const int pr = tid / 3, dxx = tid % 3;
                 double v = peak;
-                if (tid != 13) {
+                if (tid != 13 || centre_from_box) {
                     const double sfg = s_nb[pr][dxx], sg = s_nb[pr][3 + dxx], sgg = s_nb[pr][6 + dxx];
                     const double var = sgg - sg * sg / (double)G.n_tpl;
                     if (var < 1e-20) {
@@ -617,6 +624,10 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
                     }
                 }
                 s_neigh[tid] = v;
+            }
+            if (centre_from_box) {
+                __syncthreads();
+                peak = s_neigh[13];
             }
         } else {
             for (int t = warp; t < 27; t += NW) {
