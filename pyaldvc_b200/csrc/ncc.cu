@@ -72,6 +72,13 @@ __device__ __forceinline__ void copy_rows(int nrows, int ncols, Ld ld, St st) {
     }
 }
 
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
 // hint that a line is read soon: fetched into L2 without occupying a register
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
@@ -468,6 +475,29 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     __syncthreads();
     const float vmax = s_max, vmin = s_min;
     const float cmin = flat ? 0.0f : vmin;
+    const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
+    const int BX = G.sx + 2, BY = G.sy + 2, BZ = G.sz + 2;
+    float* box = psm + G.n_tpl;  // the neighbour box of the peak (shared layout above)
+    auto interior_at = [&](int q) {
+        const int qz = q / (G.vy * G.vx), qr = q - qz * G.vy * G.vx, qy = qr / G.vx, qx = qr - qy * G.vx;
+        return qx > 0 && qx < 2 * G.rx && qy > 0 && qy < 2 * G.ry && qz > 0 && qz < 2 * G.rz && !flat;
+    };
+    auto box_origin = [&](int q) {
+        const int qz = q / (G.vy * G.vx), qr = q - qz * G.vy * G.vx, qy = qr / G.vx, qx = qr - qy * G.vx;
+        return a.g + (wz0 + qz - 1) * sxy + (wy0 + qy - 1) * G.nx + (wx0 + qx - 1);
+    };
+    // the box of the FP32 maximum, copied asynchronously while the second sweep and the candidate scores run: it
+    // is the box the sub-voxel fit needs unless the FP64 re-scores move the peak
+    const int spk = s_pk;
+    const bool spec = SMEM && interior_at(spk);
+    if (spec) {
+        const float* gb0 = box_origin(spk);
+        for (int i = tid; i < BZ * BY * BX; i += NCC_THREADS) {
+            const int r = i / BX, ii = i - r * BX, k = r / BY, j = r - k * BY;
+            cp_async4(box + i, gb0 + k * sxy + (int64_t)j * G.nx + ii);
+        }
+        cp_async_commit();
+    }
     // candidates within the FP32 error bound of the maximum, and the PCE energy on the min-shifted map
     // (integer_search.py:448-452)
     double e = 0.0;
@@ -491,7 +521,6 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     e = block_sum_d(e, red) / (double)G.nmap;
     int pk = s_pk;
     double peak = (double)vmax;
-    const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
     // one candidate at an interior offset (the common case): its FP64 score is the centre of the 27-neighbourhood,
     // taken from the staged box below instead of a separate pass over the window in global memory
     bool centre_from_box = false;
@@ -543,11 +572,13 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     const bool at_border = px == 0 || px == 2 * G.rx || py == 0 || py == 2 * G.ry || pz == 0 || pz == 2 * G.rz;
     const bool interior = !at_border && G.rx > 0 && G.ry > 0 && G.rz > 0 && !flat;
     double sub[3] = {0.0, 0.0, 0.0};
+    if (spec) {  // every async copy into the box has landed before any thread reads or rewrites it
+        cp_async_wait_all();
+        __syncthreads();
+    }
     if (interior) {
-        const int BX = G.sx + 2, BY = G.sy + 2, BZ = G.sz + 2;
         const float* gb = a.g + (wz0 + pz - 1) * sxy + (wy0 + py - 1) * G.nx + (wx0 + px - 1);
-        float* box = psm + G.n_tpl;
-        if (SMEM) {
+        if (SMEM && !(spec && pk == spk)) {  // the staged box is not this peak's
             sweep_lin<8, float>(BZ * BY, BX,
                                 [&](int r, int ii) {
                                     const int k = r / BY, j = r - k * BY;
@@ -853,12 +884,6 @@ struct TiledArgs {
     int sxp;           // padded template row (floats, multiple of 4)
 };
 
-__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
 // Centred FP32 template of every node of a chunk (FP64 mean, FP64 sum of squares), rows padded to sxp floats.
 __global__ void __launch_bounds__(256) ncc_template_kernel(TiledArgs a, float* T, double* ssf) {
