@@ -92,6 +92,9 @@ typedef struct aldvc_volumes {
     const uint8_t *mask;  /* reference mask (nz, ny, nx), 0 = not material; NULL: every voxel counts */
     const float *g;       /* deformed volume prepared for the interpolation mode; NaN voxels are excluded */
     int64_t nz, ny, nx;
+    const float *g4;      /* optional (may be NULL): g as overlapping quads, 4 floats per voxel i = g[i..i+3]
+                             (aldvc_make_quads); the persistent IC-GN kernels then read each cubic tap row with
+                             one 16-byte load */
 } aldvc_volumes;
 
 /* Subset geometry of a call: one shape for every node, or per-node (uneven, anisotropic) shapes. */
@@ -191,6 +194,10 @@ int aldvc_block_downsample(const float *in, int64_t nz, int64_t ny, int64_t nx, 
 size_t aldvc_phase_correlation_workspace_size(int64_t nz, int64_t ny, int64_t nx);
 int aldvc_phase_correlation(const float *fs, const float *gs, int64_t nz, int64_t ny, int64_t nx, int64_t *peak, void *workspace,
                             size_t workspace_bytes, void *stream);
+
+/* quads[4 i + k] = vol[min(i + k, n - 1)], k = 0..3: the overlapping-quad copy of a volume read by the IC-GN
+ * kernels through aldvc_volumes.g4 (16 bytes per voxel) */
+int aldvc_make_quads(const float *vol, int64_t n_voxels, float *quads, void *stream);
 
 /* vol[i] = value wherever mask[i] == 0 (mask: uint8, same voxel count) */
 int aldvc_mask_fill(float *vol, const uint8_t *mask, int64_t n_voxels, float value, void *stream);

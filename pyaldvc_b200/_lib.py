@@ -29,7 +29,7 @@ _sz = ctypes.c_size_t
 
 class Volumes(ctypes.Structure):
     _fields_ = [("f", _p), ("gx", _p), ("gy", _p), ("gz", _p), ("mask", _p), ("g", _p), ("nz", _i64), ("ny", _i64),
-                ("nx", _i64)]
+                ("nx", _i64), ("g4", _p)]
 
 
 class Subset(ctypes.Structure):
@@ -84,6 +84,7 @@ PROTOTYPES = {
     "aldvc_normalize": (_i32, [_p, _i32, _i64, _d, _p, _p, _p, _sz, _p]),
     "aldvc_sep_filter": (_i32, [_p, _p, _i64, _i64, _i64, _i32, _p, _i32, _i32, _p]),
     "aldvc_mask_fill": (_i32, [_p, _p, _i64, ctypes.c_float, _p]),
+    "aldvc_make_quads": (_i32, [_p, _i64, _p, _p]),
     "aldvc_gradient_plane_fit": (_i32, [_p, _p, _i64, _i64, _i64, _d, _d, _d, _i32, _i32, _i32, _p, _p, _p]),
     "aldvc_gradient_fd": (_i32, [_p, _p, _i64, _i64, _i64, _d, _d, _d, _p, _p, _p]),
     "aldvc_grid_smooth_workspace_size": (_sz, [_i64, _i64, _i64]),

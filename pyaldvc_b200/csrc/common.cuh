@@ -109,6 +109,39 @@ __device__ __forceinline__ float sample_brick(const float* __restrict__ b, int b
     return acc;
 }
 
+// sample_brick over the overlapping-quad copy of the volume (q[i] = b[i..i+3]): each of the 16 tap rows of a cubic
+// sample is one 16-byte load; the same products and sums in the same order as sample_brick<MODE>.
+template <int MODE>
+__device__ __forceinline__ float sample_quad(const float4* __restrict__ q, int bx, int bxy, int ix, int iy, int iz, float fx,
+                                             float fy, float fz) {
+    float wx0, wx1, wx2, wx3, wy0, wy1, wy2, wy3, wz0, wz1, wz2, wz3;
+    if (MODE == 1) {
+        keys_w(fx, wx0, wx1, wx2, wx3);
+        keys_w(fy, wy0, wy1, wy2, wy3);
+        keys_w(fz, wz0, wz1, wz2, wz3);
+    } else {
+        bspl_w(fx, wx0, wx1, wx2, wx3);
+        bspl_w(fy, wy0, wy1, wy2, wy3);
+        bspl_w(fz, wz0, wz1, wz2, wz3);
+    }
+    const float4* p = q + ((int64_t)(iz - 1) * bxy + (int64_t)(iy - 1) * bx + (ix - 1));
+    float acc = 0.0f;
+    const float wz[4] = {wz0, wz1, wz2, wz3};
+    const float wy[4] = {wy0, wy1, wy2, wy3};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float pl = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float4 r = __ldg(p + (int64_t)k * bxy + j * bx);
+            const float row = r.x * wx0 + r.y * wx1 + r.z * wx2 + r.w * wx3;
+            pl += row * wy[j];
+        }
+        acc += pl * wz[k];
+    }
+    return acc;
+}
+
 // Stencil-7 reference gradient on the fly (numba_kernels._grad_at :188-212). The differences of two
 // float32 voxels round to float32 as in the reference; indices are clamped so the read stays inside f.
 __device__ __forceinline__ void grad_otf(const float* __restrict__ f, int nz, int ny, int nx, int zz, int yy, int xx, float& gx,

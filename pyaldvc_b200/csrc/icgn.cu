@@ -34,6 +34,7 @@ struct IcgnArgs {
     const float* gz;
     const uint8_t* mask;
     const float* g;
+    const float4* g4;  // optional overlapping-quad copy of g (cubic modes of the persistent kernel)
     int nz, ny, nx;
     // subset
     int hx, hy, hz, stride, nX, nY, nZ;
@@ -975,7 +976,9 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
                 const float fxf = floorf(xr), fyf = floorf(yr), fzf = floorf(zr);
                 const int gx_ = min(max(xci + (int)fxf, lo), hx_), gy_ = min(max(yci + (int)fyf, lo), hy_),
                           gz_ = min(max(zci + (int)fzf, lo), hz_);
-                const float gv = sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf, yr - fyf, zr - fzf);
+                const float gv = (MODE != 0 && a.g4) ? sample_quad<MODE == 0 ? 1 : MODE>(a.g4, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf,
+                                                                                         yr - fyf, zr - fzf)
+                                                     : sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf, yr - fyf, zr - fzf);
                 if (gv != gv) continue;  // NaN: masked out in the deformed frame
                 acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
             }
@@ -1425,6 +1428,7 @@ static int fill_common(IcgnArgs& a, const aldvc_volumes* vol, const aldvc_subset
     a.gz = vol->gz;
     a.mask = vol->mask;
     a.g = vol->g;
+    a.g4 = reinterpret_cast<const float4*>(vol->g4);
     a.nz = (int)vol->nz;
     a.ny = (int)vol->ny;
     a.nx = (int)vol->nx;

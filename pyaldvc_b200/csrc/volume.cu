@@ -171,6 +171,15 @@ __global__ void mask_fill_kernel(float* __restrict__ v, const uint8_t* __restric
         if (mask[i] == 0) v[i] = value;
 }
 
+// q[i] = (v[i], v[i+1], v[i+2], v[i+3]), indices clamped to the last voxel
+__global__ void make_quads_kernel(const float* __restrict__ v, int64_t n, float4* __restrict__ q) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t l = n - 1;
+        q[i] = make_float4(__ldg(v + i), __ldg(v + (i + 1 < l ? i + 1 : l)), __ldg(v + (i + 2 < l ? i + 2 : l)),
+                           __ldg(v + (i + 3 < l ? i + 3 : l)));
+    }
+}
+
 }  // namespace aldvc
 
 using namespace aldvc;
@@ -248,4 +257,13 @@ extern "C" int aldvc_mask_fill(float* vol, const uint8_t* mask, int64_t n_voxels
     const int64_t blocks = std::min<int64_t>((n_voxels + 255) / 256, 148 * 16);
     mask_fill_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vol, mask, n_voxels, value);
     return check_launch("aldvc_mask_fill");
+}
+
+extern "C" int aldvc_make_quads(const float* vol, int64_t n_voxels, float* quads, void* stream) {
+    ALDVC_REQUIRE(vol && quads, "aldvc_make_quads: null pointer");
+    ALDVC_REQUIRE((reinterpret_cast<uintptr_t>(quads) & 15) == 0, "aldvc_make_quads: quads must be 16-byte aligned");
+    if (n_voxels <= 0) return ALDVC_OK;
+    const int64_t blocks = std::min<int64_t>((n_voxels + 255) / 256, 148 * 16);
+    make_quads_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vol, n_voxels, reinterpret_cast<float4*>(quads));
+    return check_launch("aldvc_make_quads");
 }

@@ -48,11 +48,20 @@ def _workspace(nbytes: int) -> torch.Tensor:
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device="cuda")
 
 
-def volumes_struct(f, gx, gy, gz, mask, g) -> _lib.Volumes:
+def volumes_struct(f, gx, gy, gz, mask, g, g4=None) -> _lib.Volumes:
     nz, ny, nx = f.shape
     return _lib.Volumes(f.data_ptr(), None if gx is None else gx.data_ptr(), None if gy is None else gy.data_ptr(),
                         None if gz is None else gz.data_ptr(), None if mask is None else mask.data_ptr(),
-                        None if g is None else g.data_ptr(), nz, ny, nx)
+                        None if g is None else g.data_ptr(), nz, ny, nx, None if g4 is None else g4.data_ptr())
+
+
+def make_quads(vol: torch.Tensor) -> torch.Tensor:
+    """(n, 4) float32 overlapping quads of a float32 CUDA volume: row i holds vol[i], vol[i+1], vol[i+2], vol[i+3]
+    (clamped at the end): the IC-GN kernels read a cubic tap row with one 16-byte load from it."""
+    vol = dev(vol, torch.float32)
+    q = torch.empty((vol.numel(), 4), dtype=torch.float32, device=vol.device)
+    _lib.check(lib().aldvc_make_quads(_p(vol), vol.numel(), _p(q), stream_handle()), "aldvc_make_quads")
+    return q
 
 
 def subset_struct(half, stride, mode, split_index=None, split_keep=None, node_half=None) -> _lib.Subset:
@@ -132,7 +141,7 @@ def icgn_params(tol, dp_tol, max_iter, patience, noise_gain=0.0, predictive=True
 
 def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol, dp_tol, max_iter, patience, stride=1, H=None,
            pattern=None, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED, threads=0,
-           brick_floats=0, node_half=None):
+           brick_floats=0, node_half=None, g4=None):
     """Device 12-DOF IC-GN; returns (P (N,12), n_iter, status, zncc) tensors.  ``node_half``: optional (N,3)
     per-node half-widths (``half`` is then their maximum)."""
     coords = dev(coords, torch.int64)
@@ -143,7 +152,7 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
     n_iter = torch.empty(N, dtype=torch.int32, device=d)
     status = torch.empty(N, dtype=torch.int8, device=d)
     zncc = torch.empty(N, dtype=torch.float64, device=d)
-    vol = volumes_struct(f, gx, gy, gz, mask, g)
+    vol = volumes_struct(f, gx, gy, gz, mask, g, g4)
     nh = None if node_half is None else dev(node_half, torch.int32)
     sub = subset_struct(half, stride, mode, split_index, split_keep, nh)
     prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats)
@@ -160,7 +169,7 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
 
 def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, meanf, bottomf, valid, mu, tol, dp_tol, max_iter,
           patience, stride=1, n_full=0.0, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED,
-          threads=0, brick_floats=0, node_half=None):
+          threads=0, brick_floats=0, node_half=None, g4=None):
     """Device 3-DOF IC-GN (ADMM subproblem 1); returns (U (N,3), n_iter, status, zncc) tensors."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
@@ -172,7 +181,7 @@ def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, 
     n_iter = torch.empty(N, dtype=torch.int32, device=d)
     status = torch.empty(N, dtype=torch.int8, device=d)
     zncc = torch.empty(N, dtype=torch.float64, device=d)
-    vol = volumes_struct(f, gx, gy, gz, mask, g)
+    vol = volumes_struct(f, gx, gy, gz, mask, g, g4)
     nh = None if node_half is None else dev(node_half, torch.int32)
     sub = subset_struct(half, stride, mode, split_index, split_keep, nh)
     prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats, mu, n_full)

@@ -326,6 +326,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     tr.mark("init_guess")
 
     # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
+    # the persistent kernels read each cubic tap row of g as one 16-byte load from its overlapping-quad copy
+    g4 = K.make_quads(g_prep) if (mode != 0 and p.variant == K.BATCHED) else None
     P0 = torch.zeros((mesh.n, 12), dtype=torch.float64, device="cuda")
     P0[:, 9:] = U0
 
@@ -335,7 +337,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         nh = node_half if (node_half is None or idx is None) else node_half[idx]
         return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g_prep, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
                         p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
-                        node_half=nh)
+                        node_half=nh, g4=g4)
 
     th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
     P, n_iter, status, zncc = icgn12_on(None, th12, br12)
@@ -375,7 +377,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
     # every tensor the ADMM loop reads; a captured loop reads static copies of them
     T = {"f": f, "g": g_prep, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
-         "coords": mesh.coords, "elem": elem_active, "node_half": node_half}
+         "coords": mesh.coords, "elem": elem_active, "node_half": node_half, "g4": g4}
 
     def make_steps(T):
         def global_step(U1_, F1_, W_, v_):
@@ -394,7 +396,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             nh = T["node_half"] if (T["node_half"] is None or idx is None) else T["node_half"][idx]
             return K.icgn3(c, U2_, F2_, v_, mesh.half, T["f"], T["gx"], T["gy"], T["gz"], T["m"], T["g"], mode, H_, mf_, bf_, ok_,
                            p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0,
-                           p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh)
+                           p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh, g4=T["g4"])
 
         def admm_step(U2, F2, W, v, th3, br3):
             # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
