@@ -534,6 +534,60 @@ struct Acc {
         }
         ++n;
     }
+    // The same sums split by what they depend on: REF the reference-frame sums (Σ f, Σ f², Σ SD, Σ SD·f, fixed
+    // for a node), WARP the sums over the sampled g and the valid count.  Each field is updated by the same
+    // expression as in add(), so a sweep of either part gives the FP32 partials add() would give.
+    template <bool REF, bool WARP>
+    __device__ __forceinline__ void add_part(float fs, float gs, float q0, float q1, float q2, float X, float Y, float Z) {
+        if (WARP) {
+            Sg += gs;
+            Sgg += gs * gs;
+        }
+        if (REF) {
+            Sf += fs;
+            Sff += fs * fs;
+        }
+        if (WARP) Sfg += fs * gs;
+        const float q[3] = {q0, q1, q2};
+        if (NDOF == 12) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (REF) {
+                    const float qf = q[i] * fs;
+                    SD[3 * i] += q[i] * X;
+                    SD[3 * i + 1] += q[i] * Y;
+                    SD[3 * i + 2] += q[i] * Z;
+                    SD[9 + i] += q[i];
+                    SDf[3 * i] += qf * X;
+                    SDf[3 * i + 1] += qf * Y;
+                    SDf[3 * i + 2] += qf * Z;
+                    SDf[9 + i] += qf;
+                }
+                if (WARP) {
+                    const float qg = q[i] * gs;
+                    SDg[3 * i] += qg * X;
+                    SDg[3 * i + 1] += qg * Y;
+                    SDg[3 * i + 2] += qg * Z;
+                    SDg[9 + i] += qg;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (REF) {
+                    SD[i] += q[i];
+                    SDf[i] += q[i] * fs;
+                }
+                if (WARP) SDg[i] += q[i] * gs;
+            }
+        }
+        if (WARP) ++n;
+    }
+};
+
+template <int K>
+struct SweepKind {
+    static constexpr int value = K;
 };
 
 // Cross-warp FP64 totals in a fixed order (deterministic), thread 0 only.
@@ -832,28 +886,33 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
 
 // ----------------------------------------------------------------------------- lean persistent kernel
 // NW warps per node and no shared brick: the deformed volume is sampled through L1 at positions taken
-// relative to the node centre, so a CTA holds only its control block and up to 16 nodes run per SM.
-// While thread 0 of one CTA runs the FP64 control step, the other CTAs of the SM keep the pipes busy.
-// Voxel indices advance incrementally (no divisions in the loop); the per-thread FP32 moments are
-// reduced across the warp in FP64.
+// relative to the node centre, so a CTA holds only its control block and 16 (12-DOF, 128 registers a
+// thread) or 24 (3-DOF, 80) warps run per SM.  While thread 0 of one CTA runs the FP64 control step, the
+// other CTAs of the SM keep the pipes busy.  Voxel indices advance incrementally (no divisions in the loop);
+// the per-thread FP32 moments are reduced across the warp in FP64.  The reference-frame sums are swept
+// only while a node has none stored (its first iteration, or after a NaN sample).
 struct LeanCtl {
     double P[12];
     float A[9];
     float t[3];
     int slow;
     int state;
+    int use_ref;  // the node's reference-frame sums are taken from ref_tot (set by its first complete sweep)
+    int redo;     // this iteration met a NaN sample under use_ref: sweep it again with every sum
     int64_t node;
     float cf, cg;
 };
 
 template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN>
-__global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a) {
+__global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lean_kernel(IcgnArgs a) {
     constexpr int T = NW * 32;
     constexpr int NB = Acc<NDOF>::NB;
     constexpr int NV = 5 + 3 * NB;
+    constexpr int NR = 2 + 2 * NB;
     __shared__ LeanCtl sc;
     __shared__ double red[NW][NV];
     __shared__ int redi[NW][3];
+    __shared__ double ref_tot[NR];  // Σ f, Σ f², Σ SD, Σ SD·f of the node's kept voxels (FP64 totals, thread 0)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t sxy = (int64_t)a.nx * a.ny;
     const int lo = MODE == 0 ? 0 : 1, hx_ = MODE == 0 ? a.nx - 2 : a.nx - 3, hy_ = MODE == 0 ? a.ny - 2 : a.ny - 3,
@@ -894,32 +953,14 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
         const bool inside = xc - sh.hx >= 0 && xc + sh.hx < a.nx && yc - sh.hy >= 0 && yc + sh.hy < a.ny && zcn - sh.hz >= 0 &&
                             zcn + sh.hz < a.nz;
         const int xci = (int)xc, yci = (int)yc, zci = (int)zcn;
+        const float cf = sc.cf;
 
-        for (int it = 1; it <= a.max_iter; ++it) {
-            if (tid == 0) {
-                const Box bb = warp_box(a, sh, sc.P, xc, yc, zcn, 0, sh.nZ, MODE);
-                sc.slow = bb.corners_in ? 0 : 1;
-                const double* P = sc.P;
-                sc.A[0] = (float)(1.0 + P[0]);
-                sc.A[1] = (float)P[1];
-                sc.A[2] = (float)P[2];
-                sc.A[3] = (float)P[3];
-                sc.A[4] = (float)(1.0 + P[4]);
-                sc.A[5] = (float)P[5];
-                sc.A[6] = (float)P[6];
-                sc.A[7] = (float)P[7];
-                sc.A[8] = (float)(1.0 + P[8]);
-                sc.t[0] = (float)P[9];
-                sc.t[1] = (float)P[10];
-                sc.t[2] = (float)P[11];
-            }
-            __syncthreads();
-            const bool slow = sc.slow != 0;
-            const float A0 = sc.A[0], A1 = sc.A[1], A2 = sc.A[2], A3 = sc.A[3], A4 = sc.A[4], A5 = sc.A[5], A6 = sc.A[6],
-                        A7 = sc.A[7], A8 = sc.A[8];
-            const float T0 = sc.t[0], T1 = sc.t[1], T2 = sc.t[2];
-            const float cf = sc.cf, cg = sc.cg;
-            Acc<NDOF> acc;
+        // One sweep over the node's subset.  KIND 1: the sums over the sampled g and the counts; KIND 2: every sum.
+        // Both visit the same voxels in the same per-thread order, so the partials of a field do not depend on the
+        // kind that formed them.
+        auto sweep = [&](auto kind, Acc<NDOF>& acc, bool slow, float A0, float A1, float A2, float A3, float A4, float A5,
+                         float A6, float A7, float A8, float T0, float T1, float T2, float cg) {
+            constexpr int KIND = decltype(kind)::value;
             acc.zero();
             int ix = tix, iy = tiy, iz = tiz;
             for (int v = tid; v < S; v += T) {
@@ -980,35 +1021,74 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
                                                                                          yr - fyf, zr - fzf)
                                                      : sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf, yr - fyf, zr - fzf);
                 if (gv != gv) continue;  // NaN: masked out in the deformed frame
-                acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
+                if (KIND == 1)
+                    acc.template add_part<false, true>(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
+                else
+                    acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
             }
+        };
+        // per-warp FP64 totals of a sweep's partials into red / redi
+        auto reduce_warp = [&](const Acc<NDOF>& acc) {
+            float vals[NV];
+            vals[0] = acc.Sg;
+            vals[1] = acc.Sgg;
+            vals[2] = acc.Sf;
+            vals[3] = acc.Sff;
+            vals[4] = acc.Sfg;
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                vals[5 + k] = acc.SD[k];
+                vals[5 + NB + k] = acc.SDf[k];
+                vals[5 + 2 * NB + k] = acc.SDg[k];
+            }
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+                double s = (double)vals[i];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) red[warp][i] = s;
+            }
+            const int n = warp_sum_i(acc.n), nr = warp_sum_i(acc.nref);
+            const int oob = __any_sync(0xffffffffu, acc.oob != 0) ? 1 : 0;
+            if (lane == 0) {
+                redi[warp][0] = n;
+                redi[warp][1] = nr;
+                redi[warp][2] = oob;
+            }
+        };
+
+        if (tid == 0) sc.use_ref = 0;  // the first iteration sweeps every sum (read after the loop's first barrier)
+
+        for (int it = 1; it <= a.max_iter; ++it) {
+            if (tid == 0) {
+                const Box bb = warp_box(a, sh, sc.P, xc, yc, zcn, 0, sh.nZ, MODE);
+                sc.slow = bb.corners_in ? 0 : 1;
+                const double* P = sc.P;
+                sc.A[0] = (float)(1.0 + P[0]);
+                sc.A[1] = (float)P[1];
+                sc.A[2] = (float)P[2];
+                sc.A[3] = (float)P[3];
+                sc.A[4] = (float)(1.0 + P[4]);
+                sc.A[5] = (float)P[5];
+                sc.A[6] = (float)P[6];
+                sc.A[7] = (float)P[7];
+                sc.A[8] = (float)(1.0 + P[8]);
+                sc.t[0] = (float)P[9];
+                sc.t[1] = (float)P[10];
+                sc.t[2] = (float)P[11];
+            }
+            __syncthreads();
+            const bool slow = sc.slow != 0;
+            const bool use_ref = sc.use_ref != 0;
             {
-                float vals[NV];
-                vals[0] = acc.Sg;
-                vals[1] = acc.Sgg;
-                vals[2] = acc.Sf;
-                vals[3] = acc.Sff;
-                vals[4] = acc.Sfg;
-#pragma unroll
-                for (int k = 0; k < NB; ++k) {
-                    vals[5 + k] = acc.SD[k];
-                    vals[5 + NB + k] = acc.SDf[k];
-                    vals[5 + 2 * NB + k] = acc.SDg[k];
-                }
-#pragma unroll
-                for (int i = 0; i < NV; ++i) {
-                    double s = (double)vals[i];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if (lane == 0) red[warp][i] = s;
-                }
-                const int n = warp_sum_i(acc.n), nr = warp_sum_i(acc.nref);
-                const int oob = __any_sync(0xffffffffu, acc.oob != 0) ? 1 : 0;
-                if (lane == 0) {
-                    redi[warp][0] = n;
-                    redi[warp][1] = nr;
-                    redi[warp][2] = oob;
-                }
+                Acc<NDOF> acc;
+                if (use_ref)
+                    sweep(SweepKind<1>{}, acc, slow, sc.A[0], sc.A[1], sc.A[2], sc.A[3], sc.A[4], sc.A[5], sc.A[6], sc.A[7], sc.A[8],
+                          sc.t[0], sc.t[1], sc.t[2], sc.cg);
+                else
+                    sweep(SweepKind<2>{}, acc, slow, sc.A[0], sc.A[1], sc.A[2], sc.A[3], sc.A[4], sc.A[5], sc.A[6], sc.A[7], sc.A[8],
+                          sc.t[0], sc.t[1], sc.t[2], sc.cg);
+                reduce_warp(acc);
             }
             __syncthreads();
             if (tid == 0) {
@@ -1039,34 +1119,61 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW) icgn_lean_kernel(IcgnArgs a)
                     mom.SDf[k] = t[5 + NB + k];
                     mom.SDg[k] = t[5 + 2 * NB + k];
                 }
-                double b[12], bf, bg, s_cc;
-                int64_t nv;
-                const int st0 = finish_moments(mom, sc.cf, sc.cg, NB, b, bf, bg, s_cc, nv);
-                int st;
-                double zc = nan("");
-                if (st0 != 0) {
-                    st = st0;
-                } else if (NDOF == 12) {
-                    st = control12(c12, b, bf, bg, s_cc, nv, a.L + node * 144, a.H ? a.H + node * 144 : nullptr, a.pattern,
-                                   a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+                // The reference-frame sums (Σ f, Σ f², Σ SD, Σ SD·f) do not depend on the warp: a full sweep in which
+                // every kept voxel entered the sums serves the later iterations whose samples are all finite.  A NaN
+                // sample under use_ref left a kept voxel out: that iteration is swept again with every sum.
+                const bool redo = use_ref && !oo && nn != nrr;
+                sc.redo = redo ? 1 : 0;
+                if (redo) {
+                    sc.use_ref = 0;
                 } else {
-                    st = control3(c3, b, bf, bg, s_cc, nv, a.mu, a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
-                }
-                if (st >= 0) {
-                    node_end<NDOF>(a, node, c12, c3, it, st, zc);
-                    sc.state = 1;
-                } else {
-                    const double* P = NDOF == 12 ? c12.P : c3.P;
-                    for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
-                    sc.cg = (float)((double)sc.cg + mom.Sg / (double)mom.n);
-                    if (it == a.max_iter) {
-                        node_end<NDOF>(a, node, c12, c3, a.max_iter, ST_MAX_ITER, NDOF == 12 ? c12.zncc : c3.zncc);
+                    if (!use_ref && !oo && nn == nrr) {
+                        ref_tot[0] = t[2];
+                        ref_tot[1] = t[3];
+                        for (int k = 0; k < NB; ++k) {
+                            ref_tot[2 + k] = t[5 + k];
+                            ref_tot[2 + NB + k] = t[5 + NB + k];
+                        }
+                        sc.use_ref = 1;
+                    }
+                    if (use_ref) {
+                        mom.Sf = ref_tot[0];
+                        mom.Sff = ref_tot[1];
+                        for (int k = 0; k < NB; ++k) {
+                            mom.SD[k] = ref_tot[2 + k];
+                            mom.SDf[k] = ref_tot[2 + NB + k];
+                        }
+                    }
+                    double b[12], bf, bg, s_cc;
+                    int64_t nv;
+                    const int st0 = finish_moments(mom, sc.cf, sc.cg, NB, b, bf, bg, s_cc, nv);
+                    int st;
+                    double zc = nan("");
+                    if (st0 != 0) {
+                        st = st0;
+                    } else if (NDOF == 12) {
+                        st = control12(c12, b, bf, bg, s_cc, nv, a.L + node * 144, a.H ? a.H + node * 144 : nullptr, a.pattern,
+                                       a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+                    } else {
+                        st = control3(c3, b, bf, bg, s_cc, nv, a.mu, a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
+                    }
+                    if (st >= 0) {
+                        node_end<NDOF>(a, node, c12, c3, it, st, zc);
                         sc.state = 1;
+                    } else {
+                        const double* P = NDOF == 12 ? c12.P : c3.P;
+                        for (int k = 0; k < 12; ++k) sc.P[k] = P[k];
+                        sc.cg = (float)((double)sc.cg + mom.Sg / (double)mom.n);
+                        if (it == a.max_iter) {
+                            node_end<NDOF>(a, node, c12, c3, a.max_iter, ST_MAX_ITER, NDOF == 12 ? c12.zncc : c3.zncc);
+                            sc.state = 1;
+                        }
                     }
                 }
             }
             __syncthreads();
             if (sc.state != 0) break;
+            if (sc.redo) --it;  // the same iteration again, every sum swept (sc.use_ref is now 0)
         }
     }
 }
