@@ -1718,7 +1718,8 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N, N >= 48 ? 3 : 1) fftr_pa
                          [&](int r, int x, float2 v) { dst[(int64_t)r * N + x] = v; });
 }
 
-// One CTA per (ky, -ky) row pair: thread (q, c) holds the z-line of column c of its row in registers.
+// One CTA per (ky, -ky) row pair: thread (q, c) holds the z-line of column c of its row in registers.  The
+// product planes keep rows ky <= N/2 ([nb][vz][N/2 + 1][N]).
 template <int N>
 __global__ void __launch_bounds__(2 * N) fftr_pass2_kernel(FftArgs a) {
     constexpr int PITCH = N | 1;
@@ -1742,8 +1743,10 @@ __global__ void __launch_bounds__(2 * N) fftr_pass2_kernel(FftArgs a) {
         for (int k = 0; k < N; ++k) S(q, k, c) = v[k];
     }
     __syncthreads();
-    if (!active) return;
-    const int qm = self ? 0 : 1 - q, cm = (N - c) % N;
+    // rows ky > N/2 only lend their spectra: the product is Hermitian (the cross term is real), so its rows
+    // ky <= N/2 (those of q = 0) hold all of it
+    if (!active || q == 1) return;
+    const int qm = self ? 0 : 1, cm = (N - c) % N;
 #pragma unroll
     for (int kz = 0; kz < N; ++kz) {
         const float2 za = v[kz];
@@ -1755,19 +1758,32 @@ __global__ void __launch_bounds__(2 * N) fftr_pass2_kernel(FftArgs a) {
         v[kz] = fr_mul(w, tc);
     }
     fft_line<N, 1>(v);
-    float2* dst = a.P + (int64_t)blockIdx.y * G.vz * N * N + ky * N + c;
+    constexpr int NH = N / 2 + 1;
+    float2* dst = a.P + (int64_t)blockIdx.y * G.vz * NH * N + ky * N + c;
 #pragma unroll
     for (int dz = 0; dz < N; ++dz)
-        if (dz < G.vz) dst[(int64_t)dz * N * N] = v[dz];
+        if (dz < G.vz) dst[(int64_t)dz * NH * N] = v[dz];
 }
 
-// Pass 3: thread (plane, x) reads its y-column of the product straight into registers (coalesced across
-// threads) and inverts along y; thread (plane, dy < vy) inverts the row along x; the normalised map rows go out.
+// Pass 3: planes per CTA of the half-spectrum tile [N][N/2 + 1 | 1] of each plane, at most 256 threads.
 template <int N>
-__global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArgs a) {
-    constexpr int P = fftr_planes<N>();
-    constexpr int PITCH = N | 1;
-    extern __shared__ __align__(16) float2 fsm[];  // [P][N][PITCH]
+__host__ __device__ constexpr int fftr_planes3() {
+    constexpr int NH = N / 2 + 1;
+    constexpr int by_smem = 70000 / (N * (NH | 1) * 8);
+    constexpr int by_threads = 256 / NH;
+    return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
+}
+
+// Pass 3: thread (plane, kx <= N/2) reads its y-column of the product straight into registers (rows ky > N/2 as
+// the conjugates of rows N - ky at column N - kx: the product is Hermitian) and inverts along y; the columns
+// kx > N/2 are the conjugates of these, so thread (plane, j) inverts the real rows 2j and 2j + 1 along x as ONE
+// complex transform (row 2j in the real part, row 2j + 1 in the imaginary part).  The normalised map rows go out.
+template <int N>
+__global__ void __launch_bounds__(fftr_planes3<N>() * (N / 2 + 1)) fftr_pass3_kernel(FftArgs a) {
+    constexpr int NH = N / 2 + 1;
+    constexpr int P = fftr_planes3<N>();
+    constexpr int RP = NH | 1;
+    extern __shared__ __align__(16) float2 fsm[];  // [P][N][RP]: y-inverted columns kx <= N/2; then map rows
     const NccGeom& G = a.G;
     const int64_t node = a.node_base + blockIdx.y;
     const int dz0 = blockIdx.x * P;
@@ -1778,7 +1794,7 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArg
         return;
     }
     const int t = threadIdx.x;
-    const int pl = t / N, yx = t - pl * N;
+    const int pl = t / NH, kx = t - pl * NH;
     {  // the box sums of these planes are read last: start them towards L2 while the transforms run
         const int64_t sxy = (int64_t)G.nx * G.ny, wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
         const int nch = (G.vx + 31) / 32, per_row = 2 * nch;
@@ -1788,25 +1804,49 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArg
             prefetch_l2(b + (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + wx0 + 32 * (rem >> 1));
         }
     }
-    if (pl < np) {  // inverse along y, every column
-        const float2* colg = a.P + ((int64_t)blockIdx.y * G.vz + dz0 + pl) * N * N + yx;
+    if (pl < np) {  // inverse along y of column kx <= N/2
+        const float2* pg = a.P + ((int64_t)blockIdx.y * G.vz + dz0 + pl) * NH * N;
+        const int kxm = (N - kx) % N;
         float2 v[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) v[k] = colg[k * N];
-        fft_line<N, 1>(v);
-        float2* col = fsm + pl * N * PITCH + yx;
+        for (int k = 0; k < NH; ++k) v[k] = pg[k * N + kx];
 #pragma unroll
-        for (int k = 0; k < N; ++k) col[k * PITCH] = v[k];
+        for (int k = NH; k < N; ++k) {
+            const float2 w = pg[(N - k) * N + kxm];
+            v[k] = make_float2(w.x, -w.y);
+        }
+        fft_line<N, 1>(v);
+        float2* col = fsm + pl * N * RP + kx;
+#pragma unroll
+        for (int k = 0; k < N; ++k) col[k * RP] = v[k];
     }
     __syncthreads();
-    if (pl < np && yx < G.vy) {  // inverse along x, rows dy < vy
-        float2* row = fsm + (pl * N + yx) * PITCH;
+    const int nj = (G.vy + 1) / 2;  // row pairs (2j, 2j + 1), 2j + 1 <= N - 1
+    if (pl < np && kx < nj) {
+        float2* ra = fsm + (pl * N + 2 * kx) * RP;
+        float2* rb = ra + RP;
+        const bool hb = 2 * kx + 1 < G.vy;
         float2 v[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) v[k] = row[k];
-        fft_line<N, 1>(v);
+        for (int k = 0; k < NH; ++k) {  // X_a + i X_b
+            const float2 xa = ra[k], xb = hb ? rb[k] : make_float2(0.0f, 0.0f);
+            v[k] = make_float2(xa.x - xb.y, xa.y + xb.x);
+        }
 #pragma unroll
-        for (int k = 0; k < N; ++k) row[k] = v[k];
+        for (int k = NH; k < N; ++k) {  // conj X_a[N - k] + i conj X_b[N - k]
+            const float2 xa = ra[N - k], xb = hb ? rb[N - k] : make_float2(0.0f, 0.0f);
+            v[k] = make_float2(xa.x + xb.y, xb.x - xa.y);
+        }
+        fft_line<N, 1>(v);
+        // the two map rows, as floats at the start of their own tile rows (both rows were read above)
+        float* ma = reinterpret_cast<float*>(ra);
+        float* mb = reinterpret_cast<float*>(rb);
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            if (k < G.vx) {
+                ma[k] = v[k].x;
+                if (hb) mb[k] = v[k].y;
+            }
     }
     __syncthreads();
     const double scale = 1.0 / ((double)N * N * N);
@@ -1817,6 +1857,7 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArg
     // settled on FP64 re-scores
     const float fscale = (float)scale;
     const double inv_n = 1.0 / n_tpl;
+    const float* msm = reinterpret_cast<const float*>(fsm);
     sweep_lin<4, float2>(
         np * G.vy, G.vx,
         [&](int r, int dx) {
@@ -1830,7 +1871,7 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N) fftr_pass3_kernel(FftArg
             const double var = (double)bs.y - s1 * s1 * inv_n;
             float v = 0.0f;
             if (!(var < 1e-20)) {
-                v = fsm[(p_ * N + dy) * PITCH + dx].x * fscale * rsqrtf((float)(var * ssf));
+                v = msm[2 * (p_ * N + dy) * RP + dx] * fscale * rsqrtf((float)(var * ssf));
                 v = fminf(1.0f, fmaxf(-1.0f, v));
             }
             out[(int64_t)p_ * G.vy * G.vx + dy * G.vx + dx] = v;
@@ -1863,12 +1904,14 @@ static int fftr_upload() {
 template <int N>
 static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     constexpr int P = fftr_planes<N>();
+    constexpr int P3 = fftr_planes3<N>();
     constexpr size_t SM = (size_t)P * N * (N | 1) * sizeof(float2);
     constexpr size_t SM2 = (size_t)2 * N * (N | 1) * sizeof(float2);
+    constexpr size_t SM3 = (size_t)P3 * N * ((N / 2 + 1) | 1) * sizeof(float2);
     static bool attr = false;  // set once, outside any capture (the first search of this length)
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(fftr_pass1_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(fftr_pass3_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fftr_pass3_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM3);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fftr_pass2_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM2);
         if (e != cudaSuccess) return cuda_fail(e, "ncc fft: shared memory attribute");
         attr = true;
@@ -1888,7 +1931,7 @@ static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     if (rc) return rc;
     {
         KTimer kt_("fft_pass3", s);
-        fftr_pass3_kernel<N><<<dim3((G.vz + P - 1) / P, nb), P * N, SM, s>>>(a);
+        fftr_pass3_kernel<N><<<dim3((G.vz + P3 - 1) / P3, nb), P3 * (N / 2 + 1), SM3, s>>>(a);
     }
     return check_launch("ncc fft pass 3");
 }
@@ -1920,7 +1963,9 @@ static bool fft_config(const NccGeom& G, FftCfg& c, bool engine_reg = true) {
     c.smem13 = ((size_t)2 * c.ay.n * c.pitch + 2 * FFT_MAX_N) * sizeof(float2);
     // pass 2: two buffers of one whole row (Nz x pitch) or of two half rows (2 x Nz x (cb | 1))
     c.smem2 = ((size_t)2 * std::max(c.pitch, 2 * (((c.ax.n + 1) / 2) | 1)) * c.az.n + FFT_MAX_N) * sizeof(float2);
-    c.per_node = ((int64_t)G.wz + G.vz) * c.ay.n * c.ax.n * (int64_t)sizeof(float2);
+    // the in-register passes keep the product rows ky <= N/2 only
+    const int64_t p_rows = c.reg ? c.ay.n / 2 + 1 : c.ay.n;
+    c.per_node = ((int64_t)G.wz * c.ay.n + (int64_t)G.vz * p_rows) * c.ax.n * (int64_t)sizeof(float2);
     const size_t smax = (size_t)max_smem_optin() - 4096;
     return c.smem13 <= smax && c.smem2 <= smax;
 }
