@@ -1718,39 +1718,47 @@ __global__ void __launch_bounds__(fftr_planes<N>() * N, N >= 48 ? 3 : 1) fftr_pa
                          [&](int r, int x, float2 v) { dst[(int64_t)r * N + x] = v; });
 }
 
-// One CTA per (ky, -ky) row pair: thread (q, c) holds the z-line of column c of its row in registers.  The
-// product planes keep rows ky <= N/2 ([nb][vz][N/2 + 1][N]).
+// One CTA per (ky, -ky) row pair, one thread per column c: the thread transforms the z-line of column c of row
+// -ky and parks it in shared memory, then transforms that of row ky in registers, forms the product with the
+// partner lines and inverts it.  The product is Hermitian (the cross term is real), so its rows ky <= N/2 hold all
+// of it: the product planes keep only those ([nb][vz][N/2 + 1][N]) and row -ky needs no inverse.
 template <int N>
-__global__ void __launch_bounds__(2 * N) fftr_pass2_kernel(FftArgs a) {
+__global__ void __launch_bounds__(N, N > 50 ? 4 : 8) fftr_pass2_kernel(FftArgs a) {
     constexpr int PITCH = N | 1;
-    extern __shared__ __align__(16) float2 fsm[];  // the two rows' spectra [2][N][PITCH]
-    auto S = [&](int q, int k, int c) -> float2& { return fsm[(q * N + k) * PITCH + c]; };
+    constexpr int NH = N / 2 + 1;
+    extern __shared__ __align__(16) float2 fsm[];  // spectrum of row -ky (of row ky when ky = -ky) [N][PITCH]
     const NccGeom& G = a.G;
     const int64_t node = a.node_base + blockIdx.y;
     if (!fft_node_ok(a, node)) return;
     const int ky0 = blockIdx.x, ky1 = (N - ky0) % N;
     const bool self = ky0 == ky1;
-    const int t = threadIdx.x, q = t / N, c = t - q * N;
-    const bool active = !(self && q == 1);
-    const int ky = q == 0 ? ky0 : ky1;
+    const int c = threadIdx.x;
+    const float2* An = a.A + (int64_t)blockIdx.y * G.wz * N * N;
     float2 v[N];
-    if (active) {
-        const float2* col = a.A + (int64_t)blockIdx.y * G.wz * N * N + ky * N + c;
+    if (!self) {
+        const float2* col = An + ky1 * N + c;
 #pragma unroll
         for (int z = 0; z < N; ++z) v[z] = z < G.wz ? col[(int64_t)z * N * N] : make_float2(0.0f, 0.0f);
         fft_line<N, -1>(v);
 #pragma unroll
-        for (int k = 0; k < N; ++k) S(q, k, c) = v[k];
+        for (int k = 0; k < N; ++k) fsm[k * PITCH + c] = v[k];
+    }
+    {
+        const float2* col = An + ky0 * N + c;
+#pragma unroll
+        for (int z = 0; z < N; ++z) v[z] = z < G.wz ? col[(int64_t)z * N * N] : make_float2(0.0f, 0.0f);
+        fft_line<N, -1>(v);
+    }
+    if (self) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) fsm[k * PITCH + c] = v[k];
     }
     __syncthreads();
-    // rows ky > N/2 only lend their spectra: the product is Hermitian (the cross term is real), so its rows
-    // ky <= N/2 (those of q = 0) hold all of it
-    if (!active || q == 1) return;
-    const int qm = self ? 0 : 1, cm = (N - c) % N;
+    const int cm = (N - c) % N;
 #pragma unroll
     for (int kz = 0; kz < N; ++kz) {
         const float2 za = v[kz];
-        const float2 zb = S(qm, (N - kz) % N, cm);
+        const float2 zb = fsm[((N - kz) % N) * PITCH + cm];
         const float2 zbc = make_float2(zb.x, -zb.y);
         const float2 w = make_float2(0.5f * (za.x + zbc.x), 0.5f * (za.y + zbc.y));
         const float2 d = make_float2(za.x - zbc.x, za.y - zbc.y);
@@ -1758,8 +1766,7 @@ __global__ void __launch_bounds__(2 * N) fftr_pass2_kernel(FftArgs a) {
         v[kz] = fr_mul(w, tc);
     }
     fft_line<N, 1>(v);
-    constexpr int NH = N / 2 + 1;
-    float2* dst = a.P + (int64_t)blockIdx.y * G.vz * NH * N + ky * N + c;
+    float2* dst = a.P + (int64_t)blockIdx.y * G.vz * NH * N + ky0 * N + c;
 #pragma unroll
     for (int dz = 0; dz < N; ++dz)
         if (dz < G.vz) dst[(int64_t)dz * NH * N] = v[dz];
@@ -1906,7 +1913,7 @@ static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     constexpr int P = fftr_planes<N>();
     constexpr int P3 = fftr_planes3<N>();
     constexpr size_t SM = (size_t)P * N * (N | 1) * sizeof(float2);
-    constexpr size_t SM2 = (size_t)2 * N * (N | 1) * sizeof(float2);
+    constexpr size_t SM2 = (size_t)N * (N | 1) * sizeof(float2);
     constexpr size_t SM3 = (size_t)P3 * N * ((N / 2 + 1) | 1) * sizeof(float2);
     static bool attr = false;  // set once, outside any capture (the first search of this length)
     if (!attr) {
@@ -1925,7 +1932,7 @@ static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     if (rc) return rc;
     {
         KTimer kt_("fft_pass2", s);
-        fftr_pass2_kernel<N><<<dim3(N / 2 + 1, nb), 2 * N, SM2, s>>>(a);
+        fftr_pass2_kernel<N><<<dim3(N / 2 + 1, nb), N, SM2, s>>>(a);
     }
     rc = check_launch("ncc fft pass 2");
     if (rc) return rc;
