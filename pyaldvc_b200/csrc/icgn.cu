@@ -913,6 +913,7 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
     __shared__ double red[NW][NV];
     __shared__ int redi[NW][3];
     __shared__ double ref_tot[NR];  // Σ f, Σ f², Σ SD, Σ SD·f of the node's kept voxels (FP64 totals, thread 0)
+    __shared__ double Ls[NDOF == 12 ? 144 : 1];  // the node's Cholesky factor: thread 0 solves with it every iteration
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t sxy = (int64_t)a.nx * a.ny;
     const int lo = MODE == 0 ? 0 : 1, hx_ = MODE == 0 ? a.nx - 2 : a.nx - 3, hy_ = MODE == 0 ? a.ny - 2 : a.ny - 3,
@@ -1058,6 +1059,8 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
         };
 
         if (tid == 0) sc.use_ref = 0;  // the first iteration sweeps every sum (read after the loop's first barrier)
+        if (NDOF == 12)
+            for (int i = tid; i < 144; i += T) Ls[i] = a.L[node * 144 + i];  // read after the loop's first barrier
 
         for (int it = 1; it <= a.max_iter; ++it) {
             if (tid == 0) {
@@ -1152,7 +1155,7 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
                     if (st0 != 0) {
                         st = st0;
                     } else if (NDOF == 12) {
-                        st = control12(c12, b, bf, bg, s_cc, nv, a.L + node * 144, a.H ? a.H + node * 144 : nullptr, a.pattern,
+                        st = control12(c12, b, bf, bg, s_cc, nv, Ls, a.H ? a.H + node * 144 : nullptr, a.pattern,
                                        a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
                     } else {
                         st = control3(c3, b, bf, bg, s_cc, nv, a.mu, a.noise_gain, a.tol, a.dp_tol, a.patience, a.predictive, zc);
