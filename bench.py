@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=1, help="timed passes of the plain form (0 skips it)")
     ap.add_argument("--cpu-nodes", type=int, default=8, help="node block edge of the CPU baseline sample (cube root)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--icgn-threads", type=int, default=0,
+                    help="pin the batched IC-GN kernels to the lean form with this many threads per node (32/64/128) "
+                         "instead of the autotuner's choice (for profiler runs, whose timings would mislead it)")
     return ap.parse_args()
 
 
@@ -238,12 +241,16 @@ def _smooth_len(n: int) -> int:
         m += 1
 
 
+FFT_REG_SIZES = (36, 40, 48, 50, 54, 60, 64)  # cubic FFT boxes transformed a line per thread in registers
+
+
 def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
     """Roofline of every timed kernel of one pass: algorithmic work of the pass for that kernel (bytes it must move,
     or FP32 flops) over its summed device time.  Work per unit:
       fft_pass1  window + template in, spectrum planes out: (wz wy wx + sz sy sxp) 4 B + wz Ny Nx 8 B per node
-      fft_pass2  spectrum planes in, product planes out: (wz + vz) Ny Nx 8 B per node
-      fft_pass3  product planes in, box sums in, map out: vz Ny Nx 8 B + 3 n_off 4 B per node
+      fft_pass2  spectrum planes in, product planes out: (wz Ny + vz Ny') Nx 8 B per node
+      fft_pass3  product planes in, box sums in, map out: vz Ny' Nx 8 B + 3 n_off 4 B per node
+                 (Ny' = Ny / 2 + 1 for the in-register cubic boxes, which keep the product's Hermitian half; else Ny)
       ncc_peak   two sweeps of the FP32 map: 2 n_off 4 B per node
       ncc_template  template in, centred template out: (n_tpl + sz sy sxp) 4 B per node
       box_pass   16 B per voxel per launch
@@ -261,10 +268,12 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
         sxp = (s_[0] + 3) // 4 * 4
         n_tpl, n_off = float(np.prod(s_)), float(np.prod(v_))
         plane = N[0] * N[1] * 8.0  # Nx Ny complex
+        reg = N[0] == N[1] == N[2] and N[0] in FFT_REG_SIZES
+        pplane = N[0] * (N[1] // 2 + 1) * 8.0 if reg else plane  # product plane
         if engine == 2:
             byte_work["fft_pass1"] = byte_work.get("fft_pass1", 0.0) + n * ((w_[0] * w_[1] * w_[2] + s_[2] * s_[1] * sxp) * 4.0 + w_[2] * plane)
-            byte_work["fft_pass2"] = byte_work.get("fft_pass2", 0.0) + n * (w_[2] + v_[2]) * plane
-            byte_work["fft_pass3"] = byte_work.get("fft_pass3", 0.0) + n * (v_[2] * plane + 3.0 * n_off * 4.0)
+            byte_work["fft_pass2"] = byte_work.get("fft_pass2", 0.0) + n * (w_[2] * plane + v_[2] * pplane)
+            byte_work["fft_pass3"] = byte_work.get("fft_pass3", 0.0) + n * (v_[2] * pplane + 3.0 * n_off * 4.0)
         if engine in (0, 2):
             byte_work["ncc_template"] = byte_work.get("ncc_template", 0.0) + n * (n_tpl + s_[2] * s_[1] * sxp) * 4.0
         if engine == 0:
@@ -472,6 +481,8 @@ def main():
 
     cfg = args.config
     p = configs.params(cfg)
+    if args.icgn_threads:
+        p.threads, p.brick_floats = args.icgn_threads, 0
     f, g, mask, disp = configs.device_pair(cfg, seed=1000 + 17 * rank)
     torch.cuda.synchronize()
 

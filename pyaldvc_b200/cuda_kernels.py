@@ -118,6 +118,23 @@ class DeviceCache:
             self._items.popitem(last=False)
         return t
 
+    def get_quads(self, arr: np.ndarray):
+        """The overlapping-quad copy of ``arr`` (16 bytes per voxel, ``kernels.make_quads``), cached like ``get``."""
+        key = (id(arr), arr.shape, str(arr.dtype), "quads")
+        hit = self._items.get(key)
+        if hit is not None and hit[0] is arr:
+            self._items.move_to_end(key)
+            return hit[1]
+        import torch
+
+        from . import kernels
+
+        q = kernels.make_quads(self.get(arr, torch.float32))
+        self._items[key] = (arr, q)
+        while len(self._items) > self._size:
+            self._items.popitem(last=False)
+        return q
+
     def clear(self) -> None:
         self._items.clear()
 
@@ -220,12 +237,13 @@ def icgn_12dof_cuda(coords, P0, hx, hy, hz, f, gx, gy, gz, mask, g, mode, L_all,
     H_d = torch.from_numpy(np.ascontiguousarray(H_all, dtype=np.float64)).cuda() if use_noise else None
     pat = np.ascontiguousarray(pattern, dtype=np.float64) if use_noise else None
     si, sk = _split(split_index, split_keep)
+    g4 = _cache.get_quads(g) if (mode != 0 and variant == K.BATCHED) else None
     for start, stop in _chunks(N, chunk):
         sl = slice(start, stop)
         si_c = None if si is None else si[sl]
         P, it, st, zc = K.icgn12(coords_d[sl], P0_d[sl], (hx, hy, hz), f_d, gx_d, gy_d, gz_d, m_d, g_d, mode, L_d[sl], mf_d[sl],
                                  v_d[sl], tol, dp_tol, max_iter, patience, stride, None if H_d is None else H_d[sl], pat,
-                                 noise_gain if use_noise else 0.0, predictive, si_c, sk, variant, threads, brick_floats)
+                                 noise_gain if use_noise else 0.0, predictive, si_c, sk, variant, threads, brick_floats, g4=g4)
         P_out[sl] = P.cpu().numpy()
         n_iter[sl] = it.cpu().numpy()
         status[sl] = st.cpu().numpy()
@@ -261,12 +279,13 @@ def icgn_3dof_cuda(coords, U_old, F_fixed, vdual, hx, hy, hz, f, gx, gy, gz, mas
     mf_d, bf_d = up(meanf_all, (N,)), up(bottomf_all, (N,))
     v_d = torch.from_numpy(np.ascontiguousarray(valid, dtype=np.uint8)).cuda()
     si, sk = _split(split_index, split_keep)
+    g4 = _cache.get_quads(g) if (mode != 0 and variant == K.BATCHED) else None
     for start, stop in _chunks(N, chunk):
         sl = slice(start, stop)
         U, it, st, zc = K.icgn3(coords_d[sl], U_d[sl], F_d[sl], vd_d[sl], (hx, hy, hz), f_d, gx_d, gy_d, gz_d, m_d, g_d, mode,
                                 H_d[sl], mf_d[sl], bf_d[sl], v_d[sl], mu, tol, dp_tol, max_iter, patience, stride, n_full,
                                 noise_gain if noise_gain > 0.0 else 0.0, predictive, None if si is None else si[sl], sk, variant,
-                                threads, brick_floats)
+                                threads, brick_floats, g4=g4)
         U_out[sl] = U.cpu().numpy()
         n_iter[sl] = it.cpu().numpy()
         status[sl] = st.cpu().numpy()
