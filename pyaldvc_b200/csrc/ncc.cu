@@ -235,6 +235,15 @@ __global__ void __launch_bounds__(NCC_THREADS) ncc_map_kernel(MapArgs a) {
 }
 
 // ----------------------------------------------------------------------------- fused search
+// Partials of one block of a node's FP32 map (the planes one FFT pass-3 CTA writes), for the peak search: the
+// maximum with its first index, the minimum, and FP64 sums of the values and their squares (values below -1, the
+// unplaced-node marker, count as 0 as in the peak kernel's sweeps).
+struct MapPart {
+    double s1, s2;
+    float mx, mn;
+    int idx, pad;
+};
+
 struct SearchArgs {
     const float* f;
     const float* g;
@@ -254,6 +263,8 @@ struct SearchArgs {
     double* pce;
     uint8_t* clipped;
     uint8_t* ok;
+    const MapPart* part;  // per-block map partials of the chunk ([node][nblk]), or null: the peak kernel sweeps the map
+    int nblk, blk_planes;
 };
 
 // integer_search.py:374-386 window placement
@@ -372,6 +383,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     __shared__ double s_p8[NCC_THREADS / 32][9];  // the warps' partials of pair 8
     __shared__ float s_max, s_min;
     __shared__ int s_pk;
+    __shared__ double s_s1, s_s2;
     const NccGeom& G = a.G;
     const int64_t node = a.node_base + blockIdx.x;
     if (node >= a.n_nodes) return;
@@ -389,7 +401,9 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         }
         return;
     }
-    for (int i = tid * 32; i < G.nmap; i += NCC_THREADS * 32) prefetch_l2(map + i);  // the whole map towards L2
+    const bool fastp = a.part != nullptr;  // map partials from the producer: only candidate blocks are swept
+    if (!fastp)
+        for (int i = tid * 32; i < G.nmap; i += NCC_THREADS * 32) prefetch_l2(map + i);  // the whole map towards L2
     // the template first: its loads do not depend on the map, so their latency overlaps the map sweeps'
     // template: raw FP32 f (staged when SMEM), FP64 mean and sum of squares (integer_search.py:73-88)
     const int64_t x0 = a.coords[3 * node], y0 = a.coords[3 * node + 1], z0 = a.coords[3 * node + 2];
@@ -424,6 +438,31 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     const double ssf = block_sum_d(q, red);
     // flat template: the map is -2 everywhere (integer_search.py:420-421)
     const bool flat = map[0] < -1.5f;
+    const MapPart* parts = fastp ? a.part + (int64_t)blockIdx.x * a.nblk : nullptr;
+    if (fastp) {  // blocks in map order: the first maximum of the earliest block holding it is the first in the map
+        if (tid == 0) {
+            float b = -3.0f, m = 3.0f;
+            int bi = 0x7fffffff;
+            double t1 = 0.0, t2 = 0.0;
+            for (int k = 0; k < a.nblk; ++k) {
+                const MapPart q = parts[k];
+                if (q.mx > b || (q.mx == b && q.idx < bi)) {
+                    b = q.mx;
+                    bi = q.idx;
+                }
+                m = fminf(m, q.mn);
+                t1 += q.s1;
+                t2 += q.s2;
+            }
+            s_max = b;
+            s_pk = bi;
+            s_min = m;
+            s_s1 = t1;
+            s_s2 = t2;
+            s_ncand = 0;
+        }
+        __syncthreads();
+    } else {
     float best = -3.0f, mn = 3.0f;
     int bidx = 0x7fffffff;
     // eight loads in flight per thread, then the compares in ascending i (the first index wins a tie)
@@ -473,6 +512,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         s_ncand = 0;
     }
     __syncthreads();
+    }
     const float vmax = s_max, vmin = s_min;
     const float cmin = flat ? 0.0f : vmin;
     const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
@@ -501,6 +541,26 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     // candidates within the FP32 error bound of the maximum, and the PCE energy on the min-shifted map
     // (integer_search.py:448-452)
     double e = 0.0;
+    if (fastp) {
+        // only blocks whose maximum reaches the bound can hold candidates (the same FP32 comparison); the energy
+        // sum (v - c)^2 = sum v^2 - 2 c sum v + n c^2 from the blocks' FP64 sums
+        const int bsz = a.blk_planes * G.vy * G.vx;
+        for (int k = 0; k < a.nblk; ++k) {
+            if (flat || !(parts[k].mx >= vmax - NEAR_TIE)) continue;
+            const int hi = min(k * bsz + bsz, G.nmap);
+            for (int i = k * bsz + tid; i < hi; i += NCC_THREADS) {
+                const float vv = map[i];
+                const float v = vv < -1.0f ? 0.0f : vv;
+                if (v >= vmax - NEAR_TIE) {
+                    const int slot = atomicAdd(&s_ncand, 1);
+                    if (slot < MAX_CAND) s_cand[slot] = i;
+                }
+            }
+        }
+        __syncthreads();
+        const double c = (double)cmin, n = (double)G.nmap;
+        e = (s_s2 - 2.0 * c * s_s1 + n * c * c) / n;
+    } else {
     for (int i0 = tid; i0 < G.nmap; i0 += 8 * NCC_THREADS) {
         float vv[8];
 #pragma unroll
@@ -519,6 +579,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         }
     }
     e = block_sum_d(e, red) / (double)G.nmap;
+    }
     int pk = s_pk;
     double peak = (double)vmax;
     // one candidate at an interior offset (the common case): its FP64 score is the centre of the 27-neighbourhood,
@@ -1301,6 +1362,8 @@ struct FftArgs {
     float2* A;          // [nb][wz][Ny][Nx]
     float2* P;          // [nb][vz][Ny][Nx]
     float* out;         // maps of the batch
+    MapPart* part;      // per-block map partials of the batch ([node][nblk]) or null (in-register pass 3 only)
+    int nblk;
     int64_t node_base;  // first node of the batch
     int64_t n_nodes;
     int nb;
@@ -1786,7 +1849,12 @@ __host__ __device__ constexpr int fftr_planes3() {
 // kx > N/2 are the conjugates of these, so thread (plane, j) inverts the real rows 2j and 2j + 1 along x as ONE
 // complex transform (row 2j in the real part, row 2j + 1 in the imaginary part).  The normalised map rows go out.
 template <int N>
-__global__ void __launch_bounds__(fftr_planes3<N>() * (N / 2 + 1)) fftr_pass3_kernel(FftArgs a) {
+__host__ __device__ constexpr int fftr_pass3_threads() {  // whole warps (the partials reduce with full-warp shuffles)
+    return (fftr_planes3<N>() * (N / 2 + 1) + 31) / 32 * 32;
+}
+
+template <int N>
+__global__ void __launch_bounds__(fftr_pass3_threads<N>()) fftr_pass3_kernel(FftArgs a) {
     constexpr int NH = N / 2 + 1;
     constexpr int P = fftr_planes3<N>();
     constexpr int RP = NH | 1;
@@ -1798,6 +1866,14 @@ __global__ void __launch_bounds__(fftr_planes3<N>() * (N / 2 + 1)) fftr_pass3_ke
     float* out = a.out + (int64_t)blockIdx.y * G.nmap + (int64_t)dz0 * G.vy * G.vx;
     if (!fft_node_ok(a, node)) {
         for (int i = threadIdx.x; i < np * G.vy * G.vx; i += blockDim.x) out[i] = -2.0f;
+        if (a.part && threadIdx.x == 0) {  // every value counts as 0 in the peak search
+            MapPart q;
+            q.s1 = q.s2 = 0.0;
+            q.mx = q.mn = 0.0f;
+            q.idx = dz0 * G.vy * G.vx;
+            q.pad = 0;
+            a.part[(int64_t)blockIdx.y * a.nblk + blockIdx.x] = q;
+        }
         return;
     }
     const int t = threadIdx.x;
@@ -1865,6 +1941,11 @@ __global__ void __launch_bounds__(fftr_planes3<N>() * (N / 2 + 1)) fftr_pass3_ke
     const float fscale = (float)scale;
     const double inv_n = 1.0 / n_tpl;
     const float* msm = reinterpret_cast<const float*>(fsm);
+    // this block's partials for the peak search (values visited in ascending map index per thread)
+    float lmx = -3.0f, lmn = 3.0f;
+    int lidx = 0x7fffffff;
+    double ls1 = 0.0, ls2 = 0.0;
+    const int i0 = dz0 * G.vy * G.vx;
     sweep_lin<4, float2>(
         np * G.vy, G.vx,
         [&](int r, int dx) {
@@ -1882,7 +1963,53 @@ __global__ void __launch_bounds__(fftr_planes3<N>() * (N / 2 + 1)) fftr_pass3_ke
                 v = fminf(1.0f, fmaxf(-1.0f, v));
             }
             out[(int64_t)p_ * G.vy * G.vx + dy * G.vx + dx] = v;
+            if (v > lmx) {
+                lmx = v;
+                lidx = i0 + r * G.vx + dx;
+            }
+            lmn = fminf(lmn, v);
+            ls1 += (double)v;
+            ls2 += (double)v * (double)v;
         });
+    if (a.part) {
+        __shared__ MapPart wpart[fftr_pass3_threads<N>() / 32];
+        const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, lmx, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, lidx, o);
+            if (ob > lmx || (ob == lmx && oi < lidx)) {
+                lmx = ob;
+                lidx = oi;
+            }
+            lmn = fminf(lmn, __shfl_xor_sync(0xffffffffu, lmn, o));
+            ls1 += __shfl_xor_sync(0xffffffffu, ls1, o);
+            ls2 += __shfl_xor_sync(0xffffffffu, ls2, o);
+        }
+        if (lane == 0) {
+            wpart[warp].mx = lmx;
+            wpart[warp].idx = lidx;
+            wpart[warp].mn = lmn;
+            wpart[warp].s1 = ls1;
+            wpart[warp].s2 = ls2;
+        }
+        __syncthreads();
+        if (t == 0) {
+            MapPart q = wpart[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                const MapPart o = wpart[w];
+                if (o.mx > q.mx || (o.mx == q.mx && o.idx < q.idx)) {
+                    q.mx = o.mx;
+                    q.idx = o.idx;
+                }
+                q.mn = fminf(q.mn, o.mn);
+                q.s1 += o.s1;
+                q.s2 += o.s2;
+            }
+            q.pad = 0;
+            a.part[(int64_t)blockIdx.y * a.nblk + blockIdx.x] = q;
+        }
+    }
 }
 
 // twiddles of the in-register transforms, once per device (before any capture: the first FFT search does it)
@@ -1938,9 +2065,22 @@ static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     if (rc) return rc;
     {
         KTimer kt_("fft_pass3", s);
-        fftr_pass3_kernel<N><<<dim3((G.vz + P3 - 1) / P3, nb), P3 * (N / 2 + 1), SM3, s>>>(a);
+        fftr_pass3_kernel<N><<<dim3((G.vz + P3 - 1) / P3, nb), fftr_pass3_threads<N>(), SM3, s>>>(a);
     }
     return check_launch("ncc fft pass 3");
+}
+
+// map planes per pass-3 CTA of the in-register engine (the block of one map partial)
+static int fftr_planes3_n(int n) {
+    switch (n) {
+        case 36: return fftr_planes3<36>();
+        case 40: return fftr_planes3<40>();
+        case 48: return fftr_planes3<48>();
+        case 50: return fftr_planes3<50>();
+        case 54: return fftr_planes3<54>();
+        case 60: return fftr_planes3<60>();
+        default: return fftr_planes3<64>();
+    }
 }
 
 static int launch_fftr_n(int n, FftArgs& a, int nb, cudaStream_t s) {
@@ -2017,6 +2157,7 @@ static int launch_fft(FftArgs a, const FftCfg& c, int64_t n, int64_t batch, cuda
     if (rc) return rc;
     const NccGeom& G = a.G;
     float* out0 = a.out;
+    MapPart* part0 = a.part;
     const double* ssf0 = a.ssf;
     const float* T0 = a.T;
     const int64_t tsz = (int64_t)G.sz * G.sy * a.sxp;
@@ -2025,6 +2166,7 @@ static int launch_fft(FftArgs a, const FftCfg& c, int64_t n, int64_t batch, cuda
         const int nb = (int)std::min<int64_t>(batch, n - done);
         a.node_base = base0 + done;
         a.out = out0 + done * G.nmap;
+        a.part = part0 ? part0 + done * a.nblk : nullptr;
         a.ssf = ssf0 + done;
         a.T = T0 + done * tsz;
         a.nb = nb;
@@ -2159,6 +2301,11 @@ extern "C" int aldvc_ncc_map(const float* f, const float* g, int64_t nz, int64_t
     return launch_map(m, n_nodes, (cudaStream_t)stream);
 }
 
+static int fft_nblk(const NccGeom& G, const FftCfg& c) {
+    const int p3 = fftr_planes3_n(c.ax.n);
+    return (G.vz + p3 - 1) / p3;
+}
+
 static bool use_fft(const NccGeom& G, int32_t engine, FftCfg& c) {
     return (engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM) && fft_config(G, c, engine == ALDVC_NCC_FFT);
 }
@@ -2199,6 +2346,8 @@ extern "C" size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_
         b += 4 * align_up((size_t)nz * ny * nx * sizeof(float), 256) + tiled_tpl_bytes(G, chunk);
     if (fft)  // twiddles, one batch of spectra
         b += align_up(3 * FFT_MAX_N * sizeof(float2), 256) + align_up((size_t)fft_batch(fc, chunk) * fc.per_node, 256);
+    if (fft && fc.reg)  // map partials of a chunk
+        b += align_up((size_t)chunk * fft_nblk(G, fc) * sizeof(MapPart), 256);
     return b;
 }
 
@@ -2245,6 +2394,9 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
     a.pce = pce;
     a.clipped = clipped;
     a.ok = ok;
+    a.part = nullptr;
+    a.nblk = 0;
+    a.blk_planes = 0;
     ncc_place_kernel<<<(unsigned)((n_nodes + 255) / 256), 256, 0, s>>>(a);
     rc = check_launch("ncc place");
     if (rc) return rc;
@@ -2334,6 +2486,15 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
             fa.tw = tw;
             fa.A = scr;
             fa.P = scr + batch * (int64_t)G.wz * fc.ay.n * fc.ax.n;
+            fa.part = nullptr;
+            fa.nblk = 0;
+            if (fc.reg) {  // the map partials follow the spectra scratch
+                fa.nblk = fft_nblk(G, fc);
+                fa.part = (MapPart*)((char*)scr + align_up((size_t)batch * fc.per_node, 256));
+                a.part = fa.part;
+                a.nblk = fa.nblk;
+                a.blk_planes = fftr_planes3_n(fc.ax.n);
+            }
             fa.n_nodes = n_nodes;
             fa.G = G;
             fa.sxp = tc.sxp;
