@@ -251,7 +251,8 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
       fft_pass2  spectrum planes in, product planes out: (wz Ny + vz Ny') Nx 8 B per node
       fft_pass3  product planes in, box sums in, map out: vz Ny' Nx 8 B + 3 n_off 4 B per node
                  (Ny' = Ny / 2 + 1 for the in-register cubic boxes, which keep the product's Hermitian half; else Ny)
-      ncc_peak   two sweeps of the FP32 map: 2 n_off 4 B per node
+      ncc_peak   two sweeps of the FP32 map: 2 n_off 4 B per node; with the in-register FFT engine, whose pass 3 leaves
+                 per-block map partials, the partials (32 B per block) and one block of map planes
       ncc_template  template in, centred template out: (n_tpl + sz sy sxp) 4 B per node
       box_pass   16 B per voxel per launch
       ncc_tiled / ncc_map  2 n_tpl n_off flop per node (direct cross term)
@@ -280,7 +281,13 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
             flop_work["ncc_tiled"] = flop_work.get("ncc_tiled", 0.0) + n * 2.0 * n_tpl * n_off
         if engine == 1:
             flop_work["ncc_map"] = flop_work.get("ncc_map", 0.0) + n * 2.0 * n_tpl * n_off
-        byte_work["ncc_peak"] = byte_work.get("ncc_peak", 0.0) + n * 2.0 * n_off * 4.0
+        if engine == 2 and reg:
+            nh = N[1] // 2 + 1
+            p3 = max(1, min(70000 // (N[0] * (nh | 1) * 8), 256 // nh))  # map planes per pass-3 block
+            peak_b = -(-v_[2] // p3) * 32.0 + min(p3, v_[2]) * v_[1] * v_[0] * 4.0
+        else:
+            peak_b = 2.0 * n_off * 4.0
+        byte_work["ncc_peak"] = byte_work.get("ncc_peak", 0.0) + n * peak_b
     if "box_pass" in ktimes:
         byte_work["box_pass"] = ktimes["box_pass"][1] * 16.0 * nvox
     half = [int(w) // 2 for w in p.winsize]
