@@ -455,6 +455,19 @@ def run_znssd(args):
     print(json.dumps(out), flush=True)
 
 
+def max_over_ranks(x: float, world: int, device="cuda") -> float:
+    """The largest value of ``x`` over the ranks (a device time: the slowest replica sets the job's time).  Every
+    rank calls it at the same point; with one rank it returns ``x`` and makes no collective call."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     args = parse()
     if args.impl == "reference" and args.config != 4:
@@ -519,10 +532,7 @@ def main():
     if world > 1:
         dist.barrier()
     elapsed = ev0.elapsed_time(ev1) / 1e3
-    t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
+    elapsed_max = max_over_ranks(elapsed, world)
     n_nodes = int(res.coords.shape[0])
     value = world * n_nodes * args.steps / elapsed_max
     stages = {}
@@ -575,7 +585,7 @@ def main():
             res_p = one_pass(K.PLAIN, tracer=ptr[k])
         e1.record()
         torch.cuda.synchronize()
-        pe = e0.elapsed_time(e1) / 1e3
+        pe = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
         pst = {}
         for tr in ptr:
             for k_, v_ in tr.stages().items():
@@ -601,7 +611,7 @@ def main():
         U_host = r.U.to("cpu")
     e1.record()
     torch.cuda.synchronize()
-    e2e_t = e0.elapsed_time(e1) / 1e3
+    e2e_t = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
     h2d = f_h.numel() * f_h.element_size() + g_h.numel() * g_h.element_size() + (0 if m_h is None else m_h.numel())
     d2h = U_host.numel() * U_host.element_size()
     e2e_val = world * n_nodes * args.steps / e2e_t

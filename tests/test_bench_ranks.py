@@ -1,0 +1,72 @@
+"""The multi-rank plumbing of ``bench.py`` on CPU: two ``gloo`` ranks on 127.0.0.1.
+
+``bench.py --gpus N`` runs N independent replicas of the pass (no data-path collective); its only collective is the
+max over ranks of each device time (timed passes, plain form, end to end), so that the slowest replica sets the
+job's time.  These tests check that reduction with world size 2 and that one rank makes no collective call, and
+that the reference arm does its work on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import os
+import socket
+
+import pytest
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, values, out_dir: str) -> None:
+    import datetime
+
+    import torch.distributed as dist
+
+    import bench
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        got = [bench.max_over_ranks(v, world, device="cpu") for v in values[rank]]
+        with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as fh:
+            fh.write(" ".join(repr(x) for x in got))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_two_gloo_ranks(tmp_path):
+    import torch.multiprocessing as mp
+
+    # three reductions in the same order on both ranks (timed passes, plain form, end to end)
+    values = [[0.61, 9.7, 0.64], [0.58, 9.9, 0.66]]
+    mp.spawn(_rank_main, args=(2, _free_port(), values, str(tmp_path)), nprocs=2, join=True)
+    for rank in range(2):
+        got = [float(x) for x in (tmp_path / f"rank{rank}.txt").read_text().split()]
+        assert got == [0.61, 9.9, 0.66]
+
+
+def test_max_over_ranks_single_rank_makes_no_collective_call():
+    import torch.distributed as dist
+
+    import bench
+
+    assert not dist.is_initialized()
+    assert bench.max_over_ranks(0.5, 1) == 0.5  # would raise if it called a collective without a process group
+
+
+@pytest.mark.parametrize("rank", ["1", "3"])
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys, rank):
+    import bench
+
+    monkeypatch.setenv("RANK", rank)
+
+    class Args:
+        config = 5
+        cpu_nodes = 8
+
+    bench.run_reference(Args())  # returns before any work on ranks other than 0
+    assert capsys.readouterr().out == ""
