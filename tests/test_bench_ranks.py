@@ -3,7 +3,8 @@
 ``bench.py --gpus N`` runs N independent replicas of the pass (no data-path collective); its only collective is the
 max over ranks of each device time (timed passes, plain form, end to end), so that the slowest replica sets the
 job's time.  These tests check that reduction with world size 2 and that one rank makes no collective call, and
-that the reference arm does its work on rank 0 only.
+that the reference arm does its work on rank 0 only; and that the bench's FFT roofline geometry matches the
+library source.
 """
 
 from __future__ import annotations
@@ -70,3 +71,19 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys, rank):
 
     bench.run_reference(Args())  # returns before any work on ranks other than 0
     assert capsys.readouterr().out == ""
+
+
+def test_roofline_fft_geometry_matches_the_library_source():
+    """The FFT byte counts of the bench's roofline assume the library's in-register box lengths and pass-3 block
+    height (map planes per CTA); both are read here from the CUDA sources so that the two cannot drift apart."""
+    import re
+
+    import bench
+
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pyaldvc_b200", "csrc")
+    reg = open(os.path.join(csrc, "fft_reg.cuh")).read()
+    sizes = re.search(r"FFTR_SIZES\[FFTR_NSIZES\]\s*=\s*\{([^}]*)\}", reg).group(1)
+    assert tuple(int(v) for v in sizes.split(",")) == bench.FFT_REG_SIZES
+    ncc = open(os.path.join(csrc, "ncc.cu")).read()
+    body = ncc[ncc.index("constexpr int fftr_planes3()"):][:400]
+    assert "70000 / (N * (NH | 1) * 8)" in body and "256 / NH" in body
