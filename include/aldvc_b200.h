@@ -149,6 +149,13 @@ unsigned long long aldvc_launch_count(void);
  * the launch count (names: max_entries rows of name_len bytes); returns the number of distinct kernels. */
 int aldvc_kernel_timing(int enable);
 int aldvc_kernel_timing_read(int32_t max_entries, char *names, int32_t name_len, double *ms, int64_t *launches);
+/* Test hook of the bounded grid-barrier waits (no reference counterpart).  The cooperative kernels (PCG,
+ * inpainting) wait at their grid barriers for the launch's blocks plus `extra_arrivals` (default 0) and give
+ * up after `spin_limit` polls of about 64 ns each (default 2^24; <= 0 restores it), setting their error word
+ * and returning.  With extra_arrivals > 0 no barrier ever opens, so every wait runs out: the failure path of
+ * a barrier whose peer never arrives, exercised without faulting or hanging the GPU.  Applies to launches
+ * enqueued after the call, process-wide; for tests only. */
+int aldvc_test_set_barrier(int32_t extra_arrivals, int64_t spin_limit);
 /* name of device `device`, its SM count and compute capability; returns ALDVC_OK */
 int aldvc_device_info(int device, char *name, int name_len, int *sm_count, int *cc_major, int *cc_minor);
 

@@ -988,6 +988,51 @@ void orc_zncc_direct(const float *f, const float *g, int64_t nz, int64_t ny, int
     }
 }
 
+/* ------------------------------------------------------------------ window box statistics of the FFT engine
+ * integer_search._window_box_stats (:154-207): per node of W (N, wz, wy, wx) float32, the sums of W and of
+ * its float32 squares over every (sz, sy, sx) box, from an FP64 summed-area table built row by row in the
+ * reference's order; out_sum / out_sq are (N, wz-sz+1, wy-sy+1, wx-sx+1). */
+void orc_window_box_stats(const float *W, int64_t N, int64_t wz, int64_t wy, int64_t wx, int64_t sz, int64_t sy, int64_t sx,
+                          double *out_sum, double *out_sq) {
+    const int64_t vz = wz - sz + 1, vy = wy - sy + 1, vx = wx - sx + 1;
+    const int64_t sat_n = (wz + 1) * (wy + 1) * (wx + 1);
+#pragma omp parallel
+    {
+        double *S1 = (double *)malloc((size_t)sat_n * sizeof(double));
+        double *S2 = (double *)malloc((size_t)sat_n * sizeof(double));
+#define SAT(A, z, y, x) A[((z) * (wy + 1) + (y)) * (wx + 1) + (x)]
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t n = 0; n < N; ++n) {
+            const float *w = W + n * wz * wy * wx;
+            for (int64_t i = 0; i < sat_n; ++i) S1[i] = S2[i] = 0.0;
+            for (int64_t z = 0; z < wz; ++z)
+                for (int64_t y = 0; y < wy; ++y) {
+                    double r1 = 0.0, r2 = 0.0;
+                    for (int64_t x = 0; x < wx; ++x) {
+                        float v32 = w[(z * wy + y) * wx + x];
+                        r1 += (double)v32;
+                        r2 += SQ32(v32);
+                        SAT(S1, z + 1, y + 1, x + 1) = SAT(S1, z, y + 1, x + 1) + SAT(S1, z + 1, y, x + 1) - SAT(S1, z, y, x + 1) + r1;
+                        SAT(S2, z + 1, y + 1, x + 1) = SAT(S2, z, y + 1, x + 1) + SAT(S2, z + 1, y, x + 1) - SAT(S2, z, y, x + 1) + r2;
+                    }
+                }
+            double *os = out_sum + n * vz * vy * vx, *oq = out_sq + n * vz * vy * vx;
+            for (int64_t z = 0; z < vz; ++z)
+                for (int64_t y = 0; y < vy; ++y)
+                    for (int64_t x = 0; x < vx; ++x) {
+                        int64_t z1 = z + sz, y1 = y + sy, x1 = x + sx, o = (z * vy + y) * vx + x;
+                        os[o] = SAT(S1, z1, y1, x1) - SAT(S1, z, y1, x1) - SAT(S1, z1, y, x1) - SAT(S1, z1, y1, x) + SAT(S1, z, y, x1) +
+                                SAT(S1, z, y1, x) + SAT(S1, z1, y, x) - SAT(S1, z, y, x);
+                        oq[o] = SAT(S2, z1, y1, x1) - SAT(S2, z, y1, x1) - SAT(S2, z1, y, x1) - SAT(S2, z1, y1, x) + SAT(S2, z, y, x1) +
+                                SAT(S2, z, y1, x) + SAT(S2, z1, y, x) - SAT(S2, z, y, x);
+                    }
+        }
+#undef SAT
+        free(S1);
+        free(S2);
+    }
+}
+
 /* ------------------------------------------------------------------ ZNSSD cost
  * C = sum_v r_v^2 with the residual of _icgn_12dof_single (numba_kernels.py:705-708),
  * r = (float(f) - meanf) / bottomf - (g - meang) / bottomg, over the valid set and with the statistics of

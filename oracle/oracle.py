@@ -61,6 +61,7 @@ def lib():
         L.orc_zncc_direct.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]
         L.orc_znssd.argtypes = [_P, _P, _I64, _I64, _I64, _P, _I64, _I, _I, _I, _I, _P, _P]
         L.orc_sep_filter.argtypes = [_P, _P, _I64, _I64, _I64, _I, _P, _I, _I]
+        L.orc_window_box_stats.argtypes = [_P, _I64, _I64, _I64, _I64, _I64, _I64, _I64, _P, _P]
         _lib = L
     return _lib
 
@@ -349,8 +350,69 @@ def subvoxel_peak(neigh):
     return out
 
 
-def ncc_search(f, g, coords, subset, radius, shift0=None, chunk=4096):
-    """integer_search.ncc_search (:329-483) with the direct engine (FP64 map) for every size."""
+# integer_search.py:41, :395: above this many offset x template-voxel products per node the reference's CPU
+# search takes its FFT branch
+DIRECT_NCC_MAX_OPS = 3.0e7
+
+
+def window_box_stats(W, sz, sy, sx):
+    """integer_search._window_box_stats (:154-207): sums of W and of its float32 squares over every template box
+    of each node's window W (n, wz, wy, wx), FP64 summed-area tables; returns (sum, sq), (n, vz, vy, vx) each."""
+    W = np.ascontiguousarray(W, dtype=np.float32)
+    n, wz, wy, wx = W.shape
+    shape = (n, wz - sz + 1, wy - sy + 1, wx - sx + 1)
+    s1, s2 = np.empty(shape), np.empty(shape)
+    lib().orc_window_box_stats(_ptr(W), n, wz, wy, wx, int(sz), int(sy), int(sx), _ptr(s1), _ptr(s2))
+    return s1, s2
+
+
+def ncc_maps_fft(f, g, coords, half, radius, wx0, wy0, wz0):
+    """The FFT branch of integer_search.ncc_search (:418-443) for the nodes ``coords`` (templates inside f):
+    float32 windows and mean-removed float32 templates, their real FFTs over the 2,3,5-smooth padded box
+    (scipy.fft, as the reference), the product with the conjugate template spectrum, its inverse cropped to
+    the valid offsets, normalised by the FP64 window box statistics and the template norm, clipped to [-1, 1].
+    Returns (maps (n, vz, vy, vx) float64, template norms (n,))."""
+    from scipy import fft as sfft
+
+    hx, hy, hz = half
+    rx, ry, rz = radius
+    sx, sy, sz = 2 * hx + 1, 2 * hy + 1, 2 * hz + 1
+    wx, wy, wz = sx + 2 * rx, sy + 2 * ry, sz + 2 * rz
+    vx, vy, vz = 2 * rx + 1, 2 * ry + 1, 2 * rz + 1
+    n = coords.shape[0]
+    box = tuple(sfft.next_fast_len(int(w), real=True) for w in (wz, wy, wx))
+    T = np.empty((n, sz, sy, sx), dtype=np.float32)
+    W = np.empty((n, wz, wy, wx), dtype=np.float32)
+    for k in range(n):
+        x, y, z = (int(a) for a in coords[k])
+        T[k] = f[z - hz:z + hz + 1, y - hy:y + hy + 1, x - hx:x + hx + 1]
+        W[k] = g[wz0[k]:wz0[k] + wz, wy0[k]:wy0[k] + wy, wx0[k]:wx0[k] + wx]
+    # template mean in FP64, subtracted in float32; its norm in FP64
+    T -= T.mean(axis=(1, 2, 3), dtype=np.float64, keepdims=True).astype(np.float32)
+    t_norm = np.sqrt((T.astype(np.float64) ** 2).sum(axis=(1, 2, 3)))
+    spec = sfft.rfftn(W, s=box, axes=(1, 2, 3), workers=-1)
+    spec *= np.conj(sfft.rfftn(T, s=box, axes=(1, 2, 3), workers=-1))
+    cross = sfft.irfftn(spec, s=box, axes=(1, 2, 3), workers=-1)[:, :vz, :vy, :vx].astype(np.float64)
+    s1, s2 = window_box_stats(W, sz, sy, sx)
+    var = np.maximum(s2 - s1 * s1 / float(sx * sy * sz), 0.0)
+    denom = np.sqrt(var) * t_norm[:, None, None, None]
+    maps = np.zeros_like(cross)
+    np.divide(cross, denom, out=maps, where=denom > 1e-10)
+    np.clip(maps, -1.0, 1.0, out=maps)
+    return maps, t_norm
+
+
+def ncc_engine(half, radius) -> str:
+    """The reference CPU search's engine for a template half-width and radius (integer_search.py:395)."""
+    n_tpl = np.prod([2 * int(h) + 1 for h in half])
+    n_off = np.prod([2 * int(r) + 1 for r in radius])
+    return "direct" if n_tpl * n_off <= DIRECT_NCC_MAX_OPS else "fft"
+
+
+def ncc_search(f, g, coords, subset, radius, shift0=None, engine="direct"):
+    """integer_search.ncc_search (:329-483).  ``engine``: "direct" (the FP64 map of _zncc_direct for every
+    size: the exact-arithmetic map), "fft" (the reference's FP32 FFT branch) or "auto" (the reference's own
+    switch, ``ncc_engine``)."""
     f, g = _f32(f), _f32(g)
     nz, ny, nx = f.shape
     coords = np.asarray(coords, dtype=np.int64)
@@ -359,6 +421,10 @@ def ncc_search(f, g, coords, subset, radius, shift0=None, chunk=4096):
     rx, ry, rz = (int(r) for r in radius)
     sx, sy, sz = 2 * hx + 1, 2 * hy + 1, 2 * hz + 1
     wx, wy, wz = sx + 2 * rx, sy + 2 * ry, sz + 2 * rz
+    if engine == "auto":
+        engine = ncc_engine((hx, hy, hz), (rx, ry, rz))
+    if engine not in ("direct", "fft"):
+        raise ValueError(f"unknown NCC engine {engine!r}")
     if shift0 is None:
         shift0 = np.zeros((N, 3), dtype=np.int64)
     shift0 = np.asarray(np.round(shift0), dtype=np.int64)
@@ -367,7 +433,7 @@ def ncc_search(f, g, coords, subset, radius, shift0=None, chunk=4096):
     pce = np.full(N, np.nan)
     clipped = np.zeros(N, dtype=bool)
     ok = np.zeros(N, dtype=bool)
-    out = {"disp": disp, "cc": cc, "pce": pce, "clipped": clipped, "ok": ok}
+    out = {"disp": disp, "cc": cc, "pce": pce, "clipped": clipped, "ok": ok, "engine": engine}
     if wx > nx or wy > ny or wz > nz:
         return out
     cx, cy, cz = coords[:, 0], coords[:, 1], coords[:, 2]
@@ -382,13 +448,17 @@ def ncc_search(f, g, coords, subset, radius, shift0=None, chunk=4096):
     free_hi = np.column_stack([dx0 <= nx - wx, dy0 <= ny - wy, dz0 <= nz - wz])
     idx_all = np.flatnonzero(t_ok)
     vz, vy, vx = 2 * rz + 1, 2 * ry + 1, 2 * rx + 1
+    chunk = 4096 if engine == "direct" else 64
     for start in range(0, idx_all.size, chunk):
         ids = idx_all[start:start + chunk]
         n = ids.size
-        ncc = np.empty((n, vz, vy, vx))
-        zncc_direct(f, g, coords[ids], hx, hy, hz, rx, ry, rz, wx0[ids], wy0[ids], wz0[ids], np.ones(n, dtype=bool), ncc)
-        t_norm = np.where(ncc[:, 0, 0, 0] > -1.5, 1.0, 0.0)
-        ncc[ncc < -1.0] = 0.0
+        if engine == "direct":
+            ncc = np.empty((n, vz, vy, vx))
+            zncc_direct(f, g, coords[ids], hx, hy, hz, rx, ry, rz, wx0[ids], wy0[ids], wz0[ids], np.ones(n, dtype=bool), ncc)
+            t_norm = np.where(ncc[:, 0, 0, 0] > -1.5, 1.0, 0.0)  # a flat template marks its whole map -2
+            ncc[ncc < -1.0] = 0.0
+        else:
+            ncc, t_norm = ncc_maps_fft(f, g, coords[ids], (hx, hy, hz), (rx, ry, rz), wx0[ids], wy0[ids], wz0[ids])
         flat = ncc.reshape(n, -1)
         pk = np.argmax(flat, axis=1)
         pz, py, px = np.unravel_index(pk, ncc.shape[1:])
@@ -421,9 +491,10 @@ def ncc_search(f, g, coords, subset, radius, shift0=None, chunk=4096):
     return out
 
 
-def ncc_search_expanding(f, g, coords, subset, radius, shift0=None, auto_expand=True, max_expand=3):
-    """integer_search.ncc_search_expanding (:486-524)."""
-    res = ncc_search(f, g, coords, subset, radius, shift0)
+def ncc_search_expanding(f, g, coords, subset, radius, shift0=None, auto_expand=True, max_expand=3, engine="direct"):
+    """integer_search.ncc_search_expanding (:486-524); ``engine`` as in ``ncc_search`` (each radius picks its own
+    engine under "auto", as the reference's searches do)."""
+    res = ncc_search(f, g, coords, subset, radius, shift0, engine)
     res["expansions"] = 0
     res["radius"] = tuple(int(r) for r in radius)
     rad = res["radius"]
@@ -434,7 +505,7 @@ def ncc_search_expanding(f, g, coords, subset, radius, shift0=None, auto_expand=
             break
         rad = tuple(2 * r for r in rad)
         sub_shift = None if shift0 is None else np.asarray(shift0)[sel]
-        sub = ncc_search(f, g, coords[sel], subset, rad, sub_shift)
+        sub = ncc_search(f, g, coords[sel], subset, rad, sub_shift, engine)
         if not sub["ok"].any():
             break
         idx = np.flatnonzero(sel)[sub["ok"]]
@@ -597,3 +668,308 @@ def nodal_gradient(ops, U):
             F[:, i, j] = (GT @ U[:, i]) / safe
     F[~ops["active"]] = np.nan
     return F
+
+
+# --------------------------------------------------------------------------- volume normalisation
+def normalize_volume(vol):
+    """io/volume_ops.normalize_volume (:105-121) over the whole volume, on the path the reference takes for
+    integer and float inputs of two or more bytes: moments of (v - pilot) per z slice in FP64, accumulated in
+    C order with the voxel kept in its own precision before the subtraction (voi_mean_std :79-99,
+    _voi_moments :52-68), the slice totals summed, then float32((v - mean) / std) (_normalize_into :71-76)."""
+    a = np.ascontiguousarray(vol)
+    nz, ny, nx = a.shape
+    pilot = float(a[nz // 2, ny // 2, nx // 2])
+    d = a.reshape(nz, -1).astype(np.float64) - pilot
+    s = np.add.accumulate(d, axis=1)[:, -1]  # sequential per slice, like the reference's inner loops
+    ss = np.add.accumulate(d * d, axis=1)[:, -1]
+    n = float(a.size)
+    mean_shift = s.sum() / n
+    var = max(ss.sum() / n - mean_shift * mean_shift, 0.0)
+    mean, std = pilot + mean_shift, float(np.sqrt(var))
+    if std < 1e-12:
+        std = 1.0
+    return ((a.astype(np.float64) - mean) * (1.0 / std)).astype(np.float32)
+
+
+# --------------------------------------------------------------------------- node-grid post-processing
+def _neighbour_footprint():
+    fp = np.ones((3, 3, 3), dtype=bool)
+    fp[1, 1, 1] = False  # the 26 neighbours, the node itself left out
+    return fp
+
+
+def fill_nan_grid(grid):
+    """utils/inpaint.fill_nan_grid (:35-128), spring model on a (nz, ny, nx) grid: the unknown (NaN) nodes solve
+    the discrete Laplace equation with their six grid neighbours, known neighbours entering as Dirichlet data,
+    plus a 1e-10 Tikhonov term; a sparse direct solve (conjugate gradients above 60,000 unknowns).  All NaN:
+    zeros."""
+    from scipy.sparse.linalg import cg, spsolve
+
+    arr = np.array(grid, dtype=np.float64, copy=True)
+    unk = np.isnan(arr)
+    m = int(unk.sum())
+    if m == 0:
+        return arr
+    if unk.all():
+        return np.zeros_like(arr)
+    flat = arr.ravel()
+    pos = np.full(flat.size, -1, dtype=np.int64)
+    pos[np.flatnonzero(unk.ravel())] = np.arange(m)
+    ids = np.arange(flat.size).reshape(arr.shape)
+    deg = np.zeros(m)
+    rhs = np.zeros(m)
+    rows, cols = [], []
+    for ax in range(arr.ndim):
+        if arr.shape[ax] < 2:
+            continue
+        lo = ids.take(np.arange(arr.shape[ax] - 1), axis=ax).ravel()
+        hi = ids.take(np.arange(1, arr.shape[ax]), axis=ax).ravel()
+        for p, q in ((lo, hi), (hi, lo)):  # each grid edge couples both of its ends
+            pu = pos[p]
+            e = pu >= 0
+            pu, qn = pu[e], q[e]
+            np.add.at(deg, pu, 1.0)
+            qu = pos[qn]
+            kn = qu < 0
+            np.add.at(rhs, pu[kn], flat[qn[kn]])
+            rows.append(pu[~kn])
+            cols.append(qu[~kn])
+    r = np.concatenate(rows + [np.arange(m)])
+    c = np.concatenate(cols + [np.arange(m)])
+    v = np.concatenate([-np.ones(r.size - m), deg])
+    A = sparse.coo_matrix((v, (r, c)), shape=(m, m)).tocsr() + sparse.eye(m, format="csr") * 1e-10
+    if m <= 60_000:
+        x = spsolve(A.tocsc(), rhs)
+    else:
+        x, info = cg(A, rhs, rtol=1e-10, maxiter=2000)
+        if info != 0:
+            x = spsolve(A.tocsc(), rhs)
+    flat[np.flatnonzero(unk.ravel())] = x
+    return flat.reshape(arr.shape)
+
+
+def median_test(field, valid, threshold, eps=0.1):
+    """utils/outlier_detection.universal_median_test (:135-163) on an uncut grid: per component, invalid nodes
+    inpainted (fill_nan_grid), the normalised fluctuation |u - med26(u)| / (med26(|u - med26(u)|) + eps) over the
+    26-neighbourhood (scipy median filter, nearest edges), 0 at invalid nodes; a valid node is an outlier when
+    the norm of its component fluctuations exceeds ``threshold``.  field (nz, ny, nx, C) -> (nz, ny, nx) bool."""
+    from scipy.ndimage import median_filter
+
+    arr = np.asarray(field, dtype=np.float64)
+    if arr.ndim == 3:
+        arr = arr[..., None]
+    if threshold <= 0:
+        return np.zeros(arr.shape[:3], dtype=bool)
+    fp = _neighbour_footprint()
+    mag2 = np.zeros(arr.shape[:3])
+    for k in range(arr.shape[3]):
+        a = arr[..., k].copy()
+        if valid is not None:
+            a[~valid] = np.nan
+        holes = np.isnan(a)
+        if holes.all():
+            continue
+        if holes.any():
+            a = fill_nan_grid(a)
+        fl = a - median_filter(a, footprint=fp, mode="nearest")
+        nf = np.abs(fl) / (median_filter(np.abs(fl), footprint=fp, mode="nearest") + eps)
+        nf[holes] = 0.0
+        mag2 += nf * nf
+    flag = np.sqrt(mag2) > threshold
+    if valid is not None:
+        flag &= valid
+    return flag
+
+
+def _fill_bad(values, bad, grid_shape):
+    """Every column of ``values`` (N, C) with the ``bad`` rows inpainted on the node grid (local_icgn.fill_bad_nodes
+    :492-522, init_disp.clean_initial_guess :183-188); all bad: zeros."""
+    if not bad.any():
+        return values.copy()
+    if bad.all():
+        return np.zeros_like(values)
+    out = values.copy()
+    for k in range(values.shape[1]):
+        comp = values[:, k].reshape(grid_shape).copy()
+        comp[bad.reshape(grid_shape)] = np.nan
+        out[:, k] = fill_nan_grid(comp).ravel()
+    return out
+
+
+def _outliers(values, bad, grid_shape, threshold):
+    """The median test of the good nodes after a local pass, run only with more than 27 of them
+    (local_icgn.py:466-475, subpb1_solver.py:140-149, init_disp.py:166-170)."""
+    good = ~bad
+    if threshold <= 0 or good.sum() <= 27:
+        return np.zeros_like(bad)
+    return median_test(values.reshape(tuple(grid_shape) + (values.shape[1],)), good.reshape(grid_shape), threshold).ravel()
+
+
+def subset_valid_fraction(mask, coords, half):
+    """mesh/grid_mesh.subset_valid_fraction (:139-186): mask voxels inside each node's box clipped to the volume,
+    over the nominal box volume."""
+    m = np.asarray(mask) != 0
+    nz, ny, nx = m.shape
+    sat = np.zeros((nz + 1, ny + 1, nx + 1), dtype=np.int64)
+    sat[1:, 1:, 1:] = m.cumsum(0).cumsum(1).cumsum(2)
+    hx, hy, hz = half
+    cx, cy, cz = (np.asarray(coords[:, k], dtype=np.int64) for k in range(3))
+    x0, x1 = np.clip(cx - hx, 0, nx), np.clip(cx + hx + 1, 0, nx)
+    y0, y1 = np.clip(cy - hy, 0, ny), np.clip(cy + hy + 1, 0, ny)
+    z0, z1 = np.clip(cz - hz, 0, nz), np.clip(cz + hz + 1, 0, nz)
+    cnt = (sat[z1, y1, x1] - sat[z0, y1, x1] - sat[z1, y0, x1] - sat[z1, y1, x0] + sat[z0, y0, x1] + sat[z0, y1, x0]
+           + sat[z1, y0, x0] - sat[z0, y0, x0])
+    return cnt / float((2 * hx + 1) * (2 * hy + 1) * (2 * hz + 1))
+
+
+# --------------------------------------------------------------------------- one full AL-DVC pass
+PASS_DEFAULTS = dict(winsize=(32, 32, 32), search_radius=(8, 8, 8), init_subset=None, interp_method="cubic", subset_stride=1,
+                     icgn_tol=1e-2, icgn_dp_tol=1e-3, icgn_max_iter=100, icgn_patience=5, icgn_predictive_stop=True,
+                     min_valid_ratio=0.5, hessian_cond_max=1e12, init_outlier_threshold=2.0, local_outlier_threshold=2.0,
+                     ncc_auto_expand=True, ncc_max_expand=3, init_min_pce=0.0, use_global_step=True, mu=1e-3, beta=1e-3,
+                     alpha=0.0, admm_max_iter=4, admm_tol=1e-2, dual_update="accumulate", pcg_tol=1e-8, pcg_max_iter=500,
+                     gauss_pt_order=2, ncc_engine="auto")
+
+
+def aldvc_pass(f, g, coords, grid_shape, spacing, mask=None, node_half=None, **prm):
+    """One frame pair of core/pipeline.run_aldvc (:255-366) in FP64 on normalised volumes f, g: sections 3-6 with
+    the "ncc" initial guess and no global pre-shift, a fixed beta, the FEM global step and the PCG solver.
+
+    - reference-frame validity (grid_mesh.apply_mask_to_mesh :191-253 with a boolean ``mask``; precompute
+      validity, local_icgn.precompute_local_context :223-347, which then becomes the mesh's node validity);
+    - initial guess (init_disp.compute_initial_guess :53-140, clean_initial_guess :143-189): NCC search with
+      radius expansion over the valid nodes, failed / invalid / outlying nodes inpainted;
+    - local 12-DOF IC-GN (local_icgn.local_icgn :398-489): non-converged and outlying nodes inpainted, U and F;
+    - global step (subpb2_solver.solve_subpb2 :133-155, global_operators.nodal_gradient :151-170), non-finite F
+      replaced by the local F (pipeline.py:300-310);
+    - ADMM steps 2..admm_max_iter (pipeline.py:316-352): 3-DOF subproblem 1 (subpb1_solver.subpb1_solver
+      :77-164: rejected nodes keep the global estimate), global step, dual update, early stop on the RMS
+      updates.
+
+    ``node_half`` (N, 3) gives per-node subset half-widths (uneven subsets, every one within ``winsize``): each
+    shape's nodes run through the kernels together, as the reference runs one shape per call, and validity
+    uses each node's own box.  Returns a dict of per-node arrays and scalars."""
+    p = dict(PASS_DEFAULTS)
+    unknown = set(prm) - set(p)
+    if unknown:
+        raise TypeError(f"unknown pass parameters {sorted(unknown)}")
+    p.update(prm)
+    f, g = _f32(f), _f32(g)
+    grid_shape = tuple(int(s) for s in grid_shape)
+    coords = np.asarray(coords, dtype=np.int64)
+    N = coords.shape[0]
+    half = tuple(int(w) // 2 for w in p["winsize"])
+    halves = np.tile(np.asarray(half, dtype=np.int64), (N, 1)) if node_half is None else np.asarray(node_half, dtype=np.int64)
+    mode = {"linear": 0, "cubic": 1, "bspline": 2}[p["interp_method"]]
+    g_prep = prefilter_bspline(g) if mode == 2 else g
+    gx, gy, gz = compute_gradients(f)
+    m_u8 = np.ones((1, 1, 1), np.uint8) if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    stride = int(p["subset_stride"])
+    groups = [np.flatnonzero((halves == s).all(axis=1)) for s in np.unique(halves, axis=0)]
+
+    # reference-frame node validity and the active elements
+    if mask is None:
+        node_valid = np.ones(N, dtype=bool)
+    else:
+        frac = np.empty(N)
+        for sel in groups:
+            frac[sel] = subset_valid_fraction(mask, coords[sel], tuple(halves[sel[0]]))
+        node_valid = (np.asarray(mask)[coords[:, 2], coords[:, 1], coords[:, 0]] != 0) & (frac >= p["min_valid_ratio"])
+    elem_active = node_valid[grid_elements(grid_shape)].all(axis=1)
+
+    # precompute, per subset shape
+    H = np.zeros((N, 12, 12))
+    L = np.zeros((N, 12, 12))
+    meanf = np.zeros(N)
+    bottomf = np.ones(N)
+    valid = np.zeros(N, dtype=bool)
+    for sel in groups:
+        hs = tuple(int(v) for v in halves[sel[0]])
+        H[sel], L[sel], meanf[sel], bottomf[sel], _, v = precompute_nodes(coords[sel], *hs, f, gx, gy, gz, m_u8, p["min_valid_ratio"],
+                                                                           p["hessian_cond_max"], stride)
+        valid[sel] = v
+    valid &= node_valid
+
+    # section 3: initial guess over the valid nodes
+    sub0 = p["init_subset"] if p["init_subset"] is not None else tuple(min(int(w), 16) for w in p["winsize"])
+    act = np.flatnonzero(valid) if valid.any() else np.arange(N)
+    res = ncc_search_expanding(f, g, coords[act], sub0, p["search_radius"], None, p["ncc_auto_expand"], p["ncc_max_expand"],
+                               p["ncc_engine"])
+    disp = np.full((N, 3), np.nan)
+    ok = np.zeros(N, dtype=bool)
+    pce = np.full(N, np.nan)
+    disp[act], ok[act], pce[act] = res["disp"], res["ok"], res["pce"]
+    bad0 = ~ok | ~np.isfinite(disp).all(axis=1) | ~valid
+    if p["init_min_pce"] > 0:
+        bad0 |= np.isfinite(pce) & (pce < p["init_min_pce"])
+    d = np.where(bad0[:, None], np.nan, disp)
+    bad0 |= _outliers(d, bad0, grid_shape, p["init_outlier_threshold"])
+    U0 = _fill_bad(np.where(bad0[:, None], np.nan, disp), bad0, grid_shape)
+
+    # section 4: local 12-DOF IC-GN
+    P0 = np.zeros((N, 12))
+    P0[:, 9:] = U0
+    P = np.zeros((N, 12))
+    it12 = np.zeros(N, dtype=np.int32)
+    st12 = np.zeros(N, dtype=np.int8)
+    zc12 = np.zeros(N)
+    for sel in groups:
+        hs = tuple(int(v) for v in halves[sel[0]])
+        P[sel], it12[sel], st12[sel], zc12[sel] = icgn_12dof_parallel(
+            coords[sel], P0[sel], *hs, f, gx, gy, gz, m_u8, g_prep, mode, L[sel], meanf[sel], bottomf[sel], valid[sel], p["icgn_tol"],
+            p["icgn_dp_tol"], p["icgn_max_iter"], p["icgn_patience"], stride, predictive=p["icgn_predictive_stop"])
+    bad = st12 != STATUS_CONVERGED
+    bad |= _outliers(P[:, 9:], bad, grid_shape, p["local_outlier_threshold"])
+    UF = _fill_bad(P, bad, grid_shape)
+    U1, F1 = UF[:, 9:].copy(), UF[:, :9].reshape(N, 3, 3).copy()
+    out = {"U0": U0, "init_bad": bad0, "ncc_radius": np.array(res["radius"]), "ncc_expansions": res["expansions"], "valid": valid,
+           "node_valid": node_valid, "P_local": P, "status_local": st12, "n_iter_local": it12, "zncc_local": zc12,
+           "U_local": U1.copy(), "F_local": F1.copy(), "U": U1, "F": F1, "status": st12, "zncc": zc12, "n_iter": it12,
+           "admm_steps": 1}
+    if not p["use_global_step"]:
+        return out
+
+    # sections 5-6: global step and ADMM
+    ops = fem_operators(grid_shape, spacing, elem_active, p["gauss_pt_order"])
+    system = global_system(ops, p["beta"], p["mu"], p["alpha"])
+
+    def global_step(U1_, F1_, W_, v_):
+        U2_, _ = solve_subpb2(system, U1_, F1_, W_, v_, p["pcg_tol"], p["pcg_max_iter"])
+        F2_ = nodal_gradient(ops, U2_)
+        return U2_, np.where(np.isfinite(F2_), F2_, F1_)
+
+    W = np.zeros((N, 3, 3))
+    v = np.zeros((N, 3))
+    U2, F2 = global_step(U1, F1, W, v)
+    W, v = F2 - F1, U2 - U1
+    n_full = float(np.prod([(2 * h) // stride + 1 for h in half]))
+    steps, st, zc, it = 1, st12, zc12, it12
+    for step in range(2, int(p["admm_max_iter"]) + 1):
+        steps = step
+        U1_prev = U1
+        U = np.zeros((N, 3))
+        it = np.zeros(N, dtype=np.int32)
+        st = np.zeros(N, dtype=np.int8)
+        zc = np.zeros(N)
+        for sel in groups:
+            hs = tuple(int(x) for x in halves[sel[0]])
+            U[sel], it[sel], st[sel], zc[sel] = icgn_3dof_parallel(
+                coords[sel], U2[sel], F2[sel], v[sel], *hs, f, gx, gy, gz, m_u8, g_prep, mode, H[sel], meanf[sel], bottomf[sel],
+                valid[sel], p["mu"], p["icgn_tol"], p["icgn_dp_tol"], p["icgn_max_iter"], p["icgn_patience"], stride, n_full=n_full,
+                predictive=p["icgn_predictive_stop"])
+        bad3 = st != STATUS_CONVERGED
+        bad3 |= _outliers(U, bad3, grid_shape, p["local_outlier_threshold"])
+        U1 = np.where(bad3[:, None], U2, U)
+        F1 = F2
+        U2n, F2n = global_step(U1, F1, W, v)
+        du_g = float(np.sqrt(np.mean((U2n - U2) ** 2)))
+        du_l = float(np.sqrt(np.mean((U1 - U1_prev) ** 2)))
+        if p["dual_update"] == "accumulate":
+            W, v = W + (F2n - F1), v + (U2n - U1)
+        else:
+            W, v = F2n - F1, U2n - U1
+        U2, F2 = U2n, F2n
+        if du_g < p["admm_tol"] or du_l < p["admm_tol"]:
+            break
+    out.update(U=U2, F=F2, status=st, zncc=zc, n_iter=it, admm_steps=steps)
+    return out

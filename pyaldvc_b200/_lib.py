@@ -76,6 +76,7 @@ PROTOTYPES = {
     "aldvc_pcg_workspace_size": (_sz, [ctypes.POINTER(Hex8Mesh)]),
     "aldvc_pcg_hex8": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _d, _i32, _p, _sz, _p, _p, _p, _p]),
     "aldvc_pcg_hex8_noalloc_max_nodes": (_i64, []),
+    "aldvc_test_set_barrier": (_i32, [_i32, _i64]),
     "aldvc_pcg_hex8_noalloc": (_i32, [ctypes.POINTER(Hex8Mesh), _d, _d, _d, _p, _p, _d, _i32, _p, _p, _p, _p]),
     "aldvc_nodal_gradient": (_i32, [ctypes.POINTER(Hex8Mesh), _p, _p, _p]),
     "aldvc_znssd_forward": (_i32, [ctypes.POINTER(Volumes), _p, _i64, _i32, _i32, _i32, _i32, _p, _p, _p, _p]),

@@ -83,13 +83,16 @@ def auto_tune_beta_device(grid_shape, spacing, elem_active, mu: float, alpha: fl
     v0 = torch.zeros((N, 3), dtype=torch.float64, device=U1.device)
     err1 = torch.empty(len(betas), dtype=torch.float64, device=U1.device)
     err2 = torch.empty_like(err1)
+    words = K.ErrorWords()
     for k, bk in enumerate(betas):
         b = K.global_rhs(grid_shape, spacing, e, float(bk), mu, alpha, U1, F1, W0, v0, gauss_order)
-        U2, _, _ = K.pcg_hex8(grid_shape, spacing, e, float(bk), mu, alpha, b, U1, pcg_tol, pcg_max_iter, gauss_order)
+        U2, _, pe = K.pcg_hex8(grid_shape, spacing, e, float(bk), mu, alpha, b, U1, pcg_tol, pcg_max_iter, gauss_order)
+        words.add(pe, "pcg_hex8 (beta sweep)")
         F2 = K.nodal_gradient(grid_shape, spacing, e, U2, gauss_order).reshape(N, 9)
         F2 = torch.where(torch.isfinite(F2), F2, F1)
         err1[k] = torch.linalg.vector_norm((U1 - U2)[include])
         err2[k] = torch.linalg.vector_norm((F1 - F2)[include])
+    words.check()
     e1, e2 = err1.cpu().numpy(), err2.cpu().numpy()
     beta, score, k_best = score_sweep(betas, e1, e2, winstepsize, criterion)
     return beta, {"betas": betas, "err1": e1, "err2": e2, "score": score, "k_best": k_best, "beta": beta, "criterion": criterion}

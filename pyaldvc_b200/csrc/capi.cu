@@ -148,6 +148,20 @@ extern "C" int aldvc_kernel_timing_read(int32_t max_entries, char* names, int32_
     return (int)keys.size();
 }
 
+static std::atomic<unsigned int> g_bar_extra{0};
+static std::atomic<long long> g_bar_spins{aldvc::DEFAULT_SPIN_LIMIT};
+
+aldvc::BarrierParams aldvc::barrier_params() {
+    return aldvc::BarrierParams{g_bar_extra.load(std::memory_order_relaxed), g_bar_spins.load(std::memory_order_relaxed)};
+}
+
+extern "C" int aldvc_test_set_barrier(int32_t extra_arrivals, int64_t spin_limit) {
+    ALDVC_REQUIRE(extra_arrivals >= 0 && extra_arrivals <= 1024, "aldvc_test_set_barrier: extra_arrivals must be in [0, 1024]");
+    g_bar_extra.store((unsigned int)extra_arrivals, std::memory_order_relaxed);
+    g_bar_spins.store(spin_limit > 0 ? (long long)spin_limit : aldvc::DEFAULT_SPIN_LIMIT, std::memory_order_relaxed);
+    return ALDVC_OK;
+}
+
 extern "C" int aldvc_abi_version(void) { return ALDVC_ABI_VERSION; }
 
 extern "C" const char* aldvc_last_error(void) { return g_err; }

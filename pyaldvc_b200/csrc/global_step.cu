@@ -242,13 +242,13 @@ struct PcgArgs {
     double* part;  // (3 slots, nblocks, 8)
     unsigned int* bar_count;
     unsigned int* bar_gen;
+    unsigned int bar_extra;  // arrivals beyond the grid before a barrier opens (0; > 0 only in the give-up tests)
+    long long spin_limit;    // polls before a waiting block gives up
     double tol;
     int max_iter;
     int32_t* iters;
     int32_t* err;
 };
-
-constexpr long long BARRIER_SPIN_LIMIT = 1LL << 24;
 
 // Grid-wide barrier for a cooperative launch (all blocks co-resident).  The wait is bounded: on give-up
 // the error word is set and the caller leaves its loop.
@@ -261,14 +261,14 @@ __device__ bool grid_sync(const PcgArgs& a) {
         __threadfence();
         const unsigned int arrived = atomicAdd(a.bar_count, 1u) + 1u;
         int ok = 1;
-        if (arrived == gridDim.x) {
+        if (arrived == gridDim.x + a.bar_extra) {
             *a.bar_count = 0u;
             __threadfence();
             atomicAdd(a.bar_gen, 1u);
         } else {
             long long spins = 0;
             while (*gen == g0) {
-                if (++spins > BARRIER_SPIN_LIMIT) {
+                if (++spins > a.spin_limit) {
                     atomicExch(a.err, 1);
                     ok = 0;
                     break;
@@ -507,19 +507,28 @@ extern "C" int aldvc_nodal_gradient(const aldvc_hex8_mesh* mesh, const double* U
     return check_launch("aldvc_nodal_gradient");
 }
 
+static std::mutex g_pcg_grid_mu;
+static int g_pcg_grid[128] = {0};  // co-resident grid of the cooperative PCG, per device ordinal
+
+// The cooperative grid of the current device: every block resident at once.  Queried once per device
+// (no configuration call inside a stream capture after the first use).
 static int pcg_grid(int* grid_out) {
-    int* grid_out_ = grid_out;
-    static int cached = 0;  // queried once: no configuration call inside a stream capture
-    if (cached > 0) {
-        *grid_out_ = cached;
-        return ALDVC_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "pcg: current device");
+    if (dev < 0 || dev >= 128) return arg_fail("pcg: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_pcg_grid_mu);
+    if (g_pcg_grid[dev] == 0) {
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, PCG_THREADS, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "pcg: occupancy");
+        if (per_sm < 1) return arg_fail("pcg: kernel does not fit on an SM");
+        cudaDeviceProp p;
+        e = cudaGetDeviceProperties(&p, dev);
+        if (e != cudaSuccess) return cuda_fail(e, "pcg: device properties");
+        g_pcg_grid[dev] = per_sm * p.multiProcessorCount;
     }
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, PCG_THREADS, 0);
-    if (e != cudaSuccess) return cuda_fail(e, "pcg: occupancy");
-    if (per_sm < 1) return arg_fail("pcg: kernel does not fit on an SM");
-    *grid_out = per_sm * sm_count();
-    cached = *grid_out;
+    *grid_out = g_pcg_grid[dev];
     return ALDVC_OK;
 }
 
@@ -571,6 +580,9 @@ extern "C" int aldvc_pcg_hex8(const aldvc_hex8_mesh* mesh, double beta, double m
     a.active = (uint8_t*)(w + 4 * v3 + pb + align_up((size_t)n * sizeof(double), 256));
     a.bar_count = (unsigned int*)(w + 4 * v3 + pb + align_up((size_t)n * sizeof(double), 256) + align_up((size_t)n, 256));
     a.bar_gen = a.bar_count + 1;
+    const BarrierParams bp = barrier_params();
+    a.bar_extra = bp.extra;
+    a.spin_limit = bp.spin_limit;
     a.tol = tol;
     a.max_iter = max_iter;
     a.iters = iters;
@@ -676,6 +688,9 @@ extern "C" int aldvc_pcg_hex8_noalloc(const aldvc_hex8_mesh* mesh, double beta, 
     a.bar_count = (unsigned int*)(w + 4 * NOALLOC_V3 + NOALLOC_PART + (size_t)NOALLOC_PCG_MAX_NODES * sizeof(double) +
                                   (size_t)NOALLOC_PCG_MAX_NODES);
     a.bar_gen = a.bar_count + 1;
+    const BarrierParams bp = barrier_params();
+    a.bar_extra = bp.extra;
+    a.spin_limit = bp.spin_limit;
     a.tol = tol;
     a.max_iter = max_iter;
     a.iters = iters;
@@ -686,7 +701,10 @@ extern "C" int aldvc_pcg_hex8_noalloc(const aldvc_hex8_mesh* mesh, double beta, 
     e = cudaMemsetAsync(err, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: error word reset");
     void* args[] = {&a};
-    e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
+    {
+        KTimer kt_("pcg_hex8_noalloc", s);
+        e = cudaLaunchCooperativeKernel((const void*)pcg_kernel, dim3(grid), dim3(PCG_THREADS), args, 0, s);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "aldvc_pcg_hex8_noalloc: cooperative launch");
     count_launch();
     return ALDVC_OK;

@@ -49,6 +49,16 @@ struct KTimer {
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Grid-barrier parameters of the cooperative kernels: a barrier opens when the launch's blocks plus
+// `extra` have arrived, and a block stops waiting after `spin_limit` polls.  Production launches use
+// extra = 0 and DEFAULT_SPIN_LIMIT; aldvc_test_set_barrier changes both for the tests of the give-up path.
+constexpr long long DEFAULT_SPIN_LIMIT = 1LL << 24;
+struct BarrierParams {
+    unsigned int extra;
+    long long spin_limit;
+};
+BarrierParams barrier_params();
+
 }  // namespace aldvc
 
 #define ALDVC_REQUIRE(cond, msg) \

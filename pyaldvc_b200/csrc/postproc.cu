@@ -10,6 +10,7 @@
 //                        |u - med| / (median of the neighbours' |u - med| + eps), flagged above threshold.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -18,7 +19,6 @@ namespace aldvc {
 
 constexpr int PP_THREADS = 256;
 constexpr int MAX_COLS = 12;
-constexpr long long PP_SPIN_LIMIT = 1LL << 24;
 
 struct Grid3 {
     int nx, ny, nz;
@@ -45,11 +45,17 @@ struct InpArgs {
     double* X;
     double* part;
     unsigned int* bar;
+    unsigned int bar_extra;  // arrivals beyond the grid before a barrier opens (0; > 0 only in the give-up tests)
+    long long spin_limit;    // polls before a waiting block gives up
     int32_t* iters;
     int32_t* err;
 };
 
-__device__ bool pp_grid_sync(unsigned int* bar, int32_t* err) {
+// Grid-wide barrier of the cooperative inpainting kernel; bounded wait: on give-up the error word is set
+// and the caller returns.
+__device__ bool pp_grid_sync(const InpArgs& a) {
+    unsigned int* bar = a.bar;
+    int32_t* err = a.err;
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
@@ -58,14 +64,14 @@ __device__ bool pp_grid_sync(unsigned int* bar, int32_t* err) {
         __threadfence();
         const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
         int ok = 1;
-        if (arrived == gridDim.x) {
+        if (arrived == gridDim.x + a.bar_extra) {
             bar[0] = 0u;
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
             long long spins = 0;
             while (*gen == g0) {
-                if (++spins > PP_SPIN_LIMIT) {
+                if (++spins > a.spin_limit) {
                     atomicExch(err, 1);
                     ok = 0;
                     break;
@@ -168,7 +174,7 @@ __global__ void __launch_bounds__(PP_THREADS) inpaint_cg_kernel(InpArgs a) {
         }
     }
     pp_partials(a.part, 0, loc, C);
-    if (!pp_grid_sync(a.bar, a.err)) return;
+    if (!pp_grid_sync(a)) return;
     double tot[2 * MAX_COLS], rr[MAX_COLS], bn[MAX_COLS];
     pp_total(a.part, 0, C, tot);
     for (int c = 0; c < C; ++c) {
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(PP_THREADS) inpaint_cg_kernel(InpArgs a) {
                 }
             }
             pp_partials(a.part, 1, loc, C);
-            if (!pp_grid_sync(a.bar, a.err)) return;
+            if (!pp_grid_sync(a)) return;
             pp_total(a.part, 1, C, tot);
             double al[MAX_COLS];
             for (int c = 0; c < C; ++c) al[c] = tot[c] > 0.0 ? rr[c] / tot[c] : 0.0;
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(PP_THREADS) inpaint_cg_kernel(InpArgs a) {
                 }
             }
             pp_partials(a.part, 2, loc, C);
-            if (!pp_grid_sync(a.bar, a.err)) return;
+            if (!pp_grid_sync(a)) return;
             pp_total(a.part, 2, C, tot);
             bool conv = true;
             double be[MAX_COLS];
@@ -222,7 +228,7 @@ __global__ void __launch_bounds__(PP_THREADS) inpaint_cg_kernel(InpArgs a) {
                 if (!a.unk[n]) continue;
                 for (int c = 0; c < C; ++c) a.P[n * C + c] = a.R[n * C + c] + be[c] * a.P[n * C + c];
             }
-            if (!pp_grid_sync(a.bar, a.err)) return;
+            if (!pp_grid_sync(a)) return;
         }
     }
     for (int64_t n = t0; n < N; n += stride)
@@ -304,19 +310,27 @@ __global__ void nanmask_kernel(const double* field, int C, int64_t n, const uint
     out[i] = bad ? 1 : 0;
 }
 
+static std::mutex g_inp_grid_mu;
+static int g_inp_grid[128] = {0};  // co-resident grid of the cooperative inpainting kernel, per device ordinal
+
+// queried once per device: no configuration call inside a stream capture after the first use
 static int inpaint_grid(int* grid) {
-    int* grid_out_ = grid;
-    static int cached = 0;  // queried once: no configuration call inside a stream capture
-    if (cached > 0) {
-        *grid_out_ = cached;
-        return ALDVC_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "inpaint: current device");
+    if (dev < 0 || dev >= 128) return arg_fail("inpaint: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_inp_grid_mu);
+    if (g_inp_grid[dev] == 0) {
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, inpaint_cg_kernel, PP_THREADS, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "inpaint: occupancy");
+        if (per_sm < 1) return arg_fail("inpaint: kernel does not fit");
+        cudaDeviceProp p;
+        e = cudaGetDeviceProperties(&p, dev);
+        if (e != cudaSuccess) return cuda_fail(e, "inpaint: device properties");
+        g_inp_grid[dev] = per_sm * p.multiProcessorCount;
     }
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, inpaint_cg_kernel, PP_THREADS, 0);
-    if (e != cudaSuccess) return cuda_fail(e, "inpaint: occupancy");
-    if (per_sm < 1) return arg_fail("inpaint: kernel does not fit");
-    *grid = per_sm * sm_count();
-    cached = *grid;
+    *grid = g_inp_grid[dev];
     return ALDVC_OK;
 }
 
@@ -345,12 +359,18 @@ static int run_inpaint(const Grid3& g, int C, double* vals, const uint8_t* unk, 
     a.X = (double*)(ws + 3 * v);
     a.part = (double*)(ws + 4 * v);
     a.bar = (unsigned int*)(ws + 4 * v + align_up((size_t)3 * grid * 2 * MAX_COLS * sizeof(double), 256));
+    const BarrierParams bp = barrier_params();
+    a.bar_extra = bp.extra;
+    a.spin_limit = bp.spin_limit;
     a.iters = iters;
     a.err = err;
     cudaError_t e = cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned int), s);
     if (e != cudaSuccess) return cuda_fail(e, "inpaint: barrier reset");
     void* args[] = {&a};
-    e = cudaLaunchCooperativeKernel((const void*)inpaint_cg_kernel, dim3(grid), dim3(PP_THREADS), args, 0, s);
+    {
+        KTimer kt_("inpaint_cg", s);
+        e = cudaLaunchCooperativeKernel((const void*)inpaint_cg_kernel, dim3(grid), dim3(PP_THREADS), args, 0, s);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "inpaint: cooperative launch");
     count_launch();
     return ALDVC_OK;

@@ -149,24 +149,31 @@ def ncc_search_expanding_device(f, g, coords, half, radius, shift0=None, auto_ex
     return out
 
 
-def clean_field_device(disp, grid_shape, threshold: float):
+def clean_field_device(disp, grid_shape, threshold: float, errs=None):
     """``_clean_field`` (integer_search.py:545-555) on the device: median-test outliers and non-finite rows of the
-    (N,3) FP64 field are replaced by the spring inpainting of their neighbours (every row bad -> zeros)."""
+    (N,3) FP64 field are replaced by the spring inpainting of their neighbours (every row bad -> zeros).  The
+    device error words go to ``errs`` (a kernels.ErrorWords), else they are checked here."""
     import torch
 
     K = _kernels()
+    own = errs is None
+    errs = K.ErrorWords() if own else errs
     d = disp.clone()
     good = torch.isfinite(d).all(dim=1)
     if threshold > 0 and int(good.sum().item()) > 27:
-        flag, _ = K.median_test(torch.where(good[:, None], d, torch.nan).contiguous(), grid_shape,
+        flag, e = K.median_test(torch.where(good[:, None], d, torch.nan).contiguous(), grid_shape,
                                 good.to(torch.uint8).contiguous(), threshold)
+        errs.add(e, "median_test")
         good = good & (flag == 0)
     bad = ~good
     if bool(bad.all().item()):
         return torch.zeros_like(d)
     d[bad] = 0.0
     d = d.contiguous()
-    K.inpaint(d, grid_shape, bad.to(torch.uint8).contiguous())
+    _, e = K.inpaint(d, grid_shape, bad.to(torch.uint8).contiguous())
+    errs.add(e, "inpaint")
+    if own:
+        errs.check()
     return d
 
 
@@ -251,11 +258,13 @@ def auto_pyramid_levels(shape, subset, radius, max_levels: int = 3, f=None, min_
 
 def pyramid_search_device(f, g, coords, grid_shape, subset, radius, levels: int = 0, global_shift=None,
                           outlier_threshold: float = 2.0, auto_expand: bool = True, max_expand: int = 3,
-                          fine_radius: int = PYRAMID_FINE_RADIUS, valid=None, engine_of=None, calls: list | None = None) -> dict:
+                          fine_radius: int = PYRAMID_FINE_RADIUS, valid=None, engine_of=None, calls: list | None = None,
+                          errs=None) -> dict:
     """Coarse-to-fine NCC search (integer_search.py:615-694) on CUDA tensors: the coarsest level searches
     ``coarse_radius(radius)`` on block means, each finer level refines with ``fine_radius`` around the up-scaled,
     median-cleaned and inpainted estimate.  ``valid`` (N,) bool restricts the searched nodes.  Returns disp (N,3)
-    FP64 in full-resolution voxels, the last level's ok / cc / pce / clipped, and the per-level record."""
+    FP64 in full-resolution voxels, the last level's ok / cc / pce / clipped, and the per-level record.  The
+    cleaning's device error words go to ``errs`` (a kernels.ErrorWords), else they are checked per level."""
     import torch
 
     K = _kernels()
@@ -296,7 +305,7 @@ def pyramid_search_device(f, g, coords, grid_shape, subset, radius, levels: int 
         if n_ok == 0:
             info["per_level"].append(rec)
             continue
-        disp_full = clean_field_device(d, grid_shape, outlier_threshold)
+        disp_full = clean_field_device(d, grid_shape, outlier_threshold, errs)
         rec["median_cc"] = float(np.nanmedian(res["cc"].cpu().numpy()))
         rec["clipped_frac"] = float(res["clipped"][res["ok"]].double().mean().item())
         info["per_level"].append(rec)

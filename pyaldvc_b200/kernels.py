@@ -271,6 +271,47 @@ def nodal_gradient(grid_shape, spacing, elem_active, U, gauss_order=2) -> torch.
     return F
 
 
+# --------------------------------------------------------------------------- device error words
+class DeviceError(RuntimeError):
+    """A bounded device-side wait gave up: a grid barrier of a cooperative kernel (PCG, inpainting) whose peer
+    blocks did not arrive within the spin limit.  The kernel set its error word and returned; its output is
+    not a solution."""
+
+
+class ErrorWords:
+    """The device error words of a sequence of launches, read once at the end: ``add`` keeps the word (no
+    synchronisation), ``check`` reduces every word on the device, reads one scalar and raises DeviceError
+    naming the launches that gave up."""
+
+    def __init__(self):
+        self.words: list = []
+        self.names: list = []
+
+    def add(self, err, what: str) -> None:
+        self.words.append(err.reshape(-1)[:1])
+        self.names.append(what)
+
+    def extend(self, other: "ErrorWords") -> None:
+        self.words += other.words
+        self.names += other.names
+
+    def check(self) -> None:
+        if not self.words:
+            return
+        flags = torch.cat(self.words)
+        if int(flags.max().item()) == 0:
+            return
+        bad = sorted({n for n, v in zip(self.names, flags.cpu().tolist()) if v != 0})
+        raise DeviceError(f"a bounded device wait gave up in {', '.join(bad)} (grid barrier spin limit reached)")
+
+
+def test_set_barrier(extra_arrivals: int = 0, spin_limit: int = 0) -> None:
+    """Test hook of the bounded grid barriers (aldvc_test_set_barrier): the cooperative kernels wait for
+    ``extra_arrivals`` more blocks than they launch and give up after ``spin_limit`` polls; (0, 0) restores
+    the production barrier."""
+    _lib.check(lib().aldvc_test_set_barrier(int(extra_arrivals), int(spin_limit)), "aldvc_test_set_barrier")
+
+
 # --------------------------------------------------------------------------- kernel timing
 def kernel_timing(enable: bool) -> None:
     """Start (clearing earlier records) or stop the library's per-launch CUDA-event timing of its main kernels."""

@@ -146,19 +146,21 @@ class Mesh:
         self.half = tuple(int(w) // 2 for w in p.winsize)
 
 
-def _fill(values: torch.Tensor, bad: torch.Tensor, grid_shape):
+def _fill(values: torch.Tensor, bad: torch.Tensor, grid_shape, errs: K.ErrorWords):
     """fill_bad_nodes / clean_initial_guess inpainting of the rows flagged in ``bad`` (all bad -> zeros)."""
     unk = bad.to(torch.uint8).contiguous()
     v = values.clone().contiguous()
     v[bad] = 0.0
-    K.inpaint(v, grid_shape, unk)
+    _, e = K.inpaint(v, grid_shape, unk)
+    errs.add(e, "inpaint")
     return v, bad.all()
 
 
-def _median_flags(field: torch.Tensor, good: torch.Tensor, grid_shape, threshold):
+def _median_flags(field: torch.Tensor, good: torch.Tensor, grid_shape, threshold, errs: K.ErrorWords):
     if threshold <= 0:
         return torch.zeros_like(good)
-    f, _ = K.median_test(field.contiguous(), grid_shape, good.to(torch.uint8).contiguous(), threshold)
+    f, e = K.median_test(field.contiguous(), grid_shape, good.to(torch.uint8).contiguous(), threshold)
+    errs.add(e, "median_test")
     # the reference runs the test only with more than 27 good nodes (local_icgn.py:469-475)
     return (f != 0) & (good.sum() > 27)
 
@@ -212,12 +214,19 @@ def clear_graphs() -> None:
     _ADMM_GRAPHS.clear()
 
 
+def graph_count() -> int:
+    """Number of captured ADMM loops currently cached."""
+    return len(_ADMM_GRAPHS)
+
+
 def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
              tracer: Tracer | None = None, g_mask: torch.Tensor | None = None) -> PassResult:
     """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16).  ``mask``: reference-frame
     material mask; ``g_mask``: deformed-frame mask (False voxels are excluded from every correlation)."""
     tr = tracer if tracer is not None else Tracer(sync=False)
     tr.start()
+    # device error words of the bounded waits (inpainting, median test, PCG), read once at the end of the pass
+    errs = K.ErrorWords()
     f = K.normalize(f_raw) if normalize else f_raw.float().contiguous()
     g = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
     if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:197, 257
@@ -281,6 +290,9 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     rad = tuple(int(r) for r in p.search_radius)
     ncc_calls: list = []
     engine_of = lambda h, r: _ncc_engine(p, h, r)  # noqa: E731
+    # the reference makes the precompute's validity the mesh's node validity before the initial guess
+    # (core/pipeline.py:212, local_icgn.py:300): only those nodes are searched, the others are filled
+    search_valid = valid_b
     if p.init_guess_method not in ("pyramid", "ncc", "zero", "previous"):
         raise ValueError(f"unknown init_guess_method {p.init_guess_method!r}")
     if p.init_guess_method == "zero":
@@ -291,14 +303,14 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         if p.init_guess_method in ("pyramid", "previous"):  # "previous" has no earlier frame here: the reference falls back
             info = IS.pyramid_search_device(f, g, mesh.coords, mesh.grid_shape, subset0, rad, p.pyramid_levels, shift,
                                             p.init_outlier_threshold, p.ncc_auto_expand, p.ncc_max_expand, p.pyramid_fine_radius,
-                                            node_valid, engine_of, ncc_calls)
+                                            search_valid, engine_of, ncc_calls, errs)
             disp, ok, pce = info["disp"], info.get("ok"), info.get("pce")
             if ok is None:
                 ok = torch.ones(mesh.n, dtype=torch.bool, device="cuda")
             init_info = {"method": "pyramid", "levels": info["levels"], "per_level": info["per_level"],
                          "expansions": info["expansions"]}
         else:
-            act = torch.nonzero(node_valid).flatten()
+            act = torch.nonzero(search_valid).flatten()
             if act.numel() == 0:
                 act = torch.arange(mesh.n, device="cuda")
             sh0 = None
@@ -314,12 +326,12 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             pce[act] = res["pce"]
             init_info = {"method": "ncc", "radius": res["radius"], "expansions": res["expansions"]}
         init_info["global_shift"] = shift
-        bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~node_valid
+        bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~search_valid
         if p.init_min_pce > 0 and pce is not None:
             bad = bad | (torch.isfinite(pce) & (pce < p.init_min_pce))
-        flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), ~bad, mesh.grid_shape, p.init_outlier_threshold)
+        flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), ~bad, mesh.grid_shape, p.init_outlier_threshold, errs)
         bad = bad | flag
-        U0, all_bad = _fill(disp, bad, mesh.grid_shape)
+        U0, all_bad = _fill(disp, bad, mesh.grid_shape, errs)
         if bool(all_bad.item()):
             U0.zero_()
         init_info["n_bad"] = int(bad.sum().item())
@@ -342,9 +354,9 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
     P, n_iter, status, zncc = icgn12_on(None, th12, br12)
     bad = status != STATUS_CONVERGED
-    flag = _median_flags(P[:, 9:].contiguous(), ~bad, mesh.grid_shape, p.local_outlier_threshold)
+    flag = _median_flags(P[:, 9:].contiguous(), ~bad, mesh.grid_shape, p.local_outlier_threshold, errs)
     bad = bad | flag
-    UF, all_bad = _fill(P, bad, mesh.grid_shape)  # U and F inpainted together (fill_bad_nodes :492-522)
+    UF, all_bad = _fill(P, bad, mesh.grid_shape, errs)  # U and F inpainted together (fill_bad_nodes :492-522)
     if bool(all_bad.item()):
         UF.zero_()
     U1 = UF[:, 9:].contiguous()
@@ -355,6 +367,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     result = PassResult(U=U1, F=F1.reshape(-1, 3, 3), status=status, zncc=zncc, n_iter=n_iter, coords=mesh.coords,
                         grid_shape=mesh.grid_shape, valid=valid_b, U_local=U_local, U0=U0, P_local=P, status_local=status,
                         n_iter_local=n_iter)
+    result.F_local = F1.reshape(-1, 3, 3).clone()  # the local result after outlier filling
     result.tracer = tr
     result.ncc_calls = ncc_calls  # (nodes, half, radius, engine) of every integer search of the pass
     result.init_info = init_info
@@ -362,6 +375,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     result.node_half = node_half
     result.icgn3_iters = []  # n_iter tensors of every 3-DOF pass
     if not p.use_global_step:
+        errs.check()
         return result
 
     # ---------------- sections 5-6: ADMM (pipeline.py:286-352), beta fixed or tuned (pipeline.py:288-298)
@@ -379,11 +393,12 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     T = {"f": f, "g": g_prep, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
          "coords": mesh.coords, "elem": elem_active, "node_half": node_half, "g4": g4}
 
-    def make_steps(T):
+    def make_steps(T, errs_):
         def global_step(U1_, F1_, W_, v_):
             b = K.global_rhs(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
-            U2_, _, _ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, b, U1_, p.pcg_tol,
-                                   p.pcg_max_iter, p.gauss_pt_order)
+            U2_, _, e_ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, b, U1_, p.pcg_tol,
+                                    p.pcg_max_iter, p.gauss_pt_order)
+            errs_.add(e_, "pcg_hex8")
             F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, T["elem"], U2_, p.gauss_pt_order).reshape(-1, 9)
             F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
             return U2_, F2_
@@ -402,7 +417,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
             U, it3, st3, zc3 = icgn3_on(None, U2, F2, v, th3, br3)
             bad3 = st3 != STATUS_CONVERGED
-            bad3 = bad3 | _median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold)
+            bad3 = bad3 | _median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold, errs_)
             U1n = torch.where(bad3[:, None], U2, U)
             F1n = F2
             U2n, F2n = global_step(U1n, F1n, W, v)
@@ -417,7 +432,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
 
         return global_step, icgn3_on, admm_step
 
-    global_step, icgn3_on, admm_step = make_steps(T)
+    global_step, icgn3_on, admm_step = make_steps(T, errs)
     W = torch.zeros((mesh.n, 9), dtype=torch.float64, device="cuda")
     v = torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda")
     U2, F2 = global_step(U1, F1, W, v)
@@ -436,12 +451,15 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         entry = _ADMM_GRAPHS.get(key)
         if entry is None:
             static = {k: (None if t is None else t.clone()) for k, t in {**T, **state}.items()}
-            _, _, admm_static = make_steps(static)
+            warm_errs, graph_errs = K.ErrorWords(), K.ErrorWords()
+            _, _, admm_static = make_steps(static, warm_errs)
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             with torch.cuda.stream(side):  # warm-up outside capture (allocator pools, kernel attributes)
                 admm_static(static["U2"], static["F2"], static["W"], static["v"], th3, br3)
             torch.cuda.current_stream().wait_stream(side)
+            warm_errs.check()
+            _, _, admm_static = make_steps(static, graph_errs)
             graph = torch.cuda.CUDAGraph()
             with torch.cuda.graph(graph):
                 a = (static["U2"], static["F2"], static["W"], static["v"])
@@ -450,7 +468,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                     U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg = admm_static(*a, th3, br3)
                     outs.append((U1g, stg, zcg, itg))
                     a = (U2g, F2g, Wg, vg)
-            entry = {"graph": graph, "static": static, "final": a, "outs": outs[-1], "iters": [o[3] for o in outs]}
+            entry = {"graph": graph, "static": static, "final": a, "outs": outs[-1], "iters": [o[3] for o in outs],
+                     "errs": graph_errs}
             _ADMM_GRAPHS[key] = entry
             while len(_ADMM_GRAPHS) > ADMM_GRAPH_CACHE:
                 _ADMM_GRAPHS.pop(next(iter(_ADMM_GRAPHS)))
@@ -460,6 +479,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                 if t is not None:
                     entry["static"][k].copy_(t)
         entry["graph"].replay()
+        errs.extend(entry["errs"])  # the graph's error words, rewritten by this replay
         # the graph's outputs are overwritten by its next replay: the result keeps copies
         U2, F2 = entry["final"][0].clone(), entry["final"][1].clone()
         U1, st_last, zc_last, it_last = (t.clone() for t in entry["outs"])
@@ -475,6 +495,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             U1, U2, F2 = U1n, U2n, F2n
             if p.admm_early_stop and (float(du_g.item()) < p.admm_tol or float(du_l.item()) < p.admm_tol):
                 break
+    errs.check()
     tr.mark("admm")
     result.U = U2
     result.F = F2.reshape(-1, 3, 3)

@@ -77,8 +77,9 @@ def solve_subpb2(system: GlobalSystem, U1, F1, W, v):
     """``u_hat`` (N, 3); inactive nodes keep ``U1`` (subpb2_solver.solve_subpb2 :133-155)."""
     t0 = time.perf_counter()
     U2, iters, err = solve_subpb2_device(system, U1, F1, W, v)
-    if int(err.item()) != 0:
-        raise RuntimeError("aldvc_pcg_hex8: a grid barrier gave up")
+    words = _kernels().ErrorWords()
+    words.add(err, "pcg_hex8")
+    words.check()
     info = {"solver": "pcg", "iterations": int(iters.item()), "time": time.perf_counter() - t0}
     return U2.cpu().numpy(), info
 

@@ -3,7 +3,7 @@
 Run in a container that holds the pyALDVC sources (read-only) at
 ``$ALDVC_REFERENCE/src`` (default ``/root/reference/src``)::
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [kernels volume_ops init_guess strain beta pass ncc_fft]
 
 It imports the reference package, runs its own Numba CPU kernels on seeded
 bead volumes from ``pyaldvc_b200.synthetic`` and stores inputs + outputs as
@@ -411,9 +411,71 @@ def beta_fixtures():
           f"{out['bt_normalized_k_best']}, beta {out['bt_normalized_beta']}")
 
 
+def pass_fixtures():
+    """Whole frame pairs through the reference's own run_aldvc (core/pipeline.py, numba backend, PCG global
+    solver, FEM global step, fixed beta): per case the node validity, the initial guess, the local 12-DOF
+    result after outlier filling, the final U / F / status / ZNCC after the ADMM loop and its step count."""
+    from al_dvc.core.pipeline import run_aldvc
+    from al_dvc.io.volume_ops import normalize_volume
+
+    import pass_inputs as PI
+
+    out = {}
+    for name, c in PI.PASS_CASES.items():
+        f, g, mask, _ = PI.pass_pair(name)
+        para = dvcpara_default(**PI.PASS_COMMON, **c["para"], backend="numba", verbose=False)
+        r = run_aldvc(para, [f, g], masks=None if mask is None else [mask, None], compute_strain=False)
+        fr = r.result_disp[0]
+        m = r.dvc_mesh
+        infos = fr.admm.local_info
+        out.update({f"{name}_sha_f": PI.sha(normalize_volume(f)), f"{name}_sha_g": PI.sha(normalize_volume(g)),
+                    f"{name}_coords": np.round(m.coordinates).astype(np.int64), f"{name}_grid": np.array(m.grid_shape),
+                    f"{name}_spacing": np.array(m.spacing), f"{name}_node_valid": m.node_valid, f"{name}_U0": fr.U0,
+                    f"{name}_U_local": fr.U_local, f"{name}_F_local": fr.F_local, f"{name}_U": fr.U, f"{name}_F": fr.F,
+                    f"{name}_status": fr.status, f"{name}_zncc": fr.zncc, f"{name}_steps": fr.admm.n_steps,
+                    f"{name}_status_local": infos[0].status, f"{name}_n_iter_local": infos[0].n_iter,
+                    f"{name}_n_iter": infos[-1].n_iter})
+        print(f"pass {name}: grid {m.grid_shape}, {fr.admm.n_steps} ADMM steps, statuses {np.bincount(fr.status.astype(int))}")
+    path = os.path.join(HERE, "golden_pass.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
+def ncc_fft_fixtures():
+    """The reference's ncc_search where it takes its FP32 FFT branch (integer_search.py:395, :418-443): a 17^3
+    template at +-9 and +-16, an anisotropic template and radius, and the expansion from +-8 (direct) to +-16 and
+    +-32 (FFT); plus _window_box_stats on one node's window."""
+    from al_dvc.io.volume_ops import normalize_volume
+
+    import pass_inputs as PI
+
+    pair = PI.ncc_pair()
+    f, g = normalize_volume(pair.f), normalize_volume(pair.g)
+    coords = PI.ncc_coords()
+    shift = PI.ncc_shift(coords)
+    out = {"sha_f": PI.sha(f), "sha_g": PI.sha(g), "coords": coords, "shift": shift}
+    for name, c in PI.NCC_SEARCHES.items():
+        res = ris.ncc_search(f, g, coords, c["subset"], c["radius"], shift if c["shift"] else None, backend="numba")
+        for k in ("disp", "cc", "pce", "clipped", "ok"):
+            out[f"{name}_{k}"] = res[k]
+    res = ris.ncc_search_expanding(f, g, coords, PI.NCC_EXPAND["subset"], PI.NCC_EXPAND["radius"], None, True, 3, backend="numba")
+    for k in ("disp", "cc", "pce", "clipped", "ok"):
+        out[f"expand_{k}"] = res[k]
+    out["expand_expansions"] = res["expansions"]
+    out["expand_radius"] = np.array(res["radius"])
+    W = np.ascontiguousarray(g[10:40, 12:42, 14:44][None])  # one 30^3 window, boxes of (sz, sy, sx) = (13, 11, 9)
+    s1 = np.empty((1, 18, 20, 22))
+    s2 = np.empty((1, 18, 20, 22))
+    ris._window_box_stats(W, 13, 11, 9, s1, s2)
+    out.update(box_W_origin=np.array([10, 12, 14]), box_sum=s1, box_sq=s2)
+    path = os.path.join(HERE, "golden_ncc_fft.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB); expansions {res['expansions']}, radius {res['radius']}")
+
+
 if __name__ == "__main__":
-    main()
-    volume_ops_fixtures()
-    init_guess_fixtures()
-    strain_fixtures()
-    beta_fixtures()
+    which = sys.argv[1:] or ["kernels", "volume_ops", "init_guess", "strain", "beta", "pass", "ncc_fft"]
+    makers = {"kernels": main, "volume_ops": volume_ops_fixtures, "init_guess": init_guess_fixtures, "strain": strain_fixtures,
+              "beta": beta_fixtures, "pass": pass_fixtures, "ncc_fft": ncc_fft_fixtures}
+    for w in which:
+        makers[w]()

@@ -1,0 +1,113 @@
+"""GPU: the integer search against the reference's FFT branch (tests/golden/golden_ncc_fft.npz).
+
+Above 3e7 offset x template-voxel products per node the reference's CPU search correlates with FP32 FFTs
+(integer_search.py:395, :418-443) and takes the first maximum of that FP32 map.  Every engine here scores its
+FP32 map's near-maximal offsets again in FP64 (the exact map of the direct formula) and takes the first maximum
+of those.  The two rules pick the same integer peak unless the exact map's two best offsets lie within the FFT
+map's rounding of each other: the tests below require identical ok / clipped flags and integer peaks at every
+node whose exact top-two gap exceeds 1e-5, count the near-tie nodes, and require the engines' own choice there
+to be the exact map's first maximum.  Sub-voxel displacements and peak values differ from the reference's only
+by the FFT map's rounding (disp 1e-4 voxel, cc 2e-6).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import pass_inputs as PI  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+ENGINES = {"tiled": 0, "plain": 1, "fft": 2, "fft_stockham": 3}
+NEAR_TIE = 1e-5
+
+
+@pytest.fixture(scope="module")
+def gn():
+    with np.load(os.path.join(HERE, "golden", "golden_ncc_fft.npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(scope="module")
+def ncc_in(oracle_mod, gn):
+    pair = PI.ncc_pair()
+    f, g = oracle_mod.normalize_volume(pair.f), oracle_mod.normalize_volume(pair.g)
+    assert PI.sha(f) == str(gn["sha_f"]) and PI.sha(g) == str(gn["sha_g"])
+    return f, g, gn["coords"], gn["shift"]
+
+
+def _exact_top2(oracle_mod, f, g, coords, subset, radius, shift):
+    """First maximum (flat index) and the gap to the second-best offset of the exact FP64 map, per node."""
+    hx, hy, hz = (int(w) // 2 for w in subset)
+    rx, ry, rz = radius
+    nz, ny, nx = f.shape
+    wx, wy, wz = 2 * hx + 1 + 2 * rx, 2 * hy + 1 + 2 * ry, 2 * hz + 1 + 2 * rz
+    sh = np.zeros_like(coords) if shift is None else shift
+    wx0 = np.clip(coords[:, 0] + sh[:, 0] - hx - rx, 0, nx - wx)
+    wy0 = np.clip(coords[:, 1] + sh[:, 1] - hy - ry, 0, ny - wy)
+    wz0 = np.clip(coords[:, 2] + sh[:, 2] - hz - rz, 0, nz - wz)
+    maps = np.empty((len(coords), 2 * rz + 1, 2 * ry + 1, 2 * rx + 1))
+    oracle_mod.zncc_direct(f, g, coords, hx, hy, hz, rx, ry, rz, wx0, wy0, wz0, np.ones(len(coords), bool), maps)
+    flat = maps.reshape(len(coords), -1)
+    top = np.sort(flat, axis=1)[:, -2:]
+    return np.argmax(flat, axis=1), top[:, 1] - top[:, 0], (wx0, wy0, wz0)
+
+
+def _compare(oracle_mod, f, g, coords, shift, subset, radius, res, ref, what):
+    ok = ref["ok"]
+    np.testing.assert_array_equal(res["ok"], ok, err_msg=f"{what}: ok")
+    d = np.abs(res["disp"] - ref["disp"])
+    moved = np.flatnonzero(ok & (np.nanmax(d, axis=1) > 0.5))  # a different integer peak
+    same = ok.copy()
+    same[moved] = False
+    np.testing.assert_array_equal(res["clipped"][same], ref["clipped"][same], err_msg=f"{what}: clipped")
+    np.testing.assert_allclose(res["disp"][same], ref["disp"][same], rtol=0, atol=1e-4, err_msg=f"{what}: disp")
+    np.testing.assert_allclose(res["cc"][same], ref["cc"][same], rtol=0, atol=2e-6, err_msg=f"{what}: cc")
+    np.testing.assert_allclose(res["pce"][same], ref["pce"][same], rtol=2e-3, err_msg=f"{what}: pce")
+    if moved.size:
+        # the engines' peak there must be the exact map's first maximum, and the reference's a near tie of it
+        sel = moved
+        arg, gap, (wx0, wy0, wz0) = _exact_top2(oracle_mod, f, g, coords[sel], subset, radius,
+                                                None if shift is None else shift[sel])
+        assert np.all(gap < NEAR_TIE), f"{what}: peaks differ at nodes {sel} whose exact top-two gap is {gap}"
+        hx, hy, hz = (int(w) // 2 for w in subset)
+        vz, vy, vx = (2 * r + 1 for r in radius[::-1])
+        pz, py, px = np.unravel_index(arg, (vz, vy, vx))
+        exact = np.column_stack([wx0 + px + hx - coords[sel, 0], wy0 + py + hy - coords[sel, 1], wz0 + pz + hz - coords[sel, 2]])
+        np.testing.assert_array_less(np.abs(res["disp"][sel] - exact), 1.0, err_msg=f"{what}: engine peak is not the exact one")
+    return moved.size
+
+
+@pytest.mark.parametrize("engine", list(ENGINES))
+@pytest.mark.parametrize("name", list(PI.NCC_SEARCHES))
+def test_ncc_search_matches_reference_fft_branch(oracle_mod, gn, ncc_in, name, engine):
+    from pyaldvc_b200.integer_search import ncc_search
+
+    f, g, coords, shift = ncc_in
+    c = PI.NCC_SEARCHES[name]
+    sh = shift if c["shift"] else None
+    res = ncc_search(f, g, coords, c["subset"], c["radius"], sh, engine=ENGINES[engine])
+    ref = {k: gn[f"{name}_{k}"] for k in ("disp", "cc", "pce", "clipped", "ok")}
+    n_ties = _compare(oracle_mod, f, g, coords, sh, c["subset"], c["radius"], res, ref, f"{name}/{engine}")
+    assert n_ties <= 0.02 * len(coords), f"{name}/{engine}: {n_ties} near-tie nodes"
+
+
+@pytest.mark.parametrize("engine", ["tiled", "fft"])
+def test_ncc_expansion_matches_reference_fft_branch(oracle_mod, gn, ncc_in, engine):
+    """+-8 (the reference's direct branch), then +-16 and +-32 (its FFT branch) on the clipped nodes."""
+    from pyaldvc_b200.integer_search import ncc_search_expanding
+
+    f, g, coords, _ = ncc_in
+    res = ncc_search_expanding(f, g, coords, PI.NCC_EXPAND["subset"], PI.NCC_EXPAND["radius"], engine=ENGINES[engine])
+    assert res["expansions"] == int(gn["expand_expansions"]) == 2
+    assert tuple(res["radius"]) == tuple(int(r) for r in gn["expand_radius"])
+    ref = {k: gn[f"expand_{k}"] for k in ("disp", "cc", "pce", "clipped", "ok")}
+    n_ties = _compare(oracle_mod, f, g, coords, None, PI.NCC_EXPAND["subset"], tuple(res["radius"]), res, ref, f"expand/{engine}")
+    assert n_ties <= 0.02 * len(coords)
