@@ -48,7 +48,108 @@ def parse():
     ap.add_argument("--icgn-threads", type=int, default=0,
                     help="pin the batched IC-GN kernels to the lean form with this many threads per node (32/64/128) "
                          "instead of the autotuner's choice (for profiler runs, whose timings would mislead it)")
+    ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute"],
+                    help="full: the benchmark line; pass / ncc / precompute: timing of one stage on a profiling case "
+                         "(human-readable lines, no JSON), see stage_main")
+    ap.add_argument("--shape", type=int, nargs=3, default=None, help="volume (nz ny nx) of a --stage case")
+    ap.add_argument("--engine", type=int, default=2, help="--stage ncc: 0 tiled, 1 plain, 2 FFT, 3 FFT with Stockham")
+    ap.add_argument("--half", type=int, default=8, help="--stage ncc: template half-width")
+    ap.add_argument("--radius", type=int, default=16, help="--stage ncc: search radius")
+    ap.add_argument("--per-node", action="store_true", help="--stage precompute: also time the per-node kernel")
     return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- profiling cases
+def stage_main(args) -> None:
+    """Timing of one stage on a seeded case small enough for a profiler capture; prints each repetition's wall
+    time after a device synchronisation and the library's CUDA-event kernel times of the last repetition.
+
+    pass        the configuration's whole pass (its parameters; --icgn-threads pins the lean IC-GN form) on a
+                device-rendered pair of --shape (default 200 384 384 for configuration 5) with the configuration's
+                beads, noise and field; --warmup passes first, then --steps timed ones
+    ncc         the integer search (--engine, 2 FFT by default) on a 192^3 pair of Gaussian beads (0.03 / voxel,
+                sigma 1.5, rendered on the device) moved by (1.3, -2.4, 3.1), a (2 --half + 1)^3 template at
+                +- --radius (default 17^3 at +-16: the 1024 x 1024 x 306 workload's geometry), nodes every 12 voxels
+    precompute  the separable precompute on a 306 x 512 x 512 volume (--shape) of 0.005 / voxel sigma-2 beads, 33^3
+                subsets every 12 voxels (f and three gradients 1.28 GB, larger than L2); --per-node also times the
+                per-node kernel and prints the largest relative difference of H between the forms"""
+    import torch
+
+    from pyaldvc_b200 import configs
+    from pyaldvc_b200 import kernels as K
+    from pyaldvc_b200 import synthetic as S
+    from pyaldvc_b200.mesh import build_grid_axes, grid_coords
+
+    def timed(label, fn, n, unit_name):
+        out = None
+        for i in range(max(1, args.steps)):
+            if i == max(1, args.steps) - 1:
+                K.kernel_timing(True)
+            torch.cuda.synchronize()
+            t = time.time()
+            out = fn()
+            torch.cuda.synchronize()
+            dt = time.time() - t
+            print(f"{label} rep {i}: {1e3 * dt:.2f} ms, {1e6 * dt / n:.3f} us per {unit_name} ({n} {unit_name}s)", flush=True)
+        print({k: (round(v[0], 3), v[1]) for k, v in K.kernel_timing_read().items()}, flush=True)
+        K.kernel_timing(False)
+        return out
+
+    if args.stage == "pass":
+        from pyaldvc_b200.pipeline import run_pass
+
+        cfg = args.config
+        shape = tuple(args.shape) if args.shape else (200, 384, 384)
+        p = configs.params(cfg)
+        if args.icgn_threads:
+            p.threads, p.brick_floats = args.icgn_threads, 0
+        f, g, mask, _ = configs.device_pair(cfg, shape=shape)
+        for _ in range(args.warmup):
+            run_pass(f, g, p, mask)
+        res = timed(f"config {cfg} pass on {shape}", lambda: run_pass(f, g, p, mask), 1, "pass")
+        print(f"{int(res.coords.shape[0])} nodes, mean 12-DOF iterations {float(res.n_iter_local.double().mean()):.2f}")
+        return
+    if args.stage == "ncc":
+        n, h, r = 192, args.half, args.radius
+        shape = (n, n, n)
+        c, pk = S.draw_beads(shape, 0.03, 5)
+        vols = []
+        for cc in (c, S.displace_beads(c, S.translation((1.3, -2.4, 3.1)))):
+            acc = torch.zeros(shape, dtype=torch.float64, device="cuda")
+            K.render_beads(acc, cc, pk, 1.5, 6)
+            vols.append(acc.float().contiguous())
+            del acc
+        f, g = vols
+        m = h + r + 2
+        ax = np.arange(m, n - m, 12)
+        zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
+        coords = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1).astype(np.int64)
+        for _ in range(args.warmup):
+            K.ncc_search(f, g, coords, (h, h, h), (r, r, r), None, args.engine)
+        timed(f"engine {args.engine}", lambda: K.ncc_search(f, g, coords, (h, h, h), (r, r, r), None, args.engine), len(coords),
+              "node")
+        return
+    if args.stage == "precompute":
+        shape = tuple(args.shape) if args.shape else (306, 512, 512)
+        c, pk = S.draw_beads(shape, 0.005, 7)
+        acc = torch.zeros(shape, dtype=torch.float64, device="cuda")
+        K.render_beads(acc, c, pk, 2.0, 8)
+        f = K.normalize(acc.float().contiguous())
+        del acc
+        gx, gy, gz = K.gradients(f)
+        w = (32, 32, 32)
+        x0, y0, z0 = build_grid_axes(shape, w, (12, 12, 12))
+        axes = [np.round(np.asarray(a_)).astype(np.int64) for a_ in (x0, y0, z0)]
+        half = (16, 16, 16)
+        n = int(np.prod([len(a_) for a_ in axes]))
+        for _ in range(args.warmup):
+            K.precompute_grid(*axes, half, f, gx, gy, gz, 0.5, 1e12)
+        Hg = timed("grid form", lambda: K.precompute_grid(*axes, half, f, gx, gy, gz, 0.5, 1e12)[0], n, "node")
+        if args.per_node:
+            coords = torch.from_numpy(np.round(grid_coords(x0, y0, z0)).astype(np.int64)).cuda()
+            Hp = timed("per-node form", lambda: K.precompute(coords, half, f, gx, gy, gz, None, 0.5, 1e12)[0], n, "node")
+            print(f"max |dH| / max |H| = {float((Hg - Hp).abs().max() / Hp.abs().max()):.2e}", flush=True)
+        return
 
 
 # --------------------------------------------------------------------------- clocks
@@ -107,92 +208,123 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- CPU baseline (oracle, FP64)
 def node_block(mesh_shape, edge: int):
-    """Flat indices of an edge^3 block of nodes at the centre of the node grid."""
+    """(flat indices, block grid shape) of an edge^3 block of nodes at the centre of the node grid."""
     nz, ny, nx = mesh_shape
     e = [min(edge, s) for s in (nz, ny, nx)]
     st = [(s - k) // 2 for s, k in zip((nz, ny, nx), e)]
     iz, iy, ix = np.meshgrid(*[np.arange(a, a + k) for a, k in zip(st, e)], indexing="ij")
-    return (iz * ny * nx + iy * nx + ix).ravel()
+    return (iz * ny * nx + iy * nx + ix).ravel(), tuple(e)
 
 
-def cpu_sample(f, g, coords, p, block, threads: int, mask=None):
-    """The per-node chain of the pass on the host cores for the nodes ``block`` of ``coords``: NCC search, precompute,
-    12-DOF IC-GN and (with the global step) two 3-DOF passes, with the pass's reference mask and per-node subset
-    shapes (the oracle is called once per shape, as the reference calls its kernels).  Volumes are cropped to the
-    box the block touches.  Returns (seconds, n_nodes, results)."""
+def sample_box(c, spec: dict, vol_shape):
+    """The volume box ((z0, z1), (y0, y1), (x0, x1)) a block of nodes ``c`` (M, 3) [x, y, z] reads: subsets with room
+    for the displacement, and the NCC windows at the stated radius."""
+    half = [int(w) // 2 for w in spec["winsize"]]
+    h0 = [min(int(w), 16) // 2 for w in spec["winsize"]]
+    reach = np.array([max(h + 16, a + r) + 8 for h, a, r in zip(half, h0, spec["search_radius"])])
+    lo = np.maximum(c.min(axis=0) - reach, 0)
+    hi = np.minimum(c.max(axis=0) + reach + 1, [vol_shape[2], vol_shape[1], vol_shape[0]])
+    return ((int(lo[2]), int(hi[2])), (int(lo[1]), int(hi[1])), (int(lo[0]), int(hi[0])))
+
+
+def oracle_prm(spec: dict) -> dict:
+    """The oracle pass's parameters of a configuration (no early stop where the configuration runs without it)."""
+    prm = {k: spec[k] for k in ("winsize", "search_radius", "interp_method") if k in spec}
+    prm["use_global_step"] = spec.get("use_global_step", True)
+    for k in ("mu", "beta", "admm_max_iter"):
+        if k in spec:
+            prm[k] = spec[k]
+    if not spec.get("admm_early_stop", True):
+        prm["admm_tol"] = -1.0
+    return prm
+
+
+def cpu_pass_sample(fn, gn, c_local, c_global, block_grid, spec: dict, mask, threads: int):
+    """One AL-DVC pass of the FP64 oracle (the reference's CPU path restated: NCC with the reference's
+    engine switch, FFT above 3e7 products, and radius expansion; precompute; 12-DOF with outlier filling; global
+    step; ADMM) over a block of nodes as its own node grid, on normalised host volumes of the box the block reads.
+    Returns (seconds, nodes, result)."""
     from oracle import oracle as orc
 
     orc.set_num_threads(threads)
-    c = coords[block]
-    half = tuple(int(w) // 2 for w in p.winsize)
-    if p.node_winsize is not None:
-        halves = np.asarray(p.node_winsize(c), dtype=np.int64) // 2
-    else:
-        halves = np.tile(np.asarray(half, dtype=np.int64), (len(c), 1))
-    sub0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
-    h0 = tuple(int(w) // 2 for w in sub0)
-    reach = [max(h + 8, h0_ + r + 2) + 8 for h, h0_, r in zip(half, h0, p.search_radius)]
-    lo = np.maximum(c.min(axis=0) - reach, 0)
-    hi = np.minimum(c.max(axis=0) + reach + 1, [f.shape[2], f.shape[1], f.shape[0]])
-    crop = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
-    fs = np.ascontiguousarray(f[crop])
-    gs = np.ascontiguousarray(g[crop])
-    ms = np.ones((1, 1, 1), np.uint8) if mask is None else np.ascontiguousarray(mask[crop])
-    cl = (c - lo).astype(np.int64)
-    mode = {"linear": 0, "cubic": 1}[p.interp_method]
-    n = cl.shape[0]
-    P = np.zeros((n, 12))
-    st = np.zeros(n, dtype=np.int8)
+    node_half = None
+    if spec.get("node_winsize") is not None:
+        node_half = np.asarray(spec["node_winsize"](c_global), dtype=np.int64) // 2
+    spacing = tuple(float(s) for s in spec["winstepsize"])
     t0 = time.perf_counter()
-    gx, gy, gz = orc.compute_gradients(fs)
-    res = orc.ncc_search(fs, gs, cl, sub0, p.search_radius)
-    U0 = np.where(np.isfinite(res["disp"]), res["disp"], 0.0)
+    out = orc.aldvc_pass(fn, gn, c_local, block_grid, spacing, mask=None if mask is None else mask != 0, node_half=node_half,
+                         **oracle_prm(spec))
+    return time.perf_counter() - t0, int(c_local.shape[0]), out
+
+
+def oracle_local_rms(fn, gn, c_local, spec: dict, mask, U0, P_gpu, st_gpu, c_global) -> float | None:
+    """RMS difference of the device's raw 12-DOF displacements from the FP64 oracle's 12-DOF solve started at the
+    same initial guess, on the nodes both converged (per subset shape, as the reference calls its kernels)."""
+    from oracle import oracle as orc
+
+    n = c_local.shape[0]
+    half = tuple(int(w) // 2 for w in spec["winsize"])
+    halves = (np.tile(np.asarray(half), (n, 1)) if spec.get("node_winsize") is None
+              else np.asarray(spec["node_winsize"](c_global), dtype=np.int64) // 2)
+    mode = {"linear": 0, "cubic": 1, "bspline": 2}[spec["interp_method"]]
+    gx, gy, gz = orc.compute_gradients(fn)
+    m = np.ones((1, 1, 1), np.uint8) if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    P = np.full((n, 12), np.nan)
+    st = np.full(n, -1, dtype=np.int8)
     for sh in np.unique(halves, axis=0):
         sel = np.flatnonzero((halves == sh).all(axis=1))
-        cs = cl[sel]
         hs = tuple(int(v) for v in sh)
-        H, L, mf, bf, nv, valid = orc.precompute_nodes(cs, *hs, fs, gx, gy, gz, ms, p.min_valid_ratio, p.hessian_cond_max,
-                                                       p.subset_stride)
+        H, L, mf, bf, _, valid = orc.precompute_nodes(c_local[sel], *hs, fn, gx, gy, gz, m, 0.5, 1e12, 1)
         P0 = np.zeros((len(sel), 12))
         P0[:, 9:] = U0[sel]
-        Ps, it, sts, zc = orc.icgn_12dof_parallel(cs, P0, *hs, fs, gx, gy, gz, ms, gs, mode, L, mf, bf, valid, p.icgn_tol,
-                                                  p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride)
-        P[sel], st[sel] = Ps, sts
-        if p.use_global_step:
-            U, F = Ps[:, 9:], Ps[:, :9].reshape(-1, 3, 3)
-            v = np.zeros_like(U)
-            for _ in range(2, p.admm_max_iter + 1):
-                U, it3, st3, zc3 = orc.icgn_3dof_parallel(cs, U, F, v, *hs, fs, gx, gy, gz, ms, gs, mode, H, mf, bf, valid, p.mu,
-                                                          p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience,
-                                                          p.subset_stride)
-    dt = time.perf_counter() - t0
-    return dt, int(n), {"P": P, "status": st, "U0": U0}
+        P[sel], _, st[sel], _ = orc.icgn_12dof_parallel(c_local[sel], P0, *hs, fn, gx, gy, gz, m, gn, mode, L, mf, bf, valid, 1e-2,
+                                                        1e-3, 100, 5, 1)
+    ok = (st == 0) & (st_gpu == 0)
+    if not ok.any():
+        return None
+    d = P_gpu[ok, 9:] - P[ok, 9:]
+    return float(np.sqrt(np.mean(d * d)))
 
 
 def run_reference(args):
-    """CPU arm: the FP64 oracle of the reference's CPU path on the host cores, bounded sample per step."""
+    """CPU arm: the FP64 oracle restatement of the reference's CPU path (the reference is Python/Numba with no
+    compiled code to build) on the host cores, one bounded sample of the workload per step: a block of nodes of the
+    configuration's node grid, run as its own grid through the whole pass, on that block's box of the volume pair
+    rendered on the host.  Uses neither the device nor this package's CUDA library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import oracle as orc
     from pyaldvc_b200 import configs, mesh
 
-    p = configs.params(args.config)
+    spec = configs.spec(args.config)
     shape = configs.shape_of(args.config)
-    x0, y0, z0 = mesh.build_grid_axes(shape, p.winsize, p.winstepsize)
+    x0, y0, z0 = mesh.build_grid_axes(shape, spec["winsize"], spec["winstepsize"])
     coords = np.round(mesh.grid_coords(x0, y0, z0)).astype(np.int64)
     grid_shape = (len(z0), len(y0), len(x0))
-    f, g, mask = _host_volumes(args.config)
+    block, block_grid = node_block(grid_shape, args.cpu_nodes)
+    c = coords[block]
+    box = sample_box(c, spec, shape)
+    f_raw, g_raw, mask = configs.host_box(args.config, box)
+    fn, gn = orc.normalize_volume(f_raw), orc.normalize_volume(g_raw)
+    c_local = c - np.array([box[2][0], box[1][0], box[0][0]], dtype=np.int64)[None, :]
     threads = os.cpu_count() or 1
-    block = node_block(grid_shape, args.cpu_nodes)
-    for _ in range(max(0, args.warmup and 1)):
-        cpu_sample(f, g, coords, p, block[:8], threads, mask)
+    small, small_grid = node_block(block_grid, 2)
+    for _ in range(max(0, min(args.warmup, 1))):  # the first call builds the oracle library and warms its code paths
+        cpu_pass_sample(fn, gn, c_local.reshape(block_grid + (3,))[tuple(slice(0, k) for k in small_grid)].reshape(-1, 3),
+                        c.reshape(block_grid + (3,))[tuple(slice(0, k) for k in small_grid)].reshape(-1, 3), small_grid, spec,
+                        mask, threads)
     times = []
     n = 0
+    engine = orc.ncc_engine(tuple(min(int(w), 16) // 2 for w in spec["winsize"]), spec["search_radius"])
     for _ in range(args.steps):
-        dt, n, _ = cpu_sample(f, g, coords, p, block, threads, mask)
+        dt, n, _ = cpu_pass_sample(fn, gn, c_local, c, block_grid, spec, mask, threads)
         times.append(dt)
     value = n / float(np.mean(times))
-    sample = f"{n} nodes ({args.cpu_nodes}^3 block at the grid centre) per step, FP64 oracle, {threads} threads"
+    sample = (f"{n} nodes ({'x'.join(str(k) for k in block_grid)} block at the grid centre, run as its own node grid) "
+              f"per step through the whole pass (NCC on the {engine} engine with expansion, precompute, 12-DOF with filling"
+              f"{', global step and ADMM' if spec.get('use_global_step', True) else ''}), FP64 oracle, {threads} threads, "
+              f"on a {'x'.join(str(b[1] - b[0]) for b in box)} box of the pair rendered on the host")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
@@ -325,35 +457,6 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
     return out
 
 
-def _normalize_np(v):
-    a = np.asarray(v, dtype=np.float64)
-    nz, ny, nx = a.shape
-    pilot = float(a[nz // 2, ny // 2, nx // 2])
-    d = a - pilot
-    ms = d.mean()
-    sd = np.sqrt(max((d * d).mean() - ms * ms, 0.0))
-    sd = sd if sd >= 1e-12 else 1.0
-    return ((a - (pilot + ms)) * (1.0 / sd)).astype(np.float32)
-
-
-def _host_volumes(cfg: int):
-    """Normalised host volumes of the configuration and its reference mask (for the CPU arm)."""
-    from pyaldvc_b200 import configs
-
-    if cfg in (3, 5):
-        import torch
-
-        if torch.cuda.is_available():
-            f, g, m, _ = configs.device_pair(cfg)
-            from pyaldvc_b200 import kernels as K
-
-            return K.normalize(f).cpu().numpy(), K.normalize(g).cpu().numpy(), None if m is None else m.cpu().numpy()
-        if cfg == 5:
-            raise RuntimeError("configuration 5 is rendered on the device")
-    pair = configs.host_pair(cfg)
-    return _normalize_np(pair.f), _normalize_np(pair.g), pair.mask
-
-
 # --------------------------------------------------------------------------- B200 arm
 def _tuned_shapes() -> list:
     """The autotuner's choice of (threads, brick_floats) per IC-GN kernel and its timings (ms per sample launch)."""
@@ -470,6 +573,9 @@ def max_over_ranks(x: float, world: int, device="cuda") -> float:
 
 def main():
     args = parse()
+    if args.stage != "full":
+        stage_main(args)
+        return
     if args.impl == "reference" and args.config != 4:
         run_reference(args)
         return
@@ -620,18 +726,27 @@ def main():
     cpu = None
     rms_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as orc
+
         threads = os.cpu_count() or 1
-        fn = K.normalize(f).cpu().numpy()
-        gn = K.normalize(g).cpu().numpy()
-        block = node_block(res.grid_shape, args.cpu_nodes)
-        dt, nb, cres = cpu_sample(fn, gn, coords, p, block, threads, None if mask is None else mask.cpu().numpy())
+        spec = configs.spec(cfg)
+        block, block_grid = node_block(res.grid_shape, args.cpu_nodes)
+        cb = coords[block]
+        box = sample_box(cb, spec, tuple(f.shape))
+        sl = tuple(slice(a_, b_) for a_, b_ in box)
+        fn = np.ascontiguousarray(K.normalize(f)[sl].cpu().numpy())  # the device pass's own normalised volumes
+        gn = np.ascontiguousarray(K.normalize(g)[sl].cpu().numpy())
+        mb = None if mask is None else np.ascontiguousarray(mask[sl].cpu().numpy())
+        c_local = cb - np.array([box[2][0], box[1][0], box[0][0]], dtype=np.int64)[None, :]
+        dt, nb, _ = cpu_pass_sample(fn, gn, c_local, cb, block_grid, spec, mb, threads)
+        engine = orc.ncc_engine(tuple(min(int(w), 16) // 2 for w in spec["winsize"]), spec["search_radius"])
         cpu = {"value": nb / dt, "unit": "nodes/s", "cores": threads, "kind": "port",
-               "sample": f"{nb} nodes ({args.cpu_nodes}^3 block at the grid centre): NCC, precompute, 12-DOF"
-                         f"{' and 3-DOF ADMM passes' if p.use_global_step else ''}, FP64 oracle"}
-        ok = (cres["status"] == 0) & (status_local[block] == 0)
-        if ok.any():
-            d = U_local[block][ok] - cres["P"][ok, 9:]
-            rms_oracle = float(np.sqrt(np.mean(d * d)))
+               "sample": f"{nb} nodes ({'x'.join(str(k) for k in block_grid)} block at the grid centre, run as its own node "
+                         f"grid) through the whole pass (NCC on the {engine} engine with expansion, precompute, 12-DOF with "
+                         f"filling{', global step and ADMM' if p.use_global_step else ''}), FP64 oracle"}
+        U0_block = res.U0[block].cpu().numpy()
+        rms_oracle = oracle_local_rms(fn, gn, c_local, spec, mb, U0_block, res.P_local[block].cpu().numpy(), status_local[block],
+                                      cb)
 
     out = {
         "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -651,6 +766,8 @@ def main():
         "cpu_baseline": cpu,
         "plain": plain,
         "batched_over_plain": None if plain is None else value / world / plain["value"],
+        "batched_over_plain_stages": None if plain is None else
+        {k_: plain["stages_ms"][k_] / (1e3 * v_) for k_, v_ in stages.items() if k_ in plain["stages_ms"] and v_ > 0},
         "e2e": {"value": e2e_val, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "clocks": clocks.summary(),
         "icgn_launch_shapes": _tuned_shapes(),

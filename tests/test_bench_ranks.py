@@ -87,3 +87,30 @@ def test_roofline_fft_geometry_matches_the_library_source():
     ncc = open(os.path.join(csrc, "ncc.cu")).read()
     body = ncc[ncc.index("constexpr int fftr_planes3()"):][:400]
     assert "70000 / (N * (NH | 1) * 8)" in body and "256 / NH" in body
+
+
+def test_reference_arm_uses_neither_the_device_nor_the_cuda_library():
+    """bench.py --impl reference runs the oracle pass on host-rendered volumes: in a fresh process it loads no
+    library of this package, imports neither torch nor the device modules, and prints one JSON line."""
+    import json
+    import subprocess
+    import sys
+
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    probe = (
+        "import sys, runpy, io, contextlib\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--config', '1', '--cpu-nodes', '2', '--steps', '1', '--warmup', '0']\n"
+        "buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf):\n"
+        "    runpy.run_path('bench.py', run_name='__main__')\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(buf.getvalue().strip())\n"
+        "print('LOADED', 'libaldvc_b200' in maps, 'torch' in sys.modules, 'pyaldvc_b200.kernels' in sys.modules)\n"
+    )
+    r = subprocess.run([sys.executable, "-c", probe], cwd=repo, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert lines[-1] == "LOADED False False False"
+    line = json.loads(lines[-2])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0

@@ -202,5 +202,7 @@ def test_admm_graph_replay_matches_eager():
     for r_g, r_e in ((a_g, a_e), (b_g, b_e)):
         assert r_g.admm_steps == r_e.admm_steps
         for k in ("U", "F", "status", "zncc", "n_iter"):
-            assert torch.equal(getattr(r_g, k), getattr(r_e, k)), f"graph replay differs from eager in {k}"
+            x, y = getattr(r_g, k), getattr(r_e, k)
+            same = (x == y) | (torch.isnan(x) & torch.isnan(y)) if x.is_floating_point() else x == y  # NaN at rejected nodes
+            assert bool(same.all()), f"graph replay differs from eager in {k}"
     assert not torch.equal(a_g.U, b_g.U)
