@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--icgn-threads", type=int, default=0,
                     help="pin the batched IC-GN kernels to the lean form with this many threads per node (32/64/128) "
                          "instead of the autotuner's choice (for profiler runs, whose timings would mislead it)")
+    ap.add_argument("--sweep-rows", type=int, default=0,
+                    help="persistent IC-GN: subset rows per sweep tile (0 library default, -1 C order)")
     ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute"],
                     help="full: the benchmark line; pass / ncc / precompute: timing of one stage on a profiling case "
                          "(human-readable lines, no JSON), see stage_main")
@@ -100,7 +102,7 @@ def stage_main(args) -> None:
 
         cfg = args.config
         shape = tuple(args.shape) if args.shape else (200, 384, 384)
-        p = configs.params(cfg)
+        p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows)
         if args.icgn_threads:
             p.threads, p.brick_floats = args.icgn_threads, 0
         f, g, mask, _ = configs.device_pair(cfg, shape=shape)
@@ -606,7 +608,7 @@ def main():
         raise RuntimeError(f"B200 library unusable: {unavailable_reason()}")
 
     cfg = args.config
-    p = configs.params(cfg)
+    p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows)
     if args.icgn_threads:
         p.threads, p.brick_floats = args.icgn_threads, 0
     f, g, mask, disp = configs.device_pair(cfg, seed=1000 + 17 * rank)

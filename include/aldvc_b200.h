@@ -125,6 +125,10 @@ typedef struct aldvc_icgn_params {
     int32_t brick_floats; /* batched: shared-memory brick capacity in floats, 0 = library default */
     double mu;            /* 3-DOF: ADMM penalty */
     double n_full;        /* 3-DOF: sampled voxels of a full subset (noise-correction scale) */
+    int32_t sweep_rows;   /* persistent form with threads <= 128: subset rows per sweep tile (each tile swept plane by
+                             plane), 0 = library default (a tile height of 3-6 rows that pads the fewest rows),
+                             < 0 = the whole subset in C order */
+    int32_t reserved;
 } aldvc_icgn_params;
 
 /* Uniform hex8 node grid of the global step, node n = iz*ny*nx + iy*nx + ix. */

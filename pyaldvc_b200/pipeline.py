@@ -61,6 +61,7 @@ class PassParams:
     threads: int = 0  # 0: chosen by the autotuner (or the library default when autotune is off)
     brick_floats: int = 0
     autotune: bool = True
+    icgn_sweep_rows: int = 0  # persistent IC-GN: subset rows per sweep tile (0 library default, < 0 C order)
     graph: bool = False
     ncc_engine: str = "auto"  # auto | tiled | fft | plain
     # uneven subsets: coords (N,3) [x, y, z] -> (N,3) even window sizes per node, each <= winsize (which then
@@ -349,7 +350,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         nh = node_half if (node_half is None or idx is None) else node_half[idx]
         return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g_prep, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
                         p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
-                        node_half=nh, g4=g4)
+                        node_half=nh, g4=g4, sweep_rows=p.icgn_sweep_rows)
 
     th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
     P, n_iter, status, zncc = icgn12_on(None, th12, br12)
@@ -411,7 +412,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             nh = T["node_half"] if (T["node_half"] is None or idx is None) else T["node_half"][idx]
             return K.icgn3(c, U2_, F2_, v_, mesh.half, T["f"], T["gx"], T["gy"], T["gz"], T["m"], T["g"], mode, H_, mf_, bf_, ok_,
                            p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0,
-                           p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh, g4=T["g4"])
+                           p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh, g4=T["g4"],
+                           sweep_rows=p.icgn_sweep_rows)
 
         def admm_step(U2, F2, W, v, th3, br3):
             # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
