@@ -50,6 +50,9 @@ def parse():
                          "instead of the autotuner's choice (for profiler runs, whose timings would mislead it)")
     ap.add_argument("--sweep-rows", type=int, default=0,
                     help="persistent IC-GN: subset rows per sweep tile (0 library default, -1 C order)")
+    ap.add_argument("--node-order", default="morton", choices=["morton", "index"],
+                    help="persistent IC-GN work queue order")
+    ap.add_argument("--no-quads", action="store_true", help="persistent IC-GN samples g itself, not its quad copy")
     ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute"],
                     help="full: the benchmark line; pass / ncc / precompute: timing of one stage on a profiling case "
                          "(human-readable lines, no JSON), see stage_main")
@@ -102,7 +105,8 @@ def stage_main(args) -> None:
 
         cfg = args.config
         shape = tuple(args.shape) if args.shape else (200, 384, 384)
-        p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows)
+        p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows, icgn_node_order=args.node_order,
+                                icgn_quads=not args.no_quads)
         if args.icgn_threads:
             p.threads, p.brick_floats = args.icgn_threads, 0
         f, g, mask, _ = configs.device_pair(cfg, shape=shape)
@@ -608,7 +612,8 @@ def main():
         raise RuntimeError(f"B200 library unusable: {unavailable_reason()}")
 
     cfg = args.config
-    p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows)
+    p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows, icgn_node_order=args.node_order,
+                                icgn_quads=not args.no_quads)
     if args.icgn_threads:
         p.threads, p.brick_floats = args.icgn_threads, 0
     f, g, mask, disp = configs.device_pair(cfg, seed=1000 + 17 * rank)

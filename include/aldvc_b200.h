@@ -129,6 +129,9 @@ typedef struct aldvc_icgn_params {
                              plane), 0 = library default (a tile height of 3-6 rows that pads the fewest rows),
                              < 0 = the whole subset in C order */
     int32_t reserved;
+    const int32_t *node_order; /* persistent forms: (N,) a permutation of 0..N-1, the order in which the work queue
+                                  hands out the nodes (nodes solved at the same time share more of the volume in L2
+                                  when they are near each other); entries outside 0..N-1 are skipped; NULL: 0..N-1 */
 } aldvc_icgn_params;
 
 /* Uniform hex8 node grid of the global step, node n = iz*ny*nx + iy*nx + ix. */

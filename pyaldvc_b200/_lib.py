@@ -40,7 +40,7 @@ class Subset(ctypes.Structure):
 class IcgnParams(ctypes.Structure):
     _fields_ = [("tol", _d), ("dp_tol", _d), ("max_iter", _i32), ("patience", _i32), ("noise_gain", _d),
                 ("predictive", _i32), ("variant", _i32), ("threads", _i32), ("brick_floats", _i32), ("mu", _d),
-                ("n_full", _d), ("sweep_rows", _i32), ("reserved", _i32)]
+                ("n_full", _d), ("sweep_rows", _i32), ("reserved", _i32), ("node_order", _p)]
 
 
 class Hex8Mesh(ctypes.Structure):

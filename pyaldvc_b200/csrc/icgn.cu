@@ -72,7 +72,16 @@ struct IcgnArgs {
     int brick_cap;      // batched: floats of the shared brick
     const int32_t* node_half;  // (N,3) per-node half-widths (<= hx, hy, hz), NULL: one shape
     int sweep_rows;     // lean: subset rows per sweep tile (0 automatic, < 0 the whole subset)
+    const int32_t* node_order;  // persistent forms: the work queue's permutation of the nodes, NULL: index order
 };
+
+// The node the q-th work item solves: node_order[q] (entries outside 0..n-1 are skipped: -2), or q; -1 past the end.
+__device__ __forceinline__ int64_t queue_node(const IcgnArgs& a, int q) {
+    if (q >= a.n_nodes) return -1;
+    if (!a.node_order) return q;
+    const int64_t nd = a.node_order[q];
+    return (nd >= 0 && nd < a.n_nodes) ? nd : -2;
+}
 
 // Rows per sweep tile of the lean kernel.  The subset is swept tile by tile, each tile plane by plane (z) and
 // row by row, so the tap rows a plane of samples shares with the next planes are still in L1 when they are
@@ -710,7 +719,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
         __syncthreads();  // every thread has finished reading the previous node's control block
         if (tid == 0) {
             const int q = atomicAdd(a.counter, 1);
-            sc.node = q < a.n_nodes ? (int64_t)q : -1;
+            sc.node = queue_node(a, q);
             sc.state = 1;
             if (sc.node >= 0) {
                 const int64_t node = sc.node;
@@ -725,7 +734,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) icgn_batched_kernel(Ic
         }
         __syncthreads();
         const int64_t node = sc.node;
-        if (node < 0) break;
+        if (node == -1) break;  // the queue is empty (-2: a skipped order entry)
         if (sc.state != 0) continue;
         if (NDOF == 12) {
             for (int i = tid; i < 144; i += THREADS) Ls[i] = a.L[node * 144 + i];
@@ -947,7 +956,7 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
         __syncthreads();  // every thread has finished reading the previous node's control block
         if (tid == 0) {
             const int q = atomicAdd(a.counter, 1);
-            sc.node = q < a.n_nodes ? (int64_t)q : -1;
+            sc.node = queue_node(a, q);
             sc.state = 1;
             bool shape_ok = true;
             const Shape sh0 = (UNEVEN && sc.node >= 0) ? node_shape(a, sc.node, shape_ok) : Shape{a.hx, a.hy, a.hz, a.nX, a.nY, a.nZ};
@@ -961,7 +970,7 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
         }
         __syncthreads();
         const int64_t node = sc.node;
-        if (node < 0) break;
+        if (node == -1) break;  // the queue is empty (-2: a skipped order entry)
         if (sc.state != 0) continue;
         // one shape per call: the kernel parameters themselves; uneven: the node's (node_begin rejected a bad one)
         bool shape_ok = true;
@@ -1621,6 +1630,7 @@ static int run(IcgnArgs& a, int ndof, int mode, bool stored, const aldvc_icgn_pa
     const LaunchCfg c = batched_cfg(prm);
     a.brick_cap = c.brick_cap;
     a.sweep_rows = prm->sweep_rows;
+    a.node_order = prm->node_order;
     if (prm->variant != ALDVC_PLAIN) {
         const size_t smem = (size_t)c.brick_cap * sizeof(float);
         if (smem + 8192 > (size_t)max_smem_optin()) return arg_fail("icgn: brick_floats exceeds the shared memory per block");

@@ -134,14 +134,16 @@ def precompute_grid(xs, ys, zs, half, f, gx, gy, gz, min_valid_ratio, cond_max, 
 
 
 def icgn_params(tol, dp_tol, max_iter, patience, noise_gain=0.0, predictive=True, variant=BATCHED, threads=0, brick_floats=0,
-                mu=0.0, n_full=0.0, sweep_rows=0) -> _lib.IcgnParams:
+                mu=0.0, n_full=0.0, sweep_rows=0, node_order=None) -> _lib.IcgnParams:
+    """``node_order``: optional (N,) int32 CUDA tensor, the permutation the persistent work queue follows."""
     return _lib.IcgnParams(float(tol), float(dp_tol), int(max_iter), int(patience), float(noise_gain), int(bool(predictive)),
-                           int(variant), int(threads), int(brick_floats), float(mu), float(n_full), int(sweep_rows), 0)
+                           int(variant), int(threads), int(brick_floats), float(mu), float(n_full), int(sweep_rows), 0,
+                           None if node_order is None else node_order.data_ptr())
 
 
 def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol, dp_tol, max_iter, patience, stride=1, H=None,
            pattern=None, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED, threads=0,
-           brick_floats=0, node_half=None, g4=None, sweep_rows=0):
+           brick_floats=0, node_half=None, g4=None, sweep_rows=0, node_order=None):
     """Device 12-DOF IC-GN; returns (P (N,12), n_iter, status, zncc) tensors.  ``node_half``: optional (N,3)
     per-node half-widths (``half`` is then their maximum); ``sweep_rows``: rows per sweep tile of the persistent
     form (0 library default, < 0 C order)."""
@@ -156,7 +158,9 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
     vol = volumes_struct(f, gx, gy, gz, mask, g, g4)
     nh = None if node_half is None else dev(node_half, torch.int32)
     sub = subset_struct(half, stride, mode, split_index, split_keep, nh)
-    prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats, sweep_rows=sweep_rows)
+    order = None if node_order is None else dev(node_order, torch.int32)
+    prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats, sweep_rows=sweep_rows,
+                      node_order=order)
     ws_n = lib().aldvc_icgn_workspace_size(ctypes.byref(sub), N, ctypes.byref(prm))
     ws = _workspace(ws_n)
     use_noise = noise_gain > 0.0 and H is not None and pattern is not None
@@ -170,7 +174,7 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
 
 def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, meanf, bottomf, valid, mu, tol, dp_tol, max_iter,
           patience, stride=1, n_full=0.0, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED,
-          threads=0, brick_floats=0, node_half=None, g4=None, sweep_rows=0):
+          threads=0, brick_floats=0, node_half=None, g4=None, sweep_rows=0, node_order=None):
     """Device 3-DOF IC-GN (ADMM subproblem 1); returns (U (N,3), n_iter, status, zncc) tensors."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
@@ -185,8 +189,9 @@ def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, 
     vol = volumes_struct(f, gx, gy, gz, mask, g, g4)
     nh = None if node_half is None else dev(node_half, torch.int32)
     sub = subset_struct(half, stride, mode, split_index, split_keep, nh)
+    order = None if node_order is None else dev(node_order, torch.int32)
     prm = icgn_params(tol, dp_tol, max_iter, patience, noise_gain, predictive, variant, threads, brick_floats, mu, n_full,
-                      sweep_rows)
+                      sweep_rows, order)
     ws = _workspace(lib().aldvc_icgn_workspace_size(ctypes.byref(sub), N, ctypes.byref(prm)))
     _lib.check(lib().aldvc_icgn3(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, _p(U_old), _p(F_fixed), _p(vdual), _p(H),
                                  _p(meanf), _p(bottomf), _p(valid), ctypes.byref(prm), _p(ws), ws.numel(), _p(U), _p(n_iter),

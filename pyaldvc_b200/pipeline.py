@@ -62,6 +62,8 @@ class PassParams:
     brick_floats: int = 0
     autotune: bool = True
     icgn_sweep_rows: int = 0  # persistent IC-GN: subset rows per sweep tile (0 library default, < 0 C order)
+    icgn_node_order: str = "morton"  # persistent IC-GN work queue: "morton" (nodes near each other solved together) or "index"
+    icgn_quads: bool = True  # cubic / B-spline persistent IC-GN: sample g through its overlapping-quad copy
     graph: bool = False
     ncc_engine: str = "auto"  # auto | tiled | fft | plain
     # uneven subsets: coords (N,3) [x, y, z] -> (N,3) even window sizes per node, each <= winsize (which then
@@ -145,6 +147,29 @@ class Mesh:
         self.coords = torch.from_numpy(self.coords_np).cuda()
         self.n = self.coords_np.shape[0]
         self.half = tuple(int(w) // 2 for w in p.winsize)
+        self._order = None
+
+    def order(self) -> torch.Tensor:
+        """(N,) int32 CUDA tensor: the nodes sorted by the Morton code of their grid position (z, y, x bits
+        interleaved), so that nodes handed out together by a work queue lie in compact blocks of the volume."""
+        if self._order is None:
+            key = (self.grid_shape, torch.cuda.current_device())
+            if key not in _MORTON:
+                nz, ny, nx = self.grid_shape
+                iz, iy, ix = (a.ravel().astype(np.uint64) for a in np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx),
+                                                                                indexing="ij"))
+                code = np.zeros(self.n, dtype=np.uint64)
+                for b in range(21):
+                    for k, v in enumerate((ix, iy, iz)):
+                        code |= ((v >> np.uint64(b)) & np.uint64(1)) << np.uint64(3 * b + k)
+                while len(_MORTON) >= 4:
+                    _MORTON.pop(next(iter(_MORTON)))
+                _MORTON[key] = torch.from_numpy(np.argsort(code, kind="stable").astype(np.int32)).cuda()
+            self._order = _MORTON[key]
+        return self._order
+
+
+_MORTON: dict = {}  # Morton node orders by (grid shape, device), the few most recent
 
 
 def _fill(values: torch.Tensor, bad: torch.Tensor, grid_shape, errs: K.ErrorWords):
@@ -206,7 +231,7 @@ def _graph_key(p: PassParams, mesh, mode, th3, br3, n_full, tensors, beta) -> tu
     shapes = tuple((k, None if t is None else (tuple(t.shape), str(t.dtype))) for k, t in sorted(tensors.items()))
     prm = (beta, p.mu, p.alpha, p.pcg_tol, p.pcg_max_iter, p.gauss_pt_order, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
            p.icgn_patience, p.icgn_predictive_stop, p.admm_max_iter, p.dual_update, p.local_outlier_threshold, p.subset_stride,
-           p.variant)
+           p.variant, p.icgn_sweep_rows, p.icgn_node_order, p.icgn_quads)
     return (mesh.grid_shape, tuple(mesh.half), tuple(mesh.spacing), mode, th3, br3, n_full, prm, shapes)
 
 
@@ -340,7 +365,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
 
     # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
     # the persistent kernels read each cubic tap row of g as one 16-byte load from its overlapping-quad copy
-    g4 = K.make_quads(g_prep) if (mode != 0 and p.variant == K.BATCHED) else None
+    g4 = K.make_quads(g_prep) if (mode != 0 and p.variant == K.BATCHED and p.icgn_quads) else None
+    order = mesh.order() if (p.variant == K.BATCHED and p.icgn_node_order == "morton") else None
     P0 = torch.zeros((mesh.n, 12), dtype=torch.float64, device="cuda")
     P0[:, 9:] = U0
 
@@ -350,7 +376,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         nh = node_half if (node_half is None or idx is None) else node_half[idx]
         return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g_prep, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
                         p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
-                        node_half=nh, g4=g4, sweep_rows=p.icgn_sweep_rows)
+                        node_half=nh, g4=g4, sweep_rows=p.icgn_sweep_rows, node_order=order if idx is None else None)
 
     th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
     P, n_iter, status, zncc = icgn12_on(None, th12, br12)
@@ -392,7 +418,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     n_full = float(np.prod([(2 * h) // p.subset_stride + 1 for h in mesh.half]))
     # every tensor the ADMM loop reads; a captured loop reads static copies of them
     T = {"f": f, "g": g_prep, "gx": gx, "gy": gy, "gz": gz, "m": m_u8, "H": H, "meanf": meanf, "bottomf": bottomf, "valid": valid_u8,
-         "coords": mesh.coords, "elem": elem_active, "node_half": node_half, "g4": g4}
+         "coords": mesh.coords, "elem": elem_active, "node_half": node_half, "g4": g4, "order": order}
 
     def make_steps(T, errs_):
         def global_step(U1_, F1_, W_, v_):
@@ -413,7 +439,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             return K.icgn3(c, U2_, F2_, v_, mesh.half, T["f"], T["gx"], T["gy"], T["gz"], T["m"], T["g"], mode, H_, mf_, bf_, ok_,
                            p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0,
                            p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh, g4=T["g4"],
-                           sweep_rows=p.icgn_sweep_rows)
+                           sweep_rows=p.icgn_sweep_rows, node_order=T["order"] if idx is None else None)
 
         def admm_step(U2, F2, W, v, th3, br3):
             # subproblem 1 (subpb1_solver.subpb1_solver :77-164)
