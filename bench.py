@@ -113,7 +113,9 @@ def stage_main(args) -> None:
         for _ in range(args.warmup):
             run_pass(f, g, p, mask)
         res = timed(f"config {cfg} pass on {shape}", lambda: run_pass(f, g, p, mask), 1, "pass")
-        print(f"{int(res.coords.shape[0])} nodes, mean 12-DOF iterations {float(res.n_iter_local.double().mean()):.2f}")
+        it3 = [float(t.double().mean()) for t in getattr(res, "icgn3_iters", [])]
+        print(f"{int(res.coords.shape[0])} nodes, mean 12-DOF iterations {float(res.n_iter_local.double().mean()):.3f}, "
+              f"mean 3-DOF iterations per pass {[round(v, 3) for v in it3]}")
         return
     if args.stage == "ncc":
         n, h, r = 192, args.half, args.radius
@@ -381,6 +383,25 @@ def _smooth_len(n: int) -> int:
 
 FFT_REG_SIZES = (36, 40, 48, 50, 54, 60, 64)  # cubic FFT boxes transformed a line per thread in registers
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per unit of work of the dominant kernels, from ncu captures
+# of the 1024 x 1024 x 306 workload's kernels on a 200 x 384 x 384 box of the same beads, field and parameters (11,774
+# nodes; profiles/ncu_icgn_lean_config5_box.md, profiles/dram_config5_box.md), scaled here by the units a launch of
+# the measured pass processes.  Units: node-iterations for IC-GN, nodes for the NCC kernels.
+TRAFFIC_PER_UNIT = {
+    "icgn12_lean": ("node-iteration", 5.056e9 / (11774 * 2.237)),
+    "icgn3_lean": ("node-iteration", 5.358e9 / (11774 * 1.241)),
+    "fft_pass1": ("node", 787.09e6 / 811),
+    "fft_pass2": ("node", 958.01e6 / 811),
+    "fft_pass3": ("node", 367.63e6 / 811),
+    "ncc_peak": ("node", 165.55e6 / (512 * 2**20 // (33**3 * 4))),
+}
+# issue-slot, L1 and FMA-pipe utilisation of the IC-GN kernels (ncu on the same box): the FP32 roof is not what bounds
+# them; their sweeps are gathers through L1, so issue slots and L1 throughput are the roofs they run against
+ICGN_NCU_BOX = {
+    "icgn12_lean": {"issue_active": 0.617, "l1tex_throughput": 0.597, "fma_pipe": 0.354, "l1_hit": 0.801, "l2_hit": 0.855},
+    "icgn3_lean": {"issue_active": 0.663, "l1tex_throughput": 0.732, "fma_pipe": 0.347, "l1_hit": 0.778, "l2_hit": 0.788},
+}
+
 
 def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
     """Roofline of every timed kernel of one pass: algorithmic work of the pass for that kernel (bytes it must move,
@@ -447,18 +468,35 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
     for form in ("lean", "batched", "plain"):
         flop_work[f"icgn12_{form}"] = c12 * float((it12 * S_node).sum())
         flop_work[f"icgn3_{form}"] = c3 * float((it3 * S_node).sum())
+    # units of the measured pass for the traffic scaling
+    units = {"icgn12_lean": float(it12.sum()), "icgn3_lean": float(it3.sum())}
+    fft_nodes = float(sum(n for n, _, _, e in getattr(res, "ncc_calls", []) if e == 2))
+    for k in ("fft_pass1", "fft_pass2", "fft_pass3"):
+        units[k] = fft_nodes
+    units["ncc_peak"] = float(sum(n for n, _, _, _ in getattr(res, "ncc_calls", [])))
     total_ms = sum(ms for ms, _ in ktimes.values())
     out = {}
     for name, (ms, launches) in ktimes.items():
         row = {"ms": ms, "launches": launches, "ms_share": ms / total_ms if total_ms else None}
+        traffic = None
+        if name in TRAFFIC_PER_UNIT and units.get(name):
+            traffic = TRAFFIC_PER_UNIT[name][1] * units[name] / max(1, launches)  # bytes per launch
         if name in byte_work and peaks.get("hbm_gbs"):
             ach = byte_work[name] / (ms / 1e3) / 1e9
             row.update({"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
-                        "traffic": None, "peak_source": peaks["hbm_source"]})
+                        "traffic": traffic, "peak_source": peaks["hbm_source"]})
+            if traffic is not None:
+                row["traffic_over_work"] = traffic * max(1, launches) / byte_work[name]
         elif name in flop_work:
             ach = flop_work[name] / (ms / 1e3) / 1e12
             row.update({"bound": "fp32", "achieved": ach, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
-                        "frac": ach / peaks["fp32_tflops"], "traffic": None, "peak_source": peaks["fp32_source"]})
+                        "frac": ach / peaks["fp32_tflops"], "traffic": traffic, "peak_source": peaks["fp32_source"]})
+            if traffic is not None:
+                row["dram_gbs"] = traffic * max(1, launches) / (ms / 1e3) / 1e9
+            if name in ICGN_NCU_BOX:
+                row["ncu_box"] = ICGN_NCU_BOX[name]
+        if traffic is not None:
+            row["traffic_source"] = "ncu DRAM bytes per " + TRAFFIC_PER_UNIT[name][0] + " on the 200x384x384 box, scaled"
         out[name] = row
     return out
 
