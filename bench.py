@@ -50,6 +50,8 @@ def parse():
                          "instead of the autotuner's choice (for profiler runs, whose timings would mislead it)")
     ap.add_argument("--sweep-rows", type=int, default=0,
                     help="persistent IC-GN: subset rows per sweep tile (0 library default, -1 C order)")
+    ap.add_argument("--icgn-staged", action="store_true",
+                    help="pin the batched IC-GN kernels to the lean 4-warp sweep staged through TMA copies of g")
     ap.add_argument("--node-order", default="morton", choices=["morton", "index"],
                     help="persistent IC-GN work queue order")
     ap.add_argument("--no-quads", action="store_true", help="persistent IC-GN samples g itself, not its quad copy")
@@ -109,6 +111,8 @@ def stage_main(args) -> None:
                                 icgn_quads=not args.no_quads)
         if args.icgn_threads:
             p.threads, p.brick_floats = args.icgn_threads, 0
+        if args.icgn_staged:
+            p.threads, p.brick_floats = 128, -1
         f, g, mask, _ = configs.device_pair(cfg, shape=shape)
         for _ in range(args.warmup):
             run_pass(f, g, p, mask)
@@ -654,6 +658,8 @@ def main():
                                 icgn_quads=not args.no_quads)
     if args.icgn_threads:
         p.threads, p.brick_floats = args.icgn_threads, 0
+    if args.icgn_staged:
+        p.threads, p.brick_floats = 128, -1
     f, g, mask, disp = configs.device_pair(cfg, seed=1000 + 17 * rank)
     torch.cuda.synchronize()
 

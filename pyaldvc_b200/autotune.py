@@ -5,7 +5,9 @@ The batched solver has two persistent kernel forms:
 * lean: 1, 2 or 4 warps per node (``threads`` 32/64/128); the deformed volume is sampled through L1,
   so up to 16 nodes share an SM and one node's FP64 control step hides behind the others' sampling;
 * brick: 256 or 512 threads per node; the deformed subset is staged in shared memory in z-chunks
-  that fit ``brick_floats`` floats.
+  that fit ``brick_floats`` floats;
+* staged: the lean 4-warp sweep with each chunk's box of g brought into shared memory by TMA tensor copies
+  (``(128, -1)``; cubic / B-spline with stored gradients and one subset shape, else it runs as the lean form).
 
 Which is fastest depends on the subset size, the interpolation and the DOF count, so ``tune`` times
 every candidate on a sample of the real nodes (CUDA events on the current stream, one untimed launch
@@ -17,7 +19,7 @@ from __future__ import annotations
 
 import torch
 
-CANDIDATES = ((32, 0), (64, 0), (128, 0), (256, 24576), (256, 49152), (512, 24576), (512, 49152))
+CANDIDATES = ((32, 0), (64, 0), (128, 0), (128, -1), (256, 24576), (256, 49152), (512, 24576), (512, 49152))
 SAMPLE_NODES = 8 * 148 * 16  # enough work for every resident CTA of a B200 to take several nodes
 
 _cache: dict = {}

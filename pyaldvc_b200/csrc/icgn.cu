@@ -21,6 +21,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -73,7 +75,50 @@ struct IcgnArgs {
     const int32_t* node_half;  // (N,3) per-node half-widths (<= hx, hy, hz), NULL: one shape
     int sweep_rows;     // lean: subset rows per sweep tile (0 automatic, < 0 the whole subset)
     const int32_t* node_order;  // persistent forms: the work queue's permutation of the nodes, NULL: index order
+    int32_t* err;       // persistent forms: nonzero when a bounded wait on a staged copy gave up
 };
+
+// ----------------------------------------------------------------------------- TMA staging of the lean sweep
+// The staged form of the lean kernel copies, for each chunk of its sweep (a tile of `by` subset rows times
+// TMA_KZ sample planes), the box of g that the chunk's cubic taps read into shared memory with one tensor copy
+// (cp.async.bulk.tensor, completion on an mbarrier), double-buffered: the copy of chunk c + 2 runs while chunk c + 1
+// is sampled.  The box is fixed (TMA_BX x TMA_BY x TMA_BZ floats, x fastest); a chunk whose warped footprint does not
+// fit is sampled from global memory.  The tensor map covers this device's g only; no multicast.
+constexpr int TMA_BX = 48, TMA_BY = 12, TMA_BZ = 10, TMA_KZ = 3;
+constexpr int TMA_BOX = TMA_BX * TMA_BY * TMA_BZ;                // floats per buffer
+constexpr unsigned TMA_BOX_BYTES = TMA_BOX * sizeof(float);       // 23,040 bytes
+constexpr size_t TMA_SMEM = 2 * (size_t)TMA_BOX_BYTES + 128;      // two buffers, 128-byte aligned
+constexpr long long TMA_WAIT_LIMIT = 1LL << 20;                    // polls of an mbarrier before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint32_t mb, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mb), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mb, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mb, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(mb), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase `parity` of an mbarrier to complete; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t mb, uint32_t parity) {
+    for (long long i = 0; i < TMA_WAIT_LIMIT; ++i)
+        if (mbar_try_wait(mb, parity)) return true;
+    return false;
+}
+// 3-D tiled tensor copy of the box at (x, y, z) of the map into shared memory; x must be a multiple of 4 (16 bytes)
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t mb) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(mb)
+        : "memory");
+}
 
 // The node the q-th work item solves: node_order[q] (entries outside 0..n-1 are skipped: -2), or q; -1 past the end.
 __device__ __forceinline__ int64_t queue_node(const IcgnArgs& a, int q) {
@@ -934,8 +979,8 @@ struct LeanCtl {
     float cf, cg;
 };
 
-template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN>
-__global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lean_kernel(IcgnArgs a) {
+template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN, bool TMA>
+__device__ __forceinline__ void lean_body(const IcgnArgs& a, const CUtensorMap* tmap) {
     constexpr int T = NW * 32;
     constexpr int NB = Acc<NDOF>::NB;
     constexpr int NV = 5 + 3 * NB;
@@ -951,6 +996,23 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
               hz_ = MODE == 0 ? a.nz - 2 : a.nz - 3;
     Ctl12 c12;  // live in thread 0 only
     Ctl3 c3;
+    // staged form: two shared buffers, their mbarriers and the origin of the box each holds
+    extern __shared__ __align__(128) unsigned char tsm_raw[];
+    float* tbuf = reinterpret_cast<float*>(tsm_raw + ((128u - (smem_u32(tsm_raw) & 127u)) & 127u));  // 128-byte aligned
+    __shared__ __align__(8) uint64_t t_mb[2];
+    __shared__ int t_org[2][3];
+    __shared__ int t_fit[2];
+    __shared__ int t_dead;  // a wait gave up: no more staged copies in this CTA
+    uint32_t t_phase = 0;   // bit b: parity of buffer b's next completion (identical in every thread)
+    if (TMA) {
+        if (tid == 0) {
+            mbar_init(smem_u32(&t_mb[0]), 1);
+            mbar_init(smem_u32(&t_mb[1]), 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            t_dead = 0;
+        }
+        __syncthreads();
+    }
 
     for (;;) {
         __syncthreads();  // every thread has finished reading the previous node's control block
@@ -991,82 +1053,193 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
         const int xci = (int)xc, yci = (int)yc, zci = (int)zcn;
         const float cf = sc.cf;
 
-        // One sweep over the node's subset.  KIND 1: the sums over the sampled g and the counts; KIND 2: every sum.
-        // Both visit the same voxels in the same per-thread order, so the partials of a field do not depend on the
-        // kind that formed them.
+        // One voxel of a sweep (subset indices vx, vy, vz).  KIND 1: the sums over the sampled g and the counts; KIND 2:
+        // every sum.  `smp(gx, gy, gz, fx, fy, fz)` samples g at the clamped tap origin (gx, gy, gz).
+        auto visit = [&](auto kind, Acc<NDOF>& acc, bool slow, int vx, int vy, int vz, float A0, float A1, float A2, float A3,
+                         float A4, float A5, float A6, float A7, float A8, float T0, float T1, float T2, float cg, auto&& smp) {
+            constexpr int KIND = decltype(kind)::value;
+            const int dx = -sh.hx + vx * a.stride, dy = -sh.hy + vy * a.stride, dz = -sh.hz + vz * a.stride;
+            const int xx = xci + dx, yy = yci + dy, zz = zci + dz;
+            bool k;
+            if (keep || !inside) {
+                k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
+                if (k)
+                    k = keep ? kept_bit(keep, (vz * sh.nY + vy) * sh.nX + vx)
+                             : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0);
+            } else {
+                k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0;
+            }
+            if (!k) return;
+            acc.nref += 1;
+            const float X = (float)dx, Y = (float)dy, Z = (float)dz;
+            if (slow) {
+                const double* P = sc.P;
+                const double xw = (1.0 + P[0]) * dx + P[1] * dy + P[2] * dz + ((double)xc + P[9]);
+                const double yw = P[3] * dx + (1.0 + P[4]) * dy + P[5] * dz + ((double)yc + P[10]);
+                const double zw = P[6] * dx + P[7] * dy + (1.0 + P[8]) * dz + ((double)zcn + P[11]);
+                if (!margin_ok(zw, yw, xw, a.nz, a.ny, a.nx)) {
+                    acc.oob = 1;
+                    return;
+                }
+            }
+            const int64_t o = zz * sxy + (int64_t)yy * a.nx + xx;
+            // reference-frame reads first: their latency overlaps the interpolation
+            const float fv = __ldg(a.f + o);
+            float q0, q1, q2;
+            if (STORED) {
+                q0 = __ldg(a.gx + o);
+                q1 = __ldg(a.gy + o);
+                q2 = __ldg(a.gz + o);
+            } else {
+                grad_otf(a.f, a.nz, a.ny, a.nx, zz, yy, xx, q0, q1, q2);
+            }
+            const float xr = A0 * X + A1 * Y + A2 * Z + T0;
+            const float yr = A3 * X + A4 * Y + A5 * Z + T1;
+            const float zr = A6 * X + A7 * Y + A8 * Z + T2;
+            const float fxf = floorf(xr), fyf = floorf(yr), fzf = floorf(zr);
+            const int gx_ = min(max(xci + (int)fxf, lo), hx_), gy_ = min(max(yci + (int)fyf, lo), hy_),
+                      gz_ = min(max(zci + (int)fzf, lo), hz_);
+            const float gv = smp(gx_, gy_, gz_, xr - fxf, yr - fyf, zr - fzf);
+            if (gv != gv) return;  // NaN: masked out in the deformed frame
+            if (KIND == 1)
+                acc.template add_part<false, true>(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
+            else
+                acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
+        };
+        // sampling g in global memory: the overlapping-quad copy when there is one, else g itself
+        auto smp_global = [&](int gx_, int gy_, int gz_, float fx, float fy, float fz) {
+            return (MODE != 0 && a.g4) ? sample_quad<MODE == 0 ? 1 : MODE>(a.g4, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz)
+                                       : sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz);
+        };
+        // One sweep over the node's subset.  Both kinds visit the same voxels in the same per-thread order, so the
+        // partials of a field do not depend on the kind that formed them.
         auto sweep = [&](auto kind, Acc<NDOF>& acc, bool slow, float A0, float A1, float A2, float A3, float A4, float A5,
                          float A6, float A7, float A8, float T0, float T1, float T2, float cg) {
-            constexpr int KIND = decltype(kind)::value;
             acc.zero();
-            int ix = tix, ib = tib, iz = tiz, itl = tit;
-            for (int v = tid; v < Sp; v += T) {
-                const int vx = ix, vy = itl * by + ib, vz = iz;
-                ix += sx_;
-                ib += sb_;
-                iz += sz_;
-                itl += st_;
-                if (ix >= sh.nX) {
-                    ix -= sh.nX;
-                    ++ib;
+            if constexpr (!TMA) {
+                int ix = tix, ib = tib, iz = tiz, itl = tit;
+                for (int v = tid; v < Sp; v += T) {
+                    const int vx = ix, vy = itl * by + ib, vz = iz;
+                    ix += sx_;
+                    ib += sb_;
+                    iz += sz_;
+                    itl += st_;
+                    if (ix >= sh.nX) {
+                        ix -= sh.nX;
+                        ++ib;
+                    }
+                    if (ib >= by) {
+                        ib -= by;
+                        ++iz;
+                    }
+                    if (iz >= sh.nZ) {
+                        iz -= sh.nZ;
+                        ++itl;
+                    }
+                    if (vy >= sh.nY) continue;  // a padding row of the last tile
+                    visit(kind, acc, slow, vx, vy, vz, A0, A1, A2, A3, A4, A5, A6, A7, A8, T0, T1, T2, cg, smp_global);
                 }
-                if (ib >= by) {
-                    ib -= by;
-                    ++iz;
+            } else {
+                // chunks: tile t of `by` rows x sample planes [zc TMA_KZ, +TMA_KZ), in tile-major order
+                const int ntile = (sh.nY + by - 1) / by, nzc = (sh.nZ + TMA_KZ - 1) / TMA_KZ, nch = ntile * nzc;
+                // thread 0: the box of chunk ci's taps (corner positions, floors, taps -1..+2 and one voxel of margin
+                // for FP32 rounding), its copy into buffer b when it fits
+                auto issue = [&](int ci, int b) {
+                    const int t = ci / nzc, zc = ci - t * nzc;
+                    const int y0 = t * by, y1 = min(y0 + by, sh.nY) - 1, z0 = zc * TMA_KZ, z1 = min(z0 + TMA_KZ, sh.nZ) - 1;
+                    const float cx[2] = {(float)(-sh.hx), (float)(-sh.hx + (sh.nX - 1) * a.stride)};
+                    const float cy[2] = {(float)(-sh.hy + y0 * a.stride), (float)(-sh.hy + y1 * a.stride)};
+                    const float cz[2] = {(float)(-sh.hz + z0 * a.stride), (float)(-sh.hz + z1 * a.stride)};
+                    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const float X = cx[c & 1], Y = cy[(c >> 1) & 1], Z = cz[c >> 2];
+                        const float p3[3] = {A0 * X + A1 * Y + A2 * Z + T0, A3 * X + A4 * Y + A5 * Z + T1, A6 * X + A7 * Y + A8 * Z + T2};
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            mn[d] = fminf(mn[d], p3[d]);
+                            mx[d] = fmaxf(mx[d], p3[d]);
+                        }
+                    }
+                    const int cc[3] = {xci, yci, zci};
+                    const int ext[3] = {a.nx, a.ny, a.nz};
+                    int o[3], e[3];
+                    bool fit = t_dead == 0;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const float lo_f = fmaxf(floorf(mn[d]), -(float)ext[d]), hi_f = fminf(floorf(mx[d]), (float)ext[d]);
+                        o[d] = cc[d] + (int)lo_f - 2;
+                        e[d] = cc[d] + (int)hi_f + 3 - o[d] + 1;
+                    }
+                    const int ox = o[0] >= 0 ? (o[0] & ~3) : -((-o[0] + 3) & ~3);  // 16-byte aligned x origin (rounded down)
+                    fit = fit && (o[0] + e[0] - ox <= TMA_BX) && e[1] <= TMA_BY && e[2] <= TMA_BZ;
+                    t_org[b][0] = ox;
+                    t_org[b][1] = o[1];
+                    t_org[b][2] = o[2];
+                    t_fit[b] = fit ? 1 : 0;
+                    if (fit) {
+                        const uint32_t mb = smem_u32(&t_mb[b]);
+                        mbar_expect_tx(mb, TMA_BOX_BYTES);
+                        tma_load_3d(smem_u32(tbuf + b * TMA_BOX), tmap, ox, o[1], o[2], mb);
+                    }
+                };
+                if (tid == 0) {
+                    issue(0, 0);
+                    if (nch > 1) issue(1, 1);
                 }
-                if (iz >= sh.nZ) {
-                    iz -= sh.nZ;
-                    ++itl;
-                }
-                if (vy >= sh.nY) continue;  // a padding row of the last tile
-                const int dx = -sh.hx + vx * a.stride, dy = -sh.hy + vy * a.stride, dz = -sh.hz + vz * a.stride;
-                const int xx = xci + dx, yy = yci + dy, zz = zci + dz;
-                bool k;
-                if (keep || !inside) {
-                    k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
-                    if (k)
-                        k = keep ? kept_bit(keep, (vz * sh.nY + vy) * sh.nX + vx)
-                                 : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0);
-                } else {
-                    k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0;
-                }
-                if (!k) continue;
-                acc.nref += 1;
-                const float X = (float)dx, Y = (float)dy, Z = (float)dz;
-                if (slow) {
-                    const double* P = sc.P;
-                    const double xw = (1.0 + P[0]) * dx + P[1] * dy + P[2] * dz + ((double)xc + P[9]);
-                    const double yw = P[3] * dx + (1.0 + P[4]) * dy + P[5] * dz + ((double)yc + P[10]);
-                    const double zw = P[6] * dx + P[7] * dy + (1.0 + P[8]) * dz + ((double)zcn + P[11]);
-                    if (!margin_ok(zw, yw, xw, a.nz, a.ny, a.nx)) {
-                        acc.oob = 1;
-                        continue;
+                __syncthreads();
+                for (int ci = 0; ci < nch; ++ci) {
+                    const int b = ci & 1;
+                    bool fit = t_fit[b] != 0;
+                    if (fit) {
+                        const bool ok = mbar_wait(smem_u32(&t_mb[b]), (t_phase >> b) & 1u);
+                        t_phase ^= 1u << b;
+                        if (!ok) {  // never expected: the copy did not complete in time; sample from global memory
+                            if (a.err) atomicExch(a.err, 1);
+                            t_dead = 1;
+                            fit = false;
+                        }
+                    }
+                    const int t = ci / nzc, zc = ci - t * nzc;
+                    const int y0 = t * by, nyc = min(by, sh.nY - y0), z0 = zc * TMA_KZ, nzk = min(TMA_KZ, sh.nZ - z0);
+                    const int ox = t_org[b][0], oy = t_org[b][1], oz = t_org[b][2];
+                    const float* buf = tbuf + b * TMA_BOX;
+                    // taps of a staged sample: inside the box, else (a sample the box does not hold) from global memory
+                    auto smp_staged = [&](int gx_, int gy_, int gz_, float fx, float fy, float fz) {
+                        const int lx = gx_ - ox, ly = gy_ - oy, lz = gz_ - oz;
+                        if ((unsigned)(lx - 1) <= (unsigned)(TMA_BX - 4) && (unsigned)(ly - 1) <= (unsigned)(TMA_BY - 4) &&
+                            (unsigned)(lz - 1) <= (unsigned)(TMA_BZ - 4))
+                            return sample_brick<MODE>(buf, TMA_BX, TMA_BX * TMA_BY, lx, ly, lz, fx, fy, fz);
+                        return smp_global(gx_, gy_, gz_, fx, fy, fz);
+                    };
+                    // the chunk's slots (x fastest, then rows, then planes), advanced incrementally by T
+                    const int nxy = sh.nX * nyc, cnt = nxy * nzk;
+                    const int stx = T % sh.nX, sty = (T / sh.nX) % nyc, stz = T / nxy;
+                    int ix = tid % sh.nX, jy = (tid / sh.nX) % nyc, kz = tid / nxy;
+                    for (int sl = tid; sl < cnt; sl += T) {
+                        const int vx = ix, vy = y0 + jy, vz = z0 + kz;
+                        ix += stx;
+                        jy += sty;
+                        kz += stz;
+                        if (ix >= sh.nX) {
+                            ix -= sh.nX;
+                            ++jy;
+                        }
+                        if (jy >= nyc) {
+                            jy -= nyc;
+                            ++kz;
+                        }
+                        if (fit)
+                            visit(kind, acc, slow, vx, vy, vz, A0, A1, A2, A3, A4, A5, A6, A7, A8, T0, T1, T2, cg, smp_staged);
+                        else
+                            visit(kind, acc, slow, vx, vy, vz, A0, A1, A2, A3, A4, A5, A6, A7, A8, T0, T1, T2, cg, smp_global);
+                    }
+                    __syncthreads();  // buffer b is read; its next copy may start
+                    if (tid == 0 && ci + 2 < nch) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        issue(ci + 2, b);
                     }
                 }
-                const int64_t o = zz * sxy + (int64_t)yy * a.nx + xx;
-                // reference-frame reads first: their latency overlaps the interpolation
-                const float fv = __ldg(a.f + o);
-                float q0, q1, q2;
-                if (STORED) {
-                    q0 = __ldg(a.gx + o);
-                    q1 = __ldg(a.gy + o);
-                    q2 = __ldg(a.gz + o);
-                } else {
-                    grad_otf(a.f, a.nz, a.ny, a.nx, zz, yy, xx, q0, q1, q2);
-                }
-                const float xr = A0 * X + A1 * Y + A2 * Z + T0;
-                const float yr = A3 * X + A4 * Y + A5 * Z + T1;
-                const float zr = A6 * X + A7 * Y + A8 * Z + T2;
-                const float fxf = floorf(xr), fyf = floorf(yr), fzf = floorf(zr);
-                const int gx_ = min(max(xci + (int)fxf, lo), hx_), gy_ = min(max(yci + (int)fyf, lo), hy_),
-                          gz_ = min(max(zci + (int)fzf, lo), hz_);
-                const float gv = (MODE != 0 && a.g4) ? sample_quad<MODE == 0 ? 1 : MODE>(a.g4, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf,
-                                                                                         yr - fyf, zr - fzf)
-                                                     : sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, xr - fxf, yr - fyf, zr - fzf);
-                if (gv != gv) continue;  // NaN: masked out in the deformed frame
-                if (KIND == 1)
-                    acc.template add_part<false, true>(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
-                else
-                    acc.add(fv - cf, gv - cg, q0, q1, q2, X, Y, Z);
             }
         };
         // per-warp FP64 totals of a sweep's partials into red / redi
@@ -1220,6 +1393,18 @@ __global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lea
             if (sc.redo) --it;  // the same iteration again, every sum swept (sc.use_ref is now 0)
         }
     }
+}
+
+template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN>
+__global__ void __launch_bounds__(NW * 32, (NDOF == 12 ? 16 : 24) / NW) icgn_lean_kernel(IcgnArgs a) {
+    lean_body<MODE, STORED, NDOF, NW, UNEVEN, false>(a, nullptr);
+}
+
+// The staged form: 4 warps per node, stored gradients, one subset shape, cubic or B-spline sampling from the TMA
+// copies of g (two 23 KB buffers per CTA, four CTAs per SM).
+template <int MODE, int NDOF>
+__global__ void __launch_bounds__(128, 4) icgn_tma_kernel(IcgnArgs a, const __grid_constant__ CUtensorMap tmap) {
+    lean_body<MODE, true, NDOF, 4, false, true>(a, &tmap);
 }
 
 // ----------------------------------------------------------------------------- plain one-node-per-block kernel
@@ -1452,6 +1637,7 @@ constexpr int PLAIN_CHUNK = 8192;  // nodes per plain launch (sample buffer rows
 struct LaunchCfg {
     int threads;
     int brick_cap;
+    bool tma;  // 128 threads with brick_floats < 0: the lean sweep staged through TMA copies of g
 };
 
 static LaunchCfg batched_cfg(const aldvc_icgn_params* prm) {
@@ -1459,8 +1645,72 @@ static LaunchCfg batched_cfg(const aldvc_icgn_params* prm) {
     // 32/64/128: lean kernel with 1/2/4 warps per node; 256/512: shared-brick kernel
     c.threads = prm->threads > 0 ? prm->threads : 256;
     if (c.threads != 32 && c.threads != 64 && c.threads != 128 && c.threads != 256 && c.threads != 512) c.threads = 256;
+    c.tma = c.threads == 128 && prm->brick_floats < 0;
     c.brick_cap = prm->brick_floats > 0 ? prm->brick_floats : 24 * 1024;
     return c;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// The tensor map of g for the staged form: a float32 (nz, ny, nx) volume, box TMA_BX x TMA_BY x TMA_BZ, no swizzle, zero
+// fill outside.  False (the caller falls back to the L1 form) when the rows are not 16-byte multiples, g is not
+// 16-byte aligned, or the encoder is unavailable.
+static bool make_g_map(const IcgnArgs& a, CUtensorMap& map) {
+    if ((a.nx & 3) != 0 || (reinterpret_cast<uintptr_t>(a.g) & 15) != 0) return false;
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)a.nx * sizeof(float), (cuuint64_t)a.nx * a.ny * sizeof(float)};
+    const cuuint32_t box[3] = {TMA_BX, TMA_BY, TMA_BZ};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(a.g), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN = false>
+static int launch_lean_t(const IcgnArgs& a, cudaStream_t s);
+
+template <int MODE, int NDOF>
+static int launch_tma_t(const IcgnArgs& a, cudaStream_t s) {
+    auto kern = icgn_tma_kernel<MODE, NDOF>;
+    static int cached_per_sm = -1;  // queried once, outside any stream capture
+    static std::mutex mu;
+    int per_sm;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (cached_per_sm < 0) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TMA_SMEM);
+            if (e != cudaSuccess) return cuda_fail(e, "icgn staged: shared memory attribute");
+            int v = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, 128, TMA_SMEM);
+            if (e != cudaSuccess) return cuda_fail(e, "icgn staged: occupancy");
+            cached_per_sm = v;
+        }
+        per_sm = cached_per_sm;
+    }
+    if (per_sm < 1) return arg_fail("icgn staged: kernel does not fit on an SM");
+    CUtensorMap map;
+    if (!make_g_map(a, map)) return launch_lean_t<MODE, true, NDOF, 4>(a, s);
+    long long grid = (long long)per_sm * sm_count();
+    if (grid > a.n_nodes) grid = a.n_nodes;
+    {
+        KTimer kt_(NDOF == 12 ? "icgn12_tma" : "icgn3_tma", s);
+        kern<<<(unsigned)grid, 128, TMA_SMEM, s>>>(a, map);
+    }
+    return check_launch("icgn staged");
 }
 
 template <int MODE, bool STORED, int NDOF, int THREADS>
@@ -1493,7 +1743,7 @@ static int launch_batched_t(const IcgnArgs& a, int brick_cap, cudaStream_t s) {
     return check_launch("icgn batched");
 }
 
-template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN = false>
+template <int MODE, bool STORED, int NDOF, int NW, bool UNEVEN>
 static int launch_lean_t(const IcgnArgs& a, cudaStream_t s) {
     auto kern = icgn_lean_kernel<MODE, STORED, NDOF, NW, UNEVEN>;
     static int cached_per_sm = -1;  // queried once, outside any stream capture
@@ -1523,6 +1773,8 @@ template <int MODE, bool STORED, int NDOF>
 static int launch_batched_m(const IcgnArgs& a, const LaunchCfg& c, cudaStream_t s) {
     // per-node shapes run on the lean kernel with 4 warps per node (the brick kernel stages one shape per call)
     if (a.node_half) return launch_lean_t<MODE, STORED, NDOF, 4, true>(a, s);
+    if constexpr (MODE != 0 && STORED)
+        if (c.tma && !a.split_index) return launch_tma_t<MODE, NDOF>(a, s);
     switch (c.threads) {
         case 32: return launch_lean_t<MODE, STORED, NDOF, 1>(a, s);
         case 64: return launch_lean_t<MODE, STORED, NDOF, 2>(a, s);
@@ -1626,6 +1878,7 @@ static int run(IcgnArgs& a, int ndof, int mode, bool stored, const aldvc_icgn_pa
         return ALDVC_ERR_WORKSPACE;
     }
     a.counter = (int*)ws;
+    a.err = (int32_t*)ws + 1;  // next to the counter; reset with it
     a.gbuf = (float*)((char*)ws + 256);
     const LaunchCfg c = batched_cfg(prm);
     a.brick_cap = c.brick_cap;
@@ -1634,7 +1887,7 @@ static int run(IcgnArgs& a, int ndof, int mode, bool stored, const aldvc_icgn_pa
     if (prm->variant != ALDVC_PLAIN) {
         const size_t smem = (size_t)c.brick_cap * sizeof(float);
         if (smem + 8192 > (size_t)max_smem_optin()) return arg_fail("icgn: brick_floats exceeds the shared memory per block");
-        cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
+        cudaError_t e = cudaMemsetAsync(a.counter, 0, 2 * sizeof(int), s);
         if (e != cudaSuccess) return cuda_fail(e, "icgn: counter reset");
     }
     return ndof == 12 ? dispatch<12>(a, mode, stored, prm->variant, c, s) : dispatch<3>(a, mode, stored, prm->variant, c, s);

@@ -143,10 +143,11 @@ def icgn_params(tol, dp_tol, max_iter, patience, noise_gain=0.0, predictive=True
 
 def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol, dp_tol, max_iter, patience, stride=1, H=None,
            pattern=None, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED, threads=0,
-           brick_floats=0, node_half=None, g4=None, sweep_rows=0, node_order=None):
+           brick_floats=0, node_half=None, g4=None, sweep_rows=0, node_order=None, errs=None):
     """Device 12-DOF IC-GN; returns (P (N,12), n_iter, status, zncc) tensors.  ``node_half``: optional (N,3)
     per-node half-widths (``half`` is then their maximum); ``sweep_rows``: rows per sweep tile of the persistent
-    form (0 library default, < 0 C order)."""
+    form (0 library default, < 0 C order); ``threads`` 128 with ``brick_floats`` -1: the persistent sweep staged
+    through TMA copies of g; ``errs`` (an ErrorWords) receives the launch's device error word."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
     d = coords.device
@@ -169,13 +170,15 @@ def icgn12(coords, P0, half, f, gx, gy, gz, mask, g, mode, L, meanf, valid, tol,
     _lib.check(lib().aldvc_icgn12(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, _p(P0), _p(L), _p(Hd), _p(pat), _p(meanf),
                                   _p(valid), ctypes.byref(prm), _p(ws), ws.numel(), _p(P), _p(n_iter), _p(status), _p(zncc),
                                   stream_handle()), "aldvc_icgn12")
+    if errs is not None and variant == BATCHED:
+        errs.add(ws[:8].view(torch.int32)[1:2], "icgn12")  # the word after the work counter
     return P, n_iter, status, zncc
 
 
 def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, meanf, bottomf, valid, mu, tol, dp_tol, max_iter,
           patience, stride=1, n_full=0.0, noise_gain=0.0, predictive=True, split_index=None, split_keep=None, variant=BATCHED,
-          threads=0, brick_floats=0, node_half=None, g4=None, sweep_rows=0, node_order=None):
-    """Device 3-DOF IC-GN (ADMM subproblem 1); returns (U (N,3), n_iter, status, zncc) tensors."""
+          threads=0, brick_floats=0, node_half=None, g4=None, sweep_rows=0, node_order=None, errs=None):
+    """Device 3-DOF IC-GN (ADMM subproblem 1); returns (U (N,3), n_iter, status, zncc) tensors (arguments as icgn12)."""
     coords = dev(coords, torch.int64)
     N = coords.shape[0]
     d = coords.device
@@ -196,6 +199,8 @@ def icgn3(coords, U_old, F_fixed, vdual, half, f, gx, gy, gz, mask, g, mode, H, 
     _lib.check(lib().aldvc_icgn3(ctypes.byref(vol), ctypes.byref(sub), _p(coords), N, _p(U_old), _p(F_fixed), _p(vdual), _p(H),
                                  _p(meanf), _p(bottomf), _p(valid), ctypes.byref(prm), _p(ws), ws.numel(), _p(U), _p(n_iter),
                                  _p(status), _p(zncc), stream_handle()), "aldvc_icgn3")
+    if errs is not None and variant == BATCHED:
+        errs.add(ws[:8].view(torch.int32)[1:2], "icgn3")
     return U, n_iter, status, zncc
 
 

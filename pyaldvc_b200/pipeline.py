@@ -376,7 +376,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         nh = node_half if (node_half is None or idx is None) else node_half[idx]
         return K.icgn12(c, P0_, mesh.half, f, gx, gy, gz, m_u8, g_prep, mode, L_, mf_, v_, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter,
                         p.icgn_patience, p.subset_stride, None, None, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
-                        node_half=nh, g4=g4, sweep_rows=p.icgn_sweep_rows, node_order=order if idx is None else None)
+                        node_half=nh, g4=g4, sweep_rows=p.icgn_sweep_rows, node_order=order if idx is None else None,
+                        errs=errs if idx is None else None)
 
     th12, br12 = _launch_shape(p, 12, mode, mesh, m_u8, lambda idx, th, br: icgn12_on(idx, th, br))
     P, n_iter, status, zncc = icgn12_on(None, th12, br12)
@@ -439,7 +440,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
             return K.icgn3(c, U2_, F2_, v_, mesh.half, T["f"], T["gx"], T["gy"], T["gz"], T["m"], T["g"], mode, H_, mf_, bf_, ok_,
                            p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, n_full, 0.0,
                            p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=nh, g4=T["g4"],
-                           sweep_rows=p.icgn_sweep_rows, node_order=T["order"] if idx is None else None)
+                           sweep_rows=p.icgn_sweep_rows, node_order=T["order"] if idx is None else None,
+                           errs=errs_ if idx is None else None)
 
         def admm_step(U2, F2, W, v, th3, br3):
             # subproblem 1 (subpb1_solver.subpb1_solver :77-164)

@@ -67,8 +67,10 @@ def test_precompute_matches_reference(golden, ck, name):
     np.testing.assert_allclose(L[ok], Lr[ok], rtol=1e-3, atol=1e-4 * np.abs(Lr[ok]).max())
 
 
-FORMS = [(0, 0), (0, 32), (0, 64), (0, 128), (1, 0)]  # (variant, threads): brick kernel, lean kernel with 1/2/4 warps, plain
-FORM_IDS = ["brick", "lean1", "lean2", "lean4", "plain"]
+# (variant, threads, brick_floats): brick kernel, lean kernel with 1/2/4 warps, the lean 4-warp sweep staged through TMA
+# copies of g (cubic and B-spline cases with stored gradients; the others run as the lean form), plain
+FORMS = [(0, 0, 0), (0, 32, 0), (0, 64, 0), (0, 128, 0), (0, 128, -1), (1, 0, 0)]
+FORM_IDS = ["brick", "lean1", "lean2", "lean4", "staged", "plain"]
 
 
 @pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
@@ -83,7 +85,7 @@ def test_icgn12_matches_reference(golden, ck, name, form):
     args = (golden["coords"], P0, *pc["h"], golden["f"], gx, gy, gz, mask, g, c["mode"], L, mf, bf, valid, c.get("tol", 1e-2),
             c.get("dp_tol", 1e-3), c.get("max_iter", 100), c.get("patience", 5), pc["stride"], H,
             golden[f"icgn12_{name}_pattern"], gain, c.get("predictive", True))
-    got = ck.icgn_12dof_cuda(*args, **kw, variant=form[0], threads=form[1])
+    got = ck.icgn_12dof_cuda(*args, **kw, variant=form[0], threads=form[1], brick_floats=form[2])
     ref = tuple(golden[f"icgn12_{name}_{k}"] for k in ("P", "n_iter", "status", "zncc"))
     assert_parity(ref, got, what=f"icgn12/{name}")
     np.testing.assert_array_equal(P0, golden["P0_special"] if c.get("special") else P0)  # P0 not mutated
@@ -99,7 +101,8 @@ def test_icgn3_matches_reference(golden, ck, name, form):
     gain = STENCIL_NOISE_GAIN if c.get("noise") else 0.0
     got = ck.icgn_3dof_cuda(golden["coords"], golden["U_old"], golden["F_fixed"], golden["vdual"], *pc["h"], golden["f"], gx, gy,
                             gz, mask, g, c["mode"], H, mf, bf, valid, 1e-3, 1e-2, 1e-3, 100, 5, pc["stride"],
-                            float(golden[f"icgn3_{name}_n_full"]), gain, True, **kw, variant=form[0], threads=form[1])
+                            float(golden[f"icgn3_{name}_n_full"]), gain, True, **kw, variant=form[0], threads=form[1],
+                            brick_floats=form[2])
     ref = tuple(golden[f"icgn3_{name}_{k}"] for k in ("U", "n_iter", "status", "zncc"))
     assert_parity(ref, got, what=f"icgn3/{name}")
 

@@ -149,7 +149,14 @@ def _crop_config5():
     return pair.f, pair.g, None, p, None
 
 
-CROPS = {"config2": _crop_config2, "config3": _crop_config3, "config5": _crop_config5}
+def _crop_config5_staged():
+    """The configuration-5 box with the IC-GN sweeps staged through TMA copies of g."""
+    f, g, mask, p, half_of = _crop_config5()
+    p.threads, p.brick_floats = 128, -1
+    return f, g, mask, p, half_of
+
+
+CROPS = {"config2": _crop_config2, "config3": _crop_config3, "config5": _crop_config5, "config5_staged": _crop_config5_staged}
 
 
 def _oracle_pass(oracle_mod, f, g, mask, p, res, half_of):
