@@ -34,6 +34,9 @@
  *                        one axis per call
  *   aldvc_volume_stats / aldvc_normalize_voi <- io/volume_ops.py:74 voi_mean_std,
  *                        :105 normalize_volume with a VOI box
+ *   aldvc_volume_moments / aldvc_normalize_sums <- io/volume_ops.py:80-121 voi_mean_std +
+ *                        normalize_volume of a volume streamed from host memory slab by slab
+ *                        (the tiled pass; solver/tiling.py:292 ReferenceSource serves its boxes)
  *   aldvc_block_downsample <- solver/integer_search.py:235 block_downsample
  *   aldvc_phase_correlation <- solver/integer_search.py:247 phase_correlation_shift (after the
  *                        VOI crop and the block downsampling, which the caller does)
@@ -196,6 +199,16 @@ int aldvc_volume_stats(const void *vol, int32_t is_uint16, int64_t nz, int64_t n
 /* aldvc_volume_stats over the box, then (v - mean) / std over the WHOLE volume into out (std < 1e-12 -> 1) */
 int aldvc_normalize_voi(const void *vol, int32_t is_uint16, int64_t nz, int64_t ny, int64_t nx, const int64_t *box, double pilot,
                         float *out, double *stats, void *workspace, size_t workspace_bytes, void *stream);
+/* FP64 sums of (v - pilot) and (v - pilot)^2 over n_voxels of a float32 or uint16 array, ADDED to sums (device,
+ * 2 doubles, zeroed by the caller before the first slab): a volume that does not fit the device is streamed
+ * through in slabs and its moments accumulated (workspace: aldvc_normalize_workspace_size() bytes) */
+int aldvc_volume_moments(const void *vol, int32_t is_uint16, int64_t n_voxels, double pilot, double *sums, void *workspace,
+                         size_t workspace_bytes, void *stream);
+/* (v - mean) / std of n_voxels into out (float32), mean and std from the accumulated sums of n_total voxels
+ * about pilot (std < 1e-12 -> 1): one box of a streamed volume normalised with the whole volume's statistics;
+ * stats (device, 2 doubles, may be NULL) receives mean and std */
+int aldvc_normalize_sums(const void *vol, int32_t is_uint16, int64_t n_voxels, const double *sums, int64_t n_total, double pilot,
+                         float *out, double *stats, void *stream);
 
 /* Block means of factor^3 voxels (FP64 sums, float32 out); out is (nz/factor, ny/factor, nx/factor), the
  * trailing voxels of each axis dropped. */

@@ -94,6 +94,8 @@ PROTOTYPES = {
     "aldvc_stats_workspace_size": (_sz, []),
     "aldvc_volume_stats": (_i32, [_p, _i32, _i64, _i64, _i64, _p, _d, _p, _p, _sz, _p]),
     "aldvc_normalize_voi": (_i32, [_p, _i32, _i64, _i64, _i64, _p, _d, _p, _p, _p, _sz, _p]),
+    "aldvc_volume_moments": (_i32, [_p, _i32, _i64, _d, _p, _p, _sz, _p]),
+    "aldvc_normalize_sums": (_i32, [_p, _i32, _i64, _p, _i64, _d, _p, _p, _p]),
     "aldvc_block_downsample": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _p]),
     "aldvc_phase_correlation_workspace_size": (_sz, [_i64, _i64, _i64]),
     "aldvc_phase_correlation": (_i32, [_p, _p, _i64, _i64, _i64, _p, _p, _sz, _p]),

@@ -38,23 +38,35 @@ __global__ void moments_kernel(const T* __restrict__ v, int64_t n, double pilot,
     }
 }
 
-// mean/std from the partials (single thread, fixed order), then (v - mean) * (1/std) -> float32
+// mean and std of n voxels from their sums of (v - pilot) and (v - pilot)^2 (io/volume_ops.py:92-96; std < 1e-12 -> 1)
+__device__ __forceinline__ void stats_from_sums(double ts, double tq, int64_t n, double pilot, double& mean, double& sd) {
+    const double ms = ts / (double)n;
+    double var = tq / (double)n - ms * ms;
+    var = var > 0.0 ? var : 0.0;
+    sd = sqrt(var);
+    if (sd < 1e-12) sd = 1.0;
+    mean = pilot + ms;
+}
+
+// mean/std from the partials (single thread, fixed order) or, with part == NULL, from accumulated sums[2], then
+// (v - mean) * (1/std) -> float32
 template <typename T>
 __global__ void normalize_kernel(const T* __restrict__ v, int64_t n, double pilot, const double* part, int nparts, float* out,
-                                 double* stats) {
+                                 double* stats, const double* sums = nullptr, int64_t n_total = 0) {
     __shared__ double s_mean, s_inv;
     if (threadIdx.x == 0) {
-        double ts = 0.0, tq = 0.0;
-        for (int b = 0; b < nparts; ++b) {
-            ts += part[2 * b];
-            tq += part[2 * b + 1];
+        double ts = 0.0, tq = 0.0, mean, sd;
+        if (sums) {
+            ts = sums[0];
+            tq = sums[1];
+        } else {
+            for (int b = 0; b < nparts; ++b) {
+                ts += part[2 * b];
+                tq += part[2 * b + 1];
+            }
         }
-        const double ms = ts / (double)n;
-        double var = tq / (double)n - ms * ms;
-        var = var > 0.0 ? var : 0.0;
-        double sd = sqrt(var);
-        if (sd < 1e-12) sd = 1.0;
-        s_mean = pilot + ms;
+        stats_from_sums(ts, tq, sums ? n_total : n, pilot, mean, sd);
+        s_mean = mean;
         s_inv = 1.0 / sd;
         if (blockIdx.x == 0 && stats) {
             stats[0] = s_mean;
@@ -65,6 +77,17 @@ __global__ void normalize_kernel(const T* __restrict__ v, int64_t n, double pilo
     const double m = s_mean, inv = s_inv;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = (float)(((double)v[i] - m) * inv);
+}
+
+// sums[0..1] += the partials, in block order (one thread): a volume streamed slab by slab accumulates its moments
+__global__ void moments_add_kernel(const double* part, int nparts, double* sums) {
+    double ts = 0.0, tq = 0.0;
+    for (int b = 0; b < nparts; ++b) {
+        ts += part[2 * b];
+        tq += part[2 * b + 1];
+    }
+    sums[0] += ts;
+    sums[1] += tq;
 }
 
 // One block per bead: peak * exp(-|x - c|^2 / (2 sigma^2)) over the (2R+1)^3 voxels around the bead,
@@ -206,6 +229,36 @@ extern "C" int aldvc_normalize(const void* vol, int32_t is_uint16, int64_t n_vox
     ALDVC_REQUIRE(vol && out && workspace, "aldvc_normalize: null pointer");
     ALDVC_REQUIRE(n_voxels > 0, "aldvc_normalize: empty volume");
     return normalize_any(vol, is_uint16, n_voxels, pilot, out, stats, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" int aldvc_volume_moments(const void* vol, int32_t is_uint16, int64_t n_voxels, double pilot, double* sums, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+    ALDVC_REQUIRE(vol && sums && workspace, "aldvc_volume_moments: null pointer");
+    ALDVC_REQUIRE(n_voxels > 0, "aldvc_volume_moments: empty array");
+    const int parts = 1024;
+    if (workspace_bytes < (size_t)parts * 2 * sizeof(double)) return arg_fail("aldvc_volume_moments: workspace");
+    cudaStream_t s = (cudaStream_t)stream;
+    double* part = (double*)workspace;
+    if (is_uint16)
+        moments_kernel<uint16_t><<<parts, VOL_THREADS, 0, s>>>((const uint16_t*)vol, n_voxels, pilot, part);
+    else
+        moments_kernel<float><<<parts, VOL_THREADS, 0, s>>>((const float*)vol, n_voxels, pilot, part);
+    moments_add_kernel<<<1, 1, 0, s>>>(part, parts, sums);
+    return check_launch("aldvc_volume_moments");
+}
+
+extern "C" int aldvc_normalize_sums(const void* vol, int32_t is_uint16, int64_t n_voxels, const double* sums, int64_t n_total,
+                                    double pilot, float* out, double* stats, void* stream) {
+    ALDVC_REQUIRE(vol && sums && out, "aldvc_normalize_sums: null pointer");
+    ALDVC_REQUIRE(n_voxels > 0 && n_total > 0, "aldvc_normalize_sums: empty array");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int blocks = (int)std::min<int64_t>(1024, (n_voxels + VOL_THREADS - 1) / VOL_THREADS);
+    if (is_uint16)
+        normalize_kernel<uint16_t><<<blocks, VOL_THREADS, 0, s>>>((const uint16_t*)vol, n_voxels, pilot, nullptr, 0, out, stats, sums,
+                                                                  n_total);
+    else
+        normalize_kernel<float><<<blocks, VOL_THREADS, 0, s>>>((const float*)vol, n_voxels, pilot, nullptr, 0, out, stats, sums, n_total);
+    return check_launch("aldvc_normalize_sums");
 }
 
 extern "C" int aldvc_render_beads(double* accum, int64_t nz, int64_t ny, int64_t nx, const double* centres_zyx, const double* peaks,

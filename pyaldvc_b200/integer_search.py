@@ -100,11 +100,13 @@ def _window_fits(shape, half, radius) -> bool:
 
 
 def ncc_search_expanding_device(f, g, coords, half, radius, shift0=None, auto_expand: bool = True, max_expand: int = 3,
-                                engine_of=None, calls: list | None = None) -> dict:
+                                engine_of=None, calls: list | None = None, search_fn=None) -> dict:
     """Device ``ncc_search_expanding`` (integer_search.py:486-524) on CUDA tensors: ``coords`` (N,3) int64, ``half``
     the template half-widths, ``shift0`` (N,3) int64 or None.  Returns disp, cc, pce (FP64), clipped, ok (bool)
     tensors, the final ``radius`` and the number of ``expansions``.  ``engine_of(half, radius)`` picks the NCC
-    engine of each search (tiled by default); ``calls`` collects (nodes, half, radius, engine) per search."""
+    engine of each search (tiled by default); ``calls`` collects (nodes, half, radius, engine) per search.
+    ``search_fn(coords, half, radius, shift, engine)`` replaces the search over whole device volumes (the tiled
+    pass runs it box by box from host memory); ``f`` then only has to give the volume's ``shape``."""
     import torch
 
     K = _kernels()
@@ -123,7 +125,7 @@ def ncc_search_expanding_device(f, g, coords, half, radius, shift0=None, auto_ex
         eng = K.NCC_TILED if engine_of is None else engine_of(half, r)
         if calls is not None:
             calls.append((int(c.shape[0]), tuple(half), tuple(r), eng))
-        res = K.ncc_search(f, g, c, half, r, sh, eng)
+        res = K.ncc_search(f, g, c, half, r, sh, eng) if search_fn is None else search_fn(c, half, r, sh, eng)
         return {"disp": res["disp"], "cc": res["cc"], "pce": res["pce"], "clipped": res["clipped"] != 0, "ok": res["ok"] != 0}
 
     out.update(search(coords, rad, shift0))
@@ -200,9 +202,11 @@ def block_downsample(vol, factor: int):
     return out if keep else out.cpu().numpy()
 
 
-def phase_correlation_shift_device(f, g, voi=None, max_dim: int = 128) -> np.ndarray:
+def phase_correlation_shift_device(f, g, voi=None, max_dim: int = 128, downsample=None) -> np.ndarray:
     """Global integer shift (dx, dy, dz) of ``g`` against ``f`` (integer_search.py:247-291): the VOI block-
-    downsampled until no axis exceeds ``max_dim``, Hann-windowed phase correlation, peak wrapped and scaled."""
+    downsampled until no axis exceeds ``max_dim``, Hann-windowed phase correlation, peak wrapped and scaled.
+    ``downsample(factor)`` gives the block-mean pair of a volume that is not on the device (``f`` then only gives
+    the shape; no VOI)."""
     import math
 
     K = _kernels()
@@ -211,8 +215,11 @@ def phase_correlation_shift_device(f, g, voi=None, max_dim: int = 128) -> np.nda
         f = f[sl].contiguous()
         g = g[sl].contiguous()
     factor = max(1, int(math.ceil(max(f.shape) / max_dim)))
-    fs = K.block_downsample(f, factor)
-    gs = K.block_downsample(g, factor)
+    if downsample is not None and factor > 1:
+        fs, gs = downsample(factor)
+    else:
+        fs = K.block_downsample(f, factor)
+        gs = K.block_downsample(g, factor)
     peak = np.array(K.phase_correlation_peak(fs, gs), dtype=np.float64)
     for ax, n in enumerate(fs.shape):
         if peak[ax] > n // 2:
@@ -230,13 +237,18 @@ def phase_correlation_shift(f, g, voi=None, max_dim: int = 128) -> np.ndarray:
 phase_correlation_shift.__doc__ = phase_correlation_shift_device.__doc__
 
 
-def auto_pyramid_levels(shape, subset, radius, max_levels: int = 3, f=None, min_std_ratio: float = MIN_COARSE_STD_RATIO) -> int:
+def auto_pyramid_levels(shape, subset, radius, max_levels: int = 3, f=None, min_std_ratio: float = MIN_COARSE_STD_RATIO,
+                        std0: float | None = None, downsample=None) -> int:
     """Coarse levels that fit the search window and keep the texture (integer_search.py:575-612): level l
     (factor 2^l) is taken while every axis holds the level's window plus margin and, with ``f``, the block-mean
-    volume keeps at least ``min_std_ratio`` of the full-resolution standard deviation."""
+    volume keeps at least ``min_std_ratio`` of the full-resolution standard deviation.  A volume that is not on
+    the device gives its standard deviation ``std0`` and ``downsample(factor)`` (its block means, on the device)
+    instead of ``f``."""
     K = _kernels()
     fd = None if f is None else _device_volume(f)[0]
-    std0 = None if fd is None else float(K.volume_stats(fd)[1].item())
+    if fd is not None:
+        std0 = float(K.volume_stats(fd)[1].item())
+        downsample = lambda fac: K.block_downsample(fd, fac)  # noqa: E731
     levels = 0
     for lv in range(1, max_levels + 1):
         fac = 2**lv
@@ -246,7 +258,7 @@ def auto_pyramid_levels(shape, subset, radius, max_levels: int = 3, f=None, min_
             if int(n) // fac < w_l + 1 + 2 * max(r, 1) + 4:
                 fits = False
         if fits and std0 is not None and std0 > 0:
-            ds = K.block_downsample(fd, fac)
+            ds = downsample(fac)
             if float(K.volume_stats(ds)[1].item()) < min_std_ratio * std0:
                 fits = False
         if fits:
@@ -259,16 +271,22 @@ def auto_pyramid_levels(shape, subset, radius, max_levels: int = 3, f=None, min_
 def pyramid_search_device(f, g, coords, grid_shape, subset, radius, levels: int = 0, global_shift=None,
                           outlier_threshold: float = 2.0, auto_expand: bool = True, max_expand: int = 3,
                           fine_radius: int = PYRAMID_FINE_RADIUS, valid=None, engine_of=None, calls: list | None = None,
-                          errs=None) -> dict:
+                          errs=None, level_volumes=None, search_fn=None) -> dict:
     """Coarse-to-fine NCC search (integer_search.py:615-694) on CUDA tensors: the coarsest level searches
     ``coarse_radius(radius)`` on block means, each finer level refines with ``fine_radius`` around the up-scaled,
     median-cleaned and inpainted estimate.  ``valid`` (N,) bool restricts the searched nodes.  Returns disp (N,3)
     FP64 in full-resolution voxels, the last level's ok / cc / pce / clipped, and the per-level record.  The
-    cleaning's device error words go to ``errs`` (a kernels.ErrorWords), else they are checked per level."""
+    cleaning's device error words go to ``errs`` (a kernels.ErrorWords), else they are checked per level.
+    A pass over volumes streamed from host memory gives ``level_volumes(factor)`` (the block-mean pair of a
+    coarse level, on the device), ``search_fn`` (the full-resolution search, see ncc_search_expanding_device)
+    and a resolved ``levels`` (0: the full-resolution search alone); ``f`` and ``g`` then only give the volume shape."""
     import torch
 
     K = _kernels()
-    if levels <= 0:
+    streamed = level_volumes is not None
+    if level_volumes is None:
+        level_volumes = lambda fac: (K.block_downsample(f, fac), K.block_downsample(g, fac))  # noqa: E731
+    if levels <= 0 and not streamed:
         levels = auto_pyramid_levels(tuple(f.shape), subset, radius, f=f)
     N = int(coords.shape[0])
     active = torch.arange(N, device=coords.device) if valid is None else torch.nonzero(valid).flatten()
@@ -280,14 +298,14 @@ def pyramid_search_device(f, g, coords, grid_shape, subset, radius, levels: int 
     info: dict = {"levels": levels, "per_level": [], "expansions": 0, "n_searched": int(active.numel())}
     for lv in range(levels, -1, -1):
         fac = 2**lv
-        fl = K.block_downsample(f, fac) if fac > 1 else f
-        gl = K.block_downsample(g, fac) if fac > 1 else g
+        fl, gl = level_volumes(fac) if fac > 1 else (f, g)
         subset_l = tuple(max(MIN_PYRAMID_SUBSET, (int(w) // fac) // 2 * 2) for w in subset)
         half_l = tuple(w // 2 for w in subset_l)
         rad_l = coarse_radius(radius, fac) if lv == levels else (int(fine_radius),) * 3
         coords_l = torch.round(coords[active].double() / fac).long().contiguous()
         shift_l = torch.round(disp_full[active] / fac).long().contiguous()
-        sub = ncc_search_expanding_device(fl, gl, coords_l, half_l, rad_l, shift_l, auto_expand, max_expand, engine_of, calls)
+        sub = ncc_search_expanding_device(fl, gl, coords_l, half_l, rad_l, shift_l, auto_expand, max_expand, engine_of, calls,
+                                          search_fn if fac == 1 else None)
         res = {k: sub[k] for k in ("radius", "expansions")}
         for key, fill in (("disp", float("nan")), ("cc", float("nan")), ("pce", float("nan"))):
             t = torch.full((N,) + tuple(sub[key].shape[1:]), fill, dtype=torch.float64, device=coords.device)

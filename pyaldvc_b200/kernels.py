@@ -455,6 +455,26 @@ def normalize_voi(vol: torch.Tensor, box, pilot: float | None = None):
     return out, stats
 
 
+def volume_moments(vol: torch.Tensor, pilot: float, sums: torch.Tensor) -> torch.Tensor:
+    """Add the FP64 sums of (v - pilot) and (v - pilot)^2 of a float32 / uint16 CUDA array into ``sums`` (2 doubles,
+    device): the moments of a volume streamed through the device slab by slab."""
+    assert vol.is_cuda and vol.is_contiguous() and sums.dtype == torch.float64 and sums.numel() == 2
+    ws = _workspace(lib().aldvc_normalize_workspace_size())
+    _lib.check(lib().aldvc_volume_moments(_p(vol), _vol_kind(vol), vol.numel(), float(pilot), _p(sums), _p(ws), ws.numel(),
+                                          stream_handle()), "aldvc_volume_moments")
+    return sums
+
+
+def normalize_sums(vol: torch.Tensor, sums: torch.Tensor, n_total: int, pilot: float) -> torch.Tensor:
+    """(v - mean) / std of a float32 / uint16 CUDA array as float32, mean and std from the accumulated ``sums`` of a
+    volume of ``n_total`` voxels about ``pilot`` (one box of a streamed volume, the whole volume's statistics)."""
+    assert vol.is_cuda and vol.is_contiguous() and sums.dtype == torch.float64 and sums.numel() == 2
+    out = torch.empty(vol.shape, dtype=torch.float32, device=vol.device)
+    _lib.check(lib().aldvc_normalize_sums(_p(vol), _vol_kind(vol), vol.numel(), _p(sums), int(n_total), float(pilot), _p(out), None,
+                                          stream_handle()), "aldvc_normalize_sums")
+    return out
+
+
 def block_downsample(vol: torch.Tensor, factor: int) -> torch.Tensor:
     """Block means of ``factor``^3 voxels (trailing voxels dropped); ``factor <= 1`` returns a float32 copy."""
     vol = dev(vol, torch.float32)

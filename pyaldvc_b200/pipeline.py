@@ -70,6 +70,12 @@ class PassParams:
     # sets the mesh border and the maximum shape); every shape runs in the same persistent launches
     node_winsize: object = None
     prefilter_sigma: float = 0.0  # Gaussian pre-smoothing of both volumes after normalisation (0 = off)
+    # tiled pass (tiling.run_pass_tiled, core/config.py:140-142): box edge target in voxels (0 = one whole-volume
+    # box), extra halo for the displacement (0 = max(winstepsize)), halo for the subset's stretch (fraction of
+    # winsize / 2)
+    tile_local: int = 0
+    tile_disp_margin: int = 0
+    tile_strain_margin: float = 0.25
     # initial guess (core/config.py:61-71): "pyramid" (coarse-to-fine NCC), "ncc" (one full-resolution search)
     # or "zero"; an optional global phase-correlation pre-shift
     init_guess_method: str = "pyramid"
@@ -245,6 +251,95 @@ def graph_count() -> int:
     return len(_ADMM_GRAPHS)
 
 
+def node_validity(mesh, p: PassParams, node_half, valid_b: torch.Tensor, centre_ok: torch.Tensor | None, n_valid: torch.Tensor):
+    """(node validity, active elements uint8 or None): with a reference mask (``centre_ok`` set) apply_mask_to_mesh
+    (grid_mesh.py:191-253) keeps the nodes whose centre is in the mask and enough of whose subset is, and the hex
+    elements whose eight nodes are kept; without one every node and element stays."""
+    if centre_ok is None:
+        return valid_b, None
+    if node_half is None:
+        S = float(np.prod([2 * h + 1 for h in mesh.half]))
+    else:
+        S = (2 * node_half.double() + 1).prod(dim=1)
+    node_valid = centre_ok & (n_valid.double() >= p.min_valid_ratio * S)
+    valid_b = valid_b & node_valid
+    elem_node = node_valid.reshape(mesh.grid_shape)
+    e = (elem_node[:-1, :-1, :-1] & elem_node[:-1, :-1, 1:] & elem_node[:-1, 1:, 1:] & elem_node[:-1, 1:, :-1]
+         & elem_node[1:, :-1, :-1] & elem_node[1:, :-1, 1:] & elem_node[1:, 1:, 1:] & elem_node[1:, 1:, :-1])
+    return valid_b, e.reshape(-1).to(torch.uint8).contiguous()
+
+
+def initial_guess(p: PassParams, mesh, f, g, search_valid: torch.Tensor, ncc_calls: list, errs: K.ErrorWords, shift_fn=None,
+                  search_fn=None, level_volumes=None, levels: int | None = None):
+    """Section 3 of the pass (init_disp.compute_initial_guess :53-140, clean_initial_guess :143-189): (U0 (N,3)
+    FP64, record).  ``f``, ``g``: the normalised device pair, or shape-only stand-ins when ``shift_fn`` (the global
+    shift), ``search_fn`` (full-resolution searches), ``level_volumes`` (coarse pyramid pairs) and ``levels`` come
+    from a pass that streams its volumes (tiling.run_pass_tiled)."""
+    subset0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
+    half0 = tuple(int(w) // 2 for w in subset0)
+    rad = tuple(int(r) for r in p.search_radius)
+    engine_of = lambda h, r: _ncc_engine(p, h, r)  # noqa: E731
+    if p.init_guess_method not in ("pyramid", "ncc", "zero", "previous"):
+        raise ValueError(f"unknown init_guess_method {p.init_guess_method!r}")
+    if p.init_guess_method == "zero":
+        return torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda"), {"method": "zero"}
+    shift = None
+    if p.global_shift:
+        shift = shift_fn() if shift_fn is not None else IS.phase_correlation_shift_device(f, g)
+    if p.init_guess_method in ("pyramid", "previous"):  # "previous" has no earlier frame here: the reference falls back
+        info = IS.pyramid_search_device(f, g, mesh.coords, mesh.grid_shape, subset0, rad,
+                                        p.pyramid_levels if levels is None else levels, shift, p.init_outlier_threshold,
+                                        p.ncc_auto_expand, p.ncc_max_expand, p.pyramid_fine_radius, search_valid, engine_of, ncc_calls,
+                                        errs, level_volumes, search_fn)
+        disp, ok, pce = info["disp"], info.get("ok"), info.get("pce")
+        if ok is None:
+            ok = torch.ones(mesh.n, dtype=torch.bool, device="cuda")
+        init_info = {"method": "pyramid", "levels": info["levels"], "per_level": info["per_level"], "expansions": info["expansions"]}
+    else:
+        act = torch.nonzero(search_valid).flatten()
+        if act.numel() == 0:
+            act = torch.arange(mesh.n, device="cuda")
+        sh0 = None
+        if shift is not None:
+            sh0 = torch.as_tensor(np.round(shift).astype(np.int64), device="cuda")[None, :].expand(act.numel(), 3).contiguous()
+        res = IS.ncc_search_expanding_device(f, g, mesh.coords[act].contiguous(), half0, rad, sh0, p.ncc_auto_expand,
+                                             p.ncc_max_expand, engine_of, ncc_calls, search_fn)
+        disp = torch.full((mesh.n, 3), float("nan"), dtype=torch.float64, device="cuda")
+        ok = torch.zeros(mesh.n, dtype=torch.bool, device="cuda")
+        pce = torch.full((mesh.n,), float("nan"), dtype=torch.float64, device="cuda")
+        disp[act] = res["disp"]
+        ok[act] = res["ok"]
+        pce[act] = res["pce"]
+        init_info = {"method": "ncc", "radius": res["radius"], "expansions": res["expansions"]}
+    init_info["global_shift"] = shift
+    bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~search_valid
+    if p.init_min_pce > 0 and pce is not None:
+        bad = bad | (torch.isfinite(pce) & (pce < p.init_min_pce))
+    flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), ~bad, mesh.grid_shape, p.init_outlier_threshold, errs)
+    bad = bad | flag
+    U0, all_bad = _fill(disp, bad, mesh.grid_shape, errs)
+    if bool(all_bad.item()):
+        U0.zero_()
+    init_info["n_bad"] = int(bad.sum().item())
+    return U0, init_info
+
+
+def make_global_step(mesh, p: PassParams, elem_active, beta, errs: K.ErrorWords):
+    """The global step of one ADMM iteration (subpb2_solver.py, pipeline.py:300-330): right-hand side, hex8 PCG from
+    U1, nodal gradient of the result (non-finite entries keep F1).  Returns a function (U1, F1, W, v) -> (U2, F2)."""
+
+    def global_step(U1_, F1_, W_, v_):
+        b = K.global_rhs(mesh.grid_shape, mesh.spacing, elem_active, beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
+        U2_, _, e_ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, elem_active, beta, p.mu, p.alpha, b, U1_, p.pcg_tol, p.pcg_max_iter,
+                                p.gauss_pt_order)
+        errs.add(e_, "pcg_hex8")
+        F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, elem_active, U2_, p.gauss_pt_order).reshape(-1, 9)
+        F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
+        return U2_, F2_
+
+    return global_step
+
+
 def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
              tracer: Tracer | None = None, g_mask: torch.Tensor | None = None) -> PassResult:
     """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16).  ``mask``: reference-frame
@@ -290,77 +385,19 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         precompute_form = "per_node"
         H, L, meanf, bottomf, n_valid, valid = K.precompute(mesh.coords, mesh.half, f, gx, gy, gz, m_u8, p.min_valid_ratio,
                                                             p.hessian_cond_max, p.subset_stride, None, None, node_half)
-    valid_b = valid != 0
-    node_valid = torch.ones(mesh.n, dtype=torch.bool, device="cuda")  # apply_mask_to_mesh's node_valid (all without a mask)
-    if mask is not None:  # apply_mask_to_mesh (grid_mesh.py:191-253): centre in the mask, enough of the subset in it
+    centre_ok = None
+    if mask is not None:
         c = mesh.coords
         centre_ok = m_u8[c[:, 2], c[:, 1], c[:, 0]] != 0
-        if node_half is None:
-            S = float(np.prod([2 * h + 1 for h in mesh.half]))
-        else:
-            S = (2 * node_half.double() + 1).prod(dim=1)
-        node_valid = centre_ok & (n_valid.double() >= p.min_valid_ratio * S)
-        valid_b = valid_b & node_valid
-        elem_node = node_valid.reshape(mesh.grid_shape)
-        e = (elem_node[:-1, :-1, :-1] & elem_node[:-1, :-1, 1:] & elem_node[:-1, 1:, 1:] & elem_node[:-1, 1:, :-1]
-             & elem_node[1:, :-1, :-1] & elem_node[1:, :-1, 1:] & elem_node[1:, 1:, 1:] & elem_node[1:, 1:, :-1])
-        elem_active = e.reshape(-1).to(torch.uint8).contiguous()
-    else:
-        elem_active = None
+    valid_b, elem_active = node_validity(mesh, p, node_half, valid != 0, centre_ok, n_valid)
     valid_u8 = valid_b.to(torch.uint8).contiguous()
     tr.mark("precompute")
 
     # ---------------- section 3: initial guess (init_disp.compute_initial_guess :53-140, clean_initial_guess :143-189)
-    subset0 = p.init_subset if p.init_subset is not None else tuple(min(int(w), 16) for w in p.winsize)
-    half0 = tuple(int(w) // 2 for w in subset0)
-    rad = tuple(int(r) for r in p.search_radius)
-    ncc_calls: list = []
-    engine_of = lambda h, r: _ncc_engine(p, h, r)  # noqa: E731
     # the reference makes the precompute's validity the mesh's node validity before the initial guess
     # (core/pipeline.py:212, local_icgn.py:300): only those nodes are searched, the others are filled
-    search_valid = valid_b
-    if p.init_guess_method not in ("pyramid", "ncc", "zero", "previous"):
-        raise ValueError(f"unknown init_guess_method {p.init_guess_method!r}")
-    if p.init_guess_method == "zero":
-        U0 = torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda")
-        init_info = {"method": "zero"}
-    else:
-        shift = IS.phase_correlation_shift_device(f, g) if p.global_shift else None
-        if p.init_guess_method in ("pyramid", "previous"):  # "previous" has no earlier frame here: the reference falls back
-            info = IS.pyramid_search_device(f, g, mesh.coords, mesh.grid_shape, subset0, rad, p.pyramid_levels, shift,
-                                            p.init_outlier_threshold, p.ncc_auto_expand, p.ncc_max_expand, p.pyramid_fine_radius,
-                                            search_valid, engine_of, ncc_calls, errs)
-            disp, ok, pce = info["disp"], info.get("ok"), info.get("pce")
-            if ok is None:
-                ok = torch.ones(mesh.n, dtype=torch.bool, device="cuda")
-            init_info = {"method": "pyramid", "levels": info["levels"], "per_level": info["per_level"],
-                         "expansions": info["expansions"]}
-        else:
-            act = torch.nonzero(search_valid).flatten()
-            if act.numel() == 0:
-                act = torch.arange(mesh.n, device="cuda")
-            sh0 = None
-            if shift is not None:
-                sh0 = torch.as_tensor(np.round(shift).astype(np.int64), device="cuda")[None, :].expand(act.numel(), 3).contiguous()
-            res = IS.ncc_search_expanding_device(f, g, mesh.coords[act].contiguous(), half0, rad, sh0, p.ncc_auto_expand,
-                                                 p.ncc_max_expand, engine_of, ncc_calls)
-            disp = torch.full((mesh.n, 3), float("nan"), dtype=torch.float64, device="cuda")
-            ok = torch.zeros(mesh.n, dtype=torch.bool, device="cuda")
-            pce = torch.full((mesh.n,), float("nan"), dtype=torch.float64, device="cuda")
-            disp[act] = res["disp"]
-            ok[act] = res["ok"]
-            pce[act] = res["pce"]
-            init_info = {"method": "ncc", "radius": res["radius"], "expansions": res["expansions"]}
-        init_info["global_shift"] = shift
-        bad = ~ok | ~torch.isfinite(disp).all(dim=1) | ~search_valid
-        if p.init_min_pce > 0 and pce is not None:
-            bad = bad | (torch.isfinite(pce) & (pce < p.init_min_pce))
-        flag = _median_flags(torch.where(bad[:, None], torch.nan, disp), ~bad, mesh.grid_shape, p.init_outlier_threshold, errs)
-        bad = bad | flag
-        U0, all_bad = _fill(disp, bad, mesh.grid_shape, errs)
-        if bool(all_bad.item()):
-            U0.zero_()
-        init_info["n_bad"] = int(bad.sum().item())
+    ncc_calls: list = []
+    U0, init_info = initial_guess(p, mesh, f, g, valid_b, ncc_calls, errs)
     tr.mark("init_guess")
 
     # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
@@ -422,14 +459,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
          "coords": mesh.coords, "elem": elem_active, "node_half": node_half, "g4": g4, "order": order}
 
     def make_steps(T, errs_):
-        def global_step(U1_, F1_, W_, v_):
-            b = K.global_rhs(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, U1_, F1_, W_, v_, p.gauss_pt_order)
-            U2_, _, e_ = K.pcg_hex8(mesh.grid_shape, mesh.spacing, T["elem"], beta, p.mu, p.alpha, b, U1_, p.pcg_tol,
-                                    p.pcg_max_iter, p.gauss_pt_order)
-            errs_.add(e_, "pcg_hex8")
-            F2_ = K.nodal_gradient(mesh.grid_shape, mesh.spacing, T["elem"], U2_, p.gauss_pt_order).reshape(-1, 9)
-            F2_ = torch.where(torch.isfinite(F2_), F2_, F1_)
-            return U2_, F2_
+        global_step = make_global_step(mesh, p, T["elem"], beta, errs_)
 
         def icgn3_on(idx, U2_, F2_, v_, th, br):
             keys = ("coords", "H", "meanf", "bottomf", "valid")

@@ -3,7 +3,7 @@
 Run in a container that holds the pyALDVC sources (read-only) at
 ``$ALDVC_REFERENCE/src`` (default ``/root/reference/src``)::
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [kernels volume_ops init_guess strain beta pass ncc_fft]
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [kernels volume_ops init_guess strain beta pass ncc_fft tiling]
 
 It imports the reference package, runs its own Numba CPU kernels on seeded
 bead volumes from ``pyaldvc_b200.synthetic`` and stores inputs + outputs as
@@ -473,9 +473,61 @@ def ncc_fft_fixtures():
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB); expansions {res['expansions']}, radius {res['radius']}")
 
 
+# geometries of the tile plans: (volume shape, winsize, winstepsize, search radius, extra DVCPara fields, edges, disp
+# field scale (0: none), restricted-node stride (0: all nodes))
+TILING_CASES = {
+    "base": ((96, 112, 128), 16, 8, 8, {}, (96, 112, 128), 0.0, 0),
+    "disp": ((96, 112, 128), 16, 8, 8, {}, (112,), 3.7, 0),
+    "aniso": ((90, 120, 150), (20, 32, 24), (10, 12, 8), (10, 8, 6),
+              {"prefilter_sigma": 1.0, "tile_strain_margin": 0.5, "tile_disp_margin": 5}, (100, 140), 2.2, 0),
+    "nodes": ((96, 112, 128), 16, 8, 8, {}, (96,), 1.5, 7),
+    "small": ((96, 112, 128), 16, 8, 8, {}, (24, 0), 0.0, 0),
+}
+
+
+def tiling_fixtures():
+    """The reference's tile plans (solver/tiling.py tile_pad :141, plan_tiles :204) over grid meshes of several
+    geometries: halos, fallbacks, and per tile the node block and the box (origin, shape, open faces)."""
+    from al_dvc.solver.tiling import plan_tiles, tile_pad
+
+    out = {}
+    for name, (shape, ws, step, rad, extra, edges, dscale, stride) in TILING_CASES.items():
+        para = dvcpara_default(winsize=ws, winstepsize=step, search_radius=rad, verbose=False, **extra)
+        x0, y0, z0 = ref_grid_axes(para.voi, shape, para.winsize, para.winstepsize)
+        mesh = mesh_setup(x0, y0, z0)
+        coords = np.round(mesh.coordinates).astype(np.int64)
+        half = tuple(int(w) // 2 for w in np.broadcast_to(np.asarray(para.winsize), (3,)))
+        rng = np.random.default_rng(7)
+        disp = None if dscale == 0 else dscale * rng.uniform(-1.0, 1.0, size=(len(coords), 3))
+        if disp is not None:
+            disp[::11] = np.nan  # non-finite rows are ignored by the halo
+        nodes = None if stride == 0 else np.arange(3, len(coords), stride)
+        out[f"{name}_grid"] = np.array(mesh.grid_shape)
+        out[f"{name}_coords"] = coords
+        out[f"{name}_ref_pad"] = np.array(tile_pad(para, half))
+        out[f"{name}_def_pad"] = np.array(tile_pad(para, half, disp=disp, deformed=True))
+        if disp is not None:
+            out[f"{name}_disp"] = disp
+        if nodes is not None:
+            out[f"{name}_nodes"] = nodes
+        for e in edges:
+            plan = plan_tiles(mesh.grid_shape, coords, shape, para, half, disp=disp, nodes=nodes, edge=e)
+            key = f"{name}_e{e}"
+            out[f"{key}_count"] = np.array([len(n) for n, _ in plan], dtype=np.int64)
+            out[f"{key}_nodes"] = np.concatenate([n for n, _ in plan]).astype(np.int64)
+            out[f"{key}_origin"] = np.array([b.origin for _, b in plan], dtype=np.int64)
+            out[f"{key}_shape"] = np.array([b.shape for _, b in plan], dtype=np.int64)
+            out[f"{key}_faces"] = np.array([b.open_faces for _, b in plan], dtype=bool)
+            out[f"{key}_fallback"] = np.array(bool(plan.fallback))
+    out["cases"] = np.array(list(TILING_CASES))
+    path = os.path.join(HERE, "golden_tiling.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["kernels", "volume_ops", "init_guess", "strain", "beta", "pass", "ncc_fft"]
+    which = sys.argv[1:] or ["kernels", "volume_ops", "init_guess", "strain", "beta", "pass", "ncc_fft", "tiling"]
     makers = {"kernels": main, "volume_ops": volume_ops_fixtures, "init_guess": init_guess_fixtures, "strain": strain_fixtures,
-              "beta": beta_fixtures, "pass": pass_fixtures, "ncc_fft": ncc_fft_fixtures}
+              "beta": beta_fixtures, "pass": pass_fixtures, "ncc_fft": ncc_fft_fixtures, "tiling": tiling_fixtures}
     for w in which:
         makers[w]()
