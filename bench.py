@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--node-order", default="morton", choices=["morton", "index"],
                     help="persistent IC-GN work queue order")
     ap.add_argument("--no-quads", action="store_true", help="persistent IC-GN samples g itself, not its quad copy")
-    ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute"],
+    ap.add_argument("--edge", type=int, default=512, help="--stage tiled: box edge target (tile_local)")
+    ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute", "tiled"],
                     help="full: the benchmark line; pass / ncc / precompute: timing of one stage on a profiling case "
                          "(human-readable lines, no JSON), see stage_main")
     ap.add_argument("--shape", type=int, nargs=3, default=None, help="volume (nz ny nx) of a --stage case")
@@ -79,7 +80,11 @@ def stage_main(args) -> None:
                 +- --radius (default 17^3 at +-16: the 1024 x 1024 x 306 workload's geometry), nodes every 12 voxels
     precompute  the separable precompute on a 306 x 512 x 512 volume (--shape) of 0.005 / voxel sigma-2 beads, 33^3
                 subsets every 12 voxels (f and three gradients 1.28 GB, larger than L2); --per-node also times the
-                per-node kernel and prints the largest relative difference of H between the forms"""
+                per-node kernel and prints the largest relative difference of H between the forms
+    tiled       the configuration's pass (full size unless --shape) resident on the device, then tiled.run_pass_tiled
+                from host copies of the same frames with boxes of --edge voxels, once keeping the local boxes between
+                stages and once streaming every box again; prints the boxes, the bytes uploaded and the largest
+                difference to the resident result"""
     import torch
 
     from pyaldvc_b200 import configs
@@ -120,6 +125,36 @@ def stage_main(args) -> None:
         it3 = [float(t.double().mean()) for t in getattr(res, "icgn3_iters", [])]
         print(f"{int(res.coords.shape[0])} nodes, mean 12-DOF iterations {float(res.n_iter_local.double().mean()):.3f}, "
               f"mean 3-DOF iterations per pass {[round(v, 3) for v in it3]}")
+        return
+    if args.stage == "tiled":
+        from pyaldvc_b200.pipeline import run_pass
+        from pyaldvc_b200.tiling import run_pass_tiled
+
+        cfg = args.config
+        shape = tuple(args.shape) if args.shape else None
+        p = configs.params(cfg)  # the autotuner's launch shapes, shared by both passes
+        fd, gd, md, _ = configs.device_pair(cfg, shape=shape)
+        f, g = fd.cpu().numpy(), gd.cpu().numpy()
+        mask = None if md is None else md.cpu().numpy()
+        n_vox = f.size
+        for _ in range(args.warmup):
+            whole = run_pass(fd, gd, p, md)
+        whole = timed(f"config {cfg} resident pass on {f.shape}", lambda: run_pass(fd, gd, p, md), 1, "pass")
+        del fd, gd, md
+        torch.cuda.empty_cache()
+        for cache in (None, 0):
+            label = "kept boxes" if cache is None else "no box cache"
+            res = timed(f"config {cfg} tiled pass, edge {args.edge}, {label}",
+                        lambda: run_pass_tiled(f, g, p, mask=mask, edge=args.edge, cache_bytes=cache), 1, "pass")
+            fr = res.frames
+            du = float((res.U - whole.U).abs().max())
+            st = {k: (v["boxes"], v["max_voxels"], v["retried"]) for k, v in res.tiles.stages.items()}
+            print(f"  boxes (count, largest voxels, retried) {st}; {fr.bytes_uploaded / 1e9:.2f} GB uploaded "
+                  f"({fr.bytes_uploaded / (n_vox * f.itemsize):.2f} x the pair), {fr.boxes_loaded} boxes built, "
+                  f"{fr.cache_hits} cache hits; max |U - resident U| {du:.2e}; status equal "
+                  f"{bool((res.status == whole.status).all())}", flush=True)
+            del res, fr
+            torch.cuda.empty_cache()
         return
     if args.stage == "ncc":
         n, h, r = 192, args.half, args.radius

@@ -33,6 +33,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from . import autotune
 from . import beta_tuning as BT
 from . import integer_search as IS
 from . import kernels as K
@@ -588,6 +589,18 @@ def _solve_tiles(plan_fn, solve_fn, status_out, stage: str, record: TileRecord, 
     return retried
 
 
+def _launch_shape(p, ndof: int, mode: int, mesh, masked: bool, plan: TilePlan, run_tile) -> tuple:
+    """(threads, brick_floats) of the tiled IC-GN launches: the caller's, else the autotuner's choice for this kernel
+    and subset (the cache key of the whole-volume pass, so both passes share it), timed on an evenly spread sample
+    of the nodes of the plan's largest tile."""
+    if p.variant != K.BATCHED or p.threads != 0 or not p.autotune or p.node_winsize is not None:
+        return p.threads, p.brick_floats
+    k = autotune.key(ndof, mode, True, mesh.half, p.subset_stride, masked, mesh.n)
+    t = max(plan.tiles, key=lambda t_: len(t_.nodes))
+    sub = t.nodes[autotune.sample_index(len(t.nodes)).cpu().numpy()]
+    return autotune.tune(k, lambda th, br: run_tile(t, sub, (th, br)))
+
+
 def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge: int | None = None,
                    tracer: PL.Tracer | None = None, cache_bytes: int | None = None, slab_voxels: int = SLAB_VOXELS,
                    frames: HostFrames | None = None) -> PL.PassResult:
@@ -693,7 +706,6 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     # ---------------- section 4: local 12-DOF IC-GN, box by box
     quads = mode != 0 and p.variant == K.BATCHED and p.icgn_quads
     rank = _morton_rank(mesh) if (p.variant == K.BATCHED and p.icgn_node_order == "morton") else None
-    th, br = p.threads, p.brick_floats
     P0 = torch.zeros((N, 12), dtype=torch.float64, device="cuda")
     P0[:, 9:] = U0
     P = torch.zeros((N, 12), dtype=torch.float64, device="cuda")
@@ -714,18 +726,25 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
         pads = plan_tiles(mesh.grid_shape, coords_np, frames.shape, p, half, disp=disp, edge=0)
         return plan_fn, _quantised(tuple(max(a, b) for a, b in zip(pads.ref_pad, pads.def_pad)))
 
-    def icgn12_tile(t):
+    shapes = {}
+
+    def icgn12_tile(t, sub=None, shape=None):
+        """Solve tile ``t``; with ``sub`` (some of its nodes) and ``shape`` only time a launch shape (no result kept)."""
+        nodes = t.nodes if sub is None else sub
+        th_, br_ = shapes[12] if shape is None else shape
         v = frames.local_volumes(t.box, quads)
-        idx = torch.from_numpy(t.nodes).cuda()
-        cb = torch.from_numpy(t.box.shift(coords_np[t.nodes])).cuda()
+        idx = torch.from_numpy(nodes).cuda()
+        cb = torch.from_numpy(t.box.shift(coords_np[nodes])).cuda()
         res = K.icgn12(cb, P0[idx], half, v["f"], v["gx"], v["gy"], v["gz"], v["m"], v["g"], mode, L[idx], meanf[idx], valid_u8[idx],
                        p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience, p.subset_stride, None, None, 0.0,
-                       p.icgn_predictive_stop, None, None, p.variant, th, br, node_half=_gather(node_half, idx), g4=v["g4"],
-                       sweep_rows=p.icgn_sweep_rows, node_order=order_of(t.nodes), errs=errs)
-        for dst, src in zip((P, n_iter, status, zncc), res):
-            dst[idx] = src.to(dst.dtype)
+                       p.icgn_predictive_stop, None, None, p.variant, th_, br_, node_half=_gather(node_half, idx), g4=v["g4"],
+                       sweep_rows=p.icgn_sweep_rows, node_order=order_of(nodes), errs=errs if sub is None else None)
+        if sub is None:
+            for dst, src in zip((P, n_iter, status, zncc), res):
+                dst[idx] = src.to(dst.dtype)
 
     plan_fn, pad0 = plan_local(U0.cpu().numpy())
+    shapes[12] = _launch_shape(p, 12, mode, mesh, frames.mask is not None, plan_fn(None, pad0), icgn12_tile)
     _solve_tiles(plan_fn, icgn12_tile, status, "icgn12", record, pad0, extra)
     bad = status != PL.STATUS_CONVERGED
     flag = PL._median_flags(P[:, 9:].contiguous(), ~bad, mesh.grid_shape, p.local_outlier_threshold, errs)
@@ -772,20 +791,25 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
         st = torch.zeros(N, dtype=torch.int8, device="cuda")
         zc = torch.zeros(N, dtype=torch.float64, device="cuda")
 
-        def tile3(t):
+        def tile3(t, sub=None, shape=None):
+            nodes = t.nodes if sub is None else sub
+            th_, br_ = shapes[3] if shape is None else shape
             v = frames.local_volumes(t.box, quads)
-            idx = torch.from_numpy(t.nodes).cuda()
-            cb = torch.from_numpy(t.box.shift(coords_np[t.nodes])).cuda()
+            idx = torch.from_numpy(nodes).cuda()
+            cb = torch.from_numpy(t.box.shift(coords_np[nodes])).cuda()
             res = K.icgn3(cb, U2_[idx], F2_[idx], v_[idx], half, v["f"], v["gx"], v["gy"], v["gz"], v["m"], v["g"], mode, H[idx],
                           meanf[idx], bottomf[idx], valid_u8[idx], p.mu, p.icgn_tol, p.icgn_dp_tol, p.icgn_max_iter, p.icgn_patience,
-                          p.subset_stride, n_full, 0.0, p.icgn_predictive_stop, None, None, p.variant, th, br,
-                          node_half=_gather(node_half, idx), g4=v["g4"], sweep_rows=p.icgn_sweep_rows, node_order=order_of(t.nodes),
-                          errs=errs)
-            for dst, src in zip((U, it, st, zc), res):
-                dst[idx] = src.to(dst.dtype)
+                          p.subset_stride, n_full, 0.0, p.icgn_predictive_stop, None, None, p.variant, th_, br_,
+                          node_half=_gather(node_half, idx), g4=v["g4"], sweep_rows=p.icgn_sweep_rows, node_order=order_of(nodes),
+                          errs=errs if sub is None else None)
+            if sub is None:
+                for dst, src in zip((U, it, st, zc), res):
+                    dst[idx] = src.to(dst.dtype)
 
         # subpb1_solver.py:34: the halo follows the displacement the 3-DOF step starts from, U_hat + vdual
         plan_fn3, pad3 = plan_local((U2_ + v_).cpu().numpy())
+        if 3 not in shapes:
+            shapes[3] = _launch_shape(p, 3, mode, mesh, frames.mask is not None, plan_fn3(None, pad3), tile3)
         _solve_tiles(plan_fn3, tile3, st, "icgn3", record, pad3, extra)
         return U, it, st, zc
 
