@@ -28,6 +28,8 @@ box-local ``x0`` (the reference's own tiling has the same property, tests/test_t
 from __future__ import annotations
 
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -86,6 +88,10 @@ class Box:
         if tuple(vol.shape) == tuple(self.shape):
             return vol
         return np.ascontiguousarray(vol[self.slices])
+
+    def view(self, vol):
+        """The box's voxels of a host array as a view (strided unless the box is the whole volume)."""
+        return vol if tuple(vol.shape) == tuple(self.shape) else vol[self.slices]
 
     def shift(self, coords_xyz) -> np.ndarray:
         """``coords_xyz`` (N, 3) [x, y, z] in the box's frame."""
@@ -310,6 +316,66 @@ def plan_ncc_boxes(coords_xyz, half, radius, shift, volume_shape, edge: int) -> 
 
 
 # --------------------------------------------------------------------------- the frames in host memory
+STAGING_SLOTS = 3  # pinned buffers in the ring: a crop is gathered into one while earlier ones are still copying
+COPY_THREADS = max(1, min(16, os.cpu_count() or 1))  # host threads gathering one crop
+PARALLEL_GATHER_BYTES = 8 << 20  # smaller crops are gathered by one thread
+
+_TORCH_DTYPE = {np.dtype(np.float32): torch.float32, np.dtype(np.uint16): torch.uint16, np.dtype(np.uint8): torch.uint8}
+
+
+class _Staging:
+    """Host -> device copies of box crops: each crop is gathered from its (strided) host view into a pinned buffer by
+    several threads, then copied on a stream of its own, so the copy of the next box overlaps the kernels of the
+    current one.  The compute stream waits for each copy with an event; a pinned buffer is reused once the copy
+    that read it has completed."""
+
+    def __init__(self):
+        self.stream = torch.cuda.Stream()
+        self.slots: list = [(None, None)] * STAGING_SLOTS
+        self.next = 0
+        self.pool = ThreadPoolExecutor(COPY_THREADS) if COPY_THREADS > 1 else None
+
+    def _gather(self, dst: np.ndarray, src: np.ndarray) -> None:
+        if self.pool is None or src.nbytes < PARALLEL_GATHER_BYTES or src.ndim == 0:
+            np.copyto(dst, src)
+            return
+        axis = 0 if src.shape[0] >= COPY_THREADS or src.ndim == 1 else 1
+        n = src.shape[axis]
+        cuts = np.linspace(0, n, min(COPY_THREADS, n) + 1).astype(np.int64)
+
+        def part(k):
+            sl = (slice(None),) * axis + (slice(int(cuts[k]), int(cuts[k + 1])),)
+            np.copyto(dst[sl], src[sl])
+
+        list(self.pool.map(part, range(len(cuts) - 1)))
+
+    def upload(self, a: np.ndarray) -> torch.Tensor:
+        a = np.asarray(a)
+        dt = _TORCH_DTYPE.get(a.dtype)
+        if dt is None:
+            raise TypeError(f"no staging copy for dtype {a.dtype}")
+        k = self.next
+        self.next = (k + 1) % len(self.slots)
+        buf, done = self.slots[k]
+        if done is not None:
+            done.synchronize()  # the copy that last read this buffer has completed
+        nbytes = max(int(a.nbytes), 1)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        self._gather(buf[:nbytes].numpy().view(a.dtype)[: a.size].reshape(a.shape), a)
+        pinned = buf[:nbytes].view(dt)[: a.size].view(a.shape)
+        compute = torch.cuda.current_stream()
+        with torch.cuda.stream(self.stream):
+            dev = torch.empty(a.shape, dtype=dt, device="cuda")
+            dev.copy_(pinned, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(self.stream)
+        compute.wait_event(done)
+        dev.record_stream(compute)
+        self.slots[k] = (buf, done)
+        return dev
+
+
 def slab_ranges(shape, slab_voxels: int, step: int = 1) -> list:
     """z ranges [z0, z1) covering a volume of ``shape``, each of at most ``slab_voxels`` voxels where a multiple of
     ``step`` planes allows it and every one but the last a multiple of ``step`` planes."""
@@ -370,6 +436,7 @@ class HostFrames:
         self.cache_bytes = int(cache_bytes)
         self._cache: dict = {}
         self._cached = 0
+        self._staging = None
         self.stats = {}
         if normalize:
             for name in ("f", "g"):
@@ -377,9 +444,11 @@ class HostFrames:
 
     # ---- host -> device
     def _upload(self, a: np.ndarray) -> torch.Tensor:
-        a = np.ascontiguousarray(a)
+        """A device copy of the host array (or strided view) ``a``, through the pinned staging ring."""
+        if self._staging is None:
+            self._staging = _Staging()
         self.bytes_uploaded += a.nbytes
-        return torch.from_numpy(a).to("cuda")
+        return self._staging.upload(a)
 
     def slabs(self, step: int = 1):
         return slab_ranges(self.shape, self.slab_voxels, step)
@@ -393,7 +462,7 @@ class HostFrames:
         return FrameStats(sums, int(vol.size), pilot)
 
     def _normalised(self, name: str, box: Box) -> torch.Tensor:
-        raw = self._upload(box.crop(getattr(self, name)))
+        raw = self._upload(box.view(getattr(self, name)))
         if not self.normalize:
             return raw.float().contiguous()
         st = self.stats[name]
@@ -561,10 +630,34 @@ def _morton_rank(mesh) -> np.ndarray:
     return rank
 
 
-def _solve_tiles(plan_fn, solve_fn, status_out, stage: str, record: TileRecord, base_pad, extra_pad):
+MARGIN_LO, MARGIN_HI = 1.0, 3.0  # interp_kernels.interp_margin_ok: a sample needs 1 voxel below and 3 above it
+LEFT_VOLUME_TOL = 1e-9  # voxels: far above the FP64 difference between box-local and volume positions
+
+
+def left_volume(P, coords_xyz, half, stride, volume_shape) -> np.ndarray:
+    """Per node (rows of ``P`` (M, 12), the iterate a solve stopped at, and ``coords_xyz`` (M, 3) in the volume's
+    frame) whether a corner voxel of its warped subset lies outside the volume's sampling margin by more than
+    ``LEFT_VOLUME_TOL``.  The reference's sampler fails a node as soon as one unmasked warped voxel leaves that
+    margin (numba_kernels.py:563-576); for a node with no mask whose subset lies inside the volume every voxel is
+    visited and the warp is affine, so the corners decide: such a node fails at the same iterate on the whole
+    volume and needs no retry in a wider box."""
+    P = np.asarray(P, dtype=np.float64).reshape(-1, 12)
+    c = np.asarray(coords_xyz, dtype=np.float64).reshape(-1, 3)
+    hi = [-int(h) + ((2 * int(h)) // int(stride)) * int(stride) for h in half]
+    corners = np.array([[dx, dy, dz] for dz in (-half[2], hi[2]) for dy in (-half[1], hi[1]) for dx in (-half[0], hi[0])],
+                       dtype=np.float64)  # (8, 3) offsets [x, y, z]
+    A = P[:, :9].reshape(-1, 3, 3) + np.eye(3)[None]
+    w = np.einsum("nij,kj->nki", A, corners) + (c + P[:, 9:12])[:, None, :]  # (M, 8, 3) warped [x, y, z]
+    n_xyz = np.array(volume_shape[::-1], dtype=np.float64)
+    out = (w < MARGIN_LO - LEFT_VOLUME_TOL) | (w > n_xyz - MARGIN_HI + LEFT_VOLUME_TOL)
+    return out.any(axis=(1, 2))
+
+
+def _solve_tiles(plan_fn, solve_fn, status_out, stage: str, record: TileRecord, base_pad, extra_pad, left_fn=None):
     """Run ``solve_fn(tile)`` over the tiles of ``plan_fn(nodes, pad)``; nodes whose status says they left an open
     face of their box are planned again with the halo widened by ``extra_pad`` per retry (the reference retries them
-    on the whole volume, local_icgn.py:448-459)."""
+    on the whole volume, local_icgn.py:448-459).  ``left_fn(nodes)`` marks those of them whose last iterate left the
+    volume itself: they would fail on the whole volume too, and are not retried."""
     plan = plan_fn(None, base_pad)
     record.add(stage, [t.box for t in plan])
     open_face = np.zeros(status_out.shape[0], dtype=bool)
@@ -576,6 +669,8 @@ def _solve_tiles(plan_fn, solve_fn, status_out, stage: str, record: TileRecord, 
     for _ in range(ESCAPE_RETRIES):
         st = status_out.cpu().numpy()
         escaped = np.flatnonzero((st == STATUS_OUT_OF_BOUNDS) & open_face)
+        if escaped.size and left_fn is not None:
+            escaped = escaped[~left_fn(escaped)]
         if escaped.size == 0:
             break
         retried += escaped.size
@@ -715,6 +810,27 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     margin = int(p.tile_disp_margin) if p.tile_disp_margin > 0 else int(max(np.broadcast_to(np.asarray(p.winstepsize), (3,))))
     extra = tuple(int(h) + margin for h in half)
 
+    nz_, ny_, nx_ = frames.shape
+    inside = ((coords_np[:, 0] - half[0] >= 0) & (coords_np[:, 0] + half[0] < nx_) & (coords_np[:, 1] - half[1] >= 0)
+              & (coords_np[:, 1] + half[1] < ny_) & (coords_np[:, 2] - half[2] >= 0) & (coords_np[:, 2] + half[2] < nz_))
+
+    def left_of(P_of):
+        """The retry filter of a local step: with no reference mask and one subset shape, the out-of-bounds nodes
+        whose subset lies inside the volume and whose last iterate (``P_of(index tensor)``, (M, 12)) left it."""
+        if frames.mask is not None or node_half is not None:
+            return None
+
+        def left(nodes):
+            out = np.zeros(len(nodes), dtype=bool)
+            keep = inside[nodes]
+            sel = nodes[keep]
+            if sel.size:
+                Pn = P_of(torch.from_numpy(sel).cuda()).cpu().numpy()
+                out[keep] = left_volume(Pn, coords_np[sel], half, p.subset_stride, frames.shape)
+            return out
+
+        return left
+
     def order_of(nodes):
         if rank is None:
             return None
@@ -745,7 +861,7 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
 
     plan_fn, pad0 = plan_local(U0.cpu().numpy())
     shapes[12] = _launch_shape(p, 12, mode, mesh, frames.mask is not None, plan_fn(None, pad0), icgn12_tile)
-    _solve_tiles(plan_fn, icgn12_tile, status, "icgn12", record, pad0, extra)
+    _solve_tiles(plan_fn, icgn12_tile, status, "icgn12", record, pad0, extra, left_of(lambda idx: P[idx]))
     bad = status != PL.STATUS_CONVERGED
     flag = PL._median_flags(P[:, 9:].contiguous(), ~bad, mesh.grid_shape, p.local_outlier_threshold, errs)
     bad = bad | flag
@@ -810,7 +926,7 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
         plan_fn3, pad3 = plan_local((U2_ + v_).cpu().numpy())
         if 3 not in shapes:
             shapes[3] = _launch_shape(p, 3, mode, mesh, frames.mask is not None, plan_fn3(None, pad3), tile3)
-        _solve_tiles(plan_fn3, tile3, st, "icgn3", record, pad3, extra)
+        _solve_tiles(plan_fn3, tile3, st, "icgn3", record, pad3, extra, left_of(lambda idx: torch.cat([F2_[idx], U[idx]], 1)))
         return U, it, st, zc
 
     W = torch.zeros((N, 9), dtype=torch.float64, device="cuda")

@@ -197,3 +197,25 @@ def test_nodes_leaving_an_open_face_are_retried_with_a_wider_halo():
     assert retried > 0 and rec.stages["icgn_retry"]["calls"] == 2  # halos 24 (still short) and 32
     assert int((status != 0).sum()) == 0
     assert sum(rounds) == len(coords) + retried
+
+
+def test_left_volume_decides_on_the_warped_corners():
+    """A node's last iterate leaves the volume when a corner of its warped subset is outside the sampling margin
+    [1, n - 3] (interp_kernels.interp_margin_ok) of the volume; shapes (nz, ny, nx) = (40, 50, 60)."""
+    shape = (40, 50, 60)
+    half, stride = (8, 6, 5), 1
+    c = np.array([[30, 25, 20]] * 6)  # x, y, z
+    P = np.zeros((6, 12))
+    P[1, 9] = 60 - 3 - 38 + 0.5   # x corner 38 + u = 57.5 > 57
+    P[2, 9] = 60 - 3 - 38 - 1e-6  # just inside
+    P[3, 11] = -(28 - 1) - 0.25   # z corner 20 - 8 + w = -15.25 < 1
+    P[4, 0] = 0.3                 # stretch: x corner 30 + 1.3 * 8 = 40.4, inside
+    P[5, 8] = 0.9                 # z stretch alone keeps the corners inside: 20 -+ 1.9 * 8 = 4.8 .. 35.2
+    P[5, 7] = 3.0                 # plus 3 Y: 20 + 1.9 * 8 + 3 * 6 = 53.2 > 37
+    got = T.left_volume(P, c, half, stride, shape)
+    np.testing.assert_array_equal(got, [False, True, False, True, False, True])
+    # with a stride the last sample of an axis stops short of +h: 2h = 16, stride 3 -> offsets -8 .. +7
+    P2 = np.zeros((1, 12))
+    P2[0, 9] = 60 - 3 - 37 - 0.5  # corner at 30 + 7 + u = 56.5: inside with stride 3, outside the +8 corner
+    assert not T.left_volume(P2, c[:1], half, 3, shape)[0]
+    assert T.left_volume(P2, c[:1], half, 1, shape)[0]
