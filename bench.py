@@ -127,6 +127,7 @@ def stage_main(args) -> None:
               f"mean 3-DOF iterations per pass {[round(v, 3) for v in it3]}")
         return
     if args.stage == "tiled":
+        from pyaldvc_b200 import pipeline as PL
         from pyaldvc_b200.pipeline import run_pass
         from pyaldvc_b200.tiling import run_pass_tiled
 
@@ -142,10 +143,14 @@ def stage_main(args) -> None:
         whole = timed(f"config {cfg} resident pass on {f.shape}", lambda: run_pass(fd, gd, p, md), 1, "pass")
         del fd, gd, md
         torch.cuda.empty_cache()
-        for cache in (None, 0):
+        print("resident stages (ms)", {k: round(1e3 * v, 1) for k, v in whole.tracer.stages().items()}, flush=True)
+        torch.cuda.empty_cache()
+        for cache in (0, None):
             label = "kept boxes" if cache is None else "no box cache"
             res = timed(f"config {cfg} tiled pass, edge {args.edge}, {label}",
-                        lambda: run_pass_tiled(f, g, p, mask=mask, edge=args.edge, cache_bytes=cache), 1, "pass")
+                        lambda: run_pass_tiled(f, g, p, mask=mask, edge=args.edge, cache_bytes=cache,
+                                               tracer=PL.Tracer(sync=True)), 1, "pass")
+            print("  stages (ms)", {k: round(1e3 * v, 1) for k, v in res.tracer.stages().items()}, flush=True)
             fr = res.frames
             du = float((res.U - whole.U).abs().max())
             st = {k: (v["boxes"], v["max_voxels"], v["retried"]) for k, v in res.tiles.stages.items()}

@@ -333,6 +333,7 @@ class _Staging:
         self.stream = torch.cuda.Stream()
         self.slots: list = [(None, None)] * STAGING_SLOTS
         self.next = 0
+        self.size = 0  # every slot grows to the largest crop seen, so a later pass allocates nothing
         self.pool = ThreadPoolExecutor(COPY_THREADS) if COPY_THREADS > 1 else None
 
     def _gather(self, dst: np.ndarray, src: np.ndarray) -> None:
@@ -360,8 +361,10 @@ class _Staging:
         if done is not None:
             done.synchronize()  # the copy that last read this buffer has completed
         nbytes = max(int(a.nbytes), 1)
+        self.size = max(self.size, nbytes)
         if buf is None or buf.numel() < nbytes:
-            buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            buf = None
+            buf = torch.empty(self.size, dtype=torch.uint8, pin_memory=True)
         self._gather(buf[:nbytes].numpy().view(a.dtype)[: a.size].reshape(a.shape), a)
         pinned = buf[:nbytes].view(dt)[: a.size].view(a.shape)
         compute = torch.cuda.current_stream()
@@ -374,6 +377,52 @@ class _Staging:
         dev.record_stream(compute)
         self.slots[k] = (buf, done)
         return dev
+
+
+_STAGING: dict = {}  # one ring per device, kept for the process: pinned buffers are slow to allocate
+
+
+def _staging() -> _Staging:
+    d = torch.cuda.current_device()
+    if d not in _STAGING:
+        _STAGING[d] = _Staging()
+    return _STAGING[d]
+
+
+def release_staging() -> None:
+    """Free the pinned staging buffers of every device (the next tiled pass allocates them again)."""
+    for st in _STAGING.values():
+        for _, done in st.slots:
+            if done is not None:
+                done.synchronize()
+    _STAGING.clear()
+
+
+TILE_STREAMS = 2  # box solves alternate over this many streams, so one box's kernel tail overlaps the next box
+
+
+def _tile_streams() -> list:
+    d = torch.cuda.current_device()
+    if d not in _TILE_STREAM_POOL:
+        _TILE_STREAM_POOL[d] = [torch.cuda.Stream() for _ in range(TILE_STREAMS)]
+    return _TILE_STREAM_POOL[d]
+
+
+_TILE_STREAM_POOL: dict = {}
+
+
+def _on_streams(items, fn) -> None:
+    """``fn(item)`` for every item, alternating over the tile streams; each stream starts after the current
+    stream's earlier work and the current stream waits for all of them at the end."""
+    main = torch.cuda.current_stream()
+    streams = _tile_streams()
+    for st in streams:
+        st.wait_stream(main)
+    for i, it in enumerate(items):
+        with torch.cuda.stream(streams[i % len(streams)]):
+            fn(it)
+    for st in streams:
+        main.wait_stream(st)
 
 
 def slab_ranges(shape, slab_voxels: int, step: int = 1) -> list:
@@ -436,7 +485,6 @@ class HostFrames:
         self.cache_bytes = int(cache_bytes)
         self._cache: dict = {}
         self._cached = 0
-        self._staging = None
         self.stats = {}
         if normalize:
             for name in ("f", "g"):
@@ -445,10 +493,8 @@ class HostFrames:
     # ---- host -> device
     def _upload(self, a: np.ndarray) -> torch.Tensor:
         """A device copy of the host array (or strided view) ``a``, through the pinned staging ring."""
-        if self._staging is None:
-            self._staging = _Staging()
         self.bytes_uploaded += a.nbytes
-        return self._staging.upload(a)
+        return _staging().upload(a)
 
     def slabs(self, step: int = 1):
         return slab_ranges(self.shape, self.slab_voxels, step)
@@ -487,6 +533,15 @@ class HostFrames:
             self._cache[key] = vols
             self._cached += nbytes
 
+    def _hit(self, v: dict) -> dict:
+        """A kept box, read by the current stream (which may not be the one that built it)."""
+        self.cache_hits += 1
+        cur = torch.cuda.current_stream()
+        for t in v.values():
+            if isinstance(t, torch.Tensor):
+                t.record_stream(cur)
+        return v
+
     def clear_cache(self):
         self._cache.clear()
         self._cached = 0
@@ -507,8 +562,7 @@ class HostFrames:
         """f, its gradients and the mask over ``box`` (the precompute)."""
         v = self._cache.get(("local", box.origin, box.shape))
         if v is not None:
-            self.cache_hits += 1
-            return v
+            return self._hit(v)
         self.boxes_loaded += 1
         f = self._frame("f", box)
         gx, gy, gz = K.gradients(f)
@@ -521,8 +575,7 @@ class HostFrames:
         key = ("local", box.origin, box.shape)
         v = self._cache.get(key)
         if v is not None and (v["g4"] is not None or not quads):
-            self.cache_hits += 1
-            return v
+            return self._hit(v)
         v = dict(self.reference_volumes(box))
         if self.mode == 2:  # B-spline: prefilter the box grown by the filter's reach, keep the box
             big, inner = box.grown((BSPLINE_REACH,) * 3, self.shape)
@@ -661,8 +714,8 @@ def _solve_tiles(plan_fn, solve_fn, status_out, stage: str, record: TileRecord, 
     plan = plan_fn(None, base_pad)
     record.add(stage, [t.box for t in plan])
     open_face = np.zeros(status_out.shape[0], dtype=bool)
+    _on_streams(plan.tiles, solve_fn)
     for t in plan:
-        solve_fn(t)
         open_face[t.nodes] = t.box.has_open_face
     pad = base_pad
     retried = 0
@@ -678,8 +731,8 @@ def _solve_tiles(plan_fn, solve_fn, status_out, stage: str, record: TileRecord, 
         plan = plan_fn(escaped, pad)
         record.add(stage + "_retry", [t.box for t in plan], escaped.size)
         open_face[:] = False
+        _on_streams(plan.tiles, solve_fn)
         for t in plan:
-            solve_fn(t)
             open_face[t.nodes] = t.box.has_open_face
     return retried
 
@@ -710,7 +763,8 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     tr = tracer if tracer is not None else PL.Tracer(sync=False)
     tr.start()
     errs = K.ErrorWords()
-    if frames is None:
+    own_frames = frames is None
+    if own_frames:
         frames = HostFrames(f, g, p, mask, g_mask, normalize, cache_bytes, slab_voxels)
     edge = int(p.tile_local if edge is None else edge)
     record = TileRecord()
@@ -738,7 +792,8 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     pre_plan = plan_tiles(mesh.grid_shape, coords_np, frames.shape, p, half, edge=edge)
     record.add("precompute", [t.box for t in pre_plan])
     forms = set()
-    for t in pre_plan:
+
+    def precompute_tile(t):
         v = frames.reference_volumes(t.box)
         bz, by, bx = t.box.shape
         idx = torch.from_numpy(t.nodes).cuda()
@@ -756,6 +811,8 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
             forms.add("per_node")
         for dst, src in zip((H, L, meanf, bottomf, n_valid, valid), out):
             dst[idx] = src
+
+    _on_streams(pre_plan.tiles, precompute_tile)
     valid_b = valid != 0
     centre_ok = None
     if frames.mask is not None:
@@ -886,6 +943,8 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     result.frames = frames
     if not p.use_global_step:
         errs.check()
+        if own_frames:
+            frames.clear_cache()
         return result
 
     # ---------------- sections 5-6: ADMM with the 3-DOF step box by box
@@ -959,6 +1018,8 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
         if p.admm_early_stop and (float(du_g.item()) < p.admm_tol or float(du_l.item()) < p.admm_tol):
             break
     errs.check()
+    if own_frames:
+        frames.clear_cache()  # the result keeps the frames' record, not their boxes
     tr.mark("admm")
     result.U = U2
     result.F = F2.reshape(-1, 3, 3)

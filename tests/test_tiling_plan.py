@@ -168,7 +168,7 @@ def test_ncc_boxes_hold_every_read_and_clamp_like_the_volume(edge, shifted):
             assert ((c - h < 0) <= (o_xyz[k] == 0)).all() and ((c + h + 1 > n) <= (o_xyz[k] + n_xyz[k] == n)).all()
 
 
-def test_nodes_leaving_an_open_face_are_retried_with_a_wider_halo():
+def test_nodes_leaving_an_open_face_are_retried_with_a_wider_halo(monkeypatch):
     """The escape retry (local_icgn.py:448-459): a fake solve marks a node out of bounds when its box does not
     hold the 30 voxels its subset needs (clipped by the volume); the plan is repeated for those nodes with the halo
     widened until it does."""
@@ -192,6 +192,8 @@ def test_nodes_leaving_an_open_face_are_retried_with_a_wider_halo():
             ok &= (lo >= t.box.origin[k_zyx]) & (hi <= t.box.origin[k_zyx] + t.box.shape[k_zyx] - 1)
         status[torch.from_numpy(t.nodes)] = torch.from_numpy(np.where(ok, 0, T.STATUS_OUT_OF_BOUNDS).astype(np.int8))
 
+    # the host logic alone: the tiles in turn on the host instead of alternating CUDA streams
+    monkeypatch.setattr(T, "_on_streams", lambda items, fn: [fn(t) for t in items])
     rec = T.TileRecord()
     retried = T._solve_tiles(plan_fn, solve, status, "icgn", rec, (16, 16, 16), (8, 8, 8))
     assert retried > 0 and rec.stages["icgn_retry"]["calls"] == 2  # halos 24 (still short) and 32
