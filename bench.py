@@ -56,6 +56,8 @@ def parse():
                     help="persistent IC-GN work queue order")
     ap.add_argument("--no-quads", action="store_true", help="persistent IC-GN samples g itself, not its quad copy")
     ap.add_argument("--edge", type=int, default=512, help="--stage tiled: box edge target (tile_local)")
+    ap.add_argument("--ncc-engine", default="auto", choices=["auto", "tiled", "fft", "fft_cluster", "plain"],
+                    help="--stage pass: the integer search's engine")
     ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute", "tiled"],
                     help="full: the benchmark line; pass / ncc / precompute: timing of one stage on a profiling case "
                          "(human-readable lines, no JSON), see stage_main")
@@ -113,7 +115,7 @@ def stage_main(args) -> None:
         cfg = args.config
         shape = tuple(args.shape) if args.shape else (200, 384, 384)
         p = configs.params(cfg, icgn_sweep_rows=args.sweep_rows, icgn_node_order=args.node_order,
-                                icgn_quads=not args.no_quads)
+                                icgn_quads=not args.no_quads, ncc_engine=args.ncc_engine)
         if args.icgn_threads:
             p.threads, p.brick_floats = args.icgn_threads, 0
         if args.icgn_staged:

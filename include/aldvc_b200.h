@@ -316,6 +316,10 @@ int aldvc_ncc_map(const float *f, const float *g, int64_t nz, int64_t ny, int64_
 /* the FFT engine with its shared-memory Stockham transforms for every box (the in-register transforms of cubic
  * boxes of length 36, 40, 48, 50, 54, 60 or 64 turned off): a comparison form */
 #define ALDVC_NCC_FFT_STOCKHAM 3
+/* the FFT engine for cubic boxes of length 36, 40, 48, 50 or 54 as one thread-block cluster kernel per node: the
+ * node's spectrum stays in the distributed shared memory of 8 CTAs instead of an HBM scratch (other boxes run
+ * as ALDVC_NCC_FFT) */
+#define ALDVC_NCC_FFT_CLUSTER 4
 
 size_t aldvc_ncc_search_workspace_size(int64_t nz, int64_t ny, int64_t nx, int64_t n_nodes, int32_t hx, int32_t hy, int32_t hz,
                                        int32_t rx, int32_t ry, int32_t rz, int32_t engine);

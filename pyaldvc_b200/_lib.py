@@ -19,6 +19,7 @@ NCC_TILED = 0
 NCC_PLAIN = 1
 NCC_FFT = 2
 NCC_FFT_STOCKHAM = 3
+NCC_FFT_CLUSTER = 4
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32

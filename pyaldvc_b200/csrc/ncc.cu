@@ -8,6 +8,8 @@
 // aldvc_ncc_search: window placement, map, first-maximum argmax (C order), PCE, clipped flag, FP64
 //   re-scoring of every offset within NEAR_TIE of the FP32 maximum and of the 27-point neighbourhood of
 //   the winner, quadratic sub-voxel fit -- all on the device, in node chunks through a workspace.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -2012,6 +2014,313 @@ __global__ void __launch_bounds__(fftr_pass3_threads<N>()) fftr_pass3_kernel(Fft
     }
 }
 
+// ---- cubic boxes, one thread-block cluster per node: the three passes above without their HBM scratch.  The
+// node's whole spectrum (N^3 complex, 1 MB for N = 50) lives in the distributed shared memory of a cluster of C
+// CTAs, PP = ceil(N / C) z-planes each:
+//   1. CTA r transforms its window planes [r PP, r PP + PP) along x and y in its own shared memory (pass 1);
+//   2. after a cluster barrier, thread (row, column) of CTA r gathers the z-line of one (ky, kx) column of its
+//      rows from all C CTAs (ld through DSMEM), transforms it along z and keeps it in registers; after a second
+//      barrier the lines are parked in the CTA's own tile, the product W^ conj T^ is formed from row ky and its
+//      partner row -ky (the rows of a pair belong to one CTA) and inverted along z (pass 2); after a third barrier
+//      the output planes dz < vz are written straight into the shared memory of the CTA that owns them (p3 planes
+//      each, the Hermitian half ky <= N/2 only);
+//   3. after a fourth barrier each CTA inverts its output planes along y and x, normalises them and writes the map
+//      and its partials (pass 3, one block of partials per CTA).
+// Every line goes through the same fft_line calls in the same order as in the three-pass engine, so the maps are
+// identical.  Only the map and its partials reach HBM; the window and template rows are read as in pass 1.
+// The barriers are the hardware cluster barrier (no spin loop); every CTA of a cluster takes all of them, or
+// leaves before the first one together with the others (the node is the same for the whole cluster).
+namespace cg = cooperative_groups;
+
+constexpr int FFTC_C = 8;         // CTAs per cluster (the portable maximum)
+constexpr int FFTC_MAX_ROWS = 8;  // spectrum rows (ky) per CTA in the z phase
+
+// rows of the z phase: CTA r owns nrows[r] rows ky[r][.], each with the local index of its partner row (N - ky) % N
+struct FftcRows {
+    signed char nrows[FFTC_C];
+    signed char ky[FFTC_C][FFTC_MAX_ROWS];
+    signed char partner[FFTC_C][FFTC_MAX_ROWS];
+};
+
+template <int N>
+struct FftcShape {
+    static constexpr int PP = (N + FFTC_C - 1) / FFTC_C;  // z-planes per CTA in the forward phase
+    static constexpr int PITCH = N | 1;
+    static constexpr int NH = N / 2 + 1;
+    static constexpr int RP = NH | 1;
+    static constexpr int THREADS = (PP * N + 31) / 32 * 32;
+    static constexpr size_t SMEM = (size_t)PP * N * PITCH * sizeof(float2);
+};
+
+// -2 everywhere (the unplaced-node marker) in this CTA's output planes, and the matching partial
+__device__ __forceinline__ void fftc_unplaced(const FftArgs& a, int blk, int dz0, int np3) {
+    const NccGeom& G = a.G;
+    float* out = a.out + (int64_t)blockIdx.y * G.nmap + (int64_t)dz0 * G.vy * G.vx;
+    for (int i = threadIdx.x; i < np3 * G.vy * G.vx; i += blockDim.x) out[i] = -2.0f;
+    if (a.part && threadIdx.x == 0) {
+        MapPart q;
+        q.s1 = q.s2 = 0.0;
+        q.mx = q.mn = 0.0f;
+        q.idx = dz0 * G.vy * G.vx;
+        q.pad = 0;
+        a.part[(int64_t)blockIdx.y * a.nblk + blk] = q;
+    }
+}
+
+template <int N>
+__global__ void __cluster_dims__(FFTC_C, 1, 1) __launch_bounds__(FftcShape<N>::THREADS, 1)
+    fftc_kernel(FftArgs a, FftcRows rows, int p3) {
+    using Sh = FftcShape<N>;
+    constexpr int PP = Sh::PP, PITCH = Sh::PITCH, NH = Sh::NH, RP = Sh::RP;
+    extern __shared__ __align__(16) float2 fsm[];  // forward: [PP][N][PITCH]; z phase: [rows][N][PITCH]; output:
+                                                   // [p3][NH][N] then the pass-3 tile [p3][N][RP]
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const NccGeom& G = a.G;
+    const int64_t node = a.node_base + blockIdx.y;
+    const int dz0 = rank * p3;
+    const int np3 = max(0, min(p3, G.vz - dz0));
+    if (!fft_node_ok(a, node)) {  // the same for every CTA of the cluster: all leave before the first barrier
+        if (np3 > 0) fftc_unplaced(a, rank, dz0, np3);
+        return;
+    }
+    const int t = threadIdx.x;
+    const int64_t sxy = (int64_t)G.nx * G.ny;
+    const int64_t wx0 = a.wx0[node], wy0 = a.wy0[node], wz0 = a.wz0[node];
+    // ---------------- phase 1: this CTA's window planes along x, then along y
+    {
+        const int z0 = rank * PP;
+        const int np = max(0, min(PP, G.wz - z0));  // planes past the window are zero and never read
+        const float pilot = __ldg(a.pilot_at);
+        const int pl = t / N, yx = t - pl * N;
+        const int O = (int)(wx0 & 3);
+        const bool vec = (G.nx & 3) == 0 && (reinterpret_cast<uintptr_t>(a.g) & 15) == 0;
+        const float* gend = a.g + (int64_t)G.nz * sxy;
+        if (pl < np) {
+            const int z = z0 + pl, y = yx;
+            float2 v[N];
+            const float* wrow = a.g + (wz0 + z) * sxy + (wy0 + y) * G.nx + wx0;
+            const float* trow = a.T + (int64_t)blockIdx.y * G.sz * G.sy * a.sxp + ((int64_t)z * G.sy + y) * a.sxp;
+            const bool wy_in = y < G.wy, ty_in = z < G.sz && y < G.sy;
+            const bool vrow = vec && wy_in && wrow - O + 4 * ((G.wx + O + 3) / 4) <= gend;
+            if (vrow) {
+                switch (O) {
+                    case 0: fftr_row4<N, 0>(wrow, G.wx, pilot, v); break;
+                    case 1: fftr_row4<N, 1>(wrow - 1, G.wx, pilot, v); break;
+                    case 2: fftr_row4<N, 2>(wrow - 2, G.wx, pilot, v); break;
+                    default: fftr_row4<N, 3>(wrow - 3, G.wx, pilot, v); break;
+                }
+            } else {
+#pragma unroll
+                for (int x = 0; x < N; ++x) v[x].x = (wy_in && x < G.wx) ? __ldg(wrow + x) - pilot : 0.0f;
+            }
+            if (ty_in && (a.sxp & 3) == 0) {
+                fftr_trow4<N>(trow, G.sx, v);
+            } else {
+#pragma unroll
+                for (int x = 0; x < N; ++x) v[x].y = (ty_in && x < G.sx) ? __ldg(trow + x) : 0.0f;
+            }
+            if (wy_in) fft_line<N, -1>(v);
+            float2* row = fsm + (pl * N + y) * PITCH;
+#pragma unroll
+            for (int x = 0; x < N; ++x) row[x] = v[x];
+        }
+        __syncthreads();
+        if (pl < np) {
+            float2* col = fsm + pl * N * PITCH + yx;
+            float2 v[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) v[k] = col[k * PITCH];
+            fft_line<N, -1>(v);
+#pragma unroll
+            for (int k = 0; k < N; ++k) col[k * PITCH] = v[k];
+        }
+        // the box sums of this CTA's output planes are read at the end: start them towards L2
+        const int nch = (G.vx + 31) / 32, per_row = 2 * nch;
+        for (int i = t; i < np3 * G.vy * per_row; i += blockDim.x) {
+            const int r = i / per_row, rem = i - r * per_row, p_ = r / G.vy, dy = r - p_ * G.vy;
+            const float* b = (rem & 1) ? a.B2 : a.B1;
+            prefetch_l2(b + (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + wx0 + 32 * (rem >> 1));
+        }
+    }
+    cl.sync();  // barrier 1: every plane spectrum of the node is in the cluster
+    // ---------------- phase 2: thread (r, c) transforms the z-line of column c of this CTA's row r
+    const int nr = rows.nrows[rank];
+    const int r = t / N, c = t - r * N;
+    const bool has = r < nr;
+    const int ky = has ? (int)rows.ky[rank][r] : 0;
+    float2 v[N];
+    if (has) {
+        const float2* src[FFTC_C];
+#pragma unroll
+        for (int q = 0; q < FFTC_C; ++q) src[q] = cl.map_shared_rank(fsm, q) + ky * PITCH + c;
+#pragma unroll
+        for (int z = 0; z < N; ++z) v[z] = z < G.wz ? src[z / PP][(z % PP) * N * PITCH] : make_float2(0.0f, 0.0f);
+        fft_line<N, -1>(v);
+    }
+    cl.sync();  // barrier 2: every CTA has read the plane spectra it needs; the tiles are free
+    if (has) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) fsm[(r * N + k) * PITCH + c] = v[k];
+    }
+    __syncthreads();
+    const bool top = has && ky <= N / 2;  // the product is Hermitian: rows ky <= N/2 hold all of it
+    if (top) {
+        const float2* pb = fsm + (int)rows.partner[rank][r] * N * PITCH + (N - c) % N;
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            const float2 za = v[kz];
+            const float2 zb = pb[((N - kz) % N) * PITCH];
+            const float2 zbc = make_float2(zb.x, -zb.y);
+            const float2 w = make_float2(0.5f * (za.x + zbc.x), 0.5f * (za.y + zbc.y));
+            const float2 d = make_float2(za.x - zbc.x, za.y - zbc.y);
+            const float2 tc = make_float2(0.5f * d.y, 0.5f * d.x);  // conj(T^) = i conj(za - zbc) / 2
+            v[kz] = fr_mul(w, tc);
+        }
+        fft_line<N, 1>(v);
+    }
+    cl.sync();  // barrier 3: every CTA is done with its own lines; output planes may be written anywhere
+    if (top) {  // output plane dz to CTA dz / p3, plane dz % p3 of its [p3][NH][N] block
+        int owner = 0, dzl = 0;
+        float2* dst = cl.map_shared_rank(fsm, 0) + ky * N + c;
+#pragma unroll
+        for (int dz = 0; dz < N; ++dz) {
+            if (dz < G.vz) {
+                dst[dzl * NH * N] = v[dz];
+                if (++dzl == p3) {
+                    dzl = 0;
+                    ++owner;
+                    if (owner < FFTC_C) dst = cl.map_shared_rank(fsm, owner) + ky * N + c;
+                }
+            }
+        }
+    }
+    cl.sync();  // barrier 4: every output plane is in place; no CTA touches another's memory after this
+    if (np3 == 0) return;
+    // ---------------- phase 3: inverse along y of columns kx <= N/2 (rows ky > N/2 as conjugates), then along x of
+    // real row pairs, normalisation, map rows and the block's partials (as fftr_pass3_kernel)
+    float2* tile = fsm + (size_t)p3 * NH * N;  // [p3][N][RP]
+    {
+        const int pl = t / NH, kx = t - pl * NH;
+        if (pl < np3) {
+            const float2* pg = fsm + pl * NH * N;
+            const int kxm = (N - kx) % N;
+#pragma unroll
+            for (int k = 0; k < NH; ++k) v[k] = pg[k * N + kx];
+#pragma unroll
+            for (int k = NH; k < N; ++k) {
+                const float2 w = pg[(N - k) * N + kxm];
+                v[k] = make_float2(w.x, -w.y);
+            }
+            fft_line<N, 1>(v);
+            float2* col = tile + pl * N * RP + kx;
+#pragma unroll
+            for (int k = 0; k < N; ++k) col[k * RP] = v[k];
+        }
+        __syncthreads();
+        const int nj = (G.vy + 1) / 2;
+        if (pl < np3 && kx < nj) {
+            float2* ra = tile + (pl * N + 2 * kx) * RP;
+            float2* rb = ra + RP;
+            const bool hb = 2 * kx + 1 < G.vy;
+#pragma unroll
+            for (int k = 0; k < NH; ++k) {
+                const float2 xa = ra[k], xb = hb ? rb[k] : make_float2(0.0f, 0.0f);
+                v[k] = make_float2(xa.x - xb.y, xa.y + xb.x);
+            }
+#pragma unroll
+            for (int k = NH; k < N; ++k) {
+                const float2 xa = ra[N - k], xb = hb ? rb[N - k] : make_float2(0.0f, 0.0f);
+                v[k] = make_float2(xa.x + xb.y, xb.x - xa.y);
+            }
+            fft_line<N, 1>(v);
+            float* ma = reinterpret_cast<float*>(ra);
+            float* mb = reinterpret_cast<float*>(rb);
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+                if (k < G.vx) {
+                    ma[k] = v[k].x;
+                    if (hb) mb[k] = v[k].y;
+                }
+        }
+        __syncthreads();
+    }
+    float* out = a.out + (int64_t)blockIdx.y * G.nmap + (int64_t)dz0 * G.vy * G.vx;
+    const double scale = 1.0 / ((double)N * N * N);
+    const double ssf = a.ssf[blockIdx.y], n_tpl = (double)G.n_tpl;
+    const float fscale = (float)scale;
+    const double inv_n = 1.0 / n_tpl;
+    const float* msm = reinterpret_cast<const float*>(tile);
+    float lmx = -3.0f, lmn = 3.0f;
+    int lidx = 0x7fffffff;
+    double ls1 = 0.0, ls2 = 0.0;
+    const int i0 = dz0 * G.vy * G.vx;
+    sweep_lin<4, float2>(
+        np3 * G.vy, G.vx,
+        [&](int rr, int dx) {
+            const int p_ = (int)(((float)rr + 0.5f) / (float)G.vy), dy = rr - p_ * G.vy;
+            const int64_t o = (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
+            return make_float2(__ldg(a.B1 + o), __ldg(a.B2 + o));
+        },
+        [&](int rr, int dx, float2 bs) {
+            const int p_ = (int)(((float)rr + 0.5f) / (float)G.vy), dy = rr - p_ * G.vy;
+            const double s1 = (double)bs.x;
+            const double var = (double)bs.y - s1 * s1 * inv_n;
+            float vv = 0.0f;
+            if (!(var < 1e-20)) {
+                vv = msm[2 * (p_ * N + dy) * RP + dx] * fscale * rsqrtf((float)(var * ssf));
+                vv = fminf(1.0f, fmaxf(-1.0f, vv));
+            }
+            out[(int64_t)p_ * G.vy * G.vx + dy * G.vx + dx] = vv;
+            if (vv > lmx) {
+                lmx = vv;
+                lidx = i0 + rr * G.vx + dx;
+            }
+            lmn = fminf(lmn, vv);
+            ls1 += (double)vv;
+            ls2 += (double)vv * (double)vv;
+        });
+    if (a.part) {
+        __shared__ MapPart wpart[Sh::THREADS / 32];
+        const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, lmx, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, lidx, o);
+            if (ob > lmx || (ob == lmx && oi < lidx)) {
+                lmx = ob;
+                lidx = oi;
+            }
+            lmn = fminf(lmn, __shfl_xor_sync(0xffffffffu, lmn, o));
+            ls1 += __shfl_xor_sync(0xffffffffu, ls1, o);
+            ls2 += __shfl_xor_sync(0xffffffffu, ls2, o);
+        }
+        if (lane == 0) {
+            wpart[warp].mx = lmx;
+            wpart[warp].idx = lidx;
+            wpart[warp].mn = lmn;
+            wpart[warp].s1 = ls1;
+            wpart[warp].s2 = ls2;
+        }
+        __syncthreads();
+        if (t == 0) {
+            MapPart q = wpart[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                const MapPart o = wpart[w];
+                if (o.mx > q.mx || (o.mx == q.mx && o.idx < q.idx)) {
+                    q.mx = o.mx;
+                    q.idx = o.idx;
+                }
+                q.mn = fminf(q.mn, o.mn);
+                q.s1 += o.s1;
+                q.s2 += o.s2;
+            }
+            q.pad = 0;
+            a.part[(int64_t)blockIdx.y * a.nblk + rank] = q;
+        }
+    }
+}
+
 // twiddles of the in-register transforms, once per device (before any capture: the first FFT search does it)
 static int fftr_upload() {
     static std::mutex mu;
@@ -2070,6 +2379,32 @@ static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     return check_launch("ncc fft pass 3");
 }
 
+template <int N>
+static int launch_fftc(FftArgs& a, const FftcRows& rows, int p3, int nb, cudaStream_t s) {
+    using Sh = FftcShape<N>;
+    static bool attr = false;  // set once, outside any capture (the first search of this length)
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(fftc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc fft cluster: shared memory attribute");
+        attr = true;
+    }
+    {
+        KTimer kt_("fft_cluster", s);
+        fftc_kernel<N><<<dim3(FFTC_C, nb), Sh::THREADS, Sh::SMEM, s>>>(a, rows, p3);
+    }
+    return check_launch("ncc fft cluster");
+}
+
+static int launch_fftc_n(int n, FftArgs& a, const FftcRows& rows, int p3, int nb, cudaStream_t s) {
+    switch (n) {
+        case 36: return launch_fftc<36>(a, rows, p3, nb, s);
+        case 40: return launch_fftc<40>(a, rows, p3, nb, s);
+        case 48: return launch_fftc<48>(a, rows, p3, nb, s);
+        case 50: return launch_fftc<50>(a, rows, p3, nb, s);
+        default: return launch_fftc<54>(a, rows, p3, nb, s);
+    }
+}
+
 // map planes per pass-3 CTA of the in-register engine (the block of one map partial)
 static int fftr_planes3_n(int n) {
     switch (n) {
@@ -2097,22 +2432,81 @@ static int launch_fftr_n(int n, FftArgs& a, int nb, cudaStream_t s) {
 
 struct FftCfg {
     FftAxis ax, ay, az;
-    bool reg;  // cubic box of a length with an in-register transform (fftr passes)
+    bool reg;      // cubic box of a length with an in-register transform (fftr passes)
+    bool cluster;  // ... run as one cluster kernel per node (fftc_kernel): no spectra scratch
+    int p3;        // cluster form: output planes per CTA (the map block of one partial)
+    FftcRows rows; // cluster form: rows of the z phase per CTA
     int pitch;
     size_t smem13, smem2;  // dynamic shared bytes of passes 1/3 and 2
     int64_t per_node;      // scratch bytes per node (A and P)
 };
 
-static bool fft_config(const NccGeom& G, FftCfg& c, bool engine_reg = true) {
+// Cluster form of a cubic box of length n: the threads and shared bytes of fftc_kernel<n>, 0 when n has none
+static void fftc_shape(int n, int& threads, size_t& smem) {
+    threads = 0;
+    smem = 0;
+    switch (n) {
+        case 36: threads = FftcShape<36>::THREADS; smem = FftcShape<36>::SMEM; break;
+        case 40: threads = FftcShape<40>::THREADS; smem = FftcShape<40>::SMEM; break;
+        case 48: threads = FftcShape<48>::THREADS; smem = FftcShape<48>::SMEM; break;
+        case 50: threads = FftcShape<50>::THREADS; smem = FftcShape<50>::SMEM; break;
+        case 54: threads = FftcShape<54>::THREADS; smem = FftcShape<54>::SMEM; break;
+        default: break;
+    }
+}
+
+// The z-phase rows of the cluster form: the pairs (ky, N - ky) and the single rows 0 and N/2 dealt to the CTAs so
+// that no CTA holds more than PP rows (its plane tile holds PP x N lines) and a pair stays in one CTA (the
+// product needs both rows).  False when they do not fit.
+static bool fftc_rows(int n, int pp, FftcRows& r) {
+    std::memset(&r, 0, sizeof(r));
+    const int cap = std::min(pp, FFTC_MAX_ROWS);
+    auto put = [&](int ky0, int ky1) {  // ky1 < 0: a single row
+        const int need = ky1 < 0 ? 1 : 2;
+        int best = -1;
+        for (int q = 0; q < FFTC_C; ++q)  // the emptiest CTA with room
+            if (r.nrows[q] + need <= cap && (best < 0 || r.nrows[q] < r.nrows[best])) best = q;
+        if (best < 0) return false;
+        const int i0 = r.nrows[best];
+        r.ky[best][i0] = (signed char)ky0;
+        r.partner[best][i0] = (signed char)(ky1 < 0 ? i0 : i0 + 1);
+        if (ky1 >= 0) {
+            r.ky[best][i0 + 1] = (signed char)ky1;
+            r.partner[best][i0 + 1] = (signed char)i0;
+        }
+        r.nrows[best] = (signed char)(i0 + need);
+        return true;
+    };
+    for (int k = 1; k < (n + 1) / 2; ++k)
+        if (k != n - k && !put(k, n - k)) return false;
+    if (!put(0, -1)) return false;
+    if (n % 2 == 0 && !put(n / 2, -1)) return false;
+    return true;
+}
+
+static bool fftc_config(const NccGeom& G, FftCfg& c) {
+    const int n = c.ax.n;
+    int threads;
+    size_t smem;
+    fftc_shape(n, threads, smem);
+    if (threads == 0 || G.wz > n || G.vz > n) return false;
+    const int pp = (n + FFTC_C - 1) / FFTC_C, nh = n / 2 + 1;
+    c.p3 = (G.vz + FFTC_C - 1) / FFTC_C;
+    const size_t out_tile = ((size_t)c.p3 * nh * n + (size_t)c.p3 * n * (nh | 1)) * sizeof(float2);
+    return out_tile <= smem && c.p3 * nh <= threads && smem <= (size_t)max_smem_optin() - 2048 && fftc_rows(n, pp, c.rows);
+}
+
+static bool fft_config(const NccGeom& G, FftCfg& c, bool engine_reg = true, bool engine_cluster = false) {
     if (!fft_axis(smooth_len(G.wx), c.ax) || !fft_axis(smooth_len(G.wy), c.ay) || !fft_axis(smooth_len(G.wz), c.az)) return false;
     c.reg = engine_reg && c.ax.n == c.ay.n && c.ax.n == c.az.n && fftr_supported(c.ax.n);
+    c.cluster = c.reg && engine_cluster && fftc_config(G, c);
     c.pitch = c.ax.n | 1;  // odd: rows and columns of a plane fall in distinct bank pairs
     c.smem13 = ((size_t)2 * c.ay.n * c.pitch + 2 * FFT_MAX_N) * sizeof(float2);
     // pass 2: two buffers of one whole row (Nz x pitch) or of two half rows (2 x Nz x (cb | 1))
     c.smem2 = ((size_t)2 * std::max(c.pitch, 2 * (((c.ax.n + 1) / 2) | 1)) * c.az.n + FFT_MAX_N) * sizeof(float2);
     // the in-register passes keep the product rows ky <= N/2 only
     const int64_t p_rows = c.reg ? c.ay.n / 2 + 1 : c.ay.n;
-    c.per_node = ((int64_t)G.wz * c.ay.n + (int64_t)G.vz * p_rows) * c.ax.n * (int64_t)sizeof(float2);
+    c.per_node = c.cluster ? 0 : ((int64_t)G.wz * c.ay.n + (int64_t)G.vz * p_rows) * c.ax.n * (int64_t)sizeof(float2);
     const size_t smax = (size_t)max_smem_optin() - 4096;
     return c.smem13 <= smax && c.smem2 <= smax;
 }
@@ -2129,7 +2523,7 @@ static int64_t fft_batch_bytes() {
 }
 
 static int64_t fft_batch(const FftCfg& c, int64_t chunk) {
-    const int64_t b = std::min<int64_t>(chunk, fft_batch_bytes() / std::max<int64_t>(c.per_node, 1));
+    const int64_t b = c.cluster ? chunk : std::min<int64_t>(chunk, fft_batch_bytes() / std::max<int64_t>(c.per_node, 1));
     return std::max<int64_t>(1, std::min<int64_t>(b, 65535));  // grid y limit
 }
 
@@ -2171,7 +2565,7 @@ static int launch_fft(FftArgs a, const FftCfg& c, int64_t n, int64_t batch, cuda
         a.T = T0 + done * tsz;
         a.nb = nb;
         if (c.reg) {
-            rc = launch_fftr_n(c.ax.n, a, nb, s);
+            rc = c.cluster ? launch_fftc_n(c.ax.n, a, c.rows, c.p3, nb, s) : launch_fftr_n(c.ax.n, a, nb, s);
             if (rc) return rc;
             continue;
         }
@@ -2301,19 +2695,23 @@ extern "C" int aldvc_ncc_map(const float* f, const float* g, int64_t nz, int64_t
     return launch_map(m, n_nodes, (cudaStream_t)stream);
 }
 
+// map planes of one partial block: a pass-3 CTA's, or a cluster CTA's output planes
+static int fft_blk_planes(const FftCfg& c) { return c.cluster ? c.p3 : fftr_planes3_n(c.ax.n); }
+
 static int fft_nblk(const NccGeom& G, const FftCfg& c) {
-    const int p3 = fftr_planes3_n(c.ax.n);
+    const int p3 = fft_blk_planes(c);
     return (G.vz + p3 - 1) / p3;
 }
 
 static bool use_fft(const NccGeom& G, int32_t engine, FftCfg& c) {
-    return (engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM) && fft_config(G, c, engine == ALDVC_NCC_FFT);
+    const bool fft = engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM || engine == ALDVC_NCC_FFT_CLUSTER;
+    return fft && fft_config(G, c, engine != ALDVC_NCC_FFT_STOCKHAM, engine == ALDVC_NCC_FFT_CLUSTER);
 }
 
 // TILED, or FFT on a geometry the FFT engine does not take
 static bool use_tiled(const NccGeom& G, int32_t engine, TiledCfg& c) {
     FftCfg fc;
-    const bool fft = engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM;
+    const bool fft = engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM || engine == ALDVC_NCC_FFT_CLUSTER;
     return (engine == ALDVC_NCC_TILED || (fft && !fft_config(G, fc))) && tiled_config(G, c);
 }
 
@@ -2356,7 +2754,8 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
                                 const int64_t* shift0, int32_t engine, void* workspace, size_t workspace_bytes, double* disp,
                                 double* cc, double* pce, uint8_t* clipped, uint8_t* ok, void* stream) {
     ALDVC_REQUIRE(f && g && coords && disp && cc && pce && clipped && ok, "aldvc_ncc_search: null pointer");
-    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN || engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM,
+    ALDVC_REQUIRE(engine == ALDVC_NCC_TILED || engine == ALDVC_NCC_PLAIN || engine == ALDVC_NCC_FFT || engine == ALDVC_NCC_FFT_STOCKHAM ||
+                      engine == ALDVC_NCC_FFT_CLUSTER,
                   "aldvc_ncc_search: unknown engine");
     const NccGeom G = make_geom(nz, ny, nx, hx, hy, hz, rx, ry, rz);
     int rc = check_geom(G);
@@ -2493,7 +2892,7 @@ extern "C" int aldvc_ncc_search(const float* f, const float* g, int64_t nz, int6
                 fa.part = (MapPart*)((char*)scr + align_up((size_t)batch * fc.per_node, 256));
                 a.part = fa.part;
                 a.nblk = fa.nblk;
-                a.blk_planes = fftr_planes3_n(fc.ax.n);
+                a.blk_planes = fft_blk_planes(fc);
             }
             fa.n_nodes = n_nodes;
             fa.G = G;

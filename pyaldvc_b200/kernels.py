@@ -20,6 +20,7 @@ NCC_TILED = _lib.NCC_TILED
 NCC_PLAIN = _lib.NCC_PLAIN
 NCC_FFT = _lib.NCC_FFT
 NCC_FFT_STOCKHAM = _lib.NCC_FFT_STOCKHAM
+NCC_FFT_CLUSTER = _lib.NCC_FFT_CLUSTER
 INTERP_MODE_BY_NAME = {"linear": 0, "cubic": 1, "bspline": 2}
 
 

@@ -65,7 +65,7 @@ class PassParams:
     icgn_node_order: str = "morton"  # persistent IC-GN work queue: "morton" (nodes near each other solved together) or "index"
     icgn_quads: bool = True  # cubic / B-spline persistent IC-GN: sample g through its overlapping-quad copy
     graph: bool = False
-    ncc_engine: str = "auto"  # auto | tiled | fft | plain
+    ncc_engine: str = "auto"  # auto | tiled | fft | fft_cluster | plain
     # uneven subsets: coords (N,3) [x, y, z] -> (N,3) even window sizes per node, each <= winsize (which then
     # sets the mesh border and the maximum shape); every shape runs in the same persistent launches
     node_winsize: object = None
@@ -211,8 +211,8 @@ def _ncc_engine(p: PassParams, half, radius) -> int:
     engine for searches of more than ``FFT_NCC_MIN_OPS`` multiply-adds per node, else the tiled direct engine."""
     if p.variant == K.PLAIN or p.ncc_engine == "plain":
         return K.NCC_PLAIN
-    if p.ncc_engine in ("tiled", "fft"):
-        return K.NCC_TILED if p.ncc_engine == "tiled" else K.NCC_FFT
+    if p.ncc_engine in ("tiled", "fft", "fft_cluster"):
+        return {"tiled": K.NCC_TILED, "fft": K.NCC_FFT, "fft_cluster": K.NCC_FFT_CLUSTER}[p.ncc_engine]
     n_tpl = np.prod([2 * int(h) + 1 for h in half])
     n_off = np.prod([2 * int(r) + 1 for r in radius])
     return K.NCC_FFT if n_tpl * n_off > FFT_NCC_MIN_OPS else K.NCC_TILED

@@ -25,7 +25,7 @@ import pass_inputs as PI  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-ENGINES = {"tiled": 0, "plain": 1, "fft": 2, "fft_stockham": 3}
+ENGINES = {"tiled": 0, "plain": 1, "fft": 2, "fft_stockham": 3, "fft_cluster": 4}
 NEAR_TIE = 1e-5
 
 
@@ -111,3 +111,20 @@ def test_ncc_expansion_matches_reference_fft_branch(oracle_mod, gn, ncc_in, engi
     ref = {k: gn[f"expand_{k}"] for k in ("disp", "cc", "pce", "clipped", "ok")}
     n_ties = _compare(oracle_mod, f, g, coords, None, PI.NCC_EXPAND["subset"], tuple(res["radius"]), res, ref, f"expand/{engine}")
     assert n_ties <= 0.02 * len(coords)
+
+
+@pytest.mark.parametrize("name", ["r16", "r9"])
+def test_cluster_engine_equals_three_pass_engine(gn, ncc_in, name):
+    """The cluster form runs every line through the same transforms in the same order as the three passes of the
+    in-register engine: identical integer peaks, sub-voxel displacements and peak values.  The PCE energy sums the
+    map in other blocks (a cluster CTA's planes instead of a pass-3 CTA's), so it agrees to FP64 rounding.  At +-9
+    the 36-point box takes the three passes in both (its row pairs do not fit one cluster)."""
+    from pyaldvc_b200.integer_search import ncc_search
+
+    f, g, coords, shift = ncc_in
+    c = PI.NCC_SEARCHES[name]
+    a = ncc_search(f, g, coords, c["subset"], c["radius"], shift, engine=ENGINES["fft"])
+    b = ncc_search(f, g, coords, c["subset"], c["radius"], shift, engine=ENGINES["fft_cluster"])
+    for k in ("ok", "clipped", "disp", "cc"):
+        np.testing.assert_array_equal(b[k], a[k], err_msg=f"{name} {k}")
+    np.testing.assert_allclose(b["pce"], a["pce"], rtol=1e-12, equal_nan=True)
