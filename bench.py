@@ -540,7 +540,12 @@ def _kernel_roofline(ktimes: dict, res, p, vol_shape, peaks) -> dict:
             if traffic is not None:
                 row["dram_gbs"] = traffic * max(1, launches) / (ms / 1e3) / 1e9
             if name in ICGN_NCU_BOX:
-                row["ncu_box"] = ICGN_NCU_BOX[name]
+                box = ICGN_NCU_BOX[name]
+                row["ncu_box"] = box
+                # the roofs the kernel runs against, as fractions: FP32 from this run; issue slots and L1/TEX throughput
+                # from the box capture (the gather's L1 wavefronts and the sweep's instruction count bind it)
+                row["roofs"] = {"fp32": row["frac"], "issue_slots": box["issue_active"], "l1tex": box["l1tex_throughput"]}
+                row["binding_roof"] = max(row["roofs"], key=row["roofs"].get)
         if traffic is not None:
             row["traffic_source"] = "ncu DRAM bytes per " + TRAFFIC_PER_UNIT[name][0] + " on the 200x384x384 box, scaled"
         out[name] = row
