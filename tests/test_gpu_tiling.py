@@ -179,3 +179,29 @@ def test_bspline_box_coefficients_equal_the_whole_volume_prefilter():
         v = fr.local_volumes(box, quads=True)
         assert torch.equal(v["g"], whole[box.slices])
         assert torch.equal(v["g4"], K.make_quads(v["g"]))
+
+
+def test_tiled_pass_with_uneven_subsets_and_masks():
+    """Per-node subset shapes (the precompute's per-node form in every box), a reference mask and a deformed-frame
+    mask (NaN in the interpolant, 0 in the search input, each cut per box): the tiled pass equals the whole one."""
+    import torch
+
+    from pyaldvc_b200.pipeline import run_pass
+    from pyaldvc_b200.tiling import run_pass_tiled
+
+    f, g, mask, _ = PI.pass_pair("masked")
+    nz, ny, nx = f.shape
+    z, y, x = np.ogrid[:nz, :ny, :nx]
+    g_mask = ~((x - 50.0) ** 2 + (y - 20.0) ** 2 + (z - 40.0) ** 2 <= 6.0**2)  # a hole in the deformed frame
+
+    def winsize(c):  # 12 to 16 voxels per axis with the node's x position
+        c = np.asarray(c)
+        w = 12 + 2 * ((c[:, 0] // 16) % 3)
+        return np.stack([w, np.full_like(w, 16), np.full_like(w, 14)], 1)
+
+    p = _params("masked", node_winsize=winsize, interp_method="cubic")
+    cu = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    w = run_pass(cu(f), cu(g), p, cu(mask.astype(np.uint8)), g_mask=cu(g_mask.astype(np.uint8)))
+    t = run_pass_tiled(f, g, p, mask=mask, g_mask=g_mask, edge=64)
+    _compare(t, w, "uneven masked")
+    assert t.precompute_form == "per_node" and t.tiles.stages["icgn12"]["boxes"] > 1
