@@ -43,6 +43,8 @@
  *   aldvc_gradient_plane_fit <- strain/gradient_methods.py:151 gradient_plane_fit (no cut mesh)
  *   aldvc_gradient_fd <- strain/gradient_methods.py:231 gradient_fd (no cut mesh)
  *   aldvc_grid_smooth <- utils/grid_interp.py:54 smooth_grid_field
+ *   aldvc_grid_interp <- utils/grid_interp.py:18 interp_grid_field (the cumulative displacements of a
+ *                        frame series, core/pipeline.py:455-491)
  *   aldvc_strain_measures <- strain/strain_types.py:19-114 (strain_tensor, principal_strains,
  *                        von_mises_strain, max_shear_strain, volumetric_strain,
  *                        det_deformation_gradient, polar_rotation_deg)
@@ -247,6 +249,17 @@ int aldvc_gradient_fd(const double *U, const uint8_t *valid, int64_t nz, int64_t
 size_t aldvc_grid_smooth_workspace_size(int64_t nz, int64_t ny, int64_t nx);
 int aldvc_grid_smooth(const double *field, const uint8_t *valid, int64_t nz, int64_t ny, int64_t nx, const double *weights,
                       int32_t half_taps, double *out, void *workspace, size_t workspace_bytes, void *stream);
+
+/* An (nz, ny, nx, C) FP64 node-grid field at M points (M, 3) [x, y, z] (voxels; node (iz, iy, ix) sits at
+ * (ox + ix hx, oy + iy hy, oz + iz hz)) into out (M, C), FP64.  order 1: trilinear, taps clamped to the grid.
+ * order 3: cubic B-spline of the coefficient grid op_z (op_y (op_x field)), op_a an (n_a + pad_a) x n_a FP64 device
+ * matrix (the caller's padding and prefilter along that axis; node 0 at coefficient index pad_a / 2), taps clamped
+ * to the coefficient grid; workspace aldvc_grid_interp_workspace_size bytes (order 3 only). */
+size_t aldvc_grid_interp_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t C, int32_t pad_x, int32_t pad_y, int32_t pad_z);
+int aldvc_grid_interp(const double *field, int64_t nz, int64_t ny, int64_t nx, int32_t C, const double *op_x, const double *op_y,
+                      const double *op_z, int32_t pad_x, int32_t pad_y, int32_t pad_z, double ox, double oy, double oz, double hx,
+                      double hy, double hz, const double *points, int64_t M, int32_t order, double *out, void *workspace,
+                      size_t workspace_bytes, void *stream);
 /* Strain of every node from its gradient H (N, 9): E (N, 9) of type 0 infinitesimal, 1 Green-Lagrange,
  * 2 Euler-Almansi, 3 Hencky; principal strains (N, 3) descending; maximum shear, von Mises, volumetric
  * strain, det(I + H) and the polar rotation angle in degrees (N each).  NaN in, NaN out. */

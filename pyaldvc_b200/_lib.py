@@ -91,6 +91,9 @@ PROTOTYPES = {
     "aldvc_gradient_fd": (_i32, [_p, _p, _i64, _i64, _i64, _d, _d, _d, _p, _p, _p]),
     "aldvc_grid_smooth_workspace_size": (_sz, [_i64, _i64, _i64]),
     "aldvc_grid_smooth": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i32, _p, _p, _sz, _p]),
+    "aldvc_grid_interp_workspace_size": (_sz, [_i64, _i64, _i64, _i32, _i32, _i32, _i32]),
+    "aldvc_grid_interp": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _p, _p, _i32, _i32, _i32, _d, _d, _d, _d, _d, _d, _p, _i64, _i32, _p,
+                                 _p, _sz, _p]),
     "aldvc_strain_measures": (_i32, [_p, _i64, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),
     "aldvc_stats_workspace_size": (_sz, []),
     "aldvc_volume_stats": (_i32, [_p, _i32, _i64, _i64, _i64, _p, _d, _p, _p, _sz, _p]),

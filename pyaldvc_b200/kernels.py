@@ -626,6 +626,60 @@ def gaussian_presmooth(vol: torch.Tensor, sigma: float) -> torch.Tensor:
     return _three_axes(vol, gaussian_taps(sigma), BOUNDARY_NEAREST)
 
 
+GRID_ODD_PAD = 10  # utils/grid_interp.py:40-45: odd reflection continues a node grid linearly past its edge (cubic only)
+SPLINE_EDGE_PAD = 12  # SciPy's map_coordinates pads 'nearest' edges by 12 samples before its spline prefilter
+
+_SPLINE_OPS: dict = {}
+
+
+def spline_axis_operator(n: int) -> np.ndarray:
+    """((n + pad) x n) FP64: along one axis of n nodes, the odd reflection by GRID_ODD_PAD (axes longer than one node),
+    the edge padding by SPLINE_EDGE_PAD and the cubic B-spline prefilter of the edge-extended line (the 33-tap
+    impulse response of bspline_taps, |z|^33 < 2e-19): the coefficients interp_grid_field's cubic interpolation
+    evaluates, as one linear map of the axis's nodes.  Node 0 sits at coefficient index pad / 2."""
+    if n not in _SPLINE_OPS:
+        R = np.pad(np.eye(n), ((GRID_ODD_PAD, GRID_ODD_PAD), (0, 0)), mode="reflect", reflect_type="odd") if n > 1 else np.eye(n)
+        E = np.concatenate([np.repeat(R[:1], SPLINE_EDGE_PAD, 0), R, np.repeat(R[-1:], SPLINE_EDGE_PAD, 0)])
+        N = E.shape[0]
+        taps = bspline_taps()
+        J = len(taps) - 1
+        rows = np.repeat(np.arange(N), 2 * J + 1)
+        offs = np.tile(np.arange(-J, J + 1), N)
+        S = np.zeros((N, N))
+        np.add.at(S, (rows, np.clip(rows + offs, 0, N - 1)), taps[np.abs(offs)])
+        _SPLINE_OPS[n] = np.ascontiguousarray(S @ E)
+    return _SPLINE_OPS[n]
+
+
+def grid_interp(field: torch.Tensor, grid_shape, origin, spacing, points: torch.Tensor, order: int = 3) -> torch.Tensor:
+    """utils/grid_interp.py interp_grid_field on the device: the (N, C) or (N,) FP64 field of the node grid
+    ``grid_shape`` (nz, ny, nx), node (iz, iy, ix) at ``origin`` + index * ``spacing`` ([x, y, z] each), sampled at
+    ``points`` (M, 3) [x, y, z]; order 1 (trilinear) or 3 (cubic spline of the odd-reflected grid).  NaN nodes must
+    be filled by the caller (the reference inpaints them first).  Returns (M, C) or (M,) FP64."""
+    nz, ny, nx = (int(v) for v in grid_shape)
+    f = dev(field, torch.float64)
+    one = f.dim() == 1
+    C = 1 if one else int(f.shape[1])
+    pts = dev(points, torch.float64).reshape(-1, 3)
+    M = pts.shape[0]
+    out = torch.empty((M, C), dtype=torch.float64, device=f.device)
+    ops = [None, None, None]
+    pads = [0, 0, 0]
+    ws = None
+    if order == 3:
+        for k, n in enumerate((nx, ny, nz)):
+            op = spline_axis_operator(n)
+            ops[k] = torch.from_numpy(op).to(f.device)
+            pads[k] = op.shape[0] - n
+        ws = _workspace(lib().aldvc_grid_interp_workspace_size(nz, ny, nx, C, *pads))
+    ox, oy, oz = (float(v) for v in origin)
+    hx, hy, hz = (float(v) for v in spacing)
+    _lib.check(lib().aldvc_grid_interp(_p(f), nz, ny, nx, C, _p(ops[0]), _p(ops[1]), _p(ops[2]), pads[0], pads[1], pads[2], ox, oy, oz,
+                                       hx, hy, hz, _p(pts), M, int(order), _p(out), _p(ws), 0 if ws is None else ws.numel(),
+                                       stream_handle()), "aldvc_grid_interp")
+    return out[:, 0] if one else out
+
+
 def mask_fill(vol: torch.Tensor, mask: torch.Tensor, value: float) -> torch.Tensor:
     """In place: ``vol[mask == 0] = value`` (float32 volume, uint8/bool mask of the same shape)."""
     assert vol.is_cuda and vol.is_contiguous() and vol.dtype == torch.float32

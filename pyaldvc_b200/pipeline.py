@@ -270,7 +270,7 @@ def node_validity(mesh, p: PassParams, node_half, valid_b: torch.Tensor, centre_
 
 
 def initial_guess(p: PassParams, mesh, f, g, search_valid: torch.Tensor, ncc_calls: list, errs: K.ErrorWords, shift_fn=None,
-                  search_fn=None, level_volumes=None, levels: int | None = None):
+                  search_fn=None, level_volumes=None, levels: int | None = None, previous: torch.Tensor | None = None):
     """Section 3 of the pass (init_disp.compute_initial_guess :53-140, clean_initial_guess :143-189): (U0 (N,3)
     FP64, record).  ``f``, ``g``: the normalised device pair, or shape-only stand-ins when ``shift_fn`` (the global
     shift), ``search_fn`` (full-resolution searches), ``level_volumes`` (coarse pyramid pairs) and ``levels`` come
@@ -283,10 +283,15 @@ def initial_guess(p: PassParams, mesh, f, g, search_valid: torch.Tensor, ncc_cal
         raise ValueError(f"unknown init_guess_method {p.init_guess_method!r}")
     if p.init_guess_method == "zero":
         return torch.zeros((mesh.n, 3), dtype=torch.float64, device="cuda"), {"method": "zero"}
+    # the last frame's field when it was solved against the same reference and is finite everywhere, as it is (no
+    # cleaning); otherwise the pyramid (init_disp.py:70-73)
+    if p.init_guess_method == "previous" and previous is not None and tuple(previous.shape) == (mesh.n, 3) \
+            and bool(torch.isfinite(previous).all().item()):
+        return previous.to(device="cuda", dtype=torch.float64).clone(), {"method": "previous"}
     shift = None
     if p.global_shift:
         shift = shift_fn() if shift_fn is not None else IS.phase_correlation_shift_device(f, g)
-    if p.init_guess_method in ("pyramid", "previous"):  # "previous" has no earlier frame here: the reference falls back
+    if p.init_guess_method in ("pyramid", "previous"):  # "previous" without a usable field: the pyramid
         info = IS.pyramid_search_device(f, g, mesh.coords, mesh.grid_shape, subset0, rad,
                                         p.pyramid_levels if levels is None else levels, shift, p.init_outlier_threshold,
                                         p.ncc_auto_expand, p.ncc_max_expand, p.pyramid_fine_radius, search_valid, engine_of, ncc_calls,
@@ -340,34 +345,48 @@ def make_global_step(mesh, p: PassParams, elem_active, beta, errs: K.ErrorWords)
     return global_step
 
 
-def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
-             tracer: Tracer | None = None, g_mask: torch.Tensor | None = None) -> PassResult:
-    """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16).  ``mask``: reference-frame
-    material mask; ``g_mask``: deformed-frame mask (False voxels are excluded from every correlation)."""
-    tr = tracer if tracer is not None else Tracer(sync=False)
-    tr.start()
-    # device error words of the bounded waits (inpainting, median test, PCG), read once at the end of the pass
-    errs = K.ErrorWords()
+@dataclass
+class Reference:
+    """A reference frame prepared for any number of deformed frames (core/pipeline.py:187-228 get_reference): the
+    normalised (and presmoothed) volume, its gradients and mask, the node grid, the per-node precompute and the node
+    and element validity.  ``key`` holds the parameters it was prepared with."""
+
+    f: torch.Tensor
+    gx: torch.Tensor
+    gy: torch.Tensor
+    gz: torch.Tensor
+    m_u8: torch.Tensor | None
+    mesh: Mesh
+    node_half: torch.Tensor | None
+    H: torch.Tensor
+    L: torch.Tensor
+    meanf: torch.Tensor
+    bottomf: torch.Tensor
+    n_valid: torch.Tensor
+    valid_b: torch.Tensor
+    elem_active: torch.Tensor | None
+    precompute_form: str
+    key: tuple
+
+
+def _reference_key(p: PassParams, normalize: bool, shape) -> tuple:
+    return (tuple(int(s) for s in shape), tuple(p.winsize), tuple(p.winstepsize), p.min_valid_ratio, p.hessian_cond_max,
+            p.subset_stride, p.variant, id(p.node_winsize) if p.node_winsize is not None else None, p.prefilter_sigma, bool(normalize))
+
+
+def prepare_reference(f_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
+                      tracer: Tracer | None = None) -> Reference:
+    """Normalisation, presmoothing, gradients, node grid, precompute (local_icgn.precompute_local_context :223-347)
+    and node validity (grid_mesh.apply_mask_to_mesh) of a reference frame on the device.  ``tracer`` is marked
+    "preprocess" after the volume work and "precompute" at the end."""
     f = K.normalize(f_raw) if normalize else f_raw.float().contiguous()
-    g = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
-    if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:197, 257
+    if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:197
         f = K.gaussian_presmooth(f, p.prefilter_sigma)
-        g = K.gaussian_presmooth(g, p.prefilter_sigma)
-    mode = K.INTERP_MODE_BY_NAME[p.interp_method]
-    # the array the interpolation samples, and the NCC input (core/pipeline.py:258-262, io/volume_ops.py:225-244)
-    g_prep = K.bspline_prefilter(g) if p.interp_method == "bspline" else g
-    if g_mask is not None:
-        gm = g_mask.to(torch.uint8).contiguous()
-        if g_prep is g:
-            g_prep = g.clone()
-        K.mask_fill(g_prep, gm, float("nan"))
-        g = K.mask_fill(g.clone(), gm, 0.0)
     gx, gy, gz = K.gradients(f)
     mesh = Mesh(f.shape, p)
     m_u8 = None if mask is None else mask.to(torch.uint8).contiguous()
-    tr.mark("preprocess")
-
-    # ---------------- precompute (local_icgn.precompute_local_context :223-347)
+    if tracer is not None:
+        tracer.mark("preprocess")
     node_half = None
     if p.node_winsize is not None:
         ws = np.asarray(p.node_winsize(mesh.coords.cpu().numpy()), dtype=np.int64).reshape(-1, 3)
@@ -390,14 +409,53 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         c = mesh.coords
         centre_ok = m_u8[c[:, 2], c[:, 1], c[:, 0]] != 0
     valid_b, elem_active = node_validity(mesh, p, node_half, valid != 0, centre_ok, n_valid)
+    if tracer is not None:
+        tracer.mark("precompute")
+    return Reference(f, gx, gy, gz, m_u8, mesh, node_half, H, L, meanf, bottomf, n_valid, valid_b, elem_active, precompute_form,
+                     _reference_key(p, normalize, f_raw.shape))
+
+
+def run_pass(f_raw: torch.Tensor | None, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
+             tracer: Tracer | None = None, g_mask: torch.Tensor | None = None, ref: Reference | None = None,
+             previous: torch.Tensor | None = None) -> PassResult:
+    """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16).  ``mask``: reference-frame
+    material mask; ``g_mask``: deformed-frame mask (False voxels are excluded from every correlation).  ``ref``: the
+    reference frame prepared by ``prepare_reference`` (then ``f_raw`` and ``mask`` are not read); ``previous``: the
+    displacement field (N, 3) of the last frame solved against the same reference, the initial guess of
+    ``init_guess_method="previous"`` (core/pipeline.py:266, init_disp.py:70-73)."""
+    tr = tracer if tracer is not None else Tracer(sync=False)
+    tr.start()
+    # device error words of the bounded waits (inpainting, median test, PCG), read once at the end of the pass
+    errs = K.ErrorWords()
+    g = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
+    if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:257
+        g = K.gaussian_presmooth(g, p.prefilter_sigma)
+    mode = K.INTERP_MODE_BY_NAME[p.interp_method]
+    # the array the interpolation samples, and the NCC input (core/pipeline.py:258-262, io/volume_ops.py:225-244)
+    g_prep = K.bspline_prefilter(g) if p.interp_method == "bspline" else g
+    if g_mask is not None:
+        gm = g_mask.to(torch.uint8).contiguous()
+        if g_prep is g:
+            g_prep = g.clone()
+        K.mask_fill(g_prep, gm, float("nan"))
+        g = K.mask_fill(g.clone(), gm, 0.0)
+    if ref is None:
+        ref = prepare_reference(f_raw, p, mask, normalize, tr)
+    else:
+        if ref.key != _reference_key(p, normalize, g_raw.shape):
+            raise ValueError("run_pass: the prepared reference was made with other parameters or another volume shape")
+        tr.mark("preprocess")
+        tr.mark("precompute")
+    f, gx, gy, gz, m_u8, mesh, node_half = ref.f, ref.gx, ref.gy, ref.gz, ref.m_u8, ref.mesh, ref.node_half
+    H, L, meanf, bottomf, n_valid = ref.H, ref.L, ref.meanf, ref.bottomf, ref.n_valid
+    valid_b, elem_active, precompute_form = ref.valid_b, ref.elem_active, ref.precompute_form
     valid_u8 = valid_b.to(torch.uint8).contiguous()
-    tr.mark("precompute")
 
     # ---------------- section 3: initial guess (init_disp.compute_initial_guess :53-140, clean_initial_guess :143-189)
     # the reference makes the precompute's validity the mesh's node validity before the initial guess
     # (core/pipeline.py:212, local_icgn.py:300): only those nodes are searched, the others are filled
     ncc_calls: list = []
-    U0, init_info = initial_guess(p, mesh, f, g, valid_b, ncc_calls, errs)
+    U0, init_info = initial_guess(p, mesh, f, g, valid_b, ncc_calls, errs, previous=previous)
     tr.mark("init_guess")
 
     # ---------------- section 4: local 12-DOF IC-GN (local_icgn.local_icgn :398-489)
@@ -433,6 +491,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                         grid_shape=mesh.grid_shape, valid=valid_b, U_local=U_local, U0=U0, P_local=P, status_local=status,
                         n_iter_local=n_iter)
     result.F_local = F1.reshape(-1, 3, 3).clone()  # the local result after outlier filling
+    # converged, then rejected by the median test and replaced: not a measurement (core/pipeline.py:369-370)
+    result.outlier = bad & (status == STATUS_CONVERGED)
     result.tracer = tr
     result.ncc_calls = ncc_calls  # (nodes, half, radius, engine) of every integer search of the pass
     result.init_info = init_info
@@ -488,7 +548,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                 Wn = F2n - F1n
                 vn = U2n - U1n
             du_g = _rms(U2n - U2)
-            return U1n, U2n, F2n, Wn, vn, du_g, st3, zc3, it3
+            return U1n, U2n, F2n, Wn, vn, du_g, st3, zc3, it3, bad3
 
         return global_step, icgn3_on, admm_step
 
@@ -501,7 +561,7 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     th3, br3 = _launch_shape(p, 3, mode, mesh, m_u8, lambda idx, th, br: icgn3_on(idx, U2, F2, v, th, br))
 
     steps = 1
-    st_last, zc_last, it_last = status, zncc, n_iter
+    st_last, zc_last, it_last, bad_last = status, zncc, n_iter, bad
     U1_prev = U1
     if p.graph and not p.admm_early_stop and p.admm_max_iter > 1:
         # the remaining loop as one CUDA graph, captured on the first pass of this problem shape and replayed
@@ -525,8 +585,8 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
                 a = (static["U2"], static["F2"], static["W"], static["v"])
                 outs = []
                 for _ in range(2, p.admm_max_iter + 1):
-                    U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg = admm_static(*a, th3, br3)
-                    outs.append((U1g, stg, zcg, itg))
+                    U1g, U2g, F2g, Wg, vg, _, stg, zcg, itg, bdg = admm_static(*a, th3, br3)
+                    outs.append((U1g, stg, zcg, itg, bdg))
                     a = (U2g, F2g, Wg, vg)
             entry = {"graph": graph, "static": static, "final": a, "outs": outs[-1], "iters": [o[3] for o in outs],
                      "errs": graph_errs}
@@ -542,13 +602,13 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
         errs.extend(entry["errs"])  # the graph's error words, rewritten by this replay
         # the graph's outputs are overwritten by its next replay: the result keeps copies
         U2, F2 = entry["final"][0].clone(), entry["final"][1].clone()
-        U1, st_last, zc_last, it_last = (t.clone() for t in entry["outs"])
+        U1, st_last, zc_last, it_last, bad_last = (t.clone() for t in entry["outs"])
         result.icgn3_iters = [t.clone() for t in entry["iters"]]
         steps = p.admm_max_iter
     else:
         for step in range(2, p.admm_max_iter + 1):
             steps = step
-            U1n, U2n, F2n, W, v, du_g, st_last, zc_last, it_last = admm_step(U2, F2, W, v, th3, br3)
+            U1n, U2n, F2n, W, v, du_g, st_last, zc_last, it_last, bad_last = admm_step(U2, F2, W, v, th3, br3)
             result.icgn3_iters.append(it_last)
             du_l = _rms(U1n - U1_prev)
             U1_prev = U1n
@@ -561,4 +621,5 @@ def run_pass(f_raw: torch.Tensor, g_raw: torch.Tensor, p: PassParams, mask: torc
     result.F = F2.reshape(-1, 3, 3)
     result.status, result.zncc, result.n_iter = st_last, zc_last, it_last
     result.admm_steps = steps
+    result.outlier = bad_last & (st_last == STATUS_CONVERGED)
     return result

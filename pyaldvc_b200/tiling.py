@@ -933,6 +933,7 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
                            grid_shape=mesh.grid_shape, valid=valid_b, U_local=U1.clone(), U0=U0, P_local=P, status_local=status,
                            n_iter_local=n_iter)
     result.F_local = F1.reshape(-1, 3, 3).clone()
+    result.outlier = bad & (status == PL.STATUS_CONVERGED)
     result.tracer = tr
     result.ncc_calls = ncc_calls
     result.init_info = init_info
@@ -1002,6 +1003,7 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
         result.icgn3_iters.append(it_last)
         bad3 = st_last != PL.STATUS_CONVERGED
         bad3 = bad3 | PL._median_flags(U, ~bad3, mesh.grid_shape, p.local_outlier_threshold, errs)
+        result.outlier = bad3 & (st_last == PL.STATUS_CONVERGED)
         U1n = torch.where(bad3[:, None], U2, U)
         F1n = F2
         U2n, F2n = global_step(U1n, F1n, W, v)

@@ -3,7 +3,7 @@
 Run in a container that holds the pyALDVC sources (read-only) at
 ``$ALDVC_REFERENCE/src`` (default ``/root/reference/src``)::
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [kernels volume_ops init_guess strain beta pass ncc_fft tiling]
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [kernels volume_ops init_guess strain beta pass ncc_fft tiling series]
 
 It imports the reference package, runs its own Numba CPU kernels on seeded
 bead volumes from ``pyaldvc_b200.synthetic`` and stores inputs + outputs as
@@ -525,9 +525,50 @@ def tiling_fixtures():
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+def series_fixtures():
+    """The reference's run_aldvc over a three-frame series (core/pipeline.py:82-452; cumulative displacements
+    :455-491): per case and frame the reference frame, initial guess, local result, final U / F / ZNCC / statuses,
+    outlier flags, cumulative displacement and ADMM step count; plus its interp_grid_field (utils/grid_interp.py) on
+    random node grids, both orders, points inside and outside the grid."""
+    from al_dvc.core.pipeline import run_aldvc
+    from al_dvc.utils.grid_interp import interp_grid_field
+
+    import pass_inputs as PI
+
+    vols = PI.series_frames()
+    out = {"sha": np.array([PI.sha(v) for v in vols])}
+    for name, c in PI.SERIES_CASES.items():
+        common = {k: v for k, v in PI.PASS_COMMON.items() if k != "init_guess_method"}
+        para = dvcpara_default(**common, **PI.SERIES_PARA, init_guess_method=c["init_guess_method"],
+                               reference_mode=c["reference_mode"], cumulative_interp=c["cumulative_interp"], backend="numba",
+                               verbose=False)
+        r = run_aldvc(para, vols, compute_strain=False)
+        out[f"{name}_coords"] = r.dvc_mesh.coordinates
+        for k, fr in enumerate(r.result_disp):
+            key = f"{name}_f{k + 1}"
+            out.update({f"{key}_ref": np.array(fr.ref_frame), f"{key}_U0": fr.U0, f"{key}_U_local": fr.U_local, f"{key}_U": fr.U,
+                        f"{key}_F": fr.F, f"{key}_zncc": fr.zncc, f"{key}_status": fr.status, f"{key}_outlier": fr.outlier,
+                        f"{key}_U_accum": fr.U_accum, f"{key}_steps": np.array(fr.admm.n_steps)})
+        print(f"series {name}: {len(r.result_disp)} frames, steps {[fr.admm.n_steps for fr in r.result_disp]}")
+    rng = np.random.default_rng(5)
+    for gi, shape in enumerate(((5, 6, 7), (1, 6, 9), (12, 4, 3), (2, 2, 2))):
+        nz, ny, nx = shape
+        x0, y0, z0 = 10.0 + 12 * np.arange(nx), 5.0 + 12 * np.arange(ny), 7.0 + 12 * np.arange(nz)
+        field = rng.normal(size=shape)
+        q = np.stack([rng.uniform(x0[0] - 30, x0[-1] + 30, 300), rng.uniform(y0[0] - 30, y0[-1] + 30, 300),
+                      rng.uniform(z0[0] - 30, z0[-1] + 30, 300)], 1)
+        out.update({f"gi{gi}_field": field, f"gi{gi}_x0": x0, f"gi{gi}_y0": y0, f"gi{gi}_z0": z0, f"gi{gi}_q": q,
+                    f"gi{gi}_o1": interp_grid_field(field, (x0, y0, z0), q, order=1),
+                    f"gi{gi}_o3": interp_grid_field(field, (x0, y0, z0), q, order=3)})
+    path = os.path.join(HERE, "golden_series.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["kernels", "volume_ops", "init_guess", "strain", "beta", "pass", "ncc_fft", "tiling"]
+    which = sys.argv[1:] or ["kernels", "volume_ops", "init_guess", "strain", "beta", "pass", "ncc_fft", "tiling", "series"]
     makers = {"kernels": main, "volume_ops": volume_ops_fixtures, "init_guess": init_guess_fixtures, "strain": strain_fixtures,
-              "beta": beta_fixtures, "pass": pass_fixtures, "ncc_fft": ncc_fft_fixtures, "tiling": tiling_fixtures}
+              "beta": beta_fixtures, "pass": pass_fixtures, "ncc_fft": ncc_fft_fixtures, "tiling": tiling_fixtures,
+              "series": series_fixtures}
     for w in which:
         makers[w]()

@@ -100,3 +100,31 @@ def ncc_shift(coords):
     u = np.column_stack(syn.affine(NCC_F, NCC_T, centre)(*(coords[:, k].astype(float) for k in range(3))))
     off = np.stack([(np.arange(len(coords)) * 7 + k) % 5 - 2 for k in range(3)], 1)
     return np.round(u).astype(np.int64) + off
+
+
+# Frame series of golden_series.npz (the reference's run_aldvc over three frames): frame 0 and two frames of the same
+# beads moved by growing affine fields, each frame with its own noise; ws 16 / step 8, direct NCC +-4, tricubic, three
+# ADMM steps at most with the reference's early stop.  Cases: accumulative with the "previous" initial guess (frame
+# 2 starts from frame 1's field), incremental with the cubic and the linear cumulative composition.
+SERIES_SHAPE = (56, 64, 72)
+SERIES_CASES = {
+    "accum_prev": dict(reference_mode="accumulative", init_guess_method="previous", cumulative_interp="cubic"),
+    "incr_cubic": dict(reference_mode="incremental", init_guess_method="ncc", cumulative_interp="cubic"),
+    "incr_linear": dict(reference_mode="incremental", init_guess_method="ncc", cumulative_interp="linear"),
+}
+SERIES_PARA = dict(winsize=(16, 16, 16), winstepsize=(8, 8, 8), search_radius=(4, 4, 4), interp_method="cubic", admm_max_iter=3)
+
+
+def series_frames():
+    """Three float32 frames: the beads of frame 0 moved by affine fields with translations (0.9, -0.5, 0.3) and
+    (2.1, -1.3, 0.8) and gradients F_AFFINE, 2 F_AFFINE about the volume centre."""
+    shape = SERIES_SHAPE
+    centre = tuple((s - 1) / 2 for s in shape[::-1])
+    centres, peaks = syn.draw_beads(shape, 0.02, 81)
+    out = []
+    for k, (t, scale) in enumerate((((0.0, 0.0, 0.0), 0.0), ((0.9, -0.5, 0.3), 1.0), ((2.1, -1.3, 0.8), 2.0))):
+        disp = syn.affine(scale * F_AFFINE, t, centre)
+        vol = syn.render_beads(shape, syn.displace_beads(centres, disp), peaks, 1.5).astype(np.float64)
+        vol = vol + np.random.default_rng(90 + k).normal(0.0, 0.01, size=vol.shape)
+        out.append(vol.astype(np.float32))
+    return out
