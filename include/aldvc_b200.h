@@ -45,6 +45,7 @@
  *   aldvc_grid_smooth <- utils/grid_interp.py:54 smooth_grid_field
  *   aldvc_grid_interp <- utils/grid_interp.py:18 interp_grid_field (the cumulative displacements of a
  *                        frame series, core/pipeline.py:455-491)
+ *   aldvc_displacement_uncertainty <- solver/uncertainty.py:94 displacement_uncertainty
  *   aldvc_strain_measures <- strain/strain_types.py:19-114 (strain_tensor, principal_strains,
  *                        von_mises_strain, max_shear_strain, volumetric_strain,
  *                        det_deformation_gradient, polar_rotation_deg)
@@ -260,6 +261,14 @@ int aldvc_grid_interp(const double *field, int64_t nz, int64_t ny, int64_t nx, i
                       const double *op_z, int32_t pad_x, int32_t pad_y, int32_t pad_z, double ox, double oy, double oz, double hx,
                       double hy, double hz, const double *points, int64_t M, int32_t order, double *out, void *workspace,
                       size_t workspace_bytes, void *stream);
+/* Standard deviation (N, 3) of u, v, w in voxels from the IC-GN normal equations (noise-corrected two-term
+ * model): H (N, 12, 12) stored Hessians, zncc, status (NULL: every node), valid, n_valid, bottomf per node (device);
+ * pattern: HOST 12 x 12 expectation of sum J J^T for unit gradient noise over the subset (pattern[9][9] its voxel
+ * count), gain: the gradient stencil's variance gain, min_frac: the share of each translation diagonal the
+ * correction keeps.  NaN at nodes that are not converged, valid, with a finite ZNCC and more than 14 voxels. */
+int aldvc_displacement_uncertainty(const double *H, const double *zncc, const int8_t *status, const uint8_t *valid,
+                                   const int64_t *n_valid, const double *bottomf, int64_t n_nodes, const double *pattern, double gain,
+                                   double min_frac, int32_t noise_correction, double *out, void *stream);
 /* Strain of every node from its gradient H (N, 9): E (N, 9) of type 0 infinitesimal, 1 Green-Lagrange,
  * 2 Euler-Almansi, 3 Hencky; principal strains (N, 3) descending; maximum shear, von Mises, volumetric
  * strain, det(I + H) and the polar rotation angle in degrees (N each).  NaN in, NaN out. */

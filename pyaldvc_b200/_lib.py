@@ -92,6 +92,7 @@ PROTOTYPES = {
     "aldvc_grid_smooth_workspace_size": (_sz, [_i64, _i64, _i64]),
     "aldvc_grid_smooth": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i32, _p, _p, _sz, _p]),
     "aldvc_grid_interp_workspace_size": (_sz, [_i64, _i64, _i64, _i32, _i32, _i32, _i32]),
+    "aldvc_displacement_uncertainty": (_i32, [_p, _p, _p, _p, _p, _p, _i64, _p, _d, _d, _i32, _p, _p]),
     "aldvc_grid_interp": (_i32, [_p, _i64, _i64, _i64, _i32, _p, _p, _p, _i32, _i32, _i32, _d, _d, _d, _d, _d, _d, _p, _i64, _i32, _p,
                                  _p, _sz, _p]),
     "aldvc_strain_measures": (_i32, [_p, _i64, _i32, _p, _p, _p, _p, _p, _p, _p, _p]),

@@ -101,6 +101,102 @@ __global__ void grid_eval_kernel(GridInterpArgs a) {
     }
 }
 
+// ----------------------------------------------------------------------------- displacement uncertainty
+// solver/uncertainty.py:83-137: at a converged node with n_valid > 14 voxels, s^2 = (1 - ZNCC) bf^2 / n, the
+// parameter factor 2 (1 - ZNCC) bf^2 / (n - 12), the stored Hessian less the reference-gradient noise it carries
+// (gain s^2 (n / pattern[9][9]) pattern, at most (1 - min_frac) of each translation diagonal), its inverse, and
+// var = factor diag(inv)[9..11] + gain s^4 diag(inv pattern' inv)[9..11] (pattern' = pattern n / pattern[9][9]).
+// One thread per node, the 12 x 12 system in FP64, Gauss-Jordan elimination with partial pivoting; a zero pivot
+// leaves the node NaN.
+struct UncArgs {
+    const double* H;        // (N, 12, 12)
+    const double* zncc;     // (N,)
+    const int8_t* status;   // (N,) or NULL
+    const uint8_t* valid;   // (N,)
+    const int64_t* n_valid; // (N,)
+    const double* bottomf;  // (N,)
+    int64_t N;
+    double pattern[144];
+    double gain, min_frac;
+    int noise_correction;
+    double* out;  // (N, 3)
+};
+
+__global__ void uncertainty_kernel(UncArgs a) {
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < a.N; n += (int64_t)gridDim.x * blockDim.x) {
+        const double nanv = __longlong_as_double(0x7ff8000000000000LL);
+        a.out[3 * n] = a.out[3 * n + 1] = a.out[3 * n + 2] = nanv;
+        const double z = a.zncc[n];
+        const int64_t nv = a.n_valid[n];
+        if (!a.valid[n] || !isfinite(z) || nv <= 14 || (a.status && a.status[n] != 0)) continue;
+        const double bf = a.bottomf[n], omz = fmax(1.0 - z, 0.0);
+        const double factor = 2.0 * omz / (double)(nv - 12) * (bf * bf);
+        const double s2 = omz * (bf * bf) / (double)nv;
+        const double scale = (double)nv / a.pattern[9 * 12 + 9];
+        double A[144], inv[144];
+        for (int i = 0; i < 144; ++i) A[i] = a.H[n * 144 + i];
+        if (a.noise_correction) {
+            const double g = a.gain * s2 * scale;
+            double limit = 1e300;
+            for (int i = 9; i < 12; ++i) {
+                const double cd = g * a.pattern[i * 12 + i], td = A[i * 12 + i];
+                limit = fmin(limit, cd > 0.0 ? (1.0 - a.min_frac) * td / fmax(cd, 1e-300) : 1.0);
+            }
+            limit = fmin(fmax(limit, 0.0), 1.0);
+            for (int i = 0; i < 144; ++i) A[i] -= g * a.pattern[i] * limit;
+        }
+        for (int i = 0; i < 144; ++i) inv[i] = (i / 12 == i % 12) ? 1.0 : 0.0;
+        bool singular = false;
+        for (int c = 0; c < 12 && !singular; ++c) {
+            int piv = c;
+            for (int r = c + 1; r < 12; ++r)
+                if (fabs(A[r * 12 + c]) > fabs(A[piv * 12 + c])) piv = r;
+            if (A[piv * 12 + c] == 0.0) {
+                singular = true;
+                break;
+            }
+            if (piv != c)
+                for (int k = 0; k < 12; ++k) {
+                    double t = A[c * 12 + k];
+                    A[c * 12 + k] = A[piv * 12 + k];
+                    A[piv * 12 + k] = t;
+                    t = inv[c * 12 + k];
+                    inv[c * 12 + k] = inv[piv * 12 + k];
+                    inv[piv * 12 + k] = t;
+                }
+            const double d = 1.0 / A[c * 12 + c];
+            for (int k = 0; k < 12; ++k) {
+                A[c * 12 + k] *= d;
+                inv[c * 12 + k] *= d;
+            }
+            for (int r = 0; r < 12; ++r) {
+                if (r == c) continue;
+                const double m = A[r * 12 + c];
+                if (m == 0.0) continue;
+                for (int k = 0; k < 12; ++k) {
+                    A[r * 12 + k] -= m * A[c * 12 + k];
+                    inv[r * 12 + k] -= m * inv[c * 12 + k];
+                }
+            }
+        }
+        if (singular) continue;
+        for (int i = 0; i < 3; ++i) {
+            const int d = 9 + i;
+            double var = factor * inv[d * 12 + d];
+            if (a.noise_correction) {
+                double cross = 0.0;
+                for (int p = 0; p < 12; ++p) {
+                    double t = 0.0;
+                    for (int q = 0; q < 12; ++q) t += a.pattern[p * 12 + q] * scale * inv[q * 12 + d];
+                    cross += inv[d * 12 + p] * t;
+                }
+                var += a.gain * s2 * s2 * cross;
+            }
+            a.out[3 * n + i] = sqrt(fmax(var, 0.0));
+        }
+    }
+}
+
 static unsigned gi_blocks(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + GI_THREADS - 1) / GI_THREADS, 148 * 16)); }
 
 }  // namespace aldvc
@@ -165,4 +261,29 @@ extern "C" int aldvc_grid_interp(const double* field, int64_t nz, int64_t ny, in
     }
     grid_eval_kernel<<<gi_blocks(M), GI_THREADS, 0, s>>>(a);
     return check_launch("aldvc_grid_interp");
+}
+
+extern "C" int aldvc_displacement_uncertainty(const double* H, const double* zncc, const int8_t* status, const uint8_t* valid,
+                                             const int64_t* n_valid, const double* bottomf, int64_t n_nodes, const double* pattern,
+                                             double gain, double min_frac, int32_t noise_correction, double* out, void* stream) {
+    ALDVC_REQUIRE(H && zncc && valid && n_valid && bottomf && pattern && out, "aldvc_displacement_uncertainty: null pointer");
+    ALDVC_REQUIRE(pattern[9 * 12 + 9] > 0.0, "aldvc_displacement_uncertainty: pattern[9][9] must be the subset's voxel count");
+    if (n_nodes <= 0) return ALDVC_OK;
+    UncArgs a{};
+    a.H = H;
+    a.zncc = zncc;
+    a.status = status;
+    a.valid = valid;
+    a.n_valid = n_valid;
+    a.bottomf = bottomf;
+    a.N = n_nodes;
+    for (int i = 0; i < 144; ++i) a.pattern[i] = pattern[i];
+    a.gain = gain;
+    a.min_frac = min_frac;
+    a.noise_correction = noise_correction ? 1 : 0;
+    a.out = out;
+    cudaStream_t s = (cudaStream_t)stream;
+    KTimer kt_("uncertainty", s);
+    uncertainty_kernel<<<gi_blocks(n_nodes), 128, 0, s>>>(a);
+    return check_launch("aldvc_displacement_uncertainty");
 }

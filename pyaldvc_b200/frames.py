@@ -32,6 +32,7 @@ import torch
 
 from . import kernels as K
 from . import pipeline as PL
+from . import uncertainty as UN
 from .mesh import build_grid_axes, grid_coords
 
 REF_CACHE = 2  # prepared references kept at a time (core/pipeline.py:60)
@@ -98,6 +99,7 @@ class FrameResult:
     beta: float | None = None
     admm_steps: int = 0
     init_method: str = ""
+    U_std: np.ndarray | None = None  # standard deviation of u, v, w (voxels) from the normal equations
     U_accum: np.ndarray | None = None
     seconds: float = 0.0
 
@@ -275,10 +277,13 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
             res = PL.run_pass(None, g_d, pk, None, normalize, g_mask=gm_d, ref=refs[ref_idx], previous=previous)
             if p.beta is None and getattr(res, "beta", None) is not None:
                 beta_by_ref.setdefault(ref_idx, float(res.beta))
+            rf = refs[ref_idx]
+            U_std = UN.displacement_uncertainty_device(rf.H, res.zncc, res.status, rf.valid_b, rf.n_valid, rf.bottomf, rf.mesh.half,
+                                                       p.subset_stride)
             frames.append(FrameResult(U=_host(res.U), F=_host(res.F), ref_frame=ref_idx, U_local=_host(res.U_local),
                                       F_local=_host(res.F_local), U0=_host(res.U0), zncc=_host(res.zncc), status=_host(res.status),
                                       outlier=_host(res.outlier), valid=_host(res.valid), beta=getattr(res, "beta", None),
-                                      admm_steps=res.admm_steps, init_method=res.init_info.get("method", "")))
+                                      admm_steps=res.admm_steps, init_method=res.init_info.get("method", ""), U_std=_host(U_std)))
             prev_ref, prev_U = ref_idx, res.U
             # raw frames still to come: the next one and its reference when that is not prepared yet
             keep = {k + 1} | ({schedule.parent(k + 1)} if k + 1 < n_frames and schedule.parent(k + 1) not in refs else set())

@@ -548,7 +548,7 @@ def series_fixtures():
             key = f"{name}_f{k + 1}"
             out.update({f"{key}_ref": np.array(fr.ref_frame), f"{key}_U0": fr.U0, f"{key}_U_local": fr.U_local, f"{key}_U": fr.U,
                         f"{key}_F": fr.F, f"{key}_zncc": fr.zncc, f"{key}_status": fr.status, f"{key}_outlier": fr.outlier,
-                        f"{key}_U_accum": fr.U_accum, f"{key}_steps": np.array(fr.admm.n_steps)})
+                        f"{key}_U_accum": fr.U_accum, f"{key}_steps": np.array(fr.admm.n_steps), f"{key}_U_std": fr.U_std})
         print(f"series {name}: {len(r.result_disp)} frames, steps {[fr.admm.n_steps for fr in r.result_disp]}")
     rng = np.random.default_rng(5)
     for gi, shape in enumerate(((5, 6, 7), (1, 6, 9), (12, 4, 3), (2, 2, 2))):
