@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--edge", type=int, default=512, help="--stage tiled: box edge target (tile_local)")
     ap.add_argument("--ncc-engine", default="auto", choices=["auto", "tiled", "fft", "fft_cluster", "plain"],
                     help="--stage pass: the integer search's engine")
-    ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute", "tiled"],
+    ap.add_argument("--frames", type=int, default=4, help="--stage series: deformed frames of the series")
+    ap.add_argument("--stage", default="full", choices=["full", "pass", "ncc", "precompute", "tiled", "series"],
                     help="full: the benchmark line; pass / ncc / precompute: timing of one stage on a profiling case "
                          "(human-readable lines, no JSON), see stage_main")
     ap.add_argument("--shape", type=int, nargs=3, default=None, help="volume (nz ny nx) of a --stage case")
@@ -86,7 +87,10 @@ def stage_main(args) -> None:
     tiled       the configuration's pass (full size unless --shape) resident on the device, then tiled.run_pass_tiled
                 from host copies of the same frames with boxes of --edge voxels, once keeping the local boxes between
                 stages and once streaming every box again; prints the boxes, the bytes uploaded and the largest
-                difference to the resident result"""
+                difference to the resident result
+    series      --frames single passes of the configuration's pair from pinned host memory (copies timed), then
+                frames.run_series over frame 0 and the deformed frame repeated --frames times from host memory,
+                accumulative (one prepared reference) and incremental (a new reference every frame)"""
     import torch
 
     from pyaldvc_b200 import configs
@@ -162,6 +166,48 @@ def stage_main(args) -> None:
                   f"{bool((res.status == whole.status).all())}", flush=True)
             del res, fr
             torch.cuda.empty_cache()
+        return
+    if args.stage == "series":
+        from pyaldvc_b200.frames import run_series
+        from pyaldvc_b200.pipeline import run_pass
+
+        cfg = args.config
+        shape = tuple(args.shape) if args.shape else None
+        p = configs.params(cfg)
+        fd, gd, md, _ = configs.device_pair(cfg, shape=shape)
+        host = [fd.cpu().numpy()] + [gd.cpu().numpy()] * args.frames  # frame 0, then the deformed frame repeated
+        masks = None if md is None else [md.cpu().numpy()] + [None] * args.frames
+        n_nodes = None
+        for _ in range(args.warmup):
+            r = run_pass(fd, gd, p, md)
+            n_nodes = int(r.coords.shape[0])
+        del fd, gd, md
+        torch.cuda.empty_cache()
+        f_h = torch.from_numpy(host[0]).pin_memory()
+        g_h = torch.from_numpy(host[1]).pin_memory()
+        m_h = None if masks is None else torch.from_numpy(masks[0]).pin_memory()
+        torch.cuda.synchronize()
+        t = time.time()
+        for _ in range(args.frames):  # single passes from pinned host memory, copies in the timed region
+            r = run_pass(f_h.to("cuda", non_blocking=True), g_h.to("cuda", non_blocking=True), p,
+                         None if m_h is None else m_h.to("cuda", non_blocking=True))
+            r.U.cpu()
+        torch.cuda.synchronize()
+        single = time.time() - t
+        print(f"config {cfg}: {args.frames} single passes from host memory {1e3 * single:.1f} ms "
+              f"({1e3 * single / args.frames:.1f} ms per frame, {n_nodes * args.frames / single:.0f} nodes/s)", flush=True)
+        for mode in ("accumulative", "incremental"):
+            for rep in range(2):
+                torch.cuda.synchronize()
+                t = time.time()
+                res = run_series(host, p, masks=masks, reference_mode=mode)
+                torch.cuda.synchronize()
+                dt = time.time() - t
+            tm = res.timings
+            print(f"config {cfg}: {mode} series of {args.frames} frames {1e3 * dt:.1f} ms ({1e3 * dt / args.frames:.1f} ms per frame, "
+                  f"{n_nodes * args.frames / dt:.0f} nodes/s); references prepared in {1e3 * tm.get('reference_prepare', 0):.1f} ms, "
+                  f"cumulative {1e3 * tm['cumulative']:.1f} ms, {tm['h2d_bytes'] / 1e9:.2f} GB uploaded; frames (s) "
+                  f"{[round(fr.seconds, 3) for fr in res.frames]}", flush=True)
         return
     if args.stage == "ncc":
         n, h, r = 192, args.half, args.radius
