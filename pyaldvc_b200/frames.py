@@ -81,6 +81,22 @@ class FrameSchedule:
 
 
 @dataclass
+class StrainParams:
+    """Strain of every frame (DVCPara strain_* fields, core/config.py:115-122): gradient method "plane_fit", "fd",
+    "fem" or "direct" (frames against frame 0 use their own F), plane-fit half-width in nodes, strain measure,
+    voxel size (x, y, z), Gaussian smoothing of the displacement and of the strain (in nodes), and whether nodes
+    whose gradient stencil is incomplete are trimmed."""
+
+    method: str = "plane_fit"
+    halfwidth: tuple = (1, 1, 1)
+    strain_type: str = "infinitesimal"
+    voxel_size: tuple = (1.0, 1.0, 1.0)
+    disp_smoothing: float = 0.0
+    strain_smoothing: float = 0.0
+    edge_trim: bool = True
+
+
+@dataclass
 class FrameResult:
     """One deformed frame (host arrays): the pass's displacements and gradients against reference ``ref_frame``,
     the local result and initial guess, final ZNCC and statuses, the outlier flags (converged, then rejected by
@@ -101,6 +117,7 @@ class FrameResult:
     init_method: str = ""
     U_std: np.ndarray | None = None  # standard deviation of u, v, w (voxels) from the normal equations
     U_accum: np.ndarray | None = None
+    strain: object = None  # strain.StrainResult of U_accum when run_series was given StrainParams
     seconds: float = 0.0
 
 
@@ -222,12 +239,30 @@ def compose_cumulative(frames: list, schedule: FrameSchedule, coords0: np.ndarra
         fr.U_accum = pos - positions[0]
 
 
+def frame_strains(frames: list, grid_shape, spacing, valid0: np.ndarray, elem_active0, sp: StrainParams, gauss_order: int = 2) -> None:
+    """core/pipeline.py:421-433: the strain of every frame from its accumulated displacement on the node grid of the
+    first frame's reference (its node validity; the frame's own F when its reference is frame 0), on the device."""
+    from . import strain as ST
+    from .mesh import surface_nodes
+
+    boundary = np.zeros(int(np.prod(grid_shape)), dtype=bool)
+    boundary[surface_nodes(grid_shape)] = True
+    for fr in frames:
+        F_direct = fr.F if fr.ref_frame == 0 else None
+        out = ST.compute_strain_device(fr.U_accum, grid_shape, spacing, sp.method, tuple(sp.halfwidth), sp.strain_type,
+                                       tuple(sp.voxel_size), torch.from_numpy(np.asarray(valid0, dtype=bool)), F_direct,
+                                       torch.from_numpy(boundary), elem_active0, float(sp.disp_smoothing), float(sp.strain_smoothing),
+                                       bool(sp.edge_trim), gauss_order)
+        fr.strain = ST._result(_host(out["U_phys"]), _host(out["F_phys"]), _host(out["keep"]), sp.strain_type, out["method"], out)
+
+
 def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | None = None, reference_mode: str = "accumulative",
-               cumulative_interp: str = "cubic", normalize: bool = True) -> SeriesResult:
+               cumulative_interp: str = "cubic", normalize: bool = True, strain: StrainParams | None = None) -> SeriesResult:
     """run_aldvc's sections 2-7 over ``volumes`` (frame 0 first; (nz, ny, nx) uint16 or float32 host arrays or CUDA
     tensors).  ``masks``: per frame, None or a material mask, used as the reference mask when the frame is a
     reference and as the deformed-frame mask when it is solved; ``schedule`` defaults to ``reference_mode``'s.
-    Returns a SeriesResult with one FrameResult per deformed frame."""
+    ``strain``: StrainParams to add each frame's strain (of its accumulated displacement).  Returns a SeriesResult
+    with one FrameResult per deformed frame."""
     n_frames = len(volumes)
     if n_frames < 2:
         raise ValueError(f"At least 2 volumes are required (got {n_frames}).")
@@ -245,6 +280,7 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
     frames: list = []
     prev_ref, prev_U = None, None
     timings: dict = {}
+    valid0 = elem0 = spacing = None  # node validity and active elements of the first frame's reference, grid spacing
     try:
         up.prefetch(schedule.parent(1))
         up.prefetch(1)
@@ -278,6 +314,8 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
             if p.beta is None and getattr(res, "beta", None) is not None:
                 beta_by_ref.setdefault(ref_idx, float(res.beta))
             rf = refs[ref_idx]
+            if valid0 is None:
+                valid0, elem0, spacing = _host(rf.valid_b), rf.elem_active, rf.mesh.spacing
             U_std = UN.displacement_uncertainty_device(rf.H, res.zncc, res.status, rf.valid_b, rf.n_valid, rf.bottomf, rf.mesh.half,
                                                        p.subset_stride)
             frames.append(FrameResult(U=_host(res.U), F=_host(res.F), ref_frame=ref_idx, U_local=_host(res.U_local),
@@ -298,6 +336,10 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
     t7 = time.perf_counter()
     compose_cumulative(frames, schedule, coords0, (x0, y0, z0), grid_shape, 3 if cumulative_interp == "cubic" else 1)
     timings["cumulative"] = time.perf_counter() - t7
+    if strain is not None:
+        t8 = time.perf_counter()
+        frame_strains(frames, grid_shape, spacing, valid0, elem0, strain, p.gauss_pt_order)
+        timings["strain"] = time.perf_counter() - t8
     timings["h2d_bytes"] = up.h2d_bytes
     timings["total"] = time.perf_counter() - t_start
     return SeriesResult(frames, coords0, grid_shape, (x0, y0, z0), schedule, timings)

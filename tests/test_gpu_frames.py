@@ -105,3 +105,29 @@ def test_series_frames_equal_their_single_passes(vols):
     for a, b in zip(res.frames, dev.frames):
         assert np.array_equal(a.U, b.U) and np.array_equal(a.U_accum, b.U_accum)
     assert res.timings["h2d_bytes"] == sum(v.nbytes for v in vols) and dev.timings["h2d_bytes"] == 0
+
+
+def test_series_strain_is_the_strain_of_the_accumulated_field(vols):
+    """Strain per frame (core/pipeline.py:421-433): the device strain of each frame's U_accum on frame 0's node
+    grid, the frame's own F for the "direct" method when its reference is frame 0 (the strain module itself is
+    pinned to the reference's compute_strain by tests/test_gpu_strain.py)."""
+    import torch
+
+    from pyaldvc_b200 import strain as ST
+    from pyaldvc_b200.frames import StrainParams, run_series
+    from pyaldvc_b200.mesh import surface_nodes
+
+    p = _params("incr_cubic")
+    for sp in (StrainParams(), StrainParams(method="direct", strain_type="green_lagrange", voxel_size=(1.0, 1.0, 2.0))):
+        res = run_series(vols, p, reference_mode="incremental", strain=sp)
+        valid0 = res.frames[0].valid
+        bnd = np.zeros(len(valid0), dtype=bool)
+        bnd[surface_nodes(res.grid_shape)] = True
+        spacing = tuple(float(a[1] - a[0]) for a in res.axes)
+        for fr in res.frames:
+            out = ST.compute_strain_device(fr.U_accum, res.grid_shape, spacing, sp.method, sp.halfwidth, sp.strain_type, sp.voxel_size,
+                                           torch.from_numpy(valid0), fr.F if fr.ref_frame == 0 else None, torch.from_numpy(bnd))
+            E = out["E"].cpu().numpy()
+            np.testing.assert_array_equal(fr.strain.exx, E[:, 0, 0])
+            np.testing.assert_array_equal(fr.strain.eyz, E[:, 1, 2])
+            assert fr.strain.method == ("direct" if sp.method == "direct" and fr.ref_frame == 0 else "plane_fit")
