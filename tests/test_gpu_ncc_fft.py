@@ -113,7 +113,7 @@ def test_ncc_expansion_matches_reference_fft_branch(oracle_mod, gn, ncc_in, engi
     assert n_ties <= 0.02 * len(coords)
 
 
-@pytest.mark.parametrize("name", ["r16", "r9"])
+@pytest.mark.parametrize("name", ["r16", "r9", "t15r16"])
 def test_cluster_engine_equals_three_pass_engine(gn, ncc_in, name):
     """The cluster form runs every line through the same transforms in the same order as the three passes of the
     in-register engine: identical integer peaks, sub-voxel displacements and peak values.  The PCE energy sums the
@@ -122,7 +122,8 @@ def test_cluster_engine_equals_three_pass_engine(gn, ncc_in, name):
     from pyaldvc_b200.integer_search import ncc_search
 
     f, g, coords, shift = ncc_in
-    c = PI.NCC_SEARCHES[name]
+    # t15r16: a 15^3 template at +-16, a 47-voxel window in a 48-point box (the cluster form's other length)
+    c = PI.NCC_SEARCHES[name] if name in PI.NCC_SEARCHES else dict(subset=(14, 14, 14), radius=(16, 16, 16))
     a = ncc_search(f, g, coords, c["subset"], c["radius"], shift, engine=ENGINES["fft"])
     b = ncc_search(f, g, coords, c["subset"], c["radius"], shift, engine=ENGINES["fft_cluster"])
     for k in ("ok", "clipped", "disp", "cc"):
