@@ -9,7 +9,7 @@
   4-warp kernel with the overlapping-quad copy, a 17^3 template at +-16 on the in-register FFT engine).
 - CUDA-graph replay of the ADMM loop against eager execution, on two different inputs.
 
-Parity bar (the north star's): displacements within 1e-3 voxel, displacement gradients within 1e-5, identical
+Parity bar: displacements within 1e-3 voxel, displacement gradients within 1e-5, identical
 node validity and ADMM step counts, identical final statuses.
 """
 
