@@ -261,8 +261,9 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
     """run_aldvc's sections 2-7 over ``volumes`` (frame 0 first; (nz, ny, nx) uint16 or float32 host arrays or CUDA
     tensors).  ``masks``: per frame, None or a material mask, used as the reference mask when the frame is a
     reference and as the deformed-frame mask when it is solved; ``schedule`` defaults to ``reference_mode``'s.
-    ``strain``: StrainParams to add each frame's strain (of its accumulated displacement).  Returns a SeriesResult
-    with one FrameResult per deformed frame."""
+    ``strain``: StrainParams to add each frame's strain (of its accumulated displacement).  With ``p.tile_local`` > 0
+    every pass is the tiled pass (tiling.run_pass_tiled) on host frames, for volumes beyond the device's memory.
+    Returns a SeriesResult with one FrameResult per deformed frame."""
     n_frames = len(volumes)
     if n_frames < 2:
         raise ValueError(f"At least 2 volumes are required (got {n_frames}).")
@@ -273,6 +274,9 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
     if cumulative_interp not in ("linear", "cubic"):
         raise ValueError("cumulative_interp must be 'linear' or 'cubic'")
     shape = tuple(int(s) for s in volumes[0].shape)
+    tiled = int(getattr(p, "tile_local", 0) or 0) > 0
+    if tiled and any(isinstance(v, torch.Tensor) and v.is_cuda for v in volumes):
+        raise ValueError("tile_local > 0: the frames of a tiled series stay in host memory")
     t_start = time.perf_counter()
     up = _Uploader(volumes, masks)
     refs: OrderedDict = OrderedDict()
@@ -282,41 +286,51 @@ def run_series(volumes, p: PL.PassParams, masks=None, schedule: FrameSchedule | 
     timings: dict = {}
     valid0 = elem0 = spacing = None  # node validity and active elements of the first frame's reference, grid spacing
     try:
-        up.prefetch(schedule.parent(1))
-        up.prefetch(1)
+        if not tiled:
+            up.prefetch(schedule.parent(1))
+            up.prefetch(1)
         for k in range(1, n_frames):
             t_frame = time.perf_counter()
             ref_idx = schedule.parent(k)
-            if k + 1 < n_frames:  # the next frame (and a new reference) copy while this one is solved
+            if k + 1 < n_frames and not tiled:  # the next frame (and a new reference) copy while this one is solved
                 up.prefetch(k + 1)
                 if schedule.parent(k + 1) not in refs:
                     up.prefetch(schedule.parent(k + 1))
-            if ref_idx in refs:
-                refs.move_to_end(ref_idx)
-            else:
-                while len(refs) >= REF_CACHE:  # room first: a prepared reference holds about 17 bytes per voxel
-                    refs.popitem(last=False)
-                f_d, m_d = up.get(ref_idx)
-                if tuple(f_d.shape) != shape:
-                    raise ValueError(f"frame {ref_idx} has shape {tuple(f_d.shape)}, frame 0 {shape}")
-                t0 = time.perf_counter()
-                refs[ref_idx] = PL.prepare_reference(f_d, p, m_d, normalize)
-                timings["reference_prepare"] = timings.get("reference_prepare", 0.0) + time.perf_counter() - t0
-            g_d, gm_d = up.get(k)
-            if tuple(g_d.shape) != shape:
-                raise ValueError(f"frame {k} has shape {tuple(g_d.shape)}, frame 0 {shape}")
             pk = p
             if p.beta is None and ref_idx in beta_by_ref:
                 pk = copy.copy(p)
                 pk.beta = beta_by_ref[ref_idx]
             previous = prev_U if prev_ref == ref_idx else None
-            res = PL.run_pass(None, g_d, pk, None, normalize, g_mask=gm_d, ref=refs[ref_idx], previous=previous)
+            if tiled:  # volumes beyond the device: the frames stay in host memory, every pass streams its boxes
+                from .tiling import run_pass_tiled
+
+                res = run_pass_tiled(volumes[ref_idx], volumes[k], pk, None if masks is None else masks[ref_idx],
+                                     None if masks is None else masks[k], normalize, previous=previous)
+                ref_q = (res.H, res.valid, res.n_valid, res.bottomf, res.mesh, res.elem_active)
+            else:
+                if ref_idx in refs:
+                    refs.move_to_end(ref_idx)
+                else:
+                    while len(refs) >= REF_CACHE:  # room first: a prepared reference holds about 17 bytes per voxel
+                        refs.popitem(last=False)
+                    f_d, m_d = up.get(ref_idx)
+                    if tuple(f_d.shape) != shape:
+                        raise ValueError(f"frame {ref_idx} has shape {tuple(f_d.shape)}, frame 0 {shape}")
+                    t0 = time.perf_counter()
+                    refs[ref_idx] = PL.prepare_reference(f_d, p, m_d, normalize)
+                    timings["reference_prepare"] = timings.get("reference_prepare", 0.0) + time.perf_counter() - t0
+                g_d, gm_d = up.get(k)
+                if tuple(g_d.shape) != shape:
+                    raise ValueError(f"frame {k} has shape {tuple(g_d.shape)}, frame 0 {shape}")
+                rf = refs[ref_idx]
+                res = PL.run_pass(None, g_d, pk, None, normalize, g_mask=gm_d, ref=rf, previous=previous)
+                ref_q = (rf.H, rf.valid_b, rf.n_valid, rf.bottomf, rf.mesh, rf.elem_active)
             if p.beta is None and getattr(res, "beta", None) is not None:
                 beta_by_ref.setdefault(ref_idx, float(res.beta))
-            rf = refs[ref_idx]
+            H_r, valid_r, n_valid_r, bottomf_r, mesh_r, elem_r = ref_q
             if valid0 is None:
-                valid0, elem0, spacing = _host(rf.valid_b), rf.elem_active, rf.mesh.spacing
-            U_std = UN.displacement_uncertainty_device(rf.H, res.zncc, res.status, rf.valid_b, rf.n_valid, rf.bottomf, rf.mesh.half,
+                valid0, elem0, spacing = _host(valid_r), elem_r, mesh_r.spacing
+            U_std = UN.displacement_uncertainty_device(H_r, res.zncc, res.status, valid_r, n_valid_r, bottomf_r, mesh_r.half,
                                                        p.subset_stride)
             frames.append(FrameResult(U=_host(res.U), F=_host(res.F), ref_frame=ref_idx, U_local=_host(res.U_local),
                                       F_local=_host(res.F_local), U0=_host(res.U0), zncc=_host(res.zncc), status=_host(res.status),

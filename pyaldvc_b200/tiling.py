@@ -751,7 +751,7 @@ def _launch_shape(p, ndof: int, mode: int, mesh, masked: bool, plan: TilePlan, r
 
 def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge: int | None = None,
                    tracer: PL.Tracer | None = None, cache_bytes: int | None = None, slab_voxels: int = SLAB_VOXELS,
-                   frames: HostFrames | None = None) -> PL.PassResult:
+                   frames: HostFrames | None = None, previous: torch.Tensor | None = None) -> PL.PassResult:
     """One AL-DVC pass (core/pipeline.py:255-366) with every voxel-reading step run box by box from host memory.
 
     ``f``, ``g``: host volumes (NumPy arrays or memory maps, float32 or uint16; CPU tensors are accepted);
@@ -759,7 +759,8 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     (default ``p.tile_local``; 0 runs one whole-volume box).  ``cache_bytes`` bounds the device memory kept for
     boxes between stages (default half the free memory).  The result is ``run_pass``'s on the same frames, with
     ``result.tiles`` recording the boxes of every stage and ``result.frames`` the host frames (bytes uploaded,
-    boxes loaded, cache hits).  The ADMM loop runs eagerly (no graph capture: every step streams boxes)."""
+    boxes loaded, cache hits).  The ADMM loop runs eagerly (no graph capture: every step streams boxes).
+    ``previous``: the last frame's field against the same reference, for ``init_guess_method="previous"``."""
     tr = tracer if tracer is not None else PL.Tracer(sync=False)
     tr.start()
     errs = K.ErrorWords()
@@ -851,7 +852,7 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
                 levels = IS.auto_pyramid_levels(frames.shape, subset0, tuple(int(r) for r in p.search_radius),
                                                 std0=frames.f_std(), downsample=lambda k: means[k][0])
     ncc_calls: list = []
-    U0, init_info = PL.initial_guess(p, mesh, shape_only, shape_only, valid_b, ncc_calls, errs, shift_fn=shift_fn,
+    U0, init_info = PL.initial_guess(p, mesh, shape_only, shape_only, valid_b, ncc_calls, errs, previous=previous, shift_fn=shift_fn,
                                      search_fn=search_fn, level_volumes=level_volumes, levels=levels)
     tr.mark("init_guess")
 
@@ -942,6 +943,9 @@ def run_pass_tiled(f, g, p, mask=None, g_mask=None, normalize: bool = True, edge
     result.icgn3_iters = []
     result.tiles = record
     result.frames = frames
+    # the reference quantities a frame series needs (uncertainty, strain): Hessians, node statistics, grid
+    result.H, result.n_valid, result.bottomf = H, n_valid, bottomf
+    result.elem_active, result.mesh = elem_active, mesh
     if not p.use_global_step:
         errs.check()
         if own_frames:

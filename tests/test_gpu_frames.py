@@ -131,3 +131,21 @@ def test_series_strain_is_the_strain_of_the_accumulated_field(vols):
             np.testing.assert_array_equal(fr.strain.exx, E[:, 0, 0])
             np.testing.assert_array_equal(fr.strain.eyz, E[:, 1, 2])
             assert fr.strain.method == ("direct" if sp.method == "direct" and fr.ref_frame == 0 else "plane_fit")
+
+
+def test_tiled_series_equals_resident_series(vols):
+    """tile_local > 0: every frame runs the tiled pass from host memory (the reference's tile_local inside run_aldvc);
+    the frames equal the resident series' within the tiled pass's own bar (1e-9 voxel), statuses identical."""
+    from pyaldvc_b200.frames import run_series
+
+    p = _params("accum_prev")
+    p.tile_disp_margin = 2
+    whole = run_series(vols, p)
+    p.tile_local = 64
+    tiled = run_series(vols, p)
+    for a, b in zip(whole.frames, tiled.frames):
+        np.testing.assert_array_equal(a.status, b.status)
+        np.testing.assert_array_equal(a.outlier, b.outlier)
+        assert a.init_method == b.init_method and a.admm_steps == b.admm_steps
+        for k in ("U0", "U", "U_accum", "U_std"):
+            np.testing.assert_allclose(getattr(b, k), getattr(a, k), rtol=0, atol=1e-9, equal_nan=True, err_msg=k)
