@@ -111,7 +111,8 @@ __device__ __forceinline__ float sample_brick(const float* __restrict__ b, int b
 
 // sample_brick over the overlapping-quad copy of the volume (q[i] = b[i..i+3]): each of the 16 tap rows of a cubic
 // sample is one 16-byte load; the same products and sums in the same order as sample_brick<MODE>.
-template <int MODE>
+// I32: every tap index below 2^31 (the caller checks the volume), so each load takes a 32-bit index.
+template <int MODE, bool I32 = false>
 __device__ __forceinline__ float sample_quad(const float4* __restrict__ q, int bx, int bxy, int ix, int iy, int iz, float fx,
                                              float fy, float fz) {
     float wx0, wx1, wx2, wx3, wy0, wy1, wy2, wy3, wz0, wz1, wz2, wz3;
@@ -125,6 +126,7 @@ __device__ __forceinline__ float sample_quad(const float4* __restrict__ q, int b
         bspl_w(fz, wz0, wz1, wz2, wz3);
     }
     const float4* p = q + ((int64_t)(iz - 1) * bxy + (int64_t)(iy - 1) * bx + (ix - 1));
+    const int i0 = (iz - 1) * bxy + (iy - 1) * bx + (ix - 1);  // used when I32
     float acc = 0.0f;
     const float wz[4] = {wz0, wz1, wz2, wz3};
     const float wy[4] = {wy0, wy1, wy2, wy3};
@@ -133,7 +135,7 @@ __device__ __forceinline__ float sample_quad(const float4* __restrict__ q, int b
         float pl = 0.0f;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float4 r = __ldg(p + (int64_t)k * bxy + j * bx);
+            const float4 r = I32 ? __ldg(q + (i0 + k * bxy + j * bx)) : __ldg(p + (int64_t)k * bxy + j * bx);
             const float row = r.x * wx0 + r.y * wx1 + r.z * wx2 + r.w * wx3;
             pl += row * wy[j];
         }

@@ -18,6 +18,7 @@
 // FP64 across warps; thread 0 runs the per-iteration control in FP64 (Cholesky solve, stopping rules,
 // warp composition) exactly as the reference does.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -76,6 +77,7 @@ struct IcgnArgs {
     int sweep_rows;     // lean: subset rows per sweep tile (0 automatic, < 0 the whole subset)
     const int32_t* node_order;  // persistent forms: the work queue's permutation of the nodes, NULL: index order
     int32_t* err;       // persistent forms: nonzero when a bounded wait on a staged copy gave up
+    int idx32;          // every voxel index of the volumes below 2^31: the lean sweep forms 32-bit indices
 };
 
 // ----------------------------------------------------------------------------- TMA staging of the lean sweep
@@ -1061,13 +1063,15 @@ __device__ __forceinline__ void lean_body(const IcgnArgs& a, const CUtensorMap* 
             const int dx = -sh.hx + vx * a.stride, dy = -sh.hy + vy * a.stride, dz = -sh.hz + vz * a.stride;
             const int xx = xci + dx, yy = yci + dy, zz = zci + dz;
             bool k;
+            auto in_mask = [&]() {
+                return a.idx32 ? __ldg(a.mask + (zz * (int)sxy + yy * a.nx + xx)) != 0
+                               : __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0;
+            };
             if (keep || !inside) {
                 k = xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
-                if (k)
-                    k = keep ? kept_bit(keep, (vz * sh.nY + vy) * sh.nX + vx)
-                             : ((a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0);
+                if (k) k = keep ? kept_bit(keep, (vz * sh.nY + vy) * sh.nX + vx) : ((a.mask == nullptr) || in_mask());
             } else {
-                k = (a.mask == nullptr) || __ldg(a.mask + zz * sxy + (int64_t)yy * a.nx + xx) != 0;
+                k = (a.mask == nullptr) || in_mask();
             }
             if (!k) return;
             acc.nref += 1;
@@ -1082,17 +1086,22 @@ __device__ __forceinline__ void lean_body(const IcgnArgs& a, const CUtensorMap* 
                     return;
                 }
             }
-            const int64_t o = zz * sxy + (int64_t)yy * a.nx + xx;
             // reference-frame reads first: their latency overlaps the interpolation
-            const float fv = __ldg(a.f + o);
-            float q0, q1, q2;
-            if (STORED) {
-                q0 = __ldg(a.gx + o);
-                q1 = __ldg(a.gy + o);
-                q2 = __ldg(a.gz + o);
-            } else {
-                grad_otf(a.f, a.nz, a.ny, a.nx, zz, yy, xx, q0, q1, q2);
-            }
+            float fv, q0, q1, q2;
+            auto ref_reads = [&](auto o) {
+                fv = __ldg(a.f + o);
+                if (STORED) {
+                    q0 = __ldg(a.gx + o);
+                    q1 = __ldg(a.gy + o);
+                    q2 = __ldg(a.gz + o);
+                } else {
+                    grad_otf(a.f, a.nz, a.ny, a.nx, zz, yy, xx, q0, q1, q2);
+                }
+            };
+            if (a.idx32)
+                ref_reads(zz * (int)sxy + yy * a.nx + xx);
+            else
+                ref_reads(zz * sxy + (int64_t)yy * a.nx + xx);
             const float xr = A0 * X + A1 * Y + A2 * Z + T0;
             const float yr = A3 * X + A4 * Y + A5 * Z + T1;
             const float zr = A6 * X + A7 * Y + A8 * Z + T2;
@@ -1108,8 +1117,10 @@ __device__ __forceinline__ void lean_body(const IcgnArgs& a, const CUtensorMap* 
         };
         // sampling g in global memory: the overlapping-quad copy when there is one, else g itself
         auto smp_global = [&](int gx_, int gy_, int gz_, float fx, float fy, float fz) {
-            return (MODE != 0 && a.g4) ? sample_quad<MODE == 0 ? 1 : MODE>(a.g4, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz)
-                                       : sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz);
+            if (MODE != 0 && a.g4)
+                return a.idx32 ? sample_quad<MODE == 0 ? 1 : MODE, true>(a.g4, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz)
+                               : sample_quad<MODE == 0 ? 1 : MODE, false>(a.g4, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz);
+            return sample_brick<MODE>(a.g, a.nx, (int)sxy, gx_, gy_, gz_, fx, fy, fz);
         };
         // One sweep over the node's subset.  Both kinds visit the same voxels in the same per-thread order, so the
         // partials of a field do not depend on the kind that formed them.
@@ -1784,6 +1795,16 @@ static int launch_batched_m(const IcgnArgs& a, const LaunchCfg& c, cudaStream_t 
     }
 }
 
+// 32-bit voxel indices in the lean sweep (volumes below 2^31 voxels); ALDVC_ICGN_IDX32=0 keeps 64-bit indices (a
+// comparison knob, read once)
+static bool icgn_idx32() {
+    static const bool on = [] {
+        const char* e = std::getenv("ALDVC_ICGN_IDX32");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 template <int MODE, bool STORED, int NDOF>
 static int launch_plain_m(IcgnArgs a, cudaStream_t s) {
     for (int64_t start = 0; start < a.n_nodes; start += PLAIN_CHUNK) {
@@ -1832,6 +1853,7 @@ static int fill_common(IcgnArgs& a, const aldvc_volumes* vol, const aldvc_subset
     a.mask = vol->mask;
     a.g = vol->g;
     a.g4 = reinterpret_cast<const float4*>(vol->g4);
+    a.idx32 = icgn_idx32() && vol->nz * vol->ny * vol->nx < (1LL << 31) - 64 ? 1 : 0;
     a.nz = (int)vol->nz;
     a.ny = (int)vol->ny;
     a.nx = (int)vol->nx;
