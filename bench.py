@@ -480,8 +480,8 @@ FFT_REG_SIZES = (36, 40, 48, 50, 54, 60, 64)  # cubic FFT boxes transformed a li
 # nodes; profiles/ncu_icgn_lean_config5_box.md, profiles/dram_config5_box.md), scaled here by the units a launch of
 # the measured pass processes.  Units: node-iterations for IC-GN, nodes for the NCC kernels.
 TRAFFIC_PER_UNIT = {
-    "icgn12_lean": ("node-iteration", 5.056e9 / (11774 * 2.237)),
-    "icgn3_lean": ("node-iteration", 5.358e9 / (11774 * 1.241)),
+    "icgn12_lean": ("node-iteration", (4.409e9 + 0.687e9) / (11774 * 2.237)),
+    "icgn3_lean": ("node-iteration", (5.129e9 + 0.274e9) / (11774 * 1.241)),
     "fft_pass1": ("node", 787.09e6 / 811),
     "fft_pass2": ("node", 958.01e6 / 811),
     "fft_pass3": ("node", 367.63e6 / 811),
@@ -490,8 +490,8 @@ TRAFFIC_PER_UNIT = {
 # issue-slot, L1 and FMA-pipe utilisation of the IC-GN kernels (ncu on the same box): the FP32 roof is not what bounds
 # them; their sweeps are gathers through L1, so issue slots and L1 throughput are the roofs they run against
 ICGN_NCU_BOX = {
-    "icgn12_lean": {"issue_active": 0.617, "l1tex_throughput": 0.597, "fma_pipe": 0.354, "l1_hit": 0.801, "l2_hit": 0.855},
-    "icgn3_lean": {"issue_active": 0.663, "l1tex_throughput": 0.732, "fma_pipe": 0.347, "l1_hit": 0.778, "l2_hit": 0.788},
+    "icgn12_lean": {"issue_active": 0.563, "l1tex_throughput": 0.618, "fma_pipe": 0.362, "l1_hit": 0.802, "l2_hit": 0.855},
+    "icgn3_lean": {"issue_active": 0.626, "l1tex_throughput": 0.789, "fma_pipe": 0.367, "l1_hit": 0.767, "l2_hit": 0.805},
 }
 
 
