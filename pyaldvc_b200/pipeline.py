@@ -151,6 +151,7 @@ class Mesh:
         self.coords_np = np.round(grid_coords(x0, y0, z0)).astype(np.int64)
         self.axes = tuple(np.round(np.asarray(a, dtype=np.float64)).astype(np.int64) for a in (x0, y0, z0))  # xs, ys, zs
         self.coords = torch.from_numpy(self.coords_np).cuda()
+        self.axes_dev = tuple(torch.from_numpy(a).cuda() for a in self.axes)
         self.n = self.coords_np.shape[0]
         self.half = tuple(int(w) // 2 for w in p.winsize)
         self._order = None
@@ -369,21 +370,57 @@ class Reference:
     key: tuple
 
 
+_COPY_STREAMS: dict = {}
+
+
+def _upload_inputs(*inputs):
+    """Device copies of the host (CPU) tensors among a pass's inputs, issued in argument order on a copy stream of
+    this device; CUDA tensors and None pass through.  Each block is allocated on the current stream and recorded on
+    the copy stream, and the copy stream first waits for the current stream's queued work (a block may come from a
+    tensor that work still reads).  Returns the tensors and, per argument, the event after its copy (None where
+    nothing was copied).  From pinned host memory the copies run behind the kernels queued meanwhile; from pageable
+    memory each copy returns only once it is done.  Host-to-device copies share a copy engine in issue order: a
+    small copy issued after these (node coordinates and the like) waits for all of them, so the caller makes its
+    own small copies first."""
+    dev = torch.cuda.current_device()
+    cs = _COPY_STREAMS.get(dev)
+    if cs is None:
+        cs = _COPY_STREAMS[dev] = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    out, evs = [], []
+    for t in inputs:
+        if t is None or t.is_cuda:
+            out.append(t)
+            evs.append(None)
+            continue
+        d = torch.empty(t.shape, dtype=t.dtype, device="cuda")
+        d.record_stream(cs)
+        with torch.cuda.stream(cs):
+            d.copy_(t, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(cs)
+        out.append(d)
+        evs.append(ev)
+    return out, evs
+
+
 def _reference_key(p: PassParams, normalize: bool, shape) -> tuple:
     return (tuple(int(s) for s in shape), tuple(p.winsize), tuple(p.winstepsize), p.min_valid_ratio, p.hessian_cond_max,
             p.subset_stride, p.variant, id(p.node_winsize) if p.node_winsize is not None else None, p.prefilter_sigma, bool(normalize))
 
 
 def prepare_reference(f_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
-                      tracer: Tracer | None = None) -> Reference:
+                      tracer: Tracer | None = None, mesh: Mesh | None = None) -> Reference:
     """Normalisation, presmoothing, gradients, node grid, precompute (local_icgn.precompute_local_context :223-347)
     and node validity (grid_mesh.apply_mask_to_mesh) of a reference frame on the device.  ``tracer`` is marked
-    "preprocess" after the volume work and "precompute" at the end."""
+    "preprocess" after the volume work and "precompute" at the end.  ``mesh``: the node grid of this volume shape
+    and these parameters, when the caller made it already."""
     f = K.normalize(f_raw) if normalize else f_raw.float().contiguous()
     if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:197
         f = K.gaussian_presmooth(f, p.prefilter_sigma)
     gx, gy, gz = K.gradients(f)
-    mesh = Mesh(f.shape, p)
+    if mesh is None:
+        mesh = Mesh(f.shape, p)
     m_u8 = None if mask is None else mask.to(torch.uint8).contiguous()
     if tracer is not None:
         tracer.mark("preprocess")
@@ -397,7 +434,7 @@ def prepare_reference(f_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | N
     nz_, ny_, nx_ = f.shape
     if node_half is None and p.subset_stride == 1 and p.variant == K.BATCHED and nx_ <= 8192 and ny_ <= 65535:
         # a tensor grid of nodes with one subset shape: separable moment sums (the batched form)
-        H, L, meanf, bottomf, n_valid, valid = K.precompute_grid(*mesh.axes, mesh.half, f, gx, gy, gz, p.min_valid_ratio,
+        H, L, meanf, bottomf, n_valid, valid = K.precompute_grid(*mesh.axes_dev, mesh.half, f, gx, gy, gz, p.min_valid_ratio,
                                                                  p.hessian_cond_max, m_u8)
         precompute_form = "grid"
     else:
@@ -418,34 +455,60 @@ def prepare_reference(f_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | N
 def run_pass(f_raw: torch.Tensor | None, g_raw: torch.Tensor, p: PassParams, mask: torch.Tensor | None = None, normalize: bool = True,
              tracer: Tracer | None = None, g_mask: torch.Tensor | None = None, ref: Reference | None = None,
              previous: torch.Tensor | None = None) -> PassResult:
-    """Full pass on one volume pair (CUDA tensors, (nz, ny, nx) float32 or uint16).  ``mask``: reference-frame
-    material mask; ``g_mask``: deformed-frame mask (False voxels are excluded from every correlation).  ``ref``: the
-    reference frame prepared by ``prepare_reference`` (then ``f_raw`` and ``mask`` are not read); ``previous``: the
-    displacement field (N, 3) of the last frame solved against the same reference, the initial guess of
-    ``init_guess_method="previous"`` (core/pipeline.py:266, init_disp.py:70-73)."""
+    """Full pass on one volume pair ((nz, ny, nx) float32 or uint16 tensors, on the device or in host memory).
+    ``mask``: reference-frame material mask; ``g_mask``: deformed-frame mask (False voxels are excluded from every
+    correlation).  ``ref``: the reference frame prepared by ``prepare_reference`` (then ``f_raw`` and ``mask`` are
+    not read); ``previous``: the displacement field (N, 3) of the last frame solved against the same reference, the
+    initial guess of ``init_guess_method="previous"`` (core/pipeline.py:266, init_disp.py:70-73).  Host inputs are
+    copied within the pass, the reference frame first: its preparation runs while the deformed frame is copied
+    (pinned host memory lets the two overlap)."""
     tr = tracer if tracer is not None else Tracer(sync=False)
     tr.start()
     # device error words of the bounded waits (inpainting, median test, PCG), read once at the end of the pass
     errs = K.ErrorWords()
-    g = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
-    if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:257
-        g = K.gaussian_presmooth(g, p.prefilter_sigma)
+    g_ready = None
+    mesh0 = None
+    if any(t is not None and not t.is_cuda for t in (f_raw, g_raw, mask, g_mask)):
+        if ref is not None:
+            f_raw = mask = None
+        else:  # the node grid's own small copies go ahead of the volumes' in the copy engine's queue
+            mesh0 = Mesh(tuple(f_raw.shape), p)
+        (f_raw, mask, g_raw, g_mask), evs = _upload_inputs(f_raw, mask, g_raw, g_mask)
+        cur = torch.cuda.current_stream()
+        for ev in evs[:2]:
+            if ev is not None:
+                cur.wait_event(ev)
+        g_ready = [ev for ev in evs[2:] if ev is not None]
     mode = K.INTERP_MODE_BY_NAME[p.interp_method]
-    # the array the interpolation samples, and the NCC input (core/pipeline.py:258-262, io/volume_ops.py:225-244)
-    g_prep = K.bspline_prefilter(g) if p.interp_method == "bspline" else g
-    if g_mask is not None:
-        gm = g_mask.to(torch.uint8).contiguous()
-        if g_prep is g:
-            g_prep = g.clone()
-        K.mask_fill(g_prep, gm, float("nan"))
-        g = K.mask_fill(g.clone(), gm, 0.0)
+
+    def prepare_deformed():
+        g_ = K.normalize(g_raw) if normalize else g_raw.float().contiguous()
+        if p.prefilter_sigma and p.prefilter_sigma > 0:  # core/pipeline.py:257
+            g_ = K.gaussian_presmooth(g_, p.prefilter_sigma)
+        # the array the interpolation samples, and the NCC input (core/pipeline.py:258-262, io/volume_ops.py:225-244)
+        gp_ = K.bspline_prefilter(g_) if p.interp_method == "bspline" else g_
+        if g_mask is not None:
+            gm = g_mask.to(torch.uint8).contiguous()
+            if gp_ is g_:
+                gp_ = g_.clone()
+            K.mask_fill(gp_, gm, float("nan"))
+            g_ = K.mask_fill(g_.clone(), gm, 0.0)
+        return g_, gp_
+
+    if g_ready is None:
+        g, g_prep = prepare_deformed()
     if ref is None:
-        ref = prepare_reference(f_raw, p, mask, normalize, tr)
+        ref = prepare_reference(f_raw, p, mask, normalize, tr, mesh=mesh0)
     else:
         if ref.key != _reference_key(p, normalize, g_raw.shape):
             raise ValueError("run_pass: the prepared reference was made with other parameters or another volume shape")
         tr.mark("preprocess")
         tr.mark("precompute")
+    if g_ready is not None:
+        for ev in g_ready:
+            torch.cuda.current_stream().wait_event(ev)
+        g, g_prep = prepare_deformed()
+        tr.mark("preprocess")
     f, gx, gy, gz, m_u8, mesh, node_half = ref.f, ref.gx, ref.gy, ref.gz, ref.m_u8, ref.mesh, ref.node_half
     H, L, meanf, bottomf, n_valid = ref.H, ref.L, ref.meanf, ref.bottomf, ref.n_valid
     valid_b, elem_active, precompute_form = ref.valid_b, ref.elem_active, ref.precompute_form

@@ -213,3 +213,25 @@ def test_admm_graph_replay_matches_eager():
             same = (x == y) | (torch.isnan(x) & torch.isnan(y)) if x.is_floating_point() else x == y  # NaN at rejected nodes
             assert bool(same.all()), f"graph replay differs from eager in {k}"
     assert not torch.equal(a_g.U, b_g.U)
+
+
+def test_pass_from_host_buffers_equals_device_inputs():
+    """Host inputs (pinned and pageable) are copied within the pass, the reference frame first and the deformed
+    frame behind its preparation: the pass equals the one on device inputs bit for bit (configuration-3 box: uint16
+    pair with its ROI mask), with a prepared reference too (then only the deformed frame is copied)."""
+    import torch
+
+    from pyaldvc_b200.pipeline import prepare_reference, run_pass
+
+    f, g, mask, p, _ = _crop_config3()
+    dev = run_pass(_cuda(f), _cuda(g), p, _cuda(mask))
+    fh, gh, mh = (torch.from_numpy(np.ascontiguousarray(a)) for a in (f, g, mask))
+    ref = prepare_reference(_cuda(f), p, _cuda(mask))
+    for what, res in (("pinned", run_pass(fh.pin_memory(), gh.pin_memory(), p, mh.pin_memory())),
+                      ("pageable", run_pass(fh, gh, p, mh)),
+                      ("prepared reference", run_pass(None, gh.pin_memory(), p, ref=ref))):
+        assert res.admm_steps == dev.admm_steps, what
+        for k in ("U", "F", "U_local", "U0", "status", "zncc"):
+            x, y = getattr(res, k), getattr(dev, k)
+            same = (x == y) | (torch.isnan(x) & torch.isnan(y)) if x.is_floating_point() else x == y
+            assert bool(same.all()), f"{what}: {k} differs from the pass on device inputs"
