@@ -787,9 +787,16 @@ static size_t peak_smem(const NccGeom& G) {
     return b <= 160 * 1024 ? b : 0;
 }
 
+// static shared bytes of a kernel (the opt-in attribute is needed once static plus dynamic bytes pass 48 KB)
+static size_t static_smem(const void* kern) {
+    cudaFuncAttributes fa{};
+    return cudaFuncGetAttributes(&fa, kern) == cudaSuccess ? fa.sharedSizeBytes : (size_t)16 * 1024;
+}
+
 static int launch_peak(const SearchArgs& b, int64_t n, cudaStream_t s) {
     const size_t sm = peak_smem(b.G);
-    if (sm > 48 * 1024) {
+    static const size_t stat = static_smem((const void*)ncc_peak_kernel<true>);
+    if (sm && sm + stat > 48 * 1024) {
         static size_t have = 0;
         static std::mutex mu;
         std::lock_guard<std::mutex> lock(mu);
@@ -1837,6 +1844,8 @@ __global__ void __launch_bounds__(N, N > 50 ? 4 : 8) fftr_pass2_kernel(FftArgs a
         if (dz < G.vz) dst[(int64_t)dz * NH * N] = v[dz];
 }
 
+#include "fft_tensor.cuh"
+
 // Pass 3: planes per CTA of the half-spectrum tile [N][N/2 + 1 | 1] of each plane, at most 256 threads.
 template <int N>
 __host__ __device__ constexpr int fftr_planes3() {
@@ -2344,6 +2353,44 @@ static int fftr_upload() {
     return ALDVC_OK;
 }
 
+// pass 2 on the tensor pipe (fftt_pass2_kernel) when ALDVC_FFT_PASS2=tensor and the length has that form (a
+// comparison knob, read once; each launch synchronises its stream to read the kernel's error flag)
+static bool fft_pass2_tensor() {
+    static const bool on = [] {
+        const char* e = std::getenv("ALDVC_FFT_PASS2");
+        return e && std::strcmp(e, "tensor") == 0;
+    }();
+    return on;
+}
+
+template <int N>
+static int launch_fftt_pass2(FftArgs& a, int nb, cudaStream_t s) {
+    using S = FfttShape<N>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(fftt_pass2_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+        if (e != cudaSuccess) return cuda_fail(e, "ncc fft tensor pass 2: shared memory attribute");
+        attr = true;
+    }
+    const int64_t groups = ((int64_t)nb * (N / 2 + 1) * N + 127) / 128;
+    const int grid = (int)std::min<int64_t>(groups, sm_count());
+    const int zero = 0;
+    cudaError_t e = cudaMemcpyToSymbolAsync(g_fftt_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ncc fft tensor pass 2: error flag");
+    fftt_pass2_kernel<N><<<grid, FFTT_THREADS, S::SMEM, s>>>(a, groups);
+    int rc = check_launch("ncc fft tensor pass 2");
+    if (rc) return rc;
+    int err = 0;
+    e = cudaMemcpyFromSymbolAsync(&err, g_fftt_err, sizeof(int), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "ncc fft tensor pass 2");
+    if (err) {
+        set_error("ncc fft tensor pass 2: an MMA completion wait gave up");
+        return ALDVC_ERR_CUDA;
+    }
+    return ALDVC_OK;
+}
+
 template <int N>
 static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     constexpr int P = fftr_planes<N>();
@@ -2366,6 +2413,20 @@ static int launch_fftr(FftArgs& a, int nb, cudaStream_t s) {
     }
     int rc = check_launch("ncc fft pass 1");
     if (rc) return rc;
+    if constexpr (N <= 54) {
+        if (fft_pass2_tensor()) {
+            {
+                KTimer kt_("fft_pass2_tensor", s);
+                rc = launch_fftt_pass2<N>(a, nb, s);
+            }
+            if (rc) return rc;
+            {
+                KTimer kt_("fft_pass3", s);
+                fftr_pass3_kernel<N><<<dim3((G.vz + P3 - 1) / P3, nb), fftr_pass3_threads<N>(), SM3, s>>>(a);
+            }
+            return check_launch("ncc fft pass 3");
+        }
+    }
     {
         KTimer kt_("fft_pass2", s);
         fftr_pass2_kernel<N><<<dim3(N / 2 + 1, nb), N, SM2, s>>>(a);
@@ -2641,7 +2702,8 @@ static size_t tpl_smem(const NccGeom& G) { return (size_t)G.n_tpl * sizeof(float
 
 static int launch_map(const MapArgs& m, int64_t n_chunk, cudaStream_t s) {
     const size_t smem = tpl_smem(m.G);
-    static size_t attr_set = 48 * 1024;  // largest dynamic size already allowed (no call inside a capture)
+    static const size_t stat = static_smem((const void*)ncc_map_kernel);
+    static size_t attr_set = 48 * 1024 - stat;  // largest dynamic size already allowed (no call inside a capture)
     if (smem > attr_set) {
         const size_t want = (size_t)max_smem_optin() - 4096;
         cudaError_t e = cudaFuncSetAttribute(ncc_map_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);

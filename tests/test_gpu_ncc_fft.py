@@ -129,3 +129,69 @@ def test_cluster_engine_equals_three_pass_engine(gn, ncc_in, name):
     for k in ("ok", "clipped", "disp", "cc"):
         np.testing.assert_array_equal(b[k], a[k], err_msg=f"{name} {k}")
     np.testing.assert_allclose(b["pce"], a["pce"], rtol=1e-12, equal_nan=True)
+
+
+# one FFT-engine search in a fresh process (the pass-2 form is chosen by the environment)
+_TENSOR_CHILD = r"""
+import sys
+import numpy as np
+from pyaldvc_b200.integer_search import ncc_search
+d = sys.argv[1]
+z = np.load(d + "/in.npz")
+sh = z["shift"] if z["shift"].any() else None
+res = ncc_search(z["f"], z["g"], z["coords"], tuple(int(v) for v in z["subset"]), tuple(int(v) for v in z["radius"]), sh, engine=2)
+np.savez(d + "/out.npz", **{k: np.asarray(v) for k, v in res.items()})
+"""
+
+
+@pytest.mark.parametrize("name", ["r16", "r9", "t15r16"])
+def test_tensor_pass2_matches_reference_fft_branch(oracle_mod, gn, ncc_in, name, tmp_path):
+    """ALDVC_FFT_PASS2=tensor (fft_tensor.cuh): pass 2's z transforms as tcgen05 products of TF32-split operands.
+    Its FP32 maps round differently from the in-register pass, so the test holds it to the reference's FFT branch
+    under the same near-tie rule as every engine, and to the in-register form: identical ok / clipped flags, integer
+    peaks identical away from near ties, FP64 peak values equal where the peaks agree.  The knob is read once per
+    process, so the search runs in a child process."""
+    import subprocess
+
+    from pyaldvc_b200.integer_search import ncc_search
+
+    f, g, coords, shift = ncc_in
+    c = PI.NCC_SEARCHES[name] if name in PI.NCC_SEARCHES else dict(subset=(14, 14, 14), radius=(16, 16, 16), shift=True)
+    sh = shift if c["shift"] else None
+    np.savez(tmp_path / "in.npz", f=f, g=g, coords=coords, subset=np.asarray(c["subset"]), radius=np.asarray(c["radius"]),
+             shift=np.zeros_like(coords) if sh is None else sh)
+    env = dict(os.environ, ALDVC_FFT_PASS2="tensor")
+    subprocess.run([sys.executable, "-c", _TENSOR_CHILD, str(tmp_path)], env=env, check=True, timeout=900,
+                   cwd=os.path.dirname(HERE))
+    with np.load(tmp_path / "out.npz") as z:
+        res = {k: z[k] for k in z.files}
+    if name in PI.NCC_SEARCHES:
+        ref = {k: gn[f"{name}_{k}"] for k in ("disp", "cc", "pce", "clipped", "ok")}
+        n_ties = _compare(oracle_mod, f, g, coords, sh, c["subset"], c["radius"], res, ref, f"{name}/tensor pass 2")
+        assert n_ties <= 0.02 * len(coords)
+    a = ncc_search(f, g, coords, c["subset"], c["radius"], sh, engine=ENGINES["fft"])
+    np.testing.assert_array_equal(res["ok"], a["ok"])
+    np.testing.assert_array_equal(res["clipped"], a["clipped"])
+    same = np.all(res["disp"] == a["disp"], axis=1) | ~a["ok"]
+    assert (~same).sum() <= 0.01 * len(coords), f"{name}: {(~same).sum()} nodes moved against the in-register form"
+    np.testing.assert_array_equal(res["cc"][same & a["ok"]], a["cc"][same & a["ok"]])
+
+
+def test_fresh_process_first_search_with_a_15_voxel_template(ncc_in, tmp_path):
+    """A 15^3 template at +-16 as a process's first search: the peak kernel's template and neighbour box (46.6 KB)
+    plus its static shared arrays pass the 48 KB default, so the launch needs the opt-in attribute even though the
+    dynamic part alone stays under it (earlier searches with larger templates used to set it in passing)."""
+    import subprocess
+
+    from pyaldvc_b200.integer_search import ncc_search
+
+    f, g, coords, shift = ncc_in
+    np.savez(tmp_path / "in.npz", f=f, g=g, coords=coords, subset=np.asarray((14, 14, 14)), radius=np.asarray((16, 16, 16)),
+             shift=shift)
+    subprocess.run([sys.executable, "-c", _TENSOR_CHILD, str(tmp_path)], env=dict(os.environ), check=True, timeout=900,
+                   cwd=os.path.dirname(HERE))
+    with np.load(tmp_path / "out.npz") as z:
+        res = {k: z[k] for k in z.files}
+    a = ncc_search(f, g, coords, (14, 14, 14), (16, 16, 16), shift, engine=ENGINES["fft"])
+    for k in ("ok", "clipped", "disp", "cc"):
+        np.testing.assert_array_equal(res[k], a[k], err_msg=k)
