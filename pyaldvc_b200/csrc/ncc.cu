@@ -416,15 +416,39 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     // coordinates (n_tpl words)
     uint32_t* kji = reinterpret_cast<uint32_t*>(psm + G.n_tpl + (G.sx + 2) * (G.sy + 2) * (G.sz + 2));
     double sf = 0.0;
-    for (int r = warp; r < G.sz * G.sy; r += NW) {
-        const int k = r / G.sy, j = r - k * G.sy;
-        for (int ii = lane; ii < G.sx; ii += 32) {
-            const float v = __ldg(fg + k * sxy + (int64_t)j * G.nx + ii);
-            if (SMEM) {
-                psm[(k * G.sy + j) * G.sx + ii] = v;
-                kji[(k * G.sy + j) * G.sx + ii] = ((uint32_t)k << 20) | ((uint32_t)j << 10) | (uint32_t)ii;
+    const int nrow = G.sz * G.sy;
+    if (G.sx <= 32) {
+        // one sample per lane and row: eight rows' loads in flight per warp, then the sums in the same row order
+        for (int r0 = warp; r0 < nrow; r0 += 8 * NW) {
+            float vv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = r0 + u * NW, k = r / G.sy, j = r - k * G.sy;
+                vv[u] = (r < nrow && lane < G.sx) ? __ldg(fg + k * sxy + (int64_t)j * G.nx + lane) : 0.0f;
             }
-            sf += (double)v;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = r0 + u * NW, k = r / G.sy, j = r - k * G.sy;
+                if (r < nrow && lane < G.sx) {
+                    if (SMEM) {
+                        psm[r * G.sx + lane] = vv[u];
+                        kji[r * G.sx + lane] = ((uint32_t)k << 20) | ((uint32_t)j << 10) | (uint32_t)lane;
+                    }
+                    sf += (double)vv[u];
+                }
+            }
+        }
+    } else {
+        for (int r = warp; r < nrow; r += NW) {
+            const int k = r / G.sy, j = r - k * G.sy;
+            for (int ii = lane; ii < G.sx; ii += 32) {
+                const float v = __ldg(fg + k * sxy + (int64_t)j * G.nx + ii);
+                if (SMEM) {
+                    psm[r * G.sx + ii] = v;
+                    kji[r * G.sx + ii] = ((uint32_t)k << 20) | ((uint32_t)j << 10) | (uint32_t)ii;
+                }
+                sf += (double)v;
+            }
         }
     }
     sf = block_sum_d(sf, red);
@@ -446,15 +470,23 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             float b = -3.0f, m = 3.0f;
             int bi = 0x7fffffff;
             double t1 = 0.0, t2 = 0.0;
-            for (int k = 0; k < a.nblk; ++k) {
-                const MapPart q = parts[k];
-                if (q.mx > b || (q.mx == b && q.idx < bi)) {
-                    b = q.mx;
-                    bi = q.idx;
+            for (int k0 = 0; k0 < a.nblk; k0 += 4) {  // four partials' loads in flight, then in block order
+                MapPart qq[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (k0 + u < a.nblk) qq[u] = parts[k0 + u];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (k0 + u >= a.nblk) break;
+                    const MapPart& q = qq[u];
+                    if (q.mx > b || (q.mx == b && q.idx < bi)) {
+                        b = q.mx;
+                        bi = q.idx;
+                    }
+                    m = fminf(m, q.mn);
+                    t1 += q.s1;
+                    t2 += q.s2;
                 }
-                m = fminf(m, q.mn);
-                t1 += q.s1;
-                t2 += q.s2;
             }
             s_max = b;
             s_pk = bi;
@@ -550,12 +582,19 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         for (int k = 0; k < a.nblk; ++k) {
             if (flat || !(parts[k].mx >= vmax - NEAR_TIE)) continue;
             const int hi = min(k * bsz + bsz, G.nmap);
-            for (int i = k * bsz + tid; i < hi; i += NCC_THREADS) {
-                const float vv = map[i];
-                const float v = vv < -1.0f ? 0.0f : vv;
-                if (v >= vmax - NEAR_TIE) {
-                    const int slot = atomicAdd(&s_ncand, 1);
-                    if (slot < MAX_CAND) s_cand[slot] = i;
+            for (int i0 = k * bsz + tid; i0 < hi; i0 += 8 * NCC_THREADS) {  // eight map loads in flight per thread
+                float vv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) vv[u] = i0 + u * NCC_THREADS < hi ? map[i0 + u * NCC_THREADS] : -3.0f;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int i = i0 + u * NCC_THREADS;
+                    if (i >= hi) break;
+                    const float v = vv[u] < -1.0f ? 0.0f : vv[u];
+                    if (v >= vmax - NEAR_TIE) {
+                        const int slot = atomicAdd(&s_ncand, 1);
+                        if (slot < MAX_CAND) s_cand[slot] = i;
+                    }
                 }
             }
         }
