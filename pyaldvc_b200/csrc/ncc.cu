@@ -701,21 +701,26 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
                     const int k = r / G.sy, j = r - k * G.sy;
                     const float* trow = tp + (int64_t)r * G.sx;
                     const float* brow = box + ((k + dzz) * BY + (j + dyy)) * BX;
-                    float b0 = brow[0], b1 = brow[1];
+                    // the window's samples and squares carried in FP64: each box sample is converted once
+                    const float b0f = brow[0], b1f = brow[1];
+                    double d0 = (double)b0f, d1 = (double)b1f, q0 = (double)(b0f * b0f), q1 = (double)(b1f * b1f);
                     for (int i = 0; i < G.sx; ++i) {
                         const float b2 = brow[i + 2];
+                        const double d2 = (double)b2, q2 = (double)(b2 * b2);
                         const double tf = (double)trow[i] - mf;
-                        acc[0] += tf * (double)b0;
-                        acc[1] += tf * (double)b1;
-                        acc[2] += tf * (double)b2;
-                        acc[3] += (double)b0;
-                        acc[4] += (double)b1;
-                        acc[5] += (double)b2;
-                        acc[6] += (double)(b0 * b0);
-                        acc[7] += (double)(b1 * b1);
-                        acc[8] += (double)(b2 * b2);
-                        b0 = b1;
-                        b1 = b2;
+                        acc[0] += tf * d0;
+                        acc[1] += tf * d1;
+                        acc[2] += tf * d2;
+                        acc[3] += d0;
+                        acc[4] += d1;
+                        acc[5] += d2;
+                        acc[6] += q0;
+                        acc[7] += q1;
+                        acc[8] += q2;
+                        d0 = d1;
+                        d1 = d2;
+                        q0 = q1;
+                        q1 = q2;
                     }
                 }
             };
