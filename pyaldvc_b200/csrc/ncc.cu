@@ -50,6 +50,9 @@ __device__ __forceinline__ void sweep_lin(int nrows, int ncols, Ld ld, St st) {
     }
 }
 
+// r / d for 0 <= r < 2^22 from the FP32 reciprocal of d (exact in that range, as in sweep_lin)
+__device__ __forceinline__ int fdivi(int r, float inv_d) { return (int)(((float)r + 0.5f) * inv_d); }
+
 // Row-by-column sweep of an (nrows x ncols <= 128) tile, one warp per row: RB rows of loads are issued before
 // any of their stores, so each thread keeps up to 4 RB global loads in flight.
 template <int RB, typename T, typename Ld, typename St>
@@ -417,18 +420,19 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     uint32_t* kji = reinterpret_cast<uint32_t*>(psm + G.n_tpl + (G.sx + 2) * (G.sy + 2) * (G.sz + 2));
     double sf = 0.0;
     const int nrow = G.sz * G.sy;
+    const float inv_sy = 1.0f / (float)G.sy;  // template rows: r < 2^20
     if (G.sx <= 32) {
         // one sample per lane and row: eight rows' loads in flight per warp, then the sums in the same row order
         for (int r0 = warp; r0 < nrow; r0 += 8 * NW) {
             float vv[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const int r = r0 + u * NW, k = r / G.sy, j = r - k * G.sy;
+                const int r = r0 + u * NW, k = fdivi(r, inv_sy), j = r - k * G.sy;
                 vv[u] = (r < nrow && lane < G.sx) ? __ldg(fg + k * sxy + (int64_t)j * G.nx + lane) : 0.0f;
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const int r = r0 + u * NW, k = r / G.sy, j = r - k * G.sy;
+                const int r = r0 + u * NW, k = fdivi(r, inv_sy), j = r - k * G.sy;
                 if (r < nrow && lane < G.sx) {
                     if (SMEM) {
                         psm[r * G.sx + lane] = vv[u];
@@ -455,7 +459,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     const double mf = sf / (double)G.n_tpl;
     double q = 0.0;
     for (int r = warp; r < G.sz * G.sy; r += NW) {
-        const int k = r / G.sy, j = r - k * G.sy;
+        const int k = fdivi(r, inv_sy), j = r - k * G.sy;
         for (int ii = lane; ii < G.sx; ii += 32) {
             const double d = (double)tp[k * tsz + j * tsy + ii] - mf;
             q += d * d;
@@ -551,6 +555,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     const float cmin = flat ? 0.0f : vmin;
     const int64_t wz0 = a.wz0[node], wy0 = a.wy0[node], wx0 = a.wx0[node];
     const int BX = G.sx + 2, BY = G.sy + 2, BZ = G.sz + 2;
+    const float inv_bx = 1.0f / (float)BX, inv_by = 1.0f / (float)BY;  // neighbour box rows and columns: below 2^21
     float* box = psm + G.n_tpl;  // the neighbour box of the peak (shared layout above)
     auto interior_at = [&](int q) {
         const int qz = q / (G.vy * G.vx), qr = q - qz * G.vy * G.vx, qy = qr / G.vx, qx = qr - qy * G.vx;
@@ -567,7 +572,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
     if (spec) {
         const float* gb0 = box_origin(spk);
         for (int i = tid; i < BZ * BY * BX; i += NCC_THREADS) {
-            const int r = i / BX, ii = i - r * BX, k = r / BY, j = r - k * BY;
+            const int r = fdivi(i, inv_bx), ii = i - r * BX, k = fdivi(r, inv_by), j = r - k * BY;
             cp_async4(box + i, gb0 + k * sxy + (int64_t)j * G.nx + ii);
         }
         cp_async_commit();
@@ -683,7 +688,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
         if (SMEM && !(spec && pk == spk)) {  // the staged box is not this peak's
             sweep_lin<8, float>(BZ * BY, BX,
                                 [&](int r, int ii) {
-                                    const int k = r / BY, j = r - k * BY;
+                                    const int k = fdivi(r, inv_by), j = r - k * BY;
                                     return __ldg(gb + k * sxy + (int64_t)j * G.nx + ii);
                                 },
                                 [&](int r, int ii, float v) { box[r * BX + ii] = v; });
@@ -698,7 +703,7 @@ __global__ void __launch_bounds__(NCC_THREADS, 3) ncc_peak_kernel(SearchArgs a) 
             auto pair_rows = [&](int pr, int r0, int rstep, double acc[9]) {
                 const int dzz = pr / 3, dyy = pr % 3;
                 for (int r = r0; r < rows; r += rstep) {
-                    const int k = r / G.sy, j = r - k * G.sy;
+                    const int k = fdivi(r, inv_sy), j = r - k * G.sy;
                     const float* trow = tp + (int64_t)r * G.sx;
                     const float* brow = box + ((k + dzz) * BY + (j + dyy)) * BX;
                     // the window's samples and squares carried in FP64: each box sample is converted once
