@@ -1022,13 +1022,15 @@ __global__ void __launch_bounds__(256) ncc_template_kernel(TiledArgs a, float* T
         return;
     }
     const int64_t sxy = (int64_t)G.nx * G.ny;
+    const float inv_sxp = 1.0f / (float)a.sxp, inv_sy = 1.0f / (float)G.sy;  // indices below 2^22: fdivi is exact
+    auto col = [&](int i) { return i - fdivi(i, inv_sxp) * a.sxp; };
     auto at = [&](int i) {
-        const int tx = i % a.sxp, row = i / a.sxp, ty = row % G.sy, tz = row / G.sy;
+        const int row = fdivi(i, inv_sxp), tx = i - row * a.sxp, tz = fdivi(row, inv_sy), ty = row - tz * G.sy;
         return __ldg(a.f + (z0 - G.hz + tz) * sxy + (y0 - G.hy + ty) * G.nx + (x0 - G.hx + tx));
     };
     double sf = 0.0;
     for (int i = tid; i < n; i += blockDim.x)
-        if (i % a.sxp < G.sx) sf += (double)at(i);
+        if (col(i) < G.sx) sf += (double)at(i);
     const int lane = tid & 31, warp = tid >> 5;
     sf = warp_sum_d(sf);
     if (lane == 0) red[warp] = sf;
@@ -1043,7 +1045,7 @@ __global__ void __launch_bounds__(256) ncc_template_kernel(TiledArgs a, float* T
     double q = 0.0;
     for (int i = tid; i < n; i += blockDim.x) {
         float v = 0.0f;
-        if (i % a.sxp < G.sx) {
+        if (col(i) < G.sx) {
             const double d = (double)at(i) - mf;
             q += d * d;
             v = (float)d;
@@ -2006,15 +2008,16 @@ __global__ void __launch_bounds__(fftr_pass3_threads<N>()) fftr_pass3_kernel(Fft
     int lidx = 0x7fffffff;
     double ls1 = 0.0, ls2 = 0.0;
     const int i0 = dz0 * G.vy * G.vx;
+    const float inv_vy = 1.0f / (float)G.vy;  // map rows r < 2^22: fdivi is exact
     sweep_lin<4, float2>(
         np * G.vy, G.vx,
         [&](int r, int dx) {
-            const int p_ = (int)(((float)r + 0.5f) / (float)G.vy), dy = r - p_ * G.vy;
+            const int p_ = fdivi(r, inv_vy), dy = r - p_ * G.vy;
             const int64_t o = (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
             return make_float2(__ldg(a.B1 + o), __ldg(a.B2 + o));
         },
         [&](int r, int dx, float2 bs) {
-            const int p_ = (int)(((float)r + 0.5f) / (float)G.vy), dy = r - p_ * G.vy;
+            const int p_ = fdivi(r, inv_vy), dy = r - p_ * G.vy;
             const double s1 = (double)bs.x;
             const double var = (double)bs.y - s1 * s1 * inv_n;
             float v = 0.0f;
@@ -2313,15 +2316,16 @@ __global__ void __cluster_dims__(FFTC_C, 1, 1) __launch_bounds__(FftcShape<N>::T
     int lidx = 0x7fffffff;
     double ls1 = 0.0, ls2 = 0.0;
     const int i0 = dz0 * G.vy * G.vx;
+    const float inv_vy = 1.0f / (float)G.vy;  // map rows r < 2^22: fdivi is exact
     sweep_lin<4, float2>(
         np3 * G.vy, G.vx,
         [&](int rr, int dx) {
-            const int p_ = (int)(((float)rr + 0.5f) / (float)G.vy), dy = rr - p_ * G.vy;
+            const int p_ = fdivi(rr, inv_vy), dy = rr - p_ * G.vy;
             const int64_t o = (wz0 + dz0 + p_) * sxy + (wy0 + dy) * G.nx + (wx0 + dx);
             return make_float2(__ldg(a.B1 + o), __ldg(a.B2 + o));
         },
         [&](int rr, int dx, float2 bs) {
-            const int p_ = (int)(((float)rr + 0.5f) / (float)G.vy), dy = rr - p_ * G.vy;
+            const int p_ = fdivi(rr, inv_vy), dy = rr - p_ * G.vy;
             const double s1 = (double)bs.x;
             const double var = (double)bs.y - s1 * s1 * inv_n;
             float vv = 0.0f;
