@@ -850,6 +850,8 @@ def main():
     f_h = f.cpu().pin_memory()
     g_h = g.cpu().pin_memory()
     m_h = None if mask is None else mask.cpu().pin_memory()
+    # one untimed pass from the same buffers: the first copies out of freshly pinned memory carry one-time costs
+    run_pass(f_h, g_h, p, m_h).U.to("cpu")
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
